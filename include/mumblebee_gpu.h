@@ -1,0 +1,184 @@
+/*
+ * mumblebee_gpu.h — C ABI of libmbgpu.so, the B200 (sm_100a) interior-point solver that stands in
+ * for the hot path of Mumblebee.jl's `IPM` module behind its public solver API.
+ *
+ * Every entry point is `extern "C"`, takes plain pointers and sizes, returns 0 on success or a
+ * negative MB_E* code (never aborts), and copies caller-owned host inputs at create time.  Device
+ * state lives behind opaque handles.  Index arrays of block-sparse matrices are 1-based, exactly as
+ * BlockSparseMatrix stores them.  Numerical outcomes are statuses (IPMStatus), not errors.
+ *
+ * Reference interfaces replaced (paths inside the Mumblebee.jl project):
+ *   mb_problem_create       IPMProblem(Q, B, f, g, μ, K[, P1, P2])        src/IPM/src/ipm/problem.jl:49-71
+ *   mb_problem_create_csc   IPMProblem(Q::SparseMatrixCSC, B, f, g, μ, K, s; compress)
+ *                                                                          src/IPM/src/ipm/problem.jl:84-127
+ *   mb_solver_create        init(prob, settings; p0, d0, y0) → IPMSolver   src/IPM/src/ipm/solver/ipm.jl:431-491
+ *   mb_solver_step          step!(solver) → IPMStatus                      src/IPM/src/ipm/solver/ipm.jl:577-774
+ *   mb_solver_solve         solve!(solver)                                 src/IPM/src/ipm/solver/solver.jl:119-150
+ *   mb_solver_result        result(solver, status) → IPMResult            src/IPM/src/ipm/solver/ipm.jl:30-74
+ *   mb_solver_history       IPMHistory rows                                src/IPM/src/ipm/history/ipm.jl:1-71
+ *   mb_batch_solve          solve(prob, settings) over many problems      src/IPM/src/ipm/solver/ipm.jl:798-804
+ *   mb_settings             IPMSettings                                    src/IPM/src/ipm/settings/ipm.jl:1-18
+ */
+#ifndef MUMBLEBEE_GPU_H
+#define MUMBLEBEE_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* error codes */
+#define MB_OK 0
+#define MB_E_ARG (-1)      /* invalid argument or inconsistent shapes (the reference's @assert) */
+#define MB_E_CUDA (-2)     /* a CUDA runtime call failed */
+#define MB_E_NOMEM (-3)    /* device or host allocation failed */
+#define MB_E_STATE (-4)    /* call not valid in the handle's current state */
+#define MB_E_UNSUPPORTED (-5)
+
+/* cone kinds (the AbstractCone subtypes of src/IPM/src/cone/) */
+#define MB_CONE_FREE 0     /* CofreeCone        cone/noc.jl */
+#define MB_CONE_POS 1      /* PositiveCone      cone/pos.jl */
+#define MB_CONE_SOC 2      /* SecondOrderCone   cone/soc.jl */
+#define MB_CONE_SDP 3      /* SemidefiniteCone  cone/sdp.jl (svec) */
+#define MB_CONE_EXP 4      /* ExponentialCone   cone/tdc/exp.jl */
+#define MB_CONE_POW 5      /* PowerCone(α)      cone/tdc/pow.jl; α in cone_param */
+
+/* IPMStatus (src/IPM/src/ipm/ipm.jl:1), same order */
+enum mb_status {
+    MB_CONTINUE = 0, MB_OPTIMAL, MB_NEAR_OPTIMAL, MB_STALLED, MB_NUMERICAL_FAILURE, MB_ITERATION_LIMIT,
+    MB_PRIMAL_INFEASIBLE, MB_DUAL_INFEASIBLE, MB_ILL_POSED, MB_NEAR_PRIMAL_INFEASIBLE,
+    MB_NEAR_DUAL_INFEASIBLE, MB_NEAR_ILL_POSED
+};
+
+/* factor precision */
+#define MB_PREC_FP64 0     /* FP64 factor */
+#define MB_PREC_FP32 1     /* FP32 factor, FP64 refinement, residuals and termination tests */
+
+/* IPMSettings (settings/ipm.jl:2-17) + precision.  Integer fields first, then doubles. */
+typedef struct mb_settings {
+    int32_t verbose;
+    int32_t max_iter;          /* 100 */
+    int32_t scale_max_iter;    /* 10  equilibration sweeps */
+    int32_t refine_max_iter;   /* 10  KKT iterative-refinement passes */
+    int32_t newton_max_iter;   /* 100 CG iterations per KKT solve */
+    int32_t stable;            /* 0   (StableUzawaSolver not available: must be 0) */
+    int32_t precision;         /* MB_PREC_FP64 */
+    int32_t reserved;
+    double step_frac;          /* 0.99 */
+    double feas_tol;           /* 1e-8 */
+    double gap_tol;            /* 1e-8 */
+    double near_factor;        /* 1000 */
+    double stall_tol;          /* 1e-3 */
+    double refine_stall_tol;   /* 0.5 */
+    double aug_tol;            /* 1e-7 */
+    double infeas_abs;         /* 1e-8 */
+    double infeas_rel;         /* 1e-8 */
+} mb_settings;
+
+/* BlockSparseMatrix{Float64,Int64} (BlockSparseArrays/src/block_sparse_matrix.jl:10-158), 1-based */
+typedef struct mb_bsm {
+    int64_t nout, nvtx, narc, ncol, nrow, nbnz;
+    const int64_t* xsrc;   /* nvtx+1 */
+    const int64_t* xcol;   /* nvtx+1 */
+    const int64_t* xrow;   /* nout+1 */
+    const int64_t* xblk;   /* narc+1 */
+    const int64_t* tgt;    /* narc   */
+    const double* val;     /* nbnz   */
+} mb_bsm;
+
+/* SparseMatrixCSC{Float64,Int64}, 1-based colptr/rowval */
+typedef struct mb_csc {
+    int64_t m, n;
+    const int64_t* colptr;  /* n+1 */
+    const int64_t* rowval;  /* nnz */
+    const double* nzval;    /* nnz */
+} mb_csc;
+
+/* IPMResult scalars (result/ipm.jl:1-15) */
+typedef struct mb_result {
+    int32_t status;
+    int32_t niter;
+    int32_t nsolve;
+    int32_t nfactor_retry;   /* ρ-regularized refactorizations (uzawa.jl:97-112) */
+    double mu, pres, dres, pobj, dobj;
+} mb_result;
+
+/* IPMHistoryRow (history/ipm.jl:1-4), integer and status fields stored as doubles */
+typedef struct mb_history_row {
+    double pres, dres, pobj, dobj, step;
+    double piter, ppass, pstat, citer, cpass, cstat;
+    double dmin, dmax, rho, delta, mu, chi;
+} mb_history_row;
+
+typedef struct mb_ctx mb_ctx;
+typedef struct mb_problem mb_problem;
+typedef struct mb_solver mb_solver;
+
+/* library */
+int mb_version(int32_t* major, int32_t* minor);
+void mb_settings_default(mb_settings* s);
+
+/* context: one device, one stream */
+int mb_ctx_create(int32_t device, mb_ctx** out);
+int mb_ctx_destroy(mb_ctx* ctx);
+int mb_last_error(mb_ctx* ctx, char* buf, int64_t size);
+
+/* problems (host-side block form; nothing is uploaded until a solver or batch uses it).  `ctx` may be
+ * NULL for a host-only problem (front-end and symbolic analysis need no GPU); a solver needs a
+ * problem created with a context, a batch takes its context from mb_batch_prepare. */
+int mb_problem_create(mb_ctx* ctx, const mb_bsm* Q, const mb_bsm* B, const double* f, const double* g,
+                      double mu, const int32_t* cone_kind, const double* cone_param,
+                      const int64_t* P1, const int64_t* P2, mb_problem** out);
+int mb_problem_create_csc(mb_ctx* ctx, const mb_csc* Q, const mb_csc* B, const double* f, const double* g,
+                          double mu, int64_t ncone, const int32_t* cone_kind, const int64_t* cone_size,
+                          const double* cone_param, double compress, mb_problem** out);
+/* sizes of the block form: n, m, nvtx, nout, narc(B), nbnz(B), narc(Q), nbnz(Q) */
+int mb_problem_info(const mb_problem* prob, int64_t* info8);
+/* copy the block form out (arrays sized by mb_problem_info; 1-based) */
+int mb_problem_export(const mb_problem* prob, int64_t* Bxsrc, int64_t* Bxcol, int64_t* Bxrow, int64_t* Bxblk,
+                      int64_t* Btgt, double* Bval, int64_t* Qxsrc, int64_t* Qxblk, int64_t* Qtgt, double* Qval,
+                      double* f, double* g, int32_t* kind, double* param, int64_t* P1, int64_t* P2);
+int mb_problem_destroy(mb_problem* prob);
+
+/* symbolic analysis (the host stand-in for CliqueTrees.symbolic, kkt/kkt.jl:23-53):
+ * vperm (nvtx, 0-based user vertex per solver vertex, postordered), and the front partition */
+int mb_problem_symbolic(const mb_problem* prob, int64_t* vperm, int64_t* nfront, int64_t* res0, int64_t* nres,
+                        int64_t* nsep, int64_t* parent, int64_t cap);
+
+/* device bytes one instance of this problem occupies under these settings (host-only query; the
+ * serving loop admits requests by this footprint) */
+int mb_problem_footprint(mb_problem* prob, const mb_settings* settings, int64_t* bytes);
+
+/* single solver: init / step! / solve! / result */
+int mb_solver_create(mb_problem* prob, const mb_settings* settings, const double* p0, const double* d0,
+                     const double* y0, mb_solver** out);
+int mb_solver_step(mb_solver* s, int32_t* status);
+int mb_solver_solve(mb_solver* s, int32_t* status);
+int mb_solver_result(mb_solver* s, double* p, double* d, double* y, mb_result* res);
+int mb_solver_history(mb_solver* s, mb_history_row* rows, int32_t cap, int32_t* nrows);
+int mb_solver_destroy(mb_solver* s);
+
+/* batched solve: every problem solved in one persistent launch (one CTA per instance at a time).
+ * Outputs per problem i: p_out[i] (n_i), d_out[i] (n_i), y_out[i] (m_i), results[i]; any output
+ * pointer may be NULL to skip it.  `grid` = CTAs of the persistent launch (0 = one per SM). */
+int mb_batch_solve(mb_ctx* ctx, mb_problem* const* probs, int32_t nprob, const mb_settings* settings,
+                   int32_t grid, double* const* p_out, double* const* d_out, double* const* y_out,
+                   mb_result* results);
+
+/* the same with every input already resident on the device: set up once, then time solves.
+ * mb_batch_prepare uploads, mb_batch_run launches and waits (device time in *ms), mb_batch_fetch
+ * copies results back. */
+typedef struct mb_batch mb_batch;
+int mb_batch_prepare(mb_ctx* ctx, mb_problem* const* probs, int32_t nprob, const mb_settings* settings,
+                     mb_batch** out);
+int mb_batch_run(mb_batch* b, int32_t grid, float* ms);
+int mb_batch_fetch(mb_batch* b, double* const* p_out, double* const* d_out, double* const* y_out,
+                   mb_result* results);
+int mb_batch_stats(mb_batch* b, int64_t* stats8);   /* bytes: input, workspace, factor; kernel launches */
+int mb_batch_destroy(mb_batch* b);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,1039 @@
+// Batched device-resident interior-point solver for sm_100a.
+//
+// One CTA runs one complete solve of Mumblebee.jl's predictor–corrector IPM
+// (src/IPM/src/ipm/solver/ipm.jl:577-774) on one problem instance that lives in HBM: Ruiz
+// equilibration, BᵀB assembly into multifrontal front storage, NT/cone scaling, the Uzawa
+// iterative refinement + CG KKT solves over a supernodal Cholesky factor, step to the boundary,
+// termination tests and the δ augmentation schedule.  A persistent grid pulls instance indices
+// from a device work counter, so instances of any size mix in one launch and a finished CTA
+// immediately starts the next instance (continuous batching); nothing a CTA computes depends on
+// which other instances share the launch.
+//
+// Precision: iterates, residuals, refinement, cone algebra and termination checks are FP64.  The
+// KKT factor is stored and computed in FT (double, or float for the mixed-precision path).
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstdio>
+#include "mb_internal.h"
+#include "mb_device.cuh"
+#include "mb_cones.cuh"
+
+namespace mb {
+
+constexpr int TS = 64;   // trailing-update tile
+
+struct Shared {
+    double red[NW + 2];
+    double diag[32 * 33];
+    double xs[32];
+    double acc[32];
+    double ta[TS * 33];
+    double tb[TS * 33];
+    int flag;
+    int ibuf[8];
+};
+
+// ---------------------------------------------------------------------------------------------
+// dense kernels on one front (column-major, leading dimension nf)
+// ---------------------------------------------------------------------------------------------
+
+// Partial Cholesky of a front: factor the leading nres columns of the (nf x nf) lower matrix and
+// update the trailing (nf-nres) block to the Schur complement.  Returns 0 or the 1-based local
+// column whose pivot was not positive (cholesky!(…; check=false) info).
+template <class FT>
+__device__ int front_chol(FT* M, int nf, int nres, Shared& sh) {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    FT* S = reinterpret_cast<FT*>(sh.diag);
+    FT* ta = reinterpret_cast<FT*>(sh.ta);
+    FT* tb = reinterpret_cast<FT*>(sh.tb);
+    for (int k0 = 0; k0 < nres; k0 += 32) {
+        const int kb = min(32, nres - k0);
+        if (warp == 0) {
+            if (lane < kb)
+                for (int c = 0; c <= lane; ++c) S[lane * 33 + c] = M[(k0 + lane) + (int64_t)(k0 + c) * nf];
+            __syncwarp();
+            int fail = 0;
+            for (int c = 0; c < kb; ++c) {
+                if (lane == c) {
+                    FT v = S[c * 33 + c];
+                    if (!(v > FT(0))) fail = c + 1; else S[c * 33 + c] = sqrt(v);
+                }
+                fail = __shfl_sync(0xffffffffu, fail, c);
+                if (fail) break;
+                __syncwarp();
+                FT dc = S[c * 33 + c];
+                if (lane > c && lane < kb) {
+                    FT l = S[lane * 33 + c] / dc;
+                    S[lane * 33 + c] = l;
+                }
+                __syncwarp();
+                if (lane > c && lane < kb) {
+                    FT l = S[lane * 33 + c];
+                    for (int cc = c + 1; cc <= lane; ++cc) S[lane * 33 + cc] -= l * S[cc * 33 + c];
+                }
+                __syncwarp();
+            }
+            if (!fail && lane < kb)
+                for (int c = 0; c <= lane; ++c) M[(k0 + lane) + (int64_t)(k0 + c) * nf] = S[lane * 33 + c];
+            if (lane == 0) sh.flag = fail ? k0 + fail : 0;
+        }
+        __syncthreads();
+        if (sh.flag) return sh.flag;
+        // panel: L21 = A21 L11^{-T}
+        const int j0 = k0 + kb;
+        for (int i = j0 + tid; i < nf; i += NT) {
+            FT x[32];
+#pragma unroll
+            for (int c = 0; c < 32; ++c) {
+                if (c < kb) {
+                    FT t = M[i + (int64_t)(k0 + c) * nf];
+#pragma unroll
+                    for (int cc = 0; cc < c; ++cc) t -= x[cc] * S[c * 33 + cc];
+                    x[c] = t / S[c * 33 + c];
+                }
+            }
+#pragma unroll
+            for (int c = 0; c < 32; ++c) if (c < kb) M[i + (int64_t)(k0 + c) * nf] = x[c];
+        }
+        __syncthreads();
+        // trailing update: M[j0:, j0:] -= L21 L21ᵀ (lower), 64x64 tiles
+        const int nrem = nf - j0;
+        if (nrem <= 0) continue;
+        const int nt = (nrem + TS - 1) / TS;
+        const int tr = tid & 15, tc = tid >> 4;   // 16 x 32 thread grid, 4x2 outputs each
+        for (int tj = 0; tj < nt; ++tj) {
+            for (int ti = tj; ti < nt; ++ti) {
+                const int rb = j0 + ti * TS, cb = j0 + tj * TS;
+                for (int idx = tid; idx < TS * 32; idx += NT) {
+                    int r = idx % TS, c = idx / TS;
+                    FT a = 0, b = 0;
+                    if (c < kb) {
+                        if (rb + r < nf) a = M[(rb + r) + (int64_t)(k0 + c) * nf];
+                        if (cb + r < nf) b = M[(cb + r) + (int64_t)(k0 + c) * nf];
+                    }
+                    ta[r * 33 + c] = a;
+                    tb[r * 33 + c] = b;
+                }
+                __syncthreads();
+                FT acc[4][2];
+#pragma unroll
+                for (int a = 0; a < 4; ++a) { acc[a][0] = 0; acc[a][1] = 0; }
+                for (int c = 0; c < kb; ++c) {
+                    FT bv0 = tb[(tc * 2 + 0) * 33 + c], bv1 = tb[(tc * 2 + 1) * 33 + c];
+#pragma unroll
+                    for (int a = 0; a < 4; ++a) {
+                        FT av = ta[(tr * 4 + a) * 33 + c];
+                        acc[a][0] += av * bv0;
+                        acc[a][1] += av * bv1;
+                    }
+                }
+#pragma unroll
+                for (int a = 0; a < 4; ++a)
+#pragma unroll
+                    for (int b = 0; b < 2; ++b) {
+                        int row = rb + tr * 4 + a, col = cb + tc * 2 + b;
+                        if (row < nf && col < nf && row >= col) M[row + (int64_t)col * nf] -= acc[a][b];
+                    }
+                __syncthreads();
+            }
+        }
+    }
+    return 0;
+}
+
+// forward solve with front f: x[res] <- D⁻¹ x[res]; x[sep] -= L_off x[res]
+template <class FT>
+__device__ void front_lsolve(const FT* M, int nf, int nres, int r0, const int* sep, double* x, Shared& sh) {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (int k0 = 0; k0 < nres; k0 += 32) {
+        const int kb = min(32, nres - k0);
+        if (warp == 0) {
+            double xv = lane < kb ? x[r0 + k0 + lane] : 0.0;
+            for (int c = 0; c < kb; ++c) {
+                double xc = 0;
+                if (lane == c) { xv = xv / (double)M[(k0 + c) + (int64_t)(k0 + c) * nf]; }
+                xc = __shfl_sync(0xffffffffu, xv, c);
+                if (lane > c && lane < kb) xv -= (double)M[(k0 + lane) + (int64_t)(k0 + c) * nf] * xc;
+            }
+            if (lane < kb) { x[r0 + k0 + lane] = xv; sh.xs[lane] = xv; }
+        }
+        __syncthreads();
+        for (int i = k0 + kb + tid; i < nf; i += NT) {
+            double t = 0;
+            for (int c = 0; c < kb; ++c) t = fma((double)M[i + (int64_t)(k0 + c) * nf], sh.xs[c], t);
+            int tg = i < nres ? r0 + i : sep[i - nres];
+            x[tg] -= t;
+        }
+        __syncthreads();
+    }
+}
+
+// backward solve with front f: x[res] -= L_offᵀ x[sep]; x[res] <- D⁻ᵀ x[res]
+template <class FT>
+__device__ void front_usolve(const FT* M, int nf, int nres, int r0, const int* sep, double* x, Shared& sh) {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int nblk = (nres + 31) / 32;
+    for (int bk = nblk - 1; bk >= 0; --bk) {
+        const int k0 = bk * 32, kb = min(32, nres - k0);
+        for (int c = warp; c < kb; c += NW) {
+            double t = 0;
+            for (int i = k0 + kb + lane; i < nf; i += 32) {
+                int src = i < nres ? r0 + i : sep[i - nres];
+                t = fma((double)M[i + (int64_t)(k0 + c) * nf], x[src], t);
+            }
+            t = warp_sum(t);
+            if (lane == 0) sh.acc[c] = t;
+        }
+        __syncthreads();
+        if (warp == 0) {
+            double yv = lane < kb ? x[r0 + k0 + lane] - sh.acc[lane] : 0.0;
+            for (int c = kb - 1; c >= 0; --c) {
+                if (lane == c) yv = yv / (double)M[(k0 + c) + (int64_t)(k0 + c) * nf];
+                double xc = __shfl_sync(0xffffffffu, yv, c);
+                if (lane < c) yv -= (double)M[(k0 + c) + (int64_t)(k0 + lane) * nf] * xc;
+            }
+            if (lane < kb) x[r0 + k0 + lane] = yv;
+        }
+        __syncthreads();
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// the per-instance solver
+// ---------------------------------------------------------------------------------------------
+template <class FT>
+struct Ctx {
+    const DevInst& I;
+    Settings set;
+    Shared& sh;
+    double* red;
+    FT* F;
+    int n, m, nv;
+    double *Df, *Qp, *wf, *Dpa, *Dda, *Dp, *Dd, *df, *dx, *cgw, *tn;
+    double *Dg, *Dya, *Dy, *dg, *dyv, *cgp, *tm1, *tm2;
+    double *vstep, *vspsd, *vflag, *vscl, *vnrm, *vswp;
+    DevBSM Hb;              // H: Q's block pattern with the scaled Hessian values
+    double delta;
+    double nf, ng, sf, sg, nB;
+    int nrow_hist;
+    int nretry;
+    __device__ Ctx(const DevInst& I_, const Settings& s_, Shared& sh_) : I(I_), set(s_), sh(sh_) {
+        red = sh.red;
+        F = reinterpret_cast<FT*>(I.F);
+        n = I.n; m = I.m; nv = I.nvtx;
+        double* v = I.vn;
+        Df = v; Qp = v + n; wf = v + 2 * (int64_t)n; Dpa = v + 3 * (int64_t)n; Dda = v + 4 * (int64_t)n;
+        Dp = v + 5 * (int64_t)n; Dd = v + 6 * (int64_t)n; df = v + 7 * (int64_t)n; dx = v + 8 * (int64_t)n;
+        cgw = v + 9 * (int64_t)n; tn = v + 10 * (int64_t)n;
+        double* w = I.vm;
+        Dg = w; Dya = w + m; Dy = w + 2 * (int64_t)m; dg = w + 3 * (int64_t)m; dyv = w + 4 * (int64_t)m;
+        cgp = w + 5 * (int64_t)m; tm1 = w + 6 * (int64_t)m; tm2 = w + 7 * (int64_t)m;
+        double* z = I.vv;
+        vstep = z; vspsd = z + nv; vflag = z + 2 * nv; vscl = z + 3 * nv; vnrm = z + 4 * nv; vswp = z + 5 * nv;
+        delta = 1; nrow_hist = 0; nretry = 0;
+        Hb = I.Q; Hb.val = I.H;
+        nf = I.scal[5]; ng = I.scal[6]; sf = I.scal[7]; sg = I.scal[8]; nB = I.scal[9];
+        nrow_hist = I.status[1]; nretry = I.status[2];
+    }
+    __device__ void save() {
+        if (threadIdx.x == 0) {
+            I.scal[5] = nf; I.scal[6] = ng; I.scal[7] = sf; I.scal[8] = sg; I.scal[9] = nB;
+            I.status[1] = nrow_hist; I.status[2] = nretry;
+        }
+        __syncthreads();
+    }
+
+    // ---- set-up --------------------------------------------------------------------------
+    // Ruiz equilibration  (src/IPM/src/scaling/scaling.jl:52-184)
+    __device__ void equilibrate(int itmax, double tol) {
+        const DevBSM& B = I.B; const DevBSM& Q = I.Q;
+        const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+        double* rnrm = tm1; double* rswp = tm2;
+        for (int v = tid; v < nv; v += NT) { vscl[v] = 1; vswp[v] = 1; }
+        for (int i = tid; i < m; i += NT) { rswp[i] = 1; I.yscl[i] = 1; }
+        __syncthreads();
+        for (int it = 0; it < itmax; ++it) {
+            for (int i = tid; i < m; i += NT) {
+                int u = B.rowout[i]; int r = i - B.xrow[u], nr = B.xrow[u + 1] - B.xrow[u];
+                double mx = 0;
+                for (int k = B.rptr[u]; k < B.rptr[u + 1]; ++k) {
+                    int e = B.rarc[k], v = B.rvtx[k];
+                    int nc = B.xcol[v + 1] - B.xcol[v];
+                    const double* blk = B.val + B.xblk[e] + r;
+                    for (int j = 0; j < nc; ++j) mx = fmax(mx, fabs(blk[(int64_t)j * nr]));
+                }
+                rnrm[i] = mx;
+            }
+            for (int v = warp; v < nv; v += NW) {
+                double mx = 0;
+                for (int e = Q.xsrc[v]; e < Q.xsrc[v + 1]; ++e)
+                    for (int64_t b = Q.xblk[e] + lane; b < Q.xblk[e + 1]; b += 32) mx = fmax(mx, fabs(Q.val[b]));
+                for (int e = B.xsrc[v]; e < B.xsrc[v + 1]; ++e)
+                    for (int64_t b = B.xblk[e] + lane; b < B.xblk[e + 1]; b += 32) mx = fmax(mx, fabs(B.val[b]));
+                mx = warp_max(mx);
+                if (lane == 0) vnrm[v] = mx;
+            }
+            __syncthreads();
+            double dd = 0;
+            for (int v = tid; v < nv; v += NT) {
+                double nn = sqrt(vnrm[v]);
+                dd = fmax(dd, fabs(1.0 - nn));
+                if (nn != 0) { vswp[v] = 1.0 / nn; vscl[v] *= vswp[v]; }
+            }
+            for (int i = tid; i < m; i += NT) {
+                double nn = sqrt(rnrm[i]);
+                dd = fmax(dd, fabs(1.0 - nn));
+                if (nn != 0) { rswp[i] = 1.0 / nn; I.yscl[i] *= rswp[i]; }
+            }
+            dd = block_reduce(dd, red, OpMax(), 0.0);
+            // applyscaling!: B ← E B D, Q ← D Q D
+            for (int v = warp; v < nv; v += NW) {
+                double sv = vswp[v];
+                int nc = B.xcol[v + 1] - B.xcol[v];
+                for (int e = B.xsrc[v]; e < B.xsrc[v + 1]; ++e) {
+                    int u = B.tgt[e], r0 = B.xrow[u], nr = B.xrow[u + 1] - r0;
+                    double* blk = B.val + B.xblk[e];
+                    for (int t = lane; t < nr * nc; t += 32) blk[t] *= rswp[r0 + t % nr] * sv;
+                }
+                for (int e = Q.xsrc[v]; e < Q.xsrc[v + 1]; ++e) {
+                    double sc = vswp[Q.tgt[e]] * sv;
+                    for (int64_t b = Q.xblk[e] + lane; b < Q.xblk[e + 1]; b += 32) Q.val[b] *= sc;
+                }
+            }
+            __syncthreads();
+            if (dd < tol) break;
+        }
+        for (int j = tid; j < n; j += NT) { I.pscl[j] = vscl[B.colvtx[j]]; I.f[j] *= I.pscl[j]; }
+        for (int i = tid; i < m; i += NT) I.g[i] *= I.yscl[i];
+        __syncthreads();
+    }
+
+    // row position of scalar column s in front f's row list
+    __device__ int rowpos(int f, int s) const {
+        int r0 = I.fres0[f], nres = I.fnres[f];
+        if (s >= r0 && s < r0 + nres) return s - r0;
+        int lo = I.fsepp[f], hi = I.fsepp[f + 1];
+        while (lo < hi) { int md = (lo + hi) >> 1; if (I.fsep[md] < s) lo = md + 1; else hi = md; }
+        return nres + (lo - I.fsepp[f]);
+    }
+
+    // Finit ← lower part of BᵀB in front layout  (uzawa.jl:29 `B' * B`; gemm.jl:48-82;
+    // chordal.jl:1-80 scatter).  Row blocks are accumulated one after another so the sum order is
+    // fixed; within a row block every entry pair is owned by one thread.
+    __device__ void build_finit() {
+        const int* vfront = I.vfront;
+        const DevBSM& B = I.B;
+        const int tid = threadIdx.x;
+        for (int64_t i = tid; i < I.fsize; i += NT) I.Finit[i] = 0;
+        __syncthreads();
+        int* koff = reinterpret_cast<int*>(tn);    // prefix column offsets of the arcs of u (<= nvtx+1 <= 2n ints)
+        for (int u = 0; u < B.nout; ++u) {
+            const int k0 = B.rptr[u], k1 = B.rptr[u + 1], deg = k1 - k0;
+            const int r0u = B.xrow[u], nr = B.xrow[u + 1] - r0u;
+            if (tid == 0) {
+                int acc = 0;
+                for (int k = 0; k < deg; ++k) { koff[k] = acc; int v = B.rvtx[k0 + k]; acc += B.xcol[v + 1] - B.xcol[v]; }
+                koff[deg] = acc;
+            }
+            __syncthreads();
+            const int cu = koff[deg];
+            const int64_t npair = (int64_t)cu * cu;
+            for (int64_t t = tid; t < npair; t += NT) {
+                int x = (int)(t % cu), y = (int)(t / cu);
+                if (x < y) continue;
+                int lo = 0, hi = deg;   // arc of x: last k with koff[k] <= x
+                while (hi - lo > 1) { int md = (lo + hi) >> 1; if (koff[md] <= x) lo = md; else hi = md; }
+                int kx = lo;
+                lo = 0; hi = deg;
+                while (hi - lo > 1) { int md = (lo + hi) >> 1; if (koff[md] <= y) lo = md; else hi = md; }
+                int ky = lo;
+                int ex = B.rarc[k0 + kx], vx = B.rvtx[k0 + kx], ey = B.rarc[k0 + ky], vy = B.rvtx[k0 + ky];
+                int xl = x - koff[kx], yl = y - koff[ky];
+                const double* bx = B.val + B.xblk[ex] + (int64_t)xl * nr;
+                const double* by = B.val + B.xblk[ey] + (int64_t)yl * nr;
+                double s = 0;
+                for (int r = 0; r < nr; ++r) s = fma(bx[r], by[r], s);
+                int sx = B.xcol[vx] + xl, sy = B.xcol[vy] + yl;
+                int f = vfront[vy];
+                int nfr = I.fnres[f] + I.fnsep[f];
+                int64_t pos = I.fptr[f] + rowpos(f, sx) + (int64_t)(sy - I.fres0[f]) * nfr;
+                I.Finit[pos] += s;
+            }
+            __syncthreads();
+        }
+    }
+
+    __device__ void startingpoint() {  // solver/ipm.jl:331-365
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+        for (int v = warp; v < nv; v += NW) {
+            int c0 = I.B.xcol[v], nc = I.B.xcol[v + 1] - c0;
+            w_identity(I.kind[v], nc, I.p + c0);
+            w_identity(I.kind[v], nc, I.d + c0);
+        }
+        (void)lane;
+        __syncthreads();
+        bgemvN(I.B, I.p, tm1, 1, 0);
+        bgemvN(I.Q, I.p, tn, 1, 0);
+        const double eps = 2.220446049250313e-16;
+        double np = bnorm(I.p, n, red), nz = bnorm(tm1, m, red), nw = bnorm(tn, n, red);
+        double sp = nz > eps * np ? fmax(1.0, bnorm(I.g, m, red) / nz) : 1.0;
+        double sd = np > eps ? fmax(1.0, (bnorm(I.f, n, red) + sp * nw) / np) : 1.0;
+        for (int i = threadIdx.x; i < n; i += NT) { I.p[i] *= sp; I.d[i] *= sd; }
+        __syncthreads();
+    }
+
+    // ---- cone fan-outs  (cone/cone.jl:146-553) -------------------------------------------
+    __device__ bool scale_all(double& spsd_sum) {
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+        for (int v = warp; v < nv; v += NW) {
+            int k = I.kind[v];
+            int c0 = I.B.xcol[v], nc = I.B.xcol[v + 1] - c0;
+            double sp = 0; bool fl = true;
+            if (k != CONE_FREE) {
+                int e = I.qdiag[v];
+                if (e < 0) fl = false;
+                else {
+                    double* Hv = I.H + I.Q.xblk[e];
+                    const double* Qv = I.Q.val + I.Q.xblk[e];
+                    for (int t = lane; t < nc * nc; t += 32) Hv[t] = Qv[t];
+                    __syncwarp();
+                    const double* p = I.p + c0; const double* d = I.d + c0;
+                    if (k == CONE_POS) {   // pos.jl:75-84
+                        double s = 0;
+                        for (int i = lane; i < nc; i += 32) { Hv[i + (int64_t)i * nc] += d[i] / p[i]; s += 1.0 / (p[i] * d[i]); }
+                        sp = warp_sum(s);
+                    } else if (k == CONE_SOC) {
+                        fl = w_socscale(Hv, I.cache + I.cxblk[v], p, d, nc, sp);
+                    }
+                }
+            }
+            if (lane == 0) { vflag[v] = fl ? 1.0 : 0.0; vspsd[v] = sp; }
+        }
+        __syncthreads();
+        double ok = 1, s = 0;
+        for (int v = threadIdx.x; v < nv; v += NT) { ok = fmin(ok, vflag[v]); s += vspsd[v]; }
+        ok = block_reduce(ok, red, OpMin(), 1.0);
+        spsd_sum = block_reduce(s, red, OpSum(), 0.0);
+        return ok > 0;
+    }
+
+    __device__ void initcorrector(double* fr, const double* Dpv, const double* Ddv, double sm) {
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+        double* work = I.work + (int64_t)warp * I.wsize;
+        for (int v = warp; v < nv; v += NW) {
+            int k = I.kind[v];
+            int c0 = I.B.xcol[v], nc = I.B.xcol[v + 1] - c0;
+            if (k == CONE_POS) {   // pos.jl:107-120
+                for (int i = lane; i < nc; i += 32) fr[c0 + i] = (sm - Dpv[c0 + i] * Ddv[c0 + i]) / I.p[c0 + i] - I.d[c0 + i];
+            } else if (k == CONE_SOC) {
+                w_soccorr(fr + c0, I.cache + I.cxblk[v], I.p + c0, Dpv + c0, Ddv + c0, sm, nc, work);
+            } else {
+                for (int i = lane; i < nc; i += 32) fr[c0 + i] = 0;
+            }
+        }
+        __syncthreads();
+    }
+
+    __device__ void initpredictor(double* fr, double sm) {
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+        for (int v = warp; v < nv; v += NW) {
+            int k = I.kind[v];
+            int c0 = I.B.xcol[v], nc = I.B.xcol[v + 1] - c0;
+            if (k == CONE_POS) {   // pos.jl:126-137
+                for (int i = lane; i < nc; i += 32) fr[c0 + i] = sm / I.p[c0 + i] - I.d[c0 + i];
+            } else if (k == CONE_SOC) {
+                w_soccorr0(fr + c0, I.cache + I.cxblk[v], I.p + c0, sm, nc);
+            } else {
+                for (int i = lane; i < nc; i += 32) fr[c0 + i] = 0;
+            }
+        }
+        __syncthreads();
+    }
+
+    __device__ double maxsteps(const double* Dpv, const double* Ddv, double step_frac) {
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+        for (int v = warp; v < nv; v += NW) {
+            int k = I.kind[v];
+            int c0 = I.B.xcol[v], nc = I.B.xcol[v + 1] - c0;
+            double tp = 1, td = 1;
+            if (k == CONE_POS) {
+                tp = w_posmaxstep(I.p + c0, Dpv + c0, nc);
+                td = w_posmaxstep(I.d + c0, Ddv + c0, nc);
+            } else if (k == CONE_SOC) {
+                const double* c = I.cache + I.cxblk[v];
+                tp = w_socmaxstep(I.p + c0, Dpv + c0, c[1], c[3], nc);
+                td = w_socmaxstep(I.d + c0, Ddv + c0, c[2], c[4], nc);
+            }
+            if (k != CONE_FREE) { tp *= step_frac; td *= step_frac; }
+            if (lane == 0) vstep[v] = jmin(tp, td);
+        }
+        __syncthreads();
+        double mn = __longlong_as_double(0x7ff0000000000000LL);
+        for (int v = threadIdx.x; v < nv; v += NT) mn = jmin(mn, vstep[v]);
+        mn = block_reduce(mn, red, OpJmin(), __longlong_as_double(0x7ff0000000000000LL));
+        return nv == 0 ? 1.0 : mn;
+    }
+
+    __device__ void zerofree(double* x) {
+        for (int v = threadIdx.x >> 5; v < nv; v += NW)
+            if (I.kind[v] == CONE_FREE)
+                for (int j = I.B.xcol[v] + (threadIdx.x & 31); j < I.B.xcol[v + 1]; j += 32) x[j] = 0;
+        __syncthreads();
+    }
+
+    // ---- factor  (kkt/uzawa.jl:73-115) ----------------------------------------------------
+    __device__ void assemble(double dl, double rho) {
+        const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+        for (int64_t i = tid; i < I.fsize; i += NT) F[i] = (FT)I.Finit[i];
+        __syncthreads();
+        for (int v = warp; v < nv; v += NW) {
+            int nc = I.Q.xcol[v + 1] - I.Q.xcol[v];
+            for (int e = I.Q.xsrc[v]; e < I.Q.xsrc[v + 1]; ++e) {
+                int64_t pos = I.hpos[e];
+                if (pos < 0) continue;
+                int u = I.Q.tgt[e], nr = I.Q.xrow[u + 1] - I.Q.xrow[u], ld = I.hld[e];
+                const double* h = I.H + I.Q.xblk[e];
+                for (int t = lane; t < nr * nc; t += 32) {
+                    int i = t % nr, j = t / nr;
+                    int64_t q = pos + i + (int64_t)j * ld;
+                    F[q] = (FT)(I.Finit[q] + dl * h[t]);
+                }
+            }
+        }
+        __syncthreads();
+        if (rho != 0) {
+            for (int f = 0; f < I.nfront; ++f) {
+                int nres = I.fnres[f], nfr = nres + I.fnsep[f];
+                FT* M = F + I.fptr[f];
+                for (int j = tid; j < nres; j += NT) M[j + (int64_t)j * nfr] = (FT)((double)M[j + (int64_t)j * nfr] + rho);
+            }
+            __syncthreads();
+        }
+    }
+
+    __device__ double factor_lower_norm() {
+        double s = 0;
+        for (int f = 0; f < I.nfront; ++f) {
+            int nres = I.fnres[f], nfr = nres + I.fnsep[f];
+            const FT* M = F + I.fptr[f];
+            for (int64_t t = threadIdx.x; t < (int64_t)nres * nfr; t += NT) {
+                int i = (int)(t % nfr), j = (int)(t / nfr);
+                if (i >= j) { double x = (double)M[t]; s += x * x; }
+            }
+        }
+        return sqrt(block_reduce(s, red, OpSum(), 0.0));
+    }
+
+    __device__ int numeric_factor() {
+        for (int f = 0; f < I.nfront; ++f) {
+            int nres = I.fnres[f], nsep = I.fnsep[f], nfr = nres + nsep;
+            FT* M = F + I.fptr[f];
+            int info = front_chol<FT>(M, nfr, nres, sh);
+            if (info) return I.fres0[f] + info;
+            int p = I.fparent[f];
+            if (p >= 0 && nsep > 0) {
+                int np = I.fnres[p] + I.fnsep[p];
+                FT* P = F + I.fptr[p];
+                const int* rel = I.frel + I.fsepp[f];
+                for (int64_t t = threadIdx.x; t < (int64_t)nsep * nsep; t += NT) {
+                    int i = (int)(t % nsep), j = (int)(t / nsep);
+                    if (i >= j) P[rel[i] + (int64_t)rel[j] * np] += M[(nres + i) + (int64_t)(nres + j) * nfr];
+                }
+                __syncthreads();
+            }
+        }
+        return 0;
+    }
+
+    __device__ bool initkkt(double dl, double& rho) {
+        delta = dl;
+        assemble(dl, 0.0);
+        int info = numeric_factor();
+        rho = 0;
+        if (info != 0) {
+            assemble(dl, 0.0);
+            rho = 2.220446049250313e-16 * factor_lower_norm();
+            assemble(dl, rho);
+            info = numeric_factor();
+            nretry++;
+        }
+        return info == 0;
+    }
+
+    __device__ void Lsolve(double* x) {
+        for (int f = 0; f < I.nfront; ++f) {
+            int nres = I.fnres[f], nfr = nres + I.fnsep[f];
+            front_lsolve<FT>(F + I.fptr[f], nfr, nres, I.fres0[f], I.fsep + I.fsepp[f], x, sh);
+        }
+    }
+    __device__ void Usolve(double* x) {
+        for (int f = I.nfront - 1; f >= 0; --f) {
+            int nres = I.fnres[f], nfr = nres + I.fnsep[f];
+            front_usolve<FT>(F + I.fptr[f], nfr, nres, I.fres0[f], I.fsep + I.fsepp[f], x, sh);
+        }
+    }
+
+    // ---- KKT solve  (kkt/kkt.jl:9-21; kkt/cg.jl:69-167; kkt/uzawa.jl:199-227, 319-507) -------
+    __device__ void mulkkt(double* u, double* v, const DevBSM& A, const double* x, const double* yv) {
+        bgemvN(A, x, u, 1, 0);
+        bgemvT(I.B, yv, u, -1, 1);
+        bgemvN(I.B, x, v, 1, 0);
+    }
+
+    __device__ int cg(int stopmode, double* x, double* yv, double* u, double atol, int itmax, int& niter) {
+        const double eps = 2.220446049250313e-16;
+        niter = 0;
+        double nu2 = bdot(u, u, m, red), nu = sqrt(nu2);
+        if (threadIdx.x == 0) I.cghist[0] = nu;
+        double np2 = nu2;
+        bfill(yv, 0.0, m);
+        int status = CG_SOLVED;
+        bool stop0 = false;
+        if (stopmode) stop0 = bscalenorm(u, I.yscl, m, red) / (1 + sg) <= set.feas_tol;
+        if (nu > atol && !stop0) {
+            status = CG_ITMAX;
+            if (itmax > 0) {
+                bcopy(cgp, u, m);
+                status = CG_CONTINUE;
+                while (status == CG_CONTINUE) {
+                    niter += 1;
+                    bgemvT(I.B, cgp, cgw, 1, 0);
+                    Lsolve(cgw);
+                    double ep2 = bdot(cgw, cgw, n, red);
+                    if (ep2 <= eps * np2) status = CG_NUMERICAL_FAILURE;
+                    else {
+                        Usolve(cgw);
+                        double a = nu2 / ep2;
+                        for (int i = threadIdx.x; i < m; i += NT) yv[i] = fma(a, cgp[i], yv[i]);
+                        for (int i = threadIdx.x; i < n; i += NT) x[i] = fma(a, cgw[i], x[i]);
+                        __syncthreads();
+                        bgemvN(I.B, cgw, u, -a, 1);
+                        double pnu2 = nu2;
+                        nu2 = bdot(u, u, m, red); nu = sqrt(nu2);
+                        if (threadIdx.x == 0 && niter <= set.newton_max_iter) I.cghist[niter] = nu;
+                        bool st = false;
+                        if (stopmode) st = bscalenorm(u, I.yscl, m, red) / (1 + sg) <= set.feas_tol;
+                        if (nu <= atol || 1.0 + nu <= 1.0 || st) status = CG_SOLVED;
+                        else if (niter >= itmax) status = CG_ITMAX;
+                        else {
+                            double b = nu2 / pnu2;
+                            for (int i = threadIdx.x; i < m; i += NT) cgp[i] = fma(b, cgp[i], u[i]);
+                            __syncthreads();
+                            np2 = nu2 + b * b * np2;
+                        }
+                    }
+                }
+            }
+        }
+        return status;
+    }
+
+    struct KKTOut { int ncg, nir, status; double dmin, dmax; };
+
+    __device__ void kktwindow(int nir, int ncg, double ftol, double gtol, double& dmin, double& dmax) {
+        const double NaN = __longlong_as_double(0x7ff8000000000000LL);
+        dmin = dmax = NaN;
+        if (nir >= 1) {
+            double logd = log(delta), logfres = log(I.uhist[1]);
+            double loggtol = log(gtol), logftol = log(ftol);
+            int i = 0;
+            double logdmax = -__longlong_as_double(0x7ff0000000000000LL);
+            double logdmin = logd + logfres - logftol;
+            while (logdmin > logdmax && i < ncg + 1) {
+                i += 1;
+                double loggres = log(I.cghist[i - 1]);
+                logdmax = logd + (loggtol - loggres) / (double)i;
+            }
+            dmin = exp(logdmin);
+            dmax = exp(logdmax);
+        }
+    }
+
+    // stopmode 1 = solveexact!'s fstop/gstop on the scaled residual norms (solver/ipm.jl:278-315)
+    __device__ KKTOut solvekkt(int stopmode, double* x, double* yv, const DevBSM& A, const double* fv,
+                               const double* gv, bool warm, double ftol, double gtol, int irmin) {
+        const double stall = set.refine_stall_tol;
+        const int irmax = set.refine_max_iter, cgmax = set.newton_max_iter;
+        const double dl = delta, alpha = 1.0 / dl;
+        int nir = 0, ncg = 0;
+        if (warm) {
+            mulkkt(df, dg, A, x, yv);
+            for (int i = threadIdx.x; i < n; i += NT) df[i] = fv[i] - df[i];
+            for (int i = threadIdx.x; i < m; i += NT) dg[i] = gv[i] - dg[i];
+            __syncthreads();
+        } else {
+            for (int i = threadIdx.x; i < n; i += NT) { df[i] = fv[i]; x[i] = 0; }
+            for (int i = threadIdx.x; i < m; i += NT) { dg[i] = gv[i]; yv[i] = 0; }
+            __syncthreads();
+        }
+        double fres = bnorm(df, n, red), fprv = fres;
+        if (threadIdx.x == 0) I.uhist[0] = fres;
+        auto fstop = [&]() { return stopmode ? bscalenorm(df, I.pscl, n, red) / (1 + sf) <= set.feas_tol : false; };
+        int irstat;
+        if (nir >= irmin && (fres <= ftol || fstop())) irstat = KKT_SOLVED;
+        else if (nir >= irmax) irstat = KKT_IRMAX;
+        else irstat = KKT_CONTINUE;
+        while (irstat == KKT_CONTINUE) {
+            nir += 1;
+            for (int i = threadIdx.x; i < n; i += NT) dx[i] = df[i] * dl;
+            __syncthreads();
+            bgemvT(I.B, dg, dx, 1, 1);
+            Lsolve(dx);
+            Usolve(dx);
+            bgemvN(I.B, dx, dg, -1, 1);
+            for (int i = threadIdx.x; i < n; i += NT) x[i] += dx[i];
+            for (int i = threadIdx.x; i < m; i += NT) yv[i] = fma(alpha, dg[i], yv[i]);
+            __syncthreads();
+            mulkkt(df, dg, A, x, yv);
+            for (int i = threadIdx.x; i < n; i += NT) df[i] = fv[i] - df[i];
+            for (int i = threadIdx.x; i < m; i += NT) dg[i] = gv[i] - dg[i];
+            __syncthreads();
+            fres = bnorm(df, n, red);
+            if (threadIdx.x == 0) I.uhist[nir] = fres;
+            if (nir >= irmin && (fres <= ftol || fstop())) irstat = KKT_SOLVED;
+            else if (nir > 1 && fres > (1 - stall) * fprv) irstat = KKT_STAGNATED;
+            else if (nir >= irmax) irstat = KKT_IRMAX;
+            else irstat = KKT_CONTINUE;
+            fprv = fres;
+        }
+        for (int i = threadIdx.x; i < m; i += NT) yv[i] = fma(-alpha, dg[i], yv[i]);
+        __syncthreads();
+        int cgstat = cg(stopmode, x, dyv, dg, gtol, cgmax, ncg);
+        for (int i = threadIdx.x; i < m; i += NT) { yv[i] = fma(alpha, dyv[i], yv[i]); yv[i] = fma(alpha, dg[i], yv[i]); }
+        __syncthreads();
+        int status;
+        if (cgstat == CG_NUMERICAL_FAILURE) status = KKT_NUMERICAL_FAILURE;
+        else if (irstat == KKT_STAGNATED) status = KKT_STAGNATED;
+        else if (irstat == KKT_IRMAX || cgstat == CG_ITMAX) status = KKT_ITMAX;
+        else status = KKT_SOLVED;
+        KKTOut o{ncg, nir, status, 0, 0};
+        kktwindow(nir, ncg, ftol, gtol, o.dmin, o.dmax);
+        return o;
+    }
+
+    // ---- the iteration  (solver/ipm.jl:86-99, 502-571, 577-774; solver/solver.jl:20-52) ------
+    __device__ void residuals() {
+        mulkkt(Df, Dg, I.Q, I.p, I.y);
+        for (int i = threadIdx.x; i < n; i += NT) Df[i] = I.d[i] + I.f[i] - Df[i];
+        for (int i = threadIdx.x; i < m; i += NT) Dg[i] = I.g[i] - Dg[i];
+        __syncthreads();
+    }
+
+    __device__ static bool isopt(double mu, double mus, double mut, double pobj, double dobj, double pres, double dres,
+                                 int nu, double gap_tol, double feas_tol) {
+        if (!(pres < feas_tol && dres < feas_tol)) return false;
+        double tol = gap_tol * fmax(1.0, fmin(fabs(pobj), fabs(dobj)));
+        if (mut > 0 && nu > 0) return (double)nu * (mu - mut + mut * log1p(mus * mut - 1.0)) <= tol;
+        return pobj - dobj < tol;
+    }
+
+    __device__ bool isprimalinfeasible(double rtol, double atol) {
+        double gy = bdot(I.g, I.y, m, red), ny = bnorm(I.y, m, red);
+        bool fl = gy > atol * ny * (1 + ng);
+        if (fl) {
+            double nQp = bnorm(Qp, n, red);
+            for (int i = threadIdx.x; i < n; i += NT) wf[i] = Qp[i] - I.d[i];
+            __syncthreads();
+            bgemvT(I.B, I.y, wf, -1, 1);
+            double nwf = bnorm(wf, n, red), nd = bnorm(I.d, n, red);
+            fl = fmax(nQp, nwf) < rtol * gy * (1 + nd / ny);
+        }
+        return fl;
+    }
+    __device__ bool isdualinfeasible(double rtol, double atol) {
+        double fp = bdot(I.f, I.p, n, red), np = bnorm(I.p, n, red);
+        bool fl = fp > atol * np * (1 + nf);
+        if (fl) {
+            bgemvN(I.B, I.p, Dya, 1, 0);
+            double a = bnorm(Dya, m, red), b = bnorm(Qp, n, red);
+            fl = fmax(a, b) < rtol * fabs(fp);
+        }
+        return fl;
+    }
+    __device__ int nearstatus(int status, double mu, double mus, double pobj, double dobj, double pres, double dres) {
+        double fct = set.near_factor;
+        if (isopt(mu, mus, I.mut, pobj, dobj, pres, dres, I.nu, fct * set.gap_tol, fct * set.feas_tol)) status = NEAR_OPTIMAL;
+        else if (isprimalinfeasible(fct * set.infeas_rel, set.infeas_abs)) status = NEAR_PRIMAL_INFEASIBLE;
+        else if (isdualinfeasible(fct * set.infeas_rel, set.infeas_abs)) status = NEAR_DUAL_INFEASIBLE;
+        return status;
+    }
+    __device__ const Row& hrow(int i) const { return *reinterpret_cast<const Row*>(I.hist + (int64_t)i * ROW_DOUBLES); }
+    __device__ bool isstalled() const {
+        const int window = 5;
+        int nh = nrow_hist;
+        double tol = set.stall_tol;
+        if (nh > window) {
+            for (int i = nh - window; i < nh; ++i) {
+                bool muok = hrow(i).mu < (1 - tol) * hrow(i - 1).mu;
+                bool pok = hrow(i).pres < (1 - tol) * hrow(i - 1).pres;
+                bool dok = hrow(i).dres < (1 - tol) * hrow(i - 1).dres;
+                if (muok || pok || dok) return false;
+            }
+            return true;
+        }
+        return false;
+    }
+    __device__ double getaug() {
+        double s = 0;
+        for (int64_t i = threadIdx.x; i < I.Q.xblk[I.Q.narc]; i += NT) s += I.H[i] * I.H[i];
+        double nH = sqrt(block_reduce(s, red, OpSum(), 0.0));
+        if (nB == 0 || nH == 0) return 1.0;
+        if (nrow_hist == 0) return set.aug_tol * nB * nB / nH;
+        const Row& r = hrow(nrow_hist - 1);
+        double dl = r.delta, dmin = r.dmin, dmax = r.dmax;
+        if (r.ppass > 1) {
+            if (isfinite(dmin)) dl = fmax(dl, dmin);
+            dl *= 10;
+        } else if (isfinite(dmin) && isfinite(dmax) && dmin > 0 && dmax > 0) {
+            dl = sqrt(dmin) * sqrt(dmax);
+        }
+        return dl;
+    }
+
+    __device__ int step() {
+        const double NaN = __longlong_as_double(0x7ff8000000000000LL);
+        int status = CONTINUE;
+        Row row{NaN, NaN, NaN, NaN, 0.0, 0, 0, (double)KKT_SOLVED, 0, 0, (double)KKT_SOLVED, NaN, NaN, NaN, 0.0, NaN, NaN};
+        double dl = getaug();
+        double pd = bdot(I.p, I.d, n, red);
+        double spsd = 0;
+        bool ok = scale_all(spsd);
+        if (!ok) {
+            status = NUMERICAL_FAILURE;
+        } else {
+            residuals();
+            double nuf = (double)max(I.nu, 1);
+            double mu = pd / nuf, mus = spsd / nuf, chi = mu * mus - 1;
+            double pres = bscalenorm(Dg, I.yscl, m, red) / (1 + sg);
+            double dres = bscalenorm(Df, I.pscl, n, red) / (1 + sf);
+            bgemvN(I.Q, I.p, Qp, 1, 0);
+            double pQp = bdot(I.p, Qp, n, red);
+            double pobj = pQp / 2 - bdot(I.f, I.p, n, red);
+            double dobj = bdot(I.g, I.y, m, red) - pQp / 2;
+            row.mu = mu; row.chi = chi; row.pres = pres; row.dres = dres; row.pobj = pobj; row.dobj = dobj;
+            if (isopt(mu, mus, I.mut, pobj, dobj, pres, dres, I.nu, set.gap_tol, set.feas_tol)) status = OPTIMAL;
+            else if (isprimalinfeasible(set.infeas_rel, set.infeas_abs)) status = PRIMAL_INFEASIBLE;
+            else if (isdualinfeasible(set.infeas_rel, set.infeas_abs)) status = DUAL_INFEASIBLE;
+            else if (nrow_hist >= set.max_iter) status = nearstatus(ITERATION_LIMIT, mu, mus, pobj, dobj, pres, dres);
+            else if (isstalled()) status = nearstatus(STALLED, mu, mus, pobj, dobj, pres, dres);
+            else if (I.nu == 0) {
+                double rho;
+                bool iok = initkkt(dl, rho);
+                row.rho = rho;
+                if (!iok) status = nearstatus(NUMERICAL_FAILURE, mu, mus, pobj, dobj, pres, dres);
+                else {
+                    const double eps = 2.220446049250313e-16;
+                    KKTOut o = solvekkt(1, Dpa, Dya, Hb, Df, Dg, false, eps, eps, 0);
+                    row.piter = o.ncg; row.ppass = o.nir; row.pstat = o.status; row.dmin = o.dmin; row.dmax = o.dmax;
+                    for (int i = threadIdx.x; i < n; i += NT) I.p[i] += Dpa[i];
+                    for (int i = threadIdx.x; i < m; i += NT) I.y[i] += Dya[i];
+                    __syncthreads();
+                }
+            } else if (!(mu > 0)) {
+                status = nearstatus(NUMERICAL_FAILURE, mu, mus, pobj, dobj, pres, dres);
+            } else {
+                double rho;
+                bool iok = initkkt(dl, rho);
+                row.rho = rho;
+                if (!iok) status = nearstatus(NUMERICAL_FAILURE, mu, mus, pobj, dobj, pres, dres);
+                else {
+                    double mu1 = nrow_hist == 0 ? mu : hrow(0).mu;
+                    double tol;
+                    if (I.mut > 0) tol = 0.1 * fmin(fabs(mu - I.mut) / fabs(mu1 - I.mut), 1.0);
+                    else tol = 0.1 * mu / mu1;
+                    double ftol = tol * (1 + nf), gtol = tol * (1 + ng);
+                    // predictor  (solver/ipm.jl:119-163)
+                    if (I.mut > 0) initpredictor(wf, I.mut);
+                    else { for (int i = threadIdx.x; i < n; i += NT) wf[i] = -I.d[i]; __syncthreads(); }
+                    baxpy(1.0, Df, wf, n);
+                    KKTOut po = solvekkt(0, Dpa, Dya, Hb, wf, Dg, false, ftol, gtol, 1);
+                    bcopy(Dda, Df, n);
+                    bgemvT(I.B, Dya, Dda, -1, -1);
+                    bgemvN(I.Q, Dpa, Dda, 1, 1);
+                    row.piter = po.ncg; row.ppass = po.nir; row.pstat = po.status; row.dmin = po.dmin; row.dmax = po.dmax;
+                    zerofree(Dda);
+                    // corrector  (solver/ipm.jl:181-272)
+                    double taua = maxsteps(Dpa, Dda, 1.0);
+                    double sm = 0;
+                    for (int j = threadIdx.x; j < n; j += NT) sm += (I.p[j] + taua * Dpa[j]) * (I.d[j] + taua * Dda[j]);
+                    sm = block_reduce(sm, red, OpSum(), 0.0);
+                    double mua = sm / (double)I.nu;
+                    if (I.mut > 0) {
+                        double dmu = mu - I.mut;
+                        if (dmu > 0) {
+                            double dmua = fmin(fmax(mua - I.mut, 0.0), dmu);
+                            sm = I.mut + fmin(fmax(dmua * (dmua / dmu) * (dmua / dmu), 0.0), dmu);
+                        } else sm = I.mut;
+                    } else {
+                        double t = mua * (mua / mu) * (mua / mu);
+                        sm = t > mu ? mu : (t < 0 ? 0.0 : t);
+                    }
+                    initcorrector(wf, Dpa, Dda, sm);
+                    baxpy(1.0, Df, wf, n);
+                    bcopy(Dp, Dpa, n);
+                    bcopy(Dy, Dya, m);
+                    KKTOut co = solvekkt(0, Dp, Dy, Hb, wf, Dg, true, ftol, gtol, 1);
+                    bcopy(Dd, Df, n);
+                    bgemvT(I.B, Dy, Dd, -1, -1);
+                    bgemvN(I.Q, Dp, Dd, 1, 1);
+                    row.citer = co.ncg; row.cpass = co.nir; row.cstat = co.status;
+                    zerofree(Dd);
+                    if (po.status != KKT_SOLVED || co.status != KKT_SOLVED) {
+                        status = nearstatus(NUMERICAL_FAILURE, mu, mus, pobj, dobj, pres, dres);
+                    } else {
+                        double st = maxsteps(Dp, Dd, set.step_frac);
+                        row.step = st;
+                        for (int i = threadIdx.x; i < n; i += NT) { I.p[i] = fma(st, Dp[i], I.p[i]); I.d[i] = fma(st, Dd[i], I.d[i]); }
+                        for (int i = threadIdx.x; i < m; i += NT) I.y[i] = fma(st, Dy[i], I.y[i]);
+                        __syncthreads();
+                    }
+                }
+            }
+        }
+        row.delta = dl;
+        if (threadIdx.x == 0 && nrow_hist <= set.max_iter)
+            *reinterpret_cast<Row*>(I.hist + (int64_t)nrow_hist * ROW_DOUBLES) = row;
+        nrow_hist++;
+        __syncthreads();
+        return status;
+    }
+
+    // result(s, status)  (solver/ipm.jl:30-74): scalars + unscaled iterates in solver order
+    __device__ void result(int status) {
+        const double NaN = __longlong_as_double(0x7ff8000000000000LL);
+        double mu = NaN, pres = NaN, dres = NaN, pobj = NaN, dobj = NaN;
+        bool infeas = status == PRIMAL_INFEASIBLE || status == NEAR_PRIMAL_INFEASIBLE ||
+                      status == DUAL_INFEASIBLE || status == NEAR_DUAL_INFEASIBLE;
+        if (!(infeas || nrow_hist == 0)) {
+            residuals();
+            double pQp = bbdot(I.Q, I.p, I.p, red);
+            pobj = pQp / 2 - bdot(I.f, I.p, n, red);
+            dobj = bdot(I.g, I.y, m, red) - pQp / 2;
+            mu = I.nu == 0 ? NaN : bdot(I.p, I.d, n, red) / (double)I.nu;
+            pres = bscalenorm(Dg, I.yscl, m, red) / (1 + sg);
+            dres = bscalenorm(Df, I.pscl, n, red) / (1 + sf);
+        }
+        if (threadIdx.x == 0) {
+            I.scal[0] = mu; I.scal[1] = pres; I.scal[2] = dres; I.scal[3] = pobj; I.scal[4] = dobj;
+            I.scal[5] = nf; I.scal[6] = ng; I.scal[7] = sf; I.scal[8] = sg; I.scal[9] = nB;
+            I.status[0] = status; I.status[1] = nrow_hist; I.status[2] = nretry;
+        }
+        for (int i = threadIdx.x; i < n; i += NT) { I.po[i] = I.p[i] * I.pscl[i]; I.dout[i] = I.d[i] / I.pscl[i]; }
+        for (int i = threadIdx.x; i < m; i += NT) I.yo[i] = I.y[i] * I.yscl[i];
+        __syncthreads();
+    }
+};
+
+// init (solver/ipm.jl:431-478 and reinit! :375-429), then the solve_impl! loop
+// (solver/solver.jl:119-145) and result, or one of those pieces (mode)
+template <class FT>
+__device__ void solve_instance(const DevInst& I, const Settings& set, Shared& sh, int mode) {
+    const int n = I.n, m = I.m;
+    if (mode == MODE_SOLVE || mode == MODE_INIT) {
+        if (threadIdx.x == 0) { for (int k = 0; k < NSTAT; ++k) I.status[k] = 0; }
+        __syncthreads();
+    }
+    Ctx<FT> c(I, set, sh);
+    if (mode == MODE_SOLVE || mode == MODE_INIT) {
+        // working copies of the inputs: a solve never modifies the uploaded problem
+        for (int64_t i = threadIdx.x; i < I.B.xblk[I.B.narc]; i += NT) I.B.val[i] = I.Bval0[i];
+        for (int64_t i = threadIdx.x; i < I.Q.xblk[I.Q.narc]; i += NT) I.Q.val[i] = I.Qval0[i];
+        for (int i = threadIdx.x; i < n; i += NT) { I.f[i] = I.f0[i]; I.p[i] = I.p0[i]; I.d[i] = I.d0[i]; }
+        for (int i = threadIdx.x; i < m; i += NT) { I.g[i] = I.g0[i]; I.y[i] = I.y0[i]; }
+        __syncthreads();
+        // H = copy(Q) happens after equilibration (IPMSolver constructor order)
+        if (set.scale_max_iter > 0) c.equilibrate(set.scale_max_iter, 1e-3);
+        else {
+            for (int j = threadIdx.x; j < n; j += NT) I.pscl[j] = 1;
+            for (int i = threadIdx.x; i < m; i += NT) I.yscl[i] = 1;
+            __syncthreads();
+        }
+        c.build_finit();
+        int64_t nq = I.Q.xblk[I.Q.narc];
+        for (int64_t i = threadIdx.x; i < nq; i += NT) I.H[i] = I.Q.val[i];
+        double s = 0;
+        for (int64_t i = threadIdx.x; i < I.B.xblk[I.B.narc]; i += NT) s += I.B.val[i] * I.B.val[i];
+        c.nB = sqrt(block_reduce(s, c.red, OpSum(), 0.0));
+        c.nf = bnorm(I.f, n, c.red);
+        c.ng = bnorm(I.g, m, c.red);
+        c.sg = bscalenorm(I.g, I.yscl, m, c.red);
+        c.sf = bscalenorm(I.f, I.pscl, n, c.red);
+        if (!I.has_p0 && !I.has_d0) {
+            c.startingpoint();
+            if (I.has_y0) { for (int i = threadIdx.x; i < m; i += NT) I.y[i] /= I.yscl[i]; }
+            else { for (int i = threadIdx.x; i < m; i += NT) I.y[i] = 0; }
+            __syncthreads();
+        } else {
+            const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+            if (!(I.has_p0 && I.has_d0)) {
+                for (int v = warp; v < I.nvtx; v += NW) {   // dualshadow! / primalshadow!
+                    int k = I.kind[v], c0 = I.B.xcol[v], nc = I.B.xcol[v + 1] - c0;
+                    double* dst = !I.has_d0 ? I.d + c0 : I.p + c0;
+                    const double* src = !I.has_d0 ? I.p + c0 : I.d + c0;
+                    if (k == CONE_POS) { for (int i = lane; i < nc; i += 32) dst[i] = 1.0 / src[i]; }
+                    else if (k == CONE_SOC) w_socshadow(dst, src, nc);
+                    else { for (int i = lane; i < nc; i += 32) dst[i] = 0; }
+                }
+            }
+            __syncthreads();
+            if (!I.has_y0) for (int i = threadIdx.x; i < m; i += NT) I.y[i] = 0;
+            for (int i = threadIdx.x; i < n; i += NT) { I.p[i] /= I.pscl[i]; I.d[i] *= I.pscl[i]; }
+            for (int i = threadIdx.x; i < m; i += NT) I.y[i] /= I.yscl[i];
+            __syncthreads();
+        }
+        c.save();
+        if (threadIdx.x == 0) I.status[0] = CONTINUE;
+        __syncthreads();
+    }
+    if (mode == MODE_SOLVE) {
+        int status = CONTINUE;
+        while (status == CONTINUE) status = c.step();
+        c.result(status);
+    } else if (mode == MODE_STEP) {
+        int status = c.step();
+        c.save();
+        if (threadIdx.x == 0) I.status[0] = status;
+        __syncthreads();
+    } else if (mode == MODE_RESULT) {
+        c.result(I.status[0]);
+    }
+}
+
+struct BatchArgs {
+    const DevInst* inst;
+    int ninst;
+    int mode;
+    Settings set;
+    int* counter;     // work queue head
+};
+
+template <class FT>
+__global__ void __launch_bounds__(NT, 1) ipm_batch_kernel(BatchArgs a) {
+    __shared__ Shared sh;
+    __shared__ int next;
+    for (;;) {
+        if (threadIdx.x == 0) next = atomicAdd(a.counter, 1);
+        __syncthreads();
+        int k = next;
+        __syncthreads();
+        if (k >= a.ninst) break;
+        solve_instance<FT>(a.inst[k], a.set, sh, a.mode);
+    }
+}
+
+}  // namespace mb
+
+// ---------------------------------------------------------------------------------------------
+// launch entry used by the host runtime
+// ---------------------------------------------------------------------------------------------
+extern "C" int mb_launch_batch(const mb::DevInst* d_inst, int ninst, int mode, const mb::Settings* set,
+                               int* d_counter, int grid, int fp32, cudaStream_t stream) {
+    mb::BatchArgs a;
+    a.inst = d_inst; a.ninst = ninst; a.mode = mode; a.set = *set; a.counter = d_counter;
+    cudaError_t e = cudaMemsetAsync(d_counter, 0, sizeof(int), stream);
+    if (e != cudaSuccess) return -1;
+    if (fp32) mb::ipm_batch_kernel<float><<<grid, mb::NT, 0, stream>>>(a);
+    else mb::ipm_batch_kernel<double><<<grid, mb::NT, 0, stream>>>(a);
+    e = cudaGetLastError();
+    return e == cudaSuccess ? 0 : -2;
+}

@@ -1,0 +1,98 @@
+"""Seeded synthetic problem generators for the benchmark workloads.
+
+Each generator returns the reference's native CSC input of
+``IPMProblem(Q, B, f, g, μ, K, s; compress)`` (src/IPM/src/ipm/problem.jl:84-127):
+``min ½pᵀQp − fᵀp  s.t.  Bp = g,  p ∈ K`` with the cone list given as (kind, size, param).
+
+Standard-form data (min cᵀx s.t. Ax = b, x ∈ K) maps to it as Q = 0, B = A, g = b, f = −c, so the
+dual slack of the reference, d = Qp − f − Bᵀy, is c − Aᵀy.
+"""
+from __future__ import annotations
+
+import numpy as np
+import scipy.sparse as sp
+
+CONE_FREE, CONE_POS, CONE_SOC, CONE_SDP, CONE_EXP, CONE_POW = 0, 1, 2, 3, 4, 5
+
+
+def _soc_interior(rng, k):
+    u = rng.standard_normal(k - 1)
+    t = np.linalg.norm(u) + 1.0 + rng.uniform()
+    return np.concatenate([[t], u])
+
+
+def socp(n=500, m=200, ncone=25, density=0.05, seed=0):
+    """Plain SOCP: A sparse with N(0,1) entries at the given density; ``ncone`` second-order
+    cones of dimension n/ncone; feasible by construction: x0, s0 in cone interiors
+    (t = ‖u‖ + 1 + U(0,1)), y0 ~ N(0,1), b = A x0, c = Aᵀ y0 + s0."""
+    rng = np.random.default_rng(seed)
+    k = n // ncone
+    assert k * ncone == n
+    A = sp.random(m, n, density=density, format="csc", random_state=rng,
+                  data_rvs=lambda s: rng.standard_normal(s))
+    x0 = np.concatenate([_soc_interior(rng, k) for _ in range(ncone)])
+    s0 = np.concatenate([_soc_interior(rng, k) for _ in range(ncone)])
+    y0 = rng.standard_normal(m)
+    b = A @ x0
+    c = A.T @ y0 + s0
+    Q = sp.csc_matrix((n, n))
+    return dict(Q=Q, B=sp.csc_matrix(A), f=-c, g=b, mu=0.0,
+                kinds=[CONE_SOC] * ncone, sizes=[k] * ncone, params=[0.0] * ncone,
+                name=f"socp n={n} m={m} {ncone}xSOC({k}) density={density} seed={seed}")
+
+
+def portfolio(n_assets, nfac=10, gamma=1.0, seed=0, rng=None):
+    """Long-only factor-model portfolio with a risk budget (lifted form keeps Q and the SOC
+    sparse).  Variables p = [x (n, POS); y (nfac, free); s = (t, u, w) (SOC of dim 1+n+nfac)]:
+
+        min  γ (xᵀ D x + yᵀ y) − μᵀ x
+        s.t. Fᵀ x − y = 0,  1ᵀ x = 1,  t = σ,  u − D^{1/2} x = 0,  w − y = 0,
+             x ≥ 0,  ‖(u, w)‖ ≤ t.
+
+    Covariance F Fᵀ + D with F (n x nfac) N(0,1), D ~ U(0.1, 1); expected returns μ ~ N(0, 1)/10;
+    σ = 0.8 · risk of the equal-weight portfolio, so the risk bound binds on most instances."""
+    rng = rng if rng is not None else np.random.default_rng(seed)
+    n, k = n_assets, nfac
+    F = rng.standard_normal((n, k))
+    D = rng.uniform(0.1, 1.0, n)
+    mu_r = rng.standard_normal(n) / 10
+    xe = np.full(n, 1.0 / n)
+    sigma = 0.8 * np.sqrt(xe @ (D * xe) + np.sum((F.T @ xe) ** 2))
+    nx, ny, ns = n, k, 1 + n + k
+    N = nx + ny + ns
+    ox, oy, os_ = 0, nx, nx + ny
+    Qd = np.zeros(N)
+    Qd[ox:ox + nx] = 2 * gamma * D
+    Qd[oy:oy + ny] = 2 * gamma
+    Q = sp.diags(Qd).tocsc()
+    f = np.zeros(N)
+    f[ox:ox + nx] = mu_r
+    rows, cols, vals = [], [], []
+    g = []
+    r = 0
+    for j in range(k):                       # Fᵀx − y = 0
+        rows += [r] * n; cols += list(range(ox, ox + nx)); vals += list(F[:, j])
+        rows.append(r); cols.append(oy + j); vals.append(-1.0)
+        g.append(0.0); r += 1
+    rows += [r] * n; cols += list(range(ox, ox + nx)); vals += [1.0] * n   # budget
+    g.append(1.0); r += 1
+    rows.append(r); cols.append(os_); vals.append(1.0); g.append(sigma); r += 1   # t = σ
+    sD = np.sqrt(D)
+    for i in range(n):                       # u_i − √D_i x_i = 0
+        rows += [r, r]; cols += [os_ + 1 + i, ox + i]; vals += [1.0, -sD[i]]
+        g.append(0.0); r += 1
+    for j in range(k):                       # w_j − y_j = 0
+        rows += [r, r]; cols += [os_ + 1 + n + j, oy + j]; vals += [1.0, -1.0]
+        g.append(0.0); r += 1
+    B = sp.csc_matrix((vals, (rows, cols)), shape=(r, N))
+    kinds = [CONE_POS] * nx + [CONE_FREE] * ny + [CONE_SOC]
+    sizes = [1] * nx + [1] * ny + [ns]
+    return dict(Q=Q, B=B, f=f, g=np.array(g), mu=0.0, kinds=kinds, sizes=sizes,
+                params=[0.0] * len(kinds), name=f"portfolio n={n} nfac={k} seed={seed}")
+
+
+def portfolio_batch(count=4096, nmin=50, nmax=400, nfac=10, seed=0):
+    """``count`` portfolio instances with n_assets ~ U[nmin, nmax] (integers), one stream."""
+    rng = np.random.default_rng(seed)
+    sizes = rng.integers(nmin, nmax + 1, size=count)
+    return [portfolio(int(s), nfac=nfac, rng=np.random.default_rng([seed, i])) for i, s in enumerate(sizes)]

@@ -1,0 +1,459 @@
+"""Python mirror of Mumblebee.jl's `IPM` solver API over libmbgpu.so.
+
+Same names and argument meaning as the reference (src/IPM/IPM.jl:42-47 exports):
+
+    IPMProblem(Q, B, f, g, μ, K, s; compress)   problem.jl:84-127  (CSC input)
+    IPMProblem.from_blocks(Q, B, f, g, μ, K)    problem.jl:49-71   (BlockSparseMatrix input)
+    IPMSettings(...)                            settings/ipm.jl:1-18
+    init(prob, settings; p0, d0, y0)            solver/ipm.jl:485-491
+    step(solver)      — step!(solver)           solver/ipm.jl:577-774
+    solve_(solver)    — solve!(solver)          solver/solver.jl:147-150
+    solve(prob, settings)                       solver/ipm.jl:798-804
+    IPMResult / IPMHistory / IPMStatus          result/ipm.jl, history/ipm.jl, ipm/ipm.jl:1
+
+The numeric work runs on the GPU; there is no CPU path.  `batch_solve` solves many problems in one
+persistent launch.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import enum
+from dataclasses import dataclass, field, fields
+
+import numpy as np
+import scipy.sparse as sp
+
+from . import _lib
+from ._lib import check, mb_bsm, mb_csc, mb_history_row, mb_result, mb_settings, ROW_FIELDS
+
+
+class IPMStatus(enum.IntEnum):
+    CONTINUE = 0
+    OPTIMAL = 1
+    NEAR_OPTIMAL = 2
+    STALLED = 3
+    NUMERICAL_FAILURE = 4
+    ITERATION_LIMIT = 5
+    PRIMAL_INFEASIBLE = 6
+    DUAL_INFEASIBLE = 7
+    ILL_POSED = 8
+    NEAR_PRIMAL_INFEASIBLE = 9
+    NEAR_DUAL_INFEASIBLE = 10
+    NEAR_ILL_POSED = 11
+
+
+class KKTStatus(enum.IntEnum):
+    KKT_CONTINUE = 0
+    KKT_SOLVED = 1
+    KKT_STAGNATED = 2
+    KKT_ITMAX = 3
+    KKT_NUMERICAL_FAILURE = 4
+    KKT_IRMAX = 5
+
+
+# ---------------------------------------------------------------------------------------- cones
+class AbstractCone:
+    kind = -1
+    param = 0.0
+
+
+class CofreeCone(AbstractCone):
+    kind = 0
+
+
+class PositiveCone(AbstractCone):
+    kind = 1
+
+
+class SecondOrderCone(AbstractCone):
+    kind = 2
+
+
+class SemidefiniteCone(AbstractCone):
+    kind = 3
+
+
+class ExponentialCone(AbstractCone):
+    kind = 4
+
+
+class PowerCone(AbstractCone):
+    kind = 5
+
+    def __init__(self, alpha: float):
+        self.param = float(alpha)
+
+
+_CONES = {0: CofreeCone, 1: PositiveCone, 2: SecondOrderCone, 3: SemidefiniteCone, 4: ExponentialCone, 5: PowerCone}
+
+
+# ---------------------------------------------------------------------------------------- settings
+@dataclass
+class IPMSettings:
+    verbose: int = 0
+    step_frac: float = 0.99
+    feas_tol: float = 1e-8
+    gap_tol: float = 1e-8
+    max_iter: int = 100
+    near_factor: float = 1000.0
+    stall_tol: float = 1e-3
+    refine_stall_tol: float = 0.5
+    scale_max_iter: int = 10
+    refine_max_iter: int = 10
+    newton_max_iter: int = 100
+    aug_tol: float = 1e-7
+    stable: bool = False
+    infeas_abs: float = 1e-8
+    infeas_rel: float = 1e-8
+    precision: str = "fp64"          # "fp64" or "fp32" (factor precision; refinement stays FP64)
+
+    def to_c(self) -> mb_settings:
+        s = mb_settings()
+        for f in fields(self):
+            if f.name == "precision":
+                s.precision = {"fp64": 0, "fp32": 1}[self.precision]
+            elif f.name == "stable":
+                s.stable = int(self.stable)
+            else:
+                setattr(s, f.name, getattr(self, f.name))
+        return s
+
+
+# ---------------------------------------------------------------------------------------- context
+class Context:
+    """One device and one stream (mb_ctx).  `Context.host()` is a GPU-less context for problem
+    construction and symbolic analysis only."""
+    _default: dict = {}
+    _host = None
+
+    def __init__(self, device: int = 0):
+        self.L = _lib.load()
+        h = C.c_void_p()
+        rc = self.L.mb_ctx_create(device, C.byref(h))
+        if rc != 0:
+            raise _lib.MBError(f"mb_ctx_create({device}) failed with code {rc} (no CUDA device?)")
+        self.h = h
+        self.device = device
+
+    @classmethod
+    def host(cls) -> "Context":
+        if cls._host is None:
+            c = cls.__new__(cls)
+            c.L = _lib.load(); c.h = None; c.device = -1
+            cls._host = c
+        return cls._host
+
+    @classmethod
+    def default(cls, device: int = 0) -> "Context":
+        if device not in cls._default:
+            cls._default[device] = cls(device)
+        return cls._default[device]
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.L.mb_ctx_destroy(self.h)
+            self.h = None
+
+
+def _a64(x):
+    return np.ascontiguousarray(x, dtype=np.int64)
+
+
+def _f64(x):
+    return np.ascontiguousarray(x, dtype=np.float64)
+
+
+def _p(a, t):
+    return None if a is None else a.ctypes.data_as(C.POINTER(t))
+
+
+# ---------------------------------------------------------------------------------------- problem
+class IPMProblem:
+    """A primal-dual pair of conic QPs (problem.jl:1-19):
+
+        (P) min ½pᵀQp − fᵀp  s.t. Bp = g, p ∈ K
+        (D) max −½pᵀQp + gᵀy  s.t. Qp − f − Bᵀy = d ∈ K*
+    """
+
+    def __init__(self, Q, B, f, g, mu, K, s, compress: float = 1.0, ctx: Context | None = None):
+        self.ctx = ctx or Context.default()
+        L = self.ctx.L
+        Qc = sp.csc_matrix(Q); Bc = sp.csc_matrix(B)
+        Qc.sort_indices(); Bc.sort_indices()
+        keep = []
+
+        def csc(A):
+            cp = _a64(A.indptr + 1); rv = _a64(A.indices + 1); nz = _f64(A.data)
+            keep.extend([cp, rv, nz])
+            return mb_csc(A.shape[0], A.shape[1], _p(cp, C.c_int64), _p(rv, C.c_int64), _p(nz, C.c_double))
+
+        kinds = np.array([k.kind for k in K], dtype=np.int32)
+        params = _f64([k.param for k in K])
+        sizes = _a64(s)
+        fv, gv = _f64(f), _f64(g)
+        q, b = csc(Qc), csc(Bc)
+        h = C.c_void_p()
+        rc = L.mb_problem_create_csc(self.ctx.h, C.byref(q), C.byref(b), _p(fv, C.c_double), _p(gv, C.c_double),
+                                     float(mu), len(K), _p(kinds, C.c_int32), _p(sizes, C.c_int64),
+                                     _p(params, C.c_double), float(compress), C.byref(h))
+        check(rc, self.ctx.h, "IPMProblem")
+        self.h = h
+        self.mu = float(mu)
+
+    @classmethod
+    def from_blocks(cls, Q: dict, B: dict, f, g, mu, K, P1=None, P2=None, ctx: Context | None = None, params=None):
+        """IPMProblem(Q::BlockSparseMatrix, B::BlockSparseMatrix, f, g, μ, K[, P1, P2]); Q/B are dicts
+        with the 1-based BlockSparseMatrix fields (nout, nvtx, narc, ncol, nrow, nbnz, xsrc, xcol,
+        xrow, xblk, tgt, val)."""
+        self = cls.__new__(cls)
+        self.ctx = ctx or Context.default()
+        L = self.ctx.L
+        keep = []
+
+        def bsm(d):
+            a = {k: _a64(d[k]) for k in ("xsrc", "xcol", "xrow", "xblk", "tgt")}
+            a["val"] = _f64(d["val"])
+            keep.extend(a.values())
+            return mb_bsm(d["nout"], d["nvtx"], d["narc"], d["ncol"], d["nrow"], d["nbnz"],
+                          *[_p(a[k], C.c_int64) for k in ("xsrc", "xcol", "xrow", "xblk", "tgt")],
+                          _p(a["val"], C.c_double))
+
+        if len(K) and isinstance(K[0], AbstractCone):
+            kinds = np.array([k.kind for k in K], dtype=np.int32)
+            params = _f64([k.param for k in K])
+        else:
+            kinds = np.ascontiguousarray(K, dtype=np.int32)
+            params = _f64(np.zeros(len(kinds)) if params is None else params)
+        q, b = bsm(Q), bsm(B)
+        fv, gv = _f64(f), _f64(g)
+        p1 = None if P1 is None else _a64(P1)
+        p2 = None if P2 is None else _a64(P2)
+        h = C.c_void_p()
+        rc = L.mb_problem_create(self.ctx.h, C.byref(q), C.byref(b), _p(fv, C.c_double), _p(gv, C.c_double),
+                                 float(mu), _p(kinds, C.c_int32), _p(params, C.c_double), _p(p1, C.c_int64),
+                                 _p(p2, C.c_int64), C.byref(h))
+        check(rc, self.ctx.h, "IPMProblem")
+        self.h = h
+        self.mu = float(mu)
+        return self
+
+    @classmethod
+    def from_dict(cls, d: dict, ctx: Context | None = None):
+        return cls.from_blocks(d["Q"], d["B"], d["f"], d["g"], d["mu"], d["kind"], d.get("P1"), d.get("P2"), ctx=ctx,
+                               params=d.get("param"))
+
+    def info(self):
+        a = np.zeros(8, dtype=np.int64)
+        self.ctx.L.mb_problem_info(self.h, _p(a, C.c_int64))
+        return dict(zip(["n", "m", "nvtx", "nout", "narcB", "nbnzB", "narcQ", "nbnzQ"], a.tolist()))
+
+    @property
+    def n(self):
+        return self.info()["n"]
+
+    @property
+    def m(self):
+        return self.info()["m"]
+
+    def blocks(self) -> dict:
+        """The block form (BlockSparseMatrix fields, 1-based), as the reference stores IPMProblem."""
+        i = self.info()
+        nv, no, nab, nbb, naq, nbq = i["nvtx"], i["nout"], i["narcB"], i["nbnzB"], i["narcQ"], i["nbnzQ"]
+        n, m = i["n"], i["m"]
+        Bx = [np.zeros(nv + 1, np.int64), np.zeros(nv + 1, np.int64), np.zeros(no + 1, np.int64),
+              np.zeros(nab + 1, np.int64), np.zeros(nab, np.int64), np.zeros(nbb)]
+        Qx = [np.zeros(nv + 1, np.int64), np.zeros(naq + 1, np.int64), np.zeros(naq, np.int64), np.zeros(nbq)]
+        f = np.zeros(n); g = np.zeros(m); kind = np.zeros(nv, np.int32); par = np.zeros(nv)
+        P1 = np.zeros(m, np.int64); P2 = np.zeros(n, np.int64)
+        self.ctx.L.mb_problem_export(self.h, *[_p(a, C.c_int64) for a in Bx[:5]], _p(Bx[5], C.c_double),
+                                     _p(Qx[0], C.c_int64), _p(Qx[1], C.c_int64), _p(Qx[2], C.c_int64),
+                                     _p(Qx[3], C.c_double), _p(f, C.c_double), _p(g, C.c_double),
+                                     _p(kind, C.c_int32), _p(par, C.c_double), _p(P1, C.c_int64), _p(P2, C.c_int64))
+        B = dict(nout=no, nvtx=nv, narc=nab, ncol=n, nrow=m, nbnz=nbb, xsrc=Bx[0], xcol=Bx[1], xrow=Bx[2],
+                 xblk=Bx[3], tgt=Bx[4], val=Bx[5])
+        Q = dict(nout=nv, nvtx=nv, narc=naq, ncol=n, nrow=n, nbnz=nbq, xsrc=Qx[0], xcol=Bx[1], xrow=Bx[1],
+                 xblk=Qx[1], tgt=Qx[2], val=Qx[3])
+        return dict(Q=Q, B=B, f=f, g=g, mu=self.mu, kind=kind, param=par, P1=P1, P2=P2)
+
+    def footprint(self, settings: "IPMSettings | None" = None) -> int:
+        """Device bytes of one instance (mb_problem_footprint)."""
+        cs = (settings or IPMSettings()).to_c()
+        b = C.c_int64()
+        check(self.ctx.L.mb_problem_footprint(self.h, C.byref(cs), C.byref(b)), self.ctx.h, "footprint")
+        return b.value
+
+    def symbolic(self) -> dict:
+        """The host symbolic analysis: solver vertex order (0-based problem vertices) and fronts."""
+        i = self.info()
+        nv = i["nvtx"]
+        vperm = np.zeros(nv, np.int64)
+        cap = nv
+        arrs = [np.zeros(cap, np.int64) for _ in range(4)]
+        nf = C.c_int64()
+        self.ctx.L.mb_problem_symbolic(self.h, _p(vperm, C.c_int64), C.byref(nf),
+                                       *[_p(a, C.c_int64) for a in arrs], cap)
+        k = nf.value
+        return dict(vperm=vperm, nfront=k, res0=arrs[0][:k], nres=arrs[1][:k], nsep=arrs[2][:k], parent=arrs[3][:k])
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.ctx.L.mb_problem_destroy(self.h)
+            self.h = None
+
+
+# ---------------------------------------------------------------------------------------- results
+@dataclass
+class IPMHistory:
+    rows: list = field(default_factory=list)
+
+    def __len__(self):
+        return len(self.rows)
+
+    def __getitem__(self, i):
+        return self.rows[i]
+
+    def column(self, name):
+        return np.array([r[name] for r in self.rows])
+
+
+@dataclass
+class IPMResult:
+    p: np.ndarray
+    d: np.ndarray
+    y: np.ndarray
+    status: IPMStatus
+    niter: int
+    nsolve: int
+    history: IPMHistory
+    mu: float
+    pres: float
+    dres: float
+    pobj: float
+    dobj: float
+    nfactor_retry: int = 0
+
+
+class IPMSolver:
+    """Device-resident solver state (IPMSolver, solver/ipm.jl:1-28)."""
+
+    def __init__(self, prob: IPMProblem, settings: IPMSettings | None = None, p0=None, d0=None, y0=None):
+        self.prob = prob
+        self.settings = settings or IPMSettings()
+        self.L = prob.ctx.L
+        self._cs = self.settings.to_c()
+        h = C.c_void_p()
+        a = [None if x is None else _f64(x) for x in (p0, d0, y0)]
+        rc = self.L.mb_solver_create(prob.h, C.byref(self._cs), *[_p(x, C.c_double) for x in a], C.byref(h))
+        check(rc, prob.ctx.h, "init")
+        self.h = h
+        self.status = IPMStatus.CONTINUE
+
+    def step(self) -> IPMStatus:
+        st = C.c_int32()
+        check(self.L.mb_solver_step(self.h, C.byref(st)), self.prob.ctx.h, "step!")
+        self.status = IPMStatus(st.value)
+        return self.status
+
+    def solve(self) -> IPMResult:
+        st = C.c_int32()
+        check(self.L.mb_solver_solve(self.h, C.byref(st)), self.prob.ctx.h, "solve!")
+        self.status = IPMStatus(st.value)
+        return self.result()
+
+    def history(self) -> IPMHistory:
+        cap = self.settings.max_iter + 1
+        rows = (mb_history_row * cap)()
+        nr = C.c_int32()
+        check(self.L.mb_solver_history(self.h, rows, cap, C.byref(nr)), self.prob.ctx.h, "history")
+        return IPMHistory([{f: getattr(rows[i], f) for f in ROW_FIELDS} for i in range(nr.value)])
+
+    def result(self) -> IPMResult:
+        i = self.prob.info()
+        p = np.zeros(i["n"]); d = np.zeros(i["n"]); y = np.zeros(i["m"])
+        r = mb_result()
+        check(self.L.mb_solver_result(self.h, _p(p, C.c_double), _p(d, C.c_double), _p(y, C.c_double), C.byref(r)),
+              self.prob.ctx.h, "result")
+        return IPMResult(p, d, y, IPMStatus(r.status), r.niter, r.nsolve, self.history(), r.mu, r.pres, r.dres,
+                         r.pobj, r.dobj, r.nfactor_retry)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.L.mb_solver_destroy(self.h)
+            self.h = None
+
+
+def init(prob: IPMProblem, settings: IPMSettings | None = None, p0=None, d0=None, y0=None) -> IPMSolver:
+    return IPMSolver(prob, settings, p0, d0, y0)
+
+
+def step(solver: IPMSolver) -> IPMStatus:
+    """step!(solver)"""
+    return solver.step()
+
+
+def solve_(solver: IPMSolver) -> IPMResult:
+    """solve!(solver)"""
+    return solver.solve()
+
+
+def solve(prob: IPMProblem, settings: IPMSettings | None = None, p0=None, d0=None, y0=None) -> IPMResult:
+    return init(prob, settings, p0, d0, y0).solve()
+
+
+# ---------------------------------------------------------------------------------------- batches
+class Batch:
+    """Many problems resident on the device, solved by one persistent launch per `run`."""
+
+    def __init__(self, probs, settings: IPMSettings | None = None, ctx: Context | None = None):
+        self.ctx = ctx or probs[0].ctx
+        self.L = self.ctx.L
+        self.probs = list(probs)
+        self.settings = settings or IPMSettings()
+        self._cs = self.settings.to_c()
+        arr = (C.c_void_p * len(self.probs))(*[p.h.value for p in self.probs])
+        h = C.c_void_p()
+        check(self.L.mb_batch_prepare(self.ctx.h, arr, len(self.probs), C.byref(self._cs), C.byref(h)),
+              self.ctx.h, "batch prepare")
+        self.h = h
+        self.sizes = [p.info() for p in self.probs]
+
+    def run(self, grid: int = 0) -> float:
+        ms = C.c_float()
+        check(self.L.mb_batch_run(self.h, grid, C.byref(ms)), self.ctx.h, "batch run")
+        return ms.value
+
+    def fetch(self, want_vectors: bool = True):
+        k = len(self.probs)
+        res = (mb_result * k)()
+        if want_vectors:
+            ps = [np.zeros(s["n"]) for s in self.sizes]
+            ds = [np.zeros(s["n"]) for s in self.sizes]
+            ys = [np.zeros(s["m"]) for s in self.sizes]
+            mk = lambda lst: (C.POINTER(C.c_double) * k)(*[_p(a, C.c_double) for a in lst])
+            check(self.L.mb_batch_fetch(self.h, mk(ps), mk(ds), mk(ys), res), self.ctx.h, "batch fetch")
+        else:
+            ps = ds = ys = [None] * k
+            check(self.L.mb_batch_fetch(self.h, None, None, None, res), self.ctx.h, "batch fetch")
+        out = []
+        for i in range(k):
+            r = res[i]
+            out.append(IPMResult(ps[i], ds[i], ys[i], IPMStatus(r.status), r.niter, r.nsolve, IPMHistory(), r.mu,
+                                 r.pres, r.dres, r.pobj, r.dobj, r.nfactor_retry))
+        return out
+
+    def stats(self):
+        a = np.zeros(8, np.int64)
+        self.L.mb_batch_stats(self.h, _p(a, C.c_int64))
+        return dict(input_bytes=int(a[0]), work_bytes=int(a[1]), factor_bytes=int(a[2]), launches=int(a[3]),
+                    ninst=int(a[4]), output_bytes=int(a[5]))
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            self.L.mb_batch_destroy(self.h)
+            self.h = None
+
+
+def batch_solve(probs, settings: IPMSettings | None = None, grid: int = 0):
+    b = Batch(probs, settings)
+    b.run(grid)
+    return b.fetch()

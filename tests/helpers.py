@@ -1,0 +1,40 @@
+"""Shared test helpers: seeded problems, the oracle in the product's vertex order, comparisons."""
+import numpy as np
+
+import frontend
+import oracle
+from mumblebee_b200 import generators as G
+from mumblebee_b200.ipm import Context, IPMProblem
+
+
+def block_problem(pb, compress=1.0):
+    """The oracle's restated front-end: CSC problem -> block form dict (1-based)."""
+    return frontend.ipmproblem_from_csc(pb["Q"], pb["B"], pb["f"], pb["g"], pb["mu"], pb["kinds"], pb["sizes"],
+                                        pb["params"], compress)
+
+
+def product_problem(pb, ctx=None, compress=1.0):
+    K = [_cone(k, a) for k, a in zip(pb["kinds"], pb["params"])]
+    return IPMProblem(pb["Q"], pb["B"], pb["f"], pb["g"], pb["mu"], K, pb["sizes"], compress=compress,
+                      ctx=ctx or Context.host())
+
+
+def _cone(k, a):
+    from mumblebee_b200 import ipm
+    if k == 5:
+        return ipm.PowerCone(a)
+    return {0: ipm.CofreeCone, 1: ipm.PositiveCone, 2: ipm.SecondOrderCone, 3: ipm.SemidefiniteCone,
+            4: ipm.ExponentialCone}[k]()
+
+
+SMALL = {
+    "socp_tiny": lambda: G.socp(n=40, m=12, ncone=4, density=0.2, seed=1),
+    "socp_small": lambda: G.socp(n=100, m=40, ncone=5, density=0.1, seed=0),
+    "port_small": lambda: G.portfolio(30, seed=3),
+    "port_mid": lambda: G.portfolio(80, seed=7),
+}
+
+
+def oracle_solve(prob_blocks, vperm=None, threads=1, **settings):
+    s = oracle.OracleSolver(prob_blocks, oracle.default_settings(**settings), vperm=vperm, threads=threads)
+    return s, s.solve()

@@ -1,0 +1,85 @@
+"""GPU parity: the CUDA solver through the C-ABI against the FP64 oracle on seeded problems.
+
+Tolerances (FP64 factor): same IPMStatus and iteration count; objectives within 1e-9 relative
+(both sides stop at the 1e-8 gap); final iterates within 1e-6 relative (the central-path end
+point is determined only up to the stopping tolerance, and rounding orders differ between the
+device reductions and the sequential CPU loops).  History rows track each other iteration by
+iteration to 1e-6 relative for the first iterations."""
+import numpy as np
+import pytest
+
+from helpers import SMALL, block_problem, oracle_solve
+from mumblebee_b200 import generators as G
+from mumblebee_b200.ipm import Context, IPMProblem, IPMSettings, IPMStatus, batch_solve, init, solve
+
+pytestmark = pytest.mark.gpu
+
+
+def _gpu_problem(ref):
+    return IPMProblem.from_dict(ref, ctx=Context.default())
+
+
+def _rel(a, b):
+    return abs(a - b) / max(1.0, abs(b))
+
+
+@pytest.mark.parametrize("name", list(SMALL))
+def test_solve_matches_oracle(name):
+    pb = SMALL[name]()
+    ref = block_problem(pb)
+    prob = _gpu_problem(ref)
+    vperm = prob.symbolic()["vperm"]
+    _, o = oracle_solve(ref, vperm=vperm)
+    r = solve(prob, IPMSettings())
+    assert r.status == IPMStatus.OPTIMAL
+    assert o["status"] == "OPTIMAL"
+    assert r.niter == o["niter"]
+    assert _rel(r.pobj, o["pobj"]) < 1e-9 and _rel(r.dobj, o["dobj"]) < 1e-9
+    assert r.pres < 1e-8 and r.dres < 1e-8
+    for k in ("p", "d", "y"):
+        a, b = getattr(r, k), o[k]
+        assert np.linalg.norm(a - b) <= 1e-6 * max(1.0, np.linalg.norm(b)), k
+
+
+@pytest.mark.parametrize("name", ["socp_small", "port_small"])
+def test_history_tracks_oracle(name):
+    pb = SMALL[name]()
+    ref = block_problem(pb)
+    prob = _gpu_problem(ref)
+    _, o = oracle_solve(ref, vperm=prob.symbolic()["vperm"])
+    s = init(prob, IPMSettings())
+    s.solve()
+    h = s.history()
+    oh = o["history"]
+    assert len(h) == len(oh)
+    for i in range(min(4, len(h))):
+        for f in ("mu", "pres", "dres", "pobj", "dobj", "step"):
+            assert _rel(h[i][f], oh[i][f]) < 1e-6, (i, f, h[i][f], oh[i][f])
+        for f in ("piter", "ppass", "citer", "cpass"):
+            assert h[i][f] == oh[i][f], (i, f)
+
+
+def test_step_api_matches_solve():
+    ref = block_problem(SMALL["socp_tiny"]())
+    prob = _gpu_problem(ref)
+    s = init(prob, IPMSettings())
+    n = 0
+    while s.step() == IPMStatus.CONTINUE:
+        n += 1
+    r1 = s.result()
+    r2 = solve(prob, IPMSettings())
+    assert r1.status == r2.status and r1.niter == r2.niter
+    np.testing.assert_array_equal(r1.p, r2.p)
+
+
+def test_batch_equals_alone():
+    """Continuous batching: each result is bit-identical alone and inside a mixed batch."""
+    pbs = [SMALL[k]() for k in SMALL] + [G.portfolio(int(n), seed=100 + i) for i, n in enumerate([40, 120, 60])]
+    refs = [block_problem(p) for p in pbs]
+    probs = [_gpu_problem(r) for r in refs]
+    mix = batch_solve(probs, IPMSettings(), grid=3)
+    for p, rm in zip(probs, mix):
+        ra = batch_solve([p], IPMSettings())[0]
+        assert ra.status == rm.status and ra.niter == rm.niter
+        np.testing.assert_array_equal(ra.p, rm.p)
+        np.testing.assert_array_equal(ra.y, rm.y)

@@ -1,0 +1,310 @@
+#!/usr/bin/env python
+"""Benchmark: batched interior-point solves per second on B200.
+
+Workload (one "step"): one batch of synthetic portfolio QP/SOCP instances solved to the 1e-8 gap
+(n_assets ~ U[50, 400], factor model F (n x 10), D ~ U(0.1, 1), budget
+equality, long-only cone, SOC risk bound), all instances in one persistent launch.
+
+  value  — solves/s with every input resident in HBM (device time, CUDA events on the launching
+           stream, max over ranks)
+  e2e    — solves/s through the public C ABI (mb_batch_solve) from host problems to host results:
+           symbolic analysis, packing, H2D, solve and D2H inside the timed region (wall clock)
+
+Multi-GPU: one process per GPU, each solving its own batch (independent instances; no collective
+on the data path; weak scaling).  `--impl reference` times the reference algorithm's CPU
+restatement (the FP64 oracle) on the host cores.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import multiprocessing as mp
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "mumblebee.jl_b200"))
+
+import numpy as np  # noqa: E402
+
+WORKLOAD = ("batched portfolio QP/SOCP (configuration 3): n_assets~U[50,400], F n x 10 N(0,1), D~U(0.1,1), "
+            "budget equality, long-only cone, SOC risk bound; solve to 1e-8 gap")
+METRIC = "IPM solves/s & p50/p99 latency at 1e-8 gap: mixed vs FP64 GPU; factor TC%"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--count", type=int, default=4096, help="instances per step per GPU")
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--cpu-seconds", type=float, default=15.0, help="bounded CPU-baseline sample length")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+# ------------------------------------------------------------------------------------------ dist
+def dist_setup(args):
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    pg = None
+    if ws > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=600))
+        pg = dist
+    return ws, rank, local, pg
+
+
+def allreduce_max(pg, x, local):
+    if pg is None:
+        return x
+    import torch
+    dev = f"cuda:{local}" if torch.cuda.is_available() else "cpu"
+    t = torch.tensor([float(x)], dtype=torch.float64, device=dev)
+    pg.all_reduce(t, op=pg.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(pg, local):
+    if pg is not None:
+        import torch
+        if torch.cuda.is_available():
+            pg.barrier(device_ids=[local])
+        else:
+            pg.barrier()
+
+
+# ------------------------------------------------------------------------------------------ clocks
+class Clocks:
+    """nvidia-smi sampling during the timed region."""
+
+    def __init__(self, local):
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits", "-i",
+                                       str(local), "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        try:
+            self.p.wait(5)
+        except Exception:
+            self.p.kill()
+        self.f.flush(); self.f.seek(0)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.f.read().splitlines():
+            c = [x.strip() for x in line.split(",")]
+            if len(c) < 9:
+                continue
+            try:
+                sm.append(float(c[1])); mx.append(float(c[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, c[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        os.unlink(self.f.name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ------------------------------------------------------------------------------------------ peaks
+def measure_peaks():
+    """FP64 and TF32 dense GEMM peaks measured live (torch/cuBLAS, 8192^3, best of 5): the
+    denominators of the factorization roofline (MEASURED_PEAKS.json carries HBM and BF16 only)."""
+    import torch
+    out = {}
+    n = 8192
+    for name, dt, tf32 in (("fp64", torch.float64, False), ("tf32", torch.float32, True)):
+        torch.backends.cuda.matmul.allow_tf32 = tf32
+        a = torch.randn(n, n, device="cuda", dtype=dt)
+        b = torch.randn(n, n, device="cuda", dtype=dt)
+        for _ in range(2):
+            a @ b
+        best = 1e30
+        for _ in range(5):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(); a @ b; e1.record(); torch.cuda.synchronize()
+            best = min(best, e0.elapsed_time(e1) / 1e3)
+        out[name] = 2 * n ** 3 / best / 1e12
+        del a, b
+    torch.backends.cuda.matmul.allow_tf32 = False
+    torch.cuda.empty_cache()
+    return out
+
+
+# ------------------------------------------------------------------------------------------ oracle
+def _oracle_worker(args):
+    seed, deadline, count_max = args
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import frontend
+    import oracle
+    from mumblebee_b200 import generators as G
+    oracle.lib(threads=1)
+    rng = np.random.default_rng(seed)
+    done, secs = 0, 0.0
+    while time.time() < deadline and done < count_max:
+        pb = G.portfolio(int(rng.integers(50, 401)), rng=np.random.default_rng([seed, done]))
+        prob = frontend.ipmproblem_from_csc(pb["Q"], pb["B"], pb["f"], pb["g"], pb["mu"], pb["kinds"], pb["sizes"],
+                                            pb["params"])
+        adj, w = frontend.vertex_graph(prob)
+        vp = frontend.minimum_degree(adj, w)
+        t = time.perf_counter()
+        s = oracle.OracleSolver(prob, oracle.default_settings(), vperm=vp, threads=1)
+        r = s.solve()
+        secs += time.perf_counter() - t
+        done += 1
+        assert r["status"] in ("OPTIMAL", "NEAR_OPTIMAL")
+    return done, secs
+
+
+def cpu_oracle_rate(seconds, cores, seed=1234):
+    """Solves/s of the FP64 oracle on `cores` host processes (one OpenBLAS thread each), timing
+    the init+solve of each instance (problem construction excluded, as for the GPU)."""
+    ctx = mp.get_context("spawn")
+    deadline = time.time() + seconds
+    with ctx.Pool(cores) as pool:
+        res = pool.map(_oracle_worker, [(seed + k, deadline, 10 ** 6) for k in range(cores)])
+    done = sum(r[0] for r in res)
+    busy = max(r[1] for r in res) if res else 0
+    per_core = [r[0] / r[1] for r in res if r[1] > 0]
+    return sum(per_core), done, busy
+
+
+# ------------------------------------------------------------------------------------------ main
+def make_problems(count, seed, rank, ctx):
+    from mumblebee_b200 import generators as G
+    from mumblebee_b200.ipm import IPMProblem, PositiveCone, CofreeCone, SecondOrderCone
+    rng = np.random.default_rng([seed, rank])
+    sizes = rng.integers(50, 401, size=count)
+    cones = {0: CofreeCone(), 1: PositiveCone(), 2: SecondOrderCone()}
+    probs = []
+    for i, n in enumerate(sizes):
+        pb = G.portfolio(int(n), rng=np.random.default_rng([seed, rank, i]))
+        probs.append(IPMProblem(pb["Q"], pb["B"], pb["f"], pb["g"], pb["mu"], [cones[k] for k in pb["kinds"]],
+                                pb["sizes"], ctx=ctx))
+    return probs, sizes
+
+
+def run_reference(args, ws, rank):
+    if rank != 0:
+        return
+    cores = os.cpu_count() or 1
+    per_step = max(2.0, args.cpu_seconds / max(1, args.steps))
+    rates = []
+    cpu_oracle_rate(1.0, cores)     # warm-up (process spawn, library load)
+    for _ in range(args.steps):
+        r, _, _ = cpu_oracle_rate(per_step, cores)
+        rates.append(r)
+    v = statistics.median(rates)
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "solves/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * args.count / v,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "instances": args.count},
+            "cpu_baseline": {"value": v, "unit": "solves/s", "cores": cores, "kind": "port",
+                             "sample": f"FP64 oracle (CPU restatement of the reference; Julia is not installed), "
+                                       f"{cores} processes x 1 OpenBLAS thread, {per_step:.0f} s of instances per step"},
+            "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    ws, rank, local, pg = dist_setup(args)
+    if args.impl == "reference":
+        run_reference(args, ws, rank)
+        if pg is not None:
+            pg.destroy_process_group()
+        return
+    from mumblebee_b200.ipm import Batch, Context, IPMSettings, batch_solve
+    ctx = Context.default(local)
+    settings = IPMSettings(precision=args.precision)
+    t0 = time.time()
+    probs, sizes = make_problems(args.count, args.seed, rank, ctx)
+    t_gen = time.time() - t0
+    t0 = time.time()
+    batch = Batch(probs, settings, ctx=ctx)
+    t_prep = time.time() - t0
+    st = batch.stats()
+    for _ in range(args.warmup):
+        batch.run()
+    res = batch.fetch(want_vectors=False)
+    nok = sum(1 for r in res if r.status.name in ("OPTIMAL",))
+    iters = [r.niter for r in res]
+    # timed region: device time of K persistent launches (CUDA events on the launching stream)
+    barrier(pg, local)
+    clk = Clocks(local)
+    ms_steps = [batch.run() for _ in range(args.steps)]
+    clocks = clk.stop()
+    ms = sum(ms_steps) / len(ms_steps)
+    ms_max = allreduce_max(pg, ms, local)
+    value = args.count * ws / (ms_max / 1e3)
+    # roofline of the solver kernel: algorithmic factorization flops per launch / launch time
+    flops = float(sum(r.nfactor * r.factor_flops for r in res))
+    peaks = measure_peaks()
+    peak_key = "tf32" if args.precision == "fp32" else "fp64"
+    achieved = flops / (ms / 1e3) / 1e12
+    roofline = {"bound": "tensor", "achieved": achieved, "peak": peaks[peak_key], "unit": "TFLOP/s",
+                "frac": achieved / peaks[peak_key], "traffic": None,
+                "peak_source": f"measured live: torch {peak_key} GEMM 8192^3 best of 5 on this GPU",
+                "kernel": "ipm_batch_kernel", "flops_per_launch": flops}
+    # end to end through the C ABI: host problems in, host results out
+    e2e = None
+    if not args.no_e2e:
+        batch_solve(probs, settings)          # warm-up
+        barrier(pg, local)
+        t = time.perf_counter()
+        for _ in range(max(1, min(args.steps, 2))):
+            batch_solve(probs, settings)
+        dt = (time.perf_counter() - t) / max(1, min(args.steps, 2))
+        dt = allreduce_max(pg, dt, local)
+        e2e = {"value": args.count * ws / dt, "unit": "solves/s", "h2d_bytes_per_step": st["input_bytes"],
+               "d2h_bytes_per_step": st["output_bytes"]}
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        cores = os.cpu_count() or 1
+        r, done, busy = cpu_oracle_rate(args.cpu_seconds, cores)
+        cpu = {"value": r, "unit": "solves/s", "cores": cores, "kind": "port",
+               "sample": f"{done} instances of the same distribution, FP64 oracle, {cores} processes x 1 thread, "
+                         f"{args.cpu_seconds:.0f} s"}
+    if rank == 0:
+        line = {"metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": ws, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+                "config": {"workload": WORKLOAD, "instances_per_gpu": args.count, "precision": args.precision,
+                           "parallelism": f"instances sharded over {ws} GPU(s), one persistent launch per step",
+                           "l2": f"inputs larger than L2: {st['input_bytes'] / 1e9:.2f} GB uploaded + "
+                                 f"{(st['work_bytes'] + st['factor_bytes']) / 1e9:.2f} GB workspace per step",
+                           "optimal": f"{nok}/{len(res)}", "iters_mean": float(np.mean(iters)),
+                           "setup_s": {"generate": round(t_gen, 2), "prepare": round(t_prep, 2)}},
+                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": args.steps,
+                "clocks": clocks, "step_ms": ms_steps}
+        print(json.dumps(line), flush=True)
+    if pg is not None:
+        pg.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -101,7 +101,10 @@ typedef struct mb_result {
     int32_t niter;
     int32_t nsolve;
     int32_t nfactor_retry;   /* ρ-regularized refactorizations (uzawa.jl:97-112) */
+    int32_t nfactor;         /* numeric factorizations performed (including retries) */
+    int32_t reserved;
     double mu, pres, dres, pobj, dobj;
+    double factor_flops;     /* algorithmic flops of one factorization: Σ_fronts r³/3 + r²s + rs² */
 } mb_result;
 
 /* IPMHistoryRow (history/ipm.jl:1-4), integer and status fields stored as doubles */
@@ -176,6 +179,11 @@ int mb_batch_run(mb_batch* b, int32_t grid, float* ms);
 int mb_batch_fetch(mb_batch* b, double* const* p_out, double* const* d_out, double* const* y_out,
                    mb_result* results);
 int mb_batch_stats(mb_batch* b, int64_t* stats8);   /* bytes: input, workspace, factor; kernel launches */
+/* per-instance section timers after mb_batch_fetch, (NSEC + 2) doubles each: SM clocks spent in
+ * equilibrate, BᵀB, scale, initkkt, predictor, corrector, maxsteps, triangular solves, matvecs,
+ * then the number of triangular-solve sweeps and of matvecs (the TimerOutputs sections of the
+ * reference, solver/ipm.jl:137-755) */
+int mb_batch_timers(mb_batch* b, double* out, int64_t cap);
 int mb_batch_destroy(mb_batch* b);
 
 #ifdef __cplusplus

@@ -55,8 +55,9 @@ __device__ __forceinline__ void w_socroot(double* x, const double* w, double bet
     __syncwarp();
 }
 
-// NT scaling point and Hessian block  (soc.jl:192-263).  cache: beta, pdet, ddet, pdetlo, ddetlo, w[n]
-__device__ bool w_socscale(double* H, double* c, const double* p, const double* d, int n, double& spsd) {
+// NT scaling point in factored form β, w = ω/β  (soc.jl:192-230, 257-262); warp per cone.
+// cache: beta, pdet, ddet, pdetlo, ddetlo, w[n]
+__device__ bool w_socpoint(double* c, const double* p, const double* d, int n, double& spsd) {
     const int lane = threadIdx.x & 31;
     double* w = c + 5;
     double pdet, pdetlo, ddet, ddetlo;
@@ -72,29 +73,36 @@ __device__ bool w_socscale(double* H, double* c, const double* p, const double* 
         beta = sqrt(spdet / sddet);
         for (int i = lane; i < n; i += 32)
             w[i] = (i == 0 ? fma(d[0], beta, p[0] / beta) : fma(-d[i], beta, p[i] / beta)) / kappa;
-        __syncwarp();
-        double eta = 1.0 / (beta * beta), eta2 = 2 * eta;
-        double w1 = w[0];
-        // lower triangle pairs (i >= j), each written to both halves from the upper addend
-        for (int j = 0; j < n; ++j) {
-            double wj = w[j];
-            for (int i = j + lane; i < n; i += 32) {
-                if (i == j) {
-                    if (j == 0) H[0] = fma(eta2, w1 * w1, H[0] - eta);
-                    else H[(int64_t)j * n + j] = fma(eta2, wj * wj, H[(int64_t)j * n + j] + eta);
-                } else {
-                    double t = (j == 0) ? fma(-eta2 * w1, w[i], H[(int64_t)i * n])
-                                        : fma(eta2 * wj, w[i], H[j + (int64_t)i * n]);
-                    H[i + (int64_t)j * n] = t;
-                    H[j + (int64_t)i * n] = t;
-                }
-            }
-        }
         spsd = 4 * pdot / (pdet * ddet);
     }
     if (lane == 0) { c[0] = beta; c[1] = pdet; c[2] = ddet; c[3] = pdetlo; c[4] = ddetlo; }
     __syncwarp();
     return flag;
+}
+
+// H ← H + (2 (Jw)(Jw)ᵀ − J) / β² on an (n x n) block  (soc.jl:231-256), all threads of the CTA;
+// each unordered pair is written to both halves from the upper addend, as the reference does.
+__device__ void b_sochess(double* H, const double* c, int n) {
+    const double* w = c + 5;
+    const double beta = c[0];
+    const double eta = 1.0 / (beta * beta), eta2 = 2 * eta;
+    const double w1 = w[0];
+    const int64_t np = (int64_t)n * (n + 1) / 2;
+    for (int64_t t = threadIdx.x; t < np; t += NT) {
+        // column-major lower enumeration: t -> (i >= j)
+        int j = (int)((2.0 * n + 1.0 - sqrt((2.0 * n + 1.0) * (2.0 * n + 1.0) - 8.0 * (double)t)) * 0.5);
+        while (j > 0 && (int64_t)j * (2 * n - j + 1) / 2 > t) --j;
+        while ((int64_t)(j + 1) * (2 * n - j) / 2 <= t) ++j;
+        int i = j + (int)(t - (int64_t)j * (2 * n - j + 1) / 2);
+        if (i == j) {
+            if (j == 0) H[0] = fma(eta2, w1 * w1, H[0] - eta);
+            else H[(int64_t)j * n + j] = fma(eta2, w[j] * w[j], H[(int64_t)j * n + j] + eta);
+        } else {
+            double t2 = (j == 0) ? fma(-eta2 * w1, w[i], H[(int64_t)i * n]) : fma(eta2 * w[j], w[i], H[j + (int64_t)i * n]);
+            H[i + (int64_t)j * n] = t2;
+            H[j + (int64_t)i * n] = t2;
+        }
+    }
 }
 
 // Mehrotra corrector  (soc.jl:282-351); work holds 2n doubles owned by this warp

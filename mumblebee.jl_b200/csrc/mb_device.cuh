@@ -119,54 +119,60 @@ __device__ __forceinline__ void baxpy(double a, const double* x, double* y, int 
     __syncthreads();
 }
 
-// y <- alpha A x + beta y  (BlockSparseArrays/src/blas/gemv.jl:321-343, :N), one thread per row
-__device__ void bgemvN(const DevBSM& A, const double* x, double* y, double alpha, double beta) {
-    for (int i = threadIdx.x; i < A.nrow; i += NT) {
-        int u = A.rowout[i];
-        int r = i - A.xrow[u], nr = A.xrow[u + 1] - A.xrow[u];
+// Sparse products over the nonzeros of a block-sparse matrix (BlockSparseArrays/src/blas/gemv.jl:
+// 321-343 computes the same sums over the dense blocks; their explicit zeros add nothing).  A group
+// of G lanes owns one row (CSR) or one column (CSC) and reduces in a fixed order.
+constexpr int G = 16;
+
+template <class Op>
+__device__ __forceinline__ double group_reduce(double v, Op op) {
+#pragma unroll
+    for (int o = G / 2; o > 0; o >>= 1) v = op(v, __shfl_xor_sync(0xffffffffu, v, o, G));
+    return v;
+}
+
+// y <- alpha A x + beta y.  The loop bound is uniform per warp (both groups of a warp enter
+// group_reduce together).
+constexpr int GPW = 32 / G;   // groups per warp
+
+__device__ void spmv(const DevSp& A, const double* x, double* y, double alpha, double beta) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, gl = lane % G, sub = lane / G;
+    for (int i0 = warp * GPW; i0 < A.nrow; i0 += NW * GPW) {
+        const int i = i0 + sub;
         double acc = 0;
-        for (int k = A.rptr[u]; k < A.rptr[u + 1]; ++k) {
-            int e = A.rarc[k], v = A.rvtx[k];
-            int c0 = A.xcol[v], nc = A.xcol[v + 1] - c0;
-            const double* blk = A.val + A.xblk[e] + r;
-            for (int j = 0; j < nc; ++j) acc = fma(blk[(int64_t)j * nr], x[c0 + j], acc);
-        }
-        y[i] = beta == 0.0 ? alpha * acc : fma(alpha, acc, beta * y[i]);
+        if (i < A.nrow)
+            for (int k = A.rptr[i] + gl; k < A.rptr[i + 1]; k += G) acc = fma(A.val[k], x[A.cidx[k]], acc);
+        acc = group_reduce(acc, OpSum());
+        if (i < A.nrow && gl == 0) y[i] = beta == 0.0 ? alpha * acc : fma(alpha, acc, beta * y[i]);
     }
     __syncthreads();
 }
 
-// y <- alpha Aᵀ x + beta y  (gemv.jl:321-343, :T), one thread per column
-__device__ void bgemvT(const DevBSM& A, const double* x, double* y, double alpha, double beta) {
-    for (int j = threadIdx.x; j < A.ncol; j += NT) {
-        int v = A.colvtx[j];
-        int jl = j - A.xcol[v];
+// y <- alpha Aᵀ x + beta y
+__device__ void spmvT(const DevSp& A, const double* x, double* y, double alpha, double beta) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, gl = lane % G, sub = lane / G;
+    for (int j0 = warp * GPW; j0 < A.ncol; j0 += NW * GPW) {
+        const int j = j0 + sub;
         double acc = 0;
-        for (int e = A.xsrc[v]; e < A.xsrc[v + 1]; ++e) {
-            int u = A.tgt[e];
-            int r0 = A.xrow[u], nr = A.xrow[u + 1] - r0;
-            const double* blk = A.val + A.xblk[e] + (int64_t)jl * nr;
-            for (int i = 0; i < nr; ++i) acc = fma(blk[i], x[r0 + i], acc);
-        }
-        y[j] = beta == 0.0 ? alpha * acc : fma(alpha, acc, beta * y[j]);
+        if (j < A.ncol)
+            for (int k = A.cptr[j] + gl; k < A.cptr[j + 1]; k += G) acc = fma(A.val[A.cpos[k]], x[A.ridx[k]], acc);
+        acc = group_reduce(acc, OpSum());
+        if (j < A.ncol && gl == 0) y[j] = beta == 0.0 ? alpha * acc : fma(alpha, acc, beta * y[j]);
     }
     __syncthreads();
 }
 
 // dot(x, A, y)  (block_sparse_matrix.jl:1094-1109)
-__device__ double bbdot(const DevBSM& A, const double* x, const double* y, double* red) {
+__device__ double spdot(const DevSp& A, const double* x, const double* y, double* red) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, gl = lane % G, sub = lane / G;
     double s = 0;
-    for (int j = threadIdx.x; j < A.ncol; j += NT) {
-        int v = A.colvtx[j];
-        int jl = j - A.xcol[v];
+    for (int i0 = warp * GPW; i0 < A.nrow; i0 += NW * GPW) {
+        const int i = i0 + sub;
         double acc = 0;
-        for (int e = A.xsrc[v]; e < A.xsrc[v + 1]; ++e) {
-            int u = A.tgt[e];
-            int r0 = A.xrow[u], nr = A.xrow[u + 1] - r0;
-            const double* blk = A.val + A.xblk[e] + (int64_t)jl * nr;
-            for (int i = 0; i < nr; ++i) acc = fma(blk[i], x[r0 + i], acc);
-        }
-        s = fma(acc, y[j], s);
+        if (i < A.nrow)
+            for (int k = A.rptr[i] + gl; k < A.rptr[i + 1]; k += G) acc = fma(A.val[k], y[A.cidx[k]], acc);
+        acc = group_reduce(acc, OpSum());
+        if (i < A.nrow && gl == 0) s = fma(x[i], acc, s);
     }
     return block_reduce(s, red, OpSum(), 0.0);
 }

@@ -10,8 +10,10 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <atomic>
 #include <memory>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/mumblebee_gpu.h"
@@ -38,10 +40,6 @@ struct mb_problem {
     std::vector<int32_t> kind;
     std::vector<double> param;
     std::vector<i64> P1, P2;   // 0-based user row / column of each problem row / column
-    // symbolic analysis, computed once
-    bool sym = false;
-    std::vector<i64> vperm;    // problem vertex of each solver vertex
-    mbh::Fronts fr;
 };
 
 static int fail(mb_ctx* ctx, int code, const std::string& msg) {
@@ -57,8 +55,13 @@ static int fail(mb_ctx* ctx, int code, const std::string& msg) {
 // ---------------------------------------------------------------------------------------------
 // symbolic: the vertex order (minimum degree + etree postorder) and the fronts
 // ---------------------------------------------------------------------------------------------
-static void do_symbolic(mb_problem* P) {
-    if (P->sym) return;
+struct Sym {
+    std::vector<i64> vperm;    // problem vertex of each solver vertex
+    mbh::Fronts fr;
+};
+
+static Sym do_symbolic(const mb_problem* P) {
+    Sym S;
     const mbh::BSM& B = P->B;
     i64 nv = B.nvtx;
     auto adj = mbh::vertex_graph(B, P->Q);
@@ -74,10 +77,10 @@ static void do_symbolic(mb_problem* P) {
         w2[k] = w[v];
         for (i64 u : adj[v]) adj2[k].push_back(inv[u]);
     }
-    P->fr = mbh::analyze(adj2, w2);
-    P->vperm.resize(nv);
-    for (i64 k = 0; k < nv; ++k) P->vperm[k] = order[P->fr.postperm[k]];
-    P->sym = true;
+    S.fr = mbh::analyze(adj2, w2);
+    S.vperm.resize(nv);
+    for (i64 k = 0; k < nv; ++k) S.vperm[k] = order[S.fr.postperm[k]];
+    return S;
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -112,22 +115,23 @@ struct InstPlan {
     double mut;
     int wsize;
     i64 fsize;
+    double fflops;            // algorithmic flops of one factorization
+    i64 Bnnz, Qnnz, nqoff;
     // i32
-    size_t Bxsrc, Bxcol, Bxrow, Btgt, Brptr, Brarc, Brvtx, Browout, Bcolvtx;
-    size_t Qxsrc, Qtgt, Qrptr, Qrarc, Qrvtx;
-    size_t qdiag, hld, kind, fres0, fnres, fnsep, fparent, fsepp, fsep, frel, vfront, status;
-    i64 Bnout, Bnarc, Qnarc;
+    size_t xcol, colvtx, cfront, Brptr, Bcidx, Bcptr, Bridx, Bcpos, Qrptr, Qcidx, Qcptr, Qridx, Qcpos, hdld, qoffk;
+    size_t kind, fres0, fnres, fnsep, fparent, fsepp, fsep, frel;
     // i64
-    size_t Bxblk, Qxblk, hpos, cxblk, fptr;
+    size_t hdoff, hdpos, qoffpos, cxblk, fptr;
     // double in
-    size_t Bval, Qval, f, g, kpar, p, d, y;
+    size_t Bval, Qval, Qd, f, g, kpar, p, d, y;
     // work
-    size_t H, Finit, pscl, yscl, vn, vm, vv, work, uhist, cghist, cache;
-    size_t wBval, wQval, wf, wg, wp, wd, wy;   // working copies
-    // factor
+    size_t wBval, wQval, wQd, Hd, Finit, pscl, yscl, vn, vm, vv, work, uhist, cghist, cache, wf, wg, wp, wd, wy;
+    // factor (bytes)
     size_t F;
     // out
     size_t po, dout, yo, scal, hist;
+    // status words
+    size_t status;
     // host-side mapping for results
     std::vector<i64> colmap;   // user column of each solver column
     std::vector<i64> rowmap;   // user row of each solver row
@@ -139,70 +143,116 @@ struct Packed {
     Arena<double> din;
     Arena<double> work;       // device-only
     Arena<double> out;        // device-only (copied back through pinned staging)
+    Arena<int32_t> ost;       // device-only status words (copied back)
     size_t fbytes = 0;        // factor arena, bytes
     std::vector<InstPlan> plans;
-    Packed() { work.host = false; out.host = false; }
+    Packed() { work.host = false; out.host = false; ost.host = false; }
     size_t device_bytes() const {
-        return i32.size() * 4 + i64a.size() * 8 + din.size() * 8 + work.size() * 8 + out.size() * 8 + fbytes;
+        return i32.size() * 4 + i64a.size() * 8 + din.size() * 8 + work.size() * 8 + out.size() * 8 +
+               ost.size() * 4 + fbytes;
     }
 };
-
-static void bsm_rowindex(const mbh::BSM& A, std::vector<i64>& rptr, std::vector<i64>& rarc, std::vector<i64>& rvtx,
-                         std::vector<i64>& rowout, std::vector<i64>& colvtx) {
-    rptr.assign(A.nout + 1, 0);
-    for (i64 e = 0; e < A.narc; ++e) rptr[A.tgt[e] + 1]++;
-    for (i64 u = 0; u < A.nout; ++u) rptr[u + 1] += rptr[u];
-    rarc.assign(A.narc, 0); rvtx.assign(A.narc, 0);
-    std::vector<i64> c(rptr.begin(), rptr.end() - 1);
-    for (i64 v = 0; v < A.nvtx; ++v)
-        for (i64 e = A.xsrc[v]; e < A.xsrc[v + 1]; ++e) { i64 k = c[A.tgt[e]]++; rarc[k] = e; rvtx[k] = v; }
-    rowout.assign(A.nrow, 0);
-    for (i64 u = 0; u < A.nout; ++u) for (i64 i = A.xrow[u]; i < A.xrow[u + 1]; ++i) rowout[i] = u;
-    colvtx.assign(A.ncol, 0);
-    for (i64 v = 0; v < A.nvtx; ++v) for (i64 j = A.xcol[v]; j < A.xcol[v + 1]; ++j) colvtx[j] = v;
-}
 
 static int64_t cone_cachesize(int k, i64 n) { return k == MB_CONE_SOC ? 5 + n : 0; }
 static int64_t cone_workspacesize(int k, i64 n) { return k == MB_CONE_SOC ? 2 * n : 0; }
 static int64_t cone_degree(int k, i64 n) { return k == MB_CONE_POS ? n : (k == MB_CONE_SOC ? 2 : 0); }
 
-static int plan_instance(mb_problem* P, const mb_settings& set, const double* p0, const double* d0, const double* y0,
-                         Packed& pk, std::string& err) {
-    do_symbolic(P);
-    const auto& vp = P->vperm;
+// Build one instance into its own (local) Packed: symbkkt (kkt/kkt.jl:23-53) with the host ordering,
+// the device index structures, the front placement of H and every arena offset.  Thread-safe: the
+// problem is only read.
+static int plan_instance(const mb_problem* P, const mb_settings& set, const double* p0, const double* d0,
+                         const double* y0, Packed& pk, std::string& err) {
+    Sym sym = do_symbolic(P);
+    const auto& vp = sym.vperm;
     mbh::BSM B = mbh::selectvtxs(P->B, vp);
     mbh::BSM Q = mbh::halfselectvtxs(mbh::halfselectvtxs(P->Q, vp), vp);
-    const mbh::Fronts& fr = P->fr;
+    const mbh::Fronts& fr = sym.fr;
     InstPlan ip;
-    ip.n = B.ncol; ip.m = B.nrow; ip.nvtx = B.nvtx; ip.nfront = fr.nfront;
+    const i64 n = B.ncol, m = B.nrow, nv = B.nvtx;
+    ip.n = n; ip.m = m; ip.nvtx = nv; ip.nfront = fr.nfront;
     ip.mut = P->mu;
-    for (i64 v = 0; v < B.nvtx; ++v) {
+    for (i64 v = 0; v < nv; ++v) {
         int k = P->kind[vp[v]];
         if (k != MB_CONE_FREE && k != MB_CONE_POS && k != MB_CONE_SOC) { err = "cone kind not supported by this build"; return MB_E_UNSUPPORTED; }
     }
     // column map: solver column -> problem column -> user column
     std::vector<i64> cperm;
-    cperm.reserve(B.ncol);
-    for (i64 k = 0; k < B.nvtx; ++k) for (i64 j = P->B.xcol[vp[k]]; j < P->B.xcol[vp[k] + 1]; ++j) cperm.push_back(j);
-    ip.colmap.resize(B.ncol); ip.rowmap.resize(B.nrow);
-    for (i64 i = 0; i < B.ncol; ++i) ip.colmap[i] = P->P2[cperm[i]];
-    for (i64 i = 0; i < B.nrow; ++i) ip.rowmap[i] = P->P1[i];
-    // index structures
-    std::vector<i64> rptr, rarc, rvtx, rowout, colvtx;
-    bsm_rowindex(B, rptr, rarc, rvtx, rowout, colvtx);
-    ip.Bnout = B.nout; ip.Bnarc = B.narc; ip.Qnarc = Q.narc;
-    ip.Bxsrc = pk.i32.put(to32(B.xsrc)); ip.Bxcol = pk.i32.put(to32(B.xcol)); ip.Bxrow = pk.i32.put(to32(B.xrow));
-    ip.Btgt = pk.i32.put(to32(B.tgt)); ip.Brptr = pk.i32.put(to32(rptr)); ip.Brarc = pk.i32.put(to32(rarc));
-    ip.Brvtx = pk.i32.put(to32(rvtx)); ip.Browout = pk.i32.put(to32(rowout)); ip.Bcolvtx = pk.i32.put(to32(colvtx));
-    std::vector<i64> qrptr, qrarc, qrvtx, qrowout, qcolvtx;
-    bsm_rowindex(Q, qrptr, qrarc, qrvtx, qrowout, qcolvtx);
-    ip.Qxsrc = pk.i32.put(to32(Q.xsrc)); ip.Qtgt = pk.i32.put(to32(Q.tgt)); ip.Qrptr = pk.i32.put(to32(qrptr));
-    ip.Qrarc = pk.i32.put(to32(qrarc)); ip.Qrvtx = pk.i32.put(to32(qrvtx));
-    std::vector<i64> qdiag(B.nvtx, -1);
-    for (i64 v = 0; v < Q.nvtx; ++v) for (i64 e = Q.xsrc[v]; e < Q.xsrc[v + 1]; ++e) if (Q.tgt[e] == v) qdiag[v] = e;
-    // every non-free cone needs its diagonal block (cone.jl:146-174 errors otherwise)
-    for (i64 v = 0; v < B.nvtx; ++v)
-        if (qdiag[v] < 0 && P->kind[vp[v]] != MB_CONE_FREE) { err = "Q lacks the diagonal block of a cone vertex"; return MB_E_ARG; }
+    cperm.reserve(n);
+    for (i64 k = 0; k < nv; ++k) for (i64 j = P->B.xcol[vp[k]]; j < P->B.xcol[vp[k] + 1]; ++j) cperm.push_back(j);
+    ip.colmap.resize(n); ip.rowmap.resize(m);
+    for (i64 i = 0; i < n; ++i) ip.colmap[i] = P->P2[cperm[i]];
+    for (i64 i = 0; i < m; ++i) ip.rowmap[i] = P->P1[i];
+    std::vector<i64> colvtx(n), cfront(n);
+    for (i64 v = 0; v < nv; ++v) for (i64 j = B.xcol[v]; j < B.xcol[v + 1]; ++j) { colvtx[j] = v; cfront[j] = fr.vfront[v]; }
+    // scalar nonzeros: CSR + CSC (CSC entries carry their CSR position).  With `skipdiag`, the
+    // entries inside the diagonal blocks are left out (they live in the dense Qd blocks).
+    auto scalar = [&](const mbh::BSM& A, bool skipdiag, std::vector<i64>& rptr, std::vector<i64>& cidx,
+                      std::vector<double>& val, std::vector<i64>& cptr, std::vector<i64>& ridx, std::vector<i64>& cpos) {
+        std::vector<i64> tr, tc; std::vector<double> tv;   // triplets in column-major (CSC) order
+        for (i64 v = 0; v < A.nvtx; ++v) {
+            i64 nc = A.ncols(v);
+            for (i64 jl = 0; jl < nc; ++jl)
+                for (i64 e = A.xsrc[v]; e < A.xsrc[v + 1]; ++e) {
+                    i64 u = A.tgt[e];
+                    if (skipdiag && u == v) continue;
+                    i64 nr = A.nrows(u);
+                    const double* blk = A.val.data() + A.xblk[e] + jl * nr;
+                    for (i64 il = 0; il < nr; ++il)
+                        if (blk[il] != 0) { tr.push_back(A.xrow[u] + il); tc.push_back(A.xcol[v] + jl); tv.push_back(blk[il]); }
+                }
+        }
+        i64 nnz = (i64)tr.size();
+        rptr.assign(A.nrow + 1, 0); cptr.assign(A.ncol + 1, 0);
+        for (i64 k = 0; k < nnz; ++k) { rptr[tr[k] + 1]++; cptr[tc[k] + 1]++; }
+        for (i64 i = 0; i < A.nrow; ++i) rptr[i + 1] += rptr[i];
+        for (i64 j = 0; j < A.ncol; ++j) cptr[j + 1] += cptr[j];
+        cidx.assign(nnz, 0); val.assign(nnz, 0); ridx.assign(nnz, 0); cpos.assign(nnz, 0);
+        std::vector<i64> rc(rptr.begin(), rptr.end() - 1);
+        for (i64 k = 0; k < nnz; ++k) {   // CSC order == triplet order; CSR by a stable counting sort
+            i64 q = rc[tr[k]]++;
+            cidx[q] = tc[k]; val[q] = tv[k];
+            ridx[k] = tr[k]; cpos[k] = q;
+        }
+    };
+    std::vector<i64> Brptr, Bcidx, Bcptr, Bridx, Bcpos, Qrptr, Qcidx, Qcptr, Qridx, Qcpos;
+    std::vector<double> Bval, Qval;
+    scalar(B, false, Brptr, Bcidx, Bval, Bcptr, Bridx, Bcpos);
+    scalar(Q, true, Qrptr, Qcidx, Qval, Qcptr, Qridx, Qcpos);
+    ip.Bnnz = (i64)Bval.size(); ip.Qnnz = (i64)Qval.size();
+    // front row position of scalar row s in front f
+    auto rowpos = [&](i64 f, i64 srow) -> i64 {
+        i64 r0 = fr.res0[f], nres = fr.nres[f];
+        if (srow >= r0 && srow < r0 + nres) return srow - r0;
+        auto it = std::lower_bound(fr.sep[f].begin(), fr.sep[f].end(), srow);
+        if (it == fr.sep[f].end() || *it != srow) return -1;
+        return nres + (i64)(it - fr.sep[f].begin());
+    };
+    // dense diagonal blocks of Q and their place in F; every non-free cone needs one (cone.jl:146-174)
+    std::vector<i64> hdoff(nv + 1, 0), hdpos(nv, 0), hdld(nv, 0);
+    for (i64 v = 0; v < nv; ++v) hdoff[v + 1] = hdoff[v] + B.ncols(v) * B.ncols(v);
+    std::vector<double> Qd(hdoff[nv], 0.0);
+    for (i64 v = 0; v < nv; ++v) {
+        bool found = false;
+        for (i64 e = Q.xsrc[v]; e < Q.xsrc[v + 1]; ++e)
+            if (Q.tgt[e] == v) { std::copy(Q.val.begin() + Q.xblk[e], Q.val.begin() + Q.xblk[e + 1], Qd.begin() + hdoff[v]); found = true; }
+        if (!found && P->kind[vp[v]] != MB_CONE_FREE) { err = "Q lacks the diagonal block of a cone vertex"; return MB_E_ARG; }
+        i64 f = fr.vfront[v], nf = fr.nres[f] + (i64)fr.sep[f].size();
+        hdpos[v] = fr.fptr[f] + (B.xcol[v] - fr.res0[f]) * (nf + 1);
+        hdld[v] = nf;
+    }
+    // off-diagonal-block nonzeros of Q in the lower triangle and their F offsets
+    std::vector<i64> qoffk, qoffpos;
+    for (i64 i = 0; i < n; ++i)
+        for (i64 k = Qrptr[i]; k < Qrptr[i + 1]; ++k) {
+            i64 j = Qcidx[k];
+            if (i < j) continue;
+            i64 f = cfront[j], nf = fr.nres[f] + (i64)fr.sep[f].size();
+            i64 rp = rowpos(f, i);
+            if (rp < 0) { err = "internal: Q entry outside the front structure"; return MB_E_ARG; }
+            qoffk.push_back(k);
+            qoffpos.push_back(fr.fptr[f] + rp + (j - fr.res0[f]) * nf);
+        }
+    ip.nqoff = (i64)qoffk.size();
     // fronts
     std::vector<i64> fnsep(fr.nfront), fsepp(fr.nfront + 1, 0), fsep, frel;
     for (i64 f = 0; f < fr.nfront; ++f) {
@@ -212,70 +262,89 @@ static int plan_instance(mb_problem* P, const mb_settings& set, const double* p0
         if (fr.parent[f] >= 0) frel.insert(frel.end(), fr.rel[f].begin(), fr.rel[f].end());
         else frel.insert(frel.end(), fr.sep[f].size(), 0);
     }
-    // H placement in fronts: block (u, v) with u >= v lands at rows rowpos(f, xcol[u]) of front f(v)
-    std::vector<i64> hpos(Q.narc, -1), hld(Q.narc, 0);
-    for (i64 v = 0; v < Q.nvtx; ++v) {
-        i64 f = fr.vfront[v], nres = fr.nres[f], nf = nres + (i64)fr.sep[f].size(), r0 = fr.res0[f];
-        for (i64 e = Q.xsrc[v]; e < Q.xsrc[v + 1]; ++e) {
-            i64 u = Q.tgt[e];
-            if (u < v) continue;
-            i64 s = B.xcol[u], rp;
-            if (s >= r0 && s < r0 + nres) rp = s - r0;
-            else {
-                auto it = std::lower_bound(fr.sep[f].begin(), fr.sep[f].end(), s);
-                if (it == fr.sep[f].end() || *it != s) { err = "internal: Q block outside the front structure"; return MB_E_ARG; }
-                rp = nres + (i64)(it - fr.sep[f].begin());
-            }
-            hpos[e] = fr.fptr[f] + rp + (B.xcol[v] - r0) * nf;
-            hld[e] = nf;
-        }
-    }
-    std::vector<i64> kind(B.nvtx), cx(B.nvtx + 1, 0);
-    std::vector<double> kpar(B.nvtx);
+    std::vector<i64> kind(nv), cx(nv + 1, 0);
+    std::vector<double> kpar(nv);
     i64 wmax = 1;
     ip.nu = 0;
-    for (i64 v = 0; v < B.nvtx; ++v) {
+    for (i64 v = 0; v < nv; ++v) {
         kind[v] = P->kind[vp[v]]; kpar[v] = P->param[vp[v]];
         cx[v + 1] = cx[v] + cone_cachesize((int)kind[v], B.ncols(v));
         wmax = std::max<i64>(wmax, cone_workspacesize((int)kind[v], B.ncols(v)));
         ip.nu += cone_degree((int)kind[v], B.ncols(v));
     }
     ip.wsize = (int)wmax;
-    ip.qdiag = pk.i32.put(to32(qdiag)); ip.hld = pk.i32.put(to32(hld)); ip.kind = pk.i32.put(to32(kind));
+    ip.fflops = 0;
+    for (i64 f = 0; f < fr.nfront; ++f) {
+        double r = (double)fr.nres[f], sp = (double)fr.sep[f].size();
+        ip.fflops += r * r * r / 3 + r * r * sp + r * sp * sp;
+    }
+    // i32 arena
+    ip.xcol = pk.i32.put(to32(B.xcol)); ip.colvtx = pk.i32.put(to32(colvtx)); ip.cfront = pk.i32.put(to32(cfront));
+    ip.Brptr = pk.i32.put(to32(Brptr)); ip.Bcidx = pk.i32.put(to32(Bcidx)); ip.Bcptr = pk.i32.put(to32(Bcptr));
+    ip.Bridx = pk.i32.put(to32(Bridx)); ip.Bcpos = pk.i32.put(to32(Bcpos));
+    ip.Qrptr = pk.i32.put(to32(Qrptr)); ip.Qcidx = pk.i32.put(to32(Qcidx)); ip.Qcptr = pk.i32.put(to32(Qcptr));
+    ip.Qridx = pk.i32.put(to32(Qridx)); ip.Qcpos = pk.i32.put(to32(Qcpos));
+    ip.hdld = pk.i32.put(to32(hdld)); ip.qoffk = pk.i32.put(to32(qoffk)); ip.kind = pk.i32.put(to32(kind));
     ip.fres0 = pk.i32.put(to32(fr.res0)); ip.fnres = pk.i32.put(to32(fr.nres)); ip.fnsep = pk.i32.put(to32(fnsep));
     ip.fparent = pk.i32.put(to32(fr.parent)); ip.fsepp = pk.i32.put(to32(fsepp)); ip.fsep = pk.i32.put(to32(fsep));
-    ip.frel = pk.i32.put(to32(frel)); ip.vfront = pk.i32.put(to32(fr.vfront));
-    ip.status = pk.i32.take(mb::NSTAT);
-    ip.Bxblk = pk.i64a.put(B.xblk); ip.Qxblk = pk.i64a.put(Q.xblk); ip.hpos = pk.i64a.put(hpos);
+    ip.frel = pk.i32.put(to32(frel));
+    // i64 arena
+    ip.hdoff = pk.i64a.put(hdoff); ip.hdpos = pk.i64a.put(hdpos); ip.qoffpos = pk.i64a.put(qoffpos);
     ip.cxblk = pk.i64a.put(cx); ip.fptr = pk.i64a.put(fr.fptr);
     // values
-    std::vector<double> f(B.ncol), g(P->g);
-    for (i64 i = 0; i < B.ncol; ++i) f[i] = P->f[cperm[i]];
-    ip.Bval = pk.din.put(B.val); ip.Qval = pk.din.put(Q.val); ip.f = pk.din.put(f); ip.g = pk.din.put(g);
-    ip.kpar = pk.din.put(kpar);
-    std::vector<double> pv(B.ncol, 0.0), dv(B.ncol, 0.0), yv(B.nrow, 0.0);
+    std::vector<double> f(n), g(P->g);
+    for (i64 i = 0; i < n; ++i) f[i] = P->f[cperm[i]];
+    ip.Bval = pk.din.put(Bval); ip.Qval = pk.din.put(Qval); ip.Qd = pk.din.put(Qd);
+    ip.f = pk.din.put(f); ip.g = pk.din.put(g); ip.kpar = pk.din.put(kpar);
+    std::vector<double> pv(n, 0.0), dv(n, 0.0), yv(m, 0.0);
     ip.has_p0 = p0 != nullptr; ip.has_d0 = d0 != nullptr; ip.has_y0 = y0 != nullptr;
-    for (i64 i = 0; i < B.ncol; ++i) { if (p0) pv[i] = p0[ip.colmap[i]]; if (d0) dv[i] = d0[ip.colmap[i]]; }
-    if (y0) for (i64 i = 0; i < B.nrow; ++i) yv[i] = y0[ip.rowmap[i]];
+    for (i64 i = 0; i < n; ++i) { if (p0) pv[i] = p0[ip.colmap[i]]; if (d0) dv[i] = d0[ip.colmap[i]]; }
+    if (y0) for (i64 i = 0; i < m; ++i) yv[i] = y0[ip.rowmap[i]];
     ip.p = pk.din.put(pv); ip.d = pk.din.put(dv); ip.y = pk.din.put(yv);
     // workspace
     ip.fsize = fr.fsize;
-    ip.H = pk.work.take(Q.nbnz); ip.Finit = pk.work.take(fr.fsize);
-    ip.pscl = pk.work.take(B.ncol); ip.yscl = pk.work.take(B.nrow);
-    ip.vn = pk.work.take((size_t)mb::NVEC_N * B.ncol); ip.vm = pk.work.take((size_t)mb::NVEC_M * B.nrow);
-    ip.vv = pk.work.take((size_t)mb::NVEC_V * B.nvtx); ip.work = pk.work.take((size_t)(512 / 32) * wmax);
+    ip.wBval = pk.work.take(Bval.size()); ip.wQval = pk.work.take(Qval.size()); ip.wQd = pk.work.take(Qd.size());
+    ip.Hd = pk.work.take(Qd.size()); ip.Finit = pk.work.take(fr.fsize);
+    ip.pscl = pk.work.take(n); ip.yscl = pk.work.take(m);
+    ip.vn = pk.work.take((size_t)mb::NVEC_N * n); ip.vm = pk.work.take((size_t)mb::NVEC_M * m);
+    ip.vv = pk.work.take((size_t)mb::NVEC_V * nv); ip.work = pk.work.take((size_t)(512 / 32) * wmax);
     ip.uhist = pk.work.take(set.refine_max_iter + 2); ip.cghist = pk.work.take(set.newton_max_iter + 1);
-    ip.cache = pk.work.take(std::max<i64>(cx[B.nvtx], 1));
-    ip.wBval = pk.work.take(B.nbnz); ip.wQval = pk.work.take(Q.nbnz);
-    ip.wf = pk.work.take(B.ncol); ip.wg = pk.work.take(B.nrow);
-    ip.wp = pk.work.take(B.ncol); ip.wd = pk.work.take(B.ncol); ip.wy = pk.work.take(B.nrow);
+    ip.cache = pk.work.take(std::max<i64>(cx[nv], 1));
+    ip.wf = pk.work.take(n); ip.wg = pk.work.take(m); ip.wp = pk.work.take(n); ip.wd = pk.work.take(n); ip.wy = pk.work.take(m);
     size_t esz = set.precision == MB_PREC_FP32 ? 4 : 8;
     ip.F = (pk.fbytes + 255) / 256 * 256;
     pk.fbytes = ip.F + fr.fsize * esz;
-    ip.po = pk.out.take(B.ncol); ip.dout = pk.out.take(B.ncol); ip.yo = pk.out.take(B.nrow);
+    ip.po = pk.out.take(n); ip.dout = pk.out.take(n); ip.yo = pk.out.take(m);
     ip.scal = pk.out.take(mb::NSCAL); ip.hist = pk.out.take((size_t)(set.max_iter + 1) * mb::ROW_DOUBLES);
+    ip.status = pk.ost.take(mb::NSTAT);
     pk.plans.push_back(std::move(ip));
     return MB_OK;
+}
+
+// append a single-instance Packed to the batch, shifting its offsets
+static void merge(Packed& dst, Packed& src) {
+    InstPlan ip = std::move(src.plans[0]);
+    auto cat = [](auto& D, auto& S) -> size_t {
+        size_t base = D.al(D.size());
+        if (D.host) { D.h.resize(base); D.h.insert(D.h.end(), S.h.begin(), S.h.end()); }
+        else D.n = base + S.size();
+        return base;
+    };
+    size_t b32 = cat(dst.i32, src.i32), b64 = cat(dst.i64a, src.i64a), bin = cat(dst.din, src.din);
+    size_t bw = cat(dst.work, src.work), bo = cat(dst.out, src.out), bs = cat(dst.ost, src.ost);
+    for (size_t* f : {&ip.xcol, &ip.colvtx, &ip.cfront, &ip.Brptr, &ip.Bcidx, &ip.Bcptr, &ip.Bridx, &ip.Bcpos,
+                      &ip.Qrptr, &ip.Qcidx, &ip.Qcptr, &ip.Qridx, &ip.Qcpos, &ip.hdld, &ip.qoffk, &ip.kind,
+                      &ip.fres0, &ip.fnres, &ip.fnsep, &ip.fparent, &ip.fsepp, &ip.fsep, &ip.frel}) *f += b32;
+    for (size_t* f : {&ip.hdoff, &ip.hdpos, &ip.qoffpos, &ip.cxblk, &ip.fptr}) *f += b64;
+    for (size_t* f : {&ip.Bval, &ip.Qval, &ip.Qd, &ip.f, &ip.g, &ip.kpar, &ip.p, &ip.d, &ip.y}) *f += bin;
+    for (size_t* f : {&ip.wBval, &ip.wQval, &ip.wQd, &ip.Hd, &ip.Finit, &ip.pscl, &ip.yscl, &ip.vn, &ip.vm, &ip.vv,
+                      &ip.work, &ip.uhist, &ip.cghist, &ip.cache, &ip.wf, &ip.wg, &ip.wp, &ip.wd, &ip.wy}) *f += bw;
+    for (size_t* f : {&ip.po, &ip.dout, &ip.yo, &ip.scal, &ip.hist}) *f += bo;
+    ip.status += bs;
+    size_t fb = (dst.fbytes + 255) / 256 * 256;
+    ip.F += fb;
+    dst.fbytes = fb + src.fbytes;
+    dst.plans.push_back(std::move(ip));
 }
 
 struct mb_batch {
@@ -284,6 +353,7 @@ struct mb_batch {
     std::vector<mb_problem*> probs;
     Packed pk;
     int32_t* d_i32 = nullptr;
+    int32_t* d_ost = nullptr;
     i64* d_i64 = nullptr;
     double* d_din = nullptr;
     double* d_work = nullptr;
@@ -297,7 +367,7 @@ struct mb_batch {
     int64_t launches = 0;
     ~mb_batch() {
         cudaFree(d_i32); cudaFree(d_i64); cudaFree(d_din); cudaFree(d_work); cudaFree(d_out); cudaFree(d_F);
-        cudaFree(d_inst); cudaFree(d_counter);
+        cudaFree(d_inst); cudaFree(d_counter); cudaFree(d_ost);
         cudaFreeHost(h_i32); cudaFreeHost(h_out);
         if (e0) cudaEventDestroy(e0);
         if (e1) cudaEventDestroy(e1);
@@ -324,7 +394,9 @@ static int upload(mb_batch* b) {
     CUDA_TRY(ctx, cudaMalloc(&b->d_F, std::max<size_t>(pk.fbytes, 256)));
     CUDA_TRY(ctx, cudaMalloc((void**)&b->d_counter, sizeof(int)));
     CUDA_TRY(ctx, cudaMallocHost((void**)&b->h_out, std::max<size_t>(pk.out.size(), 1) * sizeof(double)));
-    CUDA_TRY(ctx, cudaMallocHost((void**)&b->h_i32, std::max<size_t>(pk.i32.size(), 1) * sizeof(int32_t)));
+    CUDA_TRY(ctx, cudaMalloc((void**)&b->d_ost, std::max<size_t>(pk.ost.size(), 1) * sizeof(int32_t)));
+    CUDA_TRY(ctx, cudaMemsetAsync(b->d_ost, 0, std::max<size_t>(pk.ost.size(), 1) * sizeof(int32_t), st));
+    CUDA_TRY(ctx, cudaMallocHost((void**)&b->h_i32, std::max<size_t>(pk.ost.size(), 1) * sizeof(int32_t)));
     std::vector<mb::DevInst> hi(pk.plans.size());
     for (size_t k = 0; k < pk.plans.size(); ++k) {
         const InstPlan& p = pk.plans[k];
@@ -332,34 +404,31 @@ static int upload(mb_batch* b) {
         int32_t* i32 = b->d_i32; i64* q64 = b->d_i64; double* dn = b->d_din; double* wk = b->d_work; double* ot = b->d_out;
         I.n = (int)p.n; I.m = (int)p.m; I.nvtx = (int)p.nvtx; I.nfront = (int)p.nfront; I.nu = (int)p.nu;
         I.has_p0 = p.has_p0; I.has_d0 = p.has_d0; I.has_y0 = p.has_y0; I.mut = p.mut;
-        auto fillbsm = [&](mb::DevBSM& A, i64 nout, i64 narc, size_t xsrc, size_t xcol, size_t xrow, size_t tgt, size_t xblk,
-                           size_t val, size_t rptr, size_t rarc, size_t rvtx, size_t rowout, size_t colvtx, i64 nrow) {
-            A.nout = (int)nout; A.nvtx = (int)p.nvtx; A.narc = (int)narc; A.ncol = (int)p.n; A.nrow = (int)nrow;
-            A.xsrc = i32 + xsrc; A.xcol = i32 + xcol; A.xrow = i32 + xrow; A.tgt = i32 + tgt;
-            A.xblk = (const int64_t*)(q64 + xblk); A.val = wk + val;
-            A.rptr = i32 + rptr; A.rarc = i32 + rarc; A.rvtx = i32 + rvtx; A.rowout = i32 + rowout; A.colvtx = i32 + colvtx;
+        I.xcol = i32 + p.xcol; I.colvtx = i32 + p.colvtx; I.cfront = i32 + p.cfront;
+        auto fillsp = [&](mb::DevSp& A, i64 nrow, i64 ncol, i64 nnz, size_t rptr, size_t cidx, size_t wval, size_t val0,
+                          size_t cptr, size_t ridx, size_t cpos) {
+            A.nrow = (int)nrow; A.ncol = (int)ncol; A.nnz = (int)nnz;
+            A.rptr = i32 + rptr; A.cidx = i32 + cidx; A.val = wk + wval; A.val0 = dn + val0;
+            A.cptr = i32 + cptr; A.ridx = i32 + ridx; A.cpos = i32 + cpos;
         };
-        fillbsm(I.B, p.Bnout, p.Bnarc, p.Bxsrc, p.Bxcol, p.Bxrow, p.Btgt, p.Bxblk, p.wBval, p.Brptr, p.Brarc, p.Brvtx,
-                p.Browout, p.Bcolvtx, p.m);
-        fillbsm(I.Q, p.nvtx, p.Qnarc, p.Qxsrc, p.Bxcol, p.Bxcol, p.Qtgt, p.Qxblk, p.wQval, p.Qrptr, p.Qrarc, p.Qrvtx,
-                p.Bcolvtx, p.Bcolvtx, p.n);
-        I.Bval0 = dn + p.Bval; I.Qval0 = dn + p.Qval; I.f0 = dn + p.f; I.g0 = dn + p.g;
-        I.p0 = dn + p.p; I.d0 = dn + p.d; I.y0 = dn + p.y;
-        I.H = wk + p.H;
-        I.qdiag = i32 + p.qdiag; I.hpos = (const int64_t*)(q64 + p.hpos); I.hld = i32 + p.hld;
+        fillsp(I.B, p.m, p.n, p.Bnnz, p.Brptr, p.Bcidx, p.wBval, p.Bval, p.Bcptr, p.Bridx, p.Bcpos);
+        fillsp(I.Q, p.n, p.n, p.Qnnz, p.Qrptr, p.Qcidx, p.wQval, p.Qval, p.Qcptr, p.Qridx, p.Qcpos);
+        I.hdoff = (const int64_t*)(q64 + p.hdoff); I.Qd = wk + p.wQd; I.Qd0 = dn + p.Qd; I.Hd = wk + p.Hd;
+        I.hdpos = (const int64_t*)(q64 + p.hdpos); I.hdld = i32 + p.hdld;
+        I.nqoff = (int)p.nqoff; I.qoffk = i32 + p.qoffk; I.qoffpos = (const int64_t*)(q64 + p.qoffpos);
         I.kind = i32 + p.kind; I.kpar = dn + p.kpar; I.cxblk = (const int64_t*)(q64 + p.cxblk); I.cache = wk + p.cache;
         I.wsize = p.wsize;
         I.fres0 = i32 + p.fres0; I.fnres = i32 + p.fnres; I.fnsep = i32 + p.fnsep; I.fparent = i32 + p.fparent;
         I.fptr = (const int64_t*)(q64 + p.fptr); I.fsepp = i32 + p.fsepp; I.fsep = i32 + p.fsep; I.frel = i32 + p.frel;
         I.fsize = p.fsize;
         I.Finit = wk + p.Finit; I.F = (char*)b->d_F + p.F;
+        I.f0 = dn + p.f; I.g0 = dn + p.g; I.p0 = dn + p.p; I.d0 = dn + p.d; I.y0 = dn + p.y;
         I.f = wk + p.wf; I.g = wk + p.wg; I.pscl = wk + p.pscl; I.yscl = wk + p.yscl;
         I.p = wk + p.wp; I.d = wk + p.wd; I.y = wk + p.wy;
         I.vn = wk + p.vn; I.vm = wk + p.vm; I.vv = wk + p.vv; I.work = wk + p.work;
-        I.vfront = i32 + p.vfront;
         I.po = ot + p.po; I.dout = ot + p.dout; I.yo = ot + p.yo;
         I.hist = ot + p.hist; I.uhist = wk + p.uhist; I.cghist = wk + p.cghist;
-        I.status = i32 + p.status; I.scal = ot + p.scal;
+        I.status = b->d_ost + p.status; I.scal = ot + p.scal;
     }
     CUDA_TRY(ctx, cudaMalloc((void**)&b->d_inst, hi.size() * sizeof(mb::DevInst)));
     CUDA_TRY(ctx, cudaMemcpyAsync(b->d_inst, hi.data(), hi.size() * sizeof(mb::DevInst), cudaMemcpyHostToDevice, st));
@@ -379,11 +448,27 @@ static int make_batch(mb_ctx* ctx, mb_problem* const* probs, int32_t nprob, cons
     auto b = std::make_unique<mb_batch>();
     b->ctx = ctx; b->set = s;
     CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+    for (int32_t k = 0; k < nprob; ++k) if (!probs[k]) return fail(ctx, MB_E_ARG, "null problem");
+    std::vector<Packed> local(nprob);
+    std::vector<int> rcs(nprob, 0);
+    std::vector<std::string> errs(nprob);
+    std::atomic<int32_t> next{0};
+    auto worker = [&]() {
+        for (;;) {
+            int32_t k = next.fetch_add(1);
+            if (k >= nprob) break;
+            rcs[k] = plan_instance(probs[k], s, p0, d0, y0, local[k], errs[k]);
+        }
+    };
+    int nth = (int)std::min<unsigned>(std::max(1u, std::thread::hardware_concurrency()), (unsigned)std::max(1, nprob));
+    std::vector<std::thread> th;
+    for (int t = 1; t < nth; ++t) th.emplace_back(worker);
+    worker();
+    for (auto& t : th) t.join();
     for (int32_t k = 0; k < nprob; ++k) {
-        if (!probs[k]) return fail(ctx, MB_E_ARG, "null problem");
-        std::string err;
-        int rc = plan_instance(probs[k], s, p0, d0, y0, b->pk, err);
-        if (rc) return fail(ctx, rc, err);
+        if (rcs[k]) return fail(ctx, rcs[k], errs[k]);
+        merge(b->pk, local[k]);
+        Packed().i32.h.swap(local[k].i32.h);
         b->probs.push_back(probs[k]);
     }
     int rc = upload(b.get());
@@ -415,7 +500,7 @@ static int run_batch(mb_batch* b, int mode, int32_t grid, float* ms) {
 static int fetch_batch(mb_batch* b) {
     mb_ctx* ctx = b->ctx;
     CUDA_TRY(ctx, cudaMemcpyAsync(b->h_out, b->d_out, std::max<size_t>(b->pk.out.size(), 1) * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-    CUDA_TRY(ctx, cudaMemcpyAsync(b->h_i32, b->d_i32, std::max<size_t>(b->pk.i32.size(), 1) * sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
+    CUDA_TRY(ctx, cudaMemcpyAsync(b->h_i32, b->d_ost, std::max<size_t>(b->pk.ost.size(), 1) * sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
     CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
     return MB_OK;
 }
@@ -428,7 +513,8 @@ static void unpack_one(const mb_batch* b, size_t k, double* p, double* d, double
     if (y) for (i64 i = 0; i < ip.m; ++i) y[ip.rowmap[i]] = o[ip.yo + i];
     if (r) {
         const int32_t* st = b->h_i32 + ip.status;
-        r->status = st[0]; r->niter = st[1]; r->nfactor_retry = st[2];
+        r->status = st[0]; r->niter = st[1]; r->nfactor_retry = st[2]; r->nfactor = st[3]; r->reserved = 0;
+        r->factor_flops = ip.fflops;
         const double* sc = o + ip.scal;
         r->mu = sc[0]; r->pres = sc[1]; r->dres = sc[2]; r->pobj = sc[3]; r->dobj = sc[4];
         int ns = 0;
@@ -722,15 +808,14 @@ int mb_problem_destroy(mb_problem* P) {
 int mb_problem_symbolic(const mb_problem* Pc, int64_t* vperm, int64_t* nfront, int64_t* res0, int64_t* nres,
                         int64_t* nsep, int64_t* parent, int64_t cap) {
     if (!Pc) return MB_E_ARG;
-    mb_problem* P = const_cast<mb_problem*>(Pc);
-    do_symbolic(P);
-    if (vperm) for (size_t k = 0; k < P->vperm.size(); ++k) vperm[k] = P->vperm[k];
-    if (nfront) *nfront = P->fr.nfront;
-    for (i64 f = 0; f < P->fr.nfront && f < cap; ++f) {
-        if (res0) res0[f] = P->fr.res0[f];
-        if (nres) nres[f] = P->fr.nres[f];
-        if (nsep) nsep[f] = (i64)P->fr.sep[f].size();
-        if (parent) parent[f] = P->fr.parent[f];
+    Sym S = do_symbolic(Pc);
+    if (vperm) for (size_t k = 0; k < S.vperm.size(); ++k) vperm[k] = S.vperm[k];
+    if (nfront) *nfront = S.fr.nfront;
+    for (i64 f = 0; f < S.fr.nfront && f < cap; ++f) {
+        if (res0) res0[f] = S.fr.res0[f];
+        if (nres) nres[f] = S.fr.nres[f];
+        if (nsep) nsep[f] = (i64)S.fr.sep[f].size();
+        if (parent) parent[f] = S.fr.parent[f];
     }
     return MB_OK;
 }
@@ -769,7 +854,7 @@ int mb_solver_step(mb_solver* s, int32_t* status) {
     int rc = run_batch(s->b.get(), mb::MODE_STEP, 1, nullptr);
     if (rc) return rc;
     int32_t st = 0;
-    CUDA_TRY(s->prob->ctx, cudaMemcpy(&st, s->b->d_i32 + s->b->pk.plans[0].status, sizeof(int32_t), cudaMemcpyDeviceToHost));
+    CUDA_TRY(s->prob->ctx, cudaMemcpy(&st, s->b->d_ost + s->b->pk.plans[0].status, sizeof(int32_t), cudaMemcpyDeviceToHost));
     s->status = st;
     if (st != MB_CONTINUE) s->done = true;
     if (status) *status = st;
@@ -841,8 +926,21 @@ int mb_batch_stats(mb_batch* b, int64_t* s) {
     s[2] = (int64_t)b->pk.fbytes;
     s[3] = b->launches;
     s[4] = (int64_t)b->pk.plans.size();
-    s[5] = (int64_t)(b->pk.out.size() * 8);
+    s[5] = (int64_t)(b->pk.out.size() * 8 + b->pk.ost.size() * 4);
     s[6] = 0; s[7] = 0;
+    return MB_OK;
+}
+
+int mb_batch_timers(mb_batch* b, double* out, int64_t cap) {
+    if (!b || !out) return MB_E_ARG;
+    // per instance: NSEC section clocks, trsv sweeps, gemv calls (needs a prior mb_batch_fetch)
+    const int W = mb::NSEC + 2;
+    for (size_t k = 0; k < b->pk.plans.size() && (int64_t)((k + 1) * W) <= cap; ++k) {
+        const double* sc = b->h_out + b->pk.plans[k].scal;
+        for (int j = 0; j < mb::NSEC; ++j) out[k * W + j] = sc[mb::SCAL_SEC + j];
+        out[k * W + mb::NSEC] = sc[mb::SCAL_NTRSV];
+        out[k * W + mb::NSEC + 1] = sc[mb::SCAL_NGEMV];
+    }
     return MB_OK;
 }
 

@@ -29,21 +29,18 @@ struct Row {
 };
 constexpr int ROW_DOUBLES = 17;
 
-// Block-sparse matrix on the device, 0-based: block-CSC by vertex (column blocks) plus a
-// block-CSR arc index by out-vertex (row blocks) so both A x and Aᵀ x are gathers.
-struct DevBSM {
-    int nout, nvtx, narc, ncol, nrow;
-    const int* xsrc;        // nvtx+1
-    const int* xcol;        // nvtx+1
-    const int* xrow;        // nout+1
-    const int* tgt;         // narc
-    const int64_t* xblk;    // narc+1
-    double* val;            // nbnz (mutable: equilibration scales in place)
-    const int* rptr;        // nout+1: arcs of out-vertex u are rarc[rptr[u] .. rptr[u+1])
-    const int* rarc;        // arc ids grouped by target
-    const int* rvtx;        // the source vertex of each grouped arc
-    const int* rowout;      // nrow: out-vertex of each row
-    const int* colvtx;      // ncol: vertex of each column
+// Scalar sparse matrix on the device: the nonzeros of a BlockSparseMatrix (explicit zeros of its
+// dense blocks dropped; they contribute nothing to any sum), CSR order, with a CSC index into the
+// same value array so that A x and Aᵀ x are both gathers.
+struct DevSp {
+    int nrow, ncol, nnz;
+    const int* rptr;        // nrow+1
+    const int* cidx;        // nnz: column of each CSR entry (ascending within a row)
+    double* val;            // nnz, CSR order (mutable: equilibration scales in place)
+    const double* val0;     // nnz, pristine copy
+    const int* cptr;        // ncol+1
+    const int* ridx;        // nnz: row of each CSC entry (ascending within a column)
+    const int* cpos;        // nnz: CSR position of each CSC entry
 };
 
 struct DevInst {
@@ -51,11 +48,18 @@ struct DevInst {
     int nu;                 // cone degree ν
     int has_p0, has_d0, has_y0;
     double mut;             // barrier target μ′ (0 = exact solve)
-    DevBSM B, Q;            // Q shares B's vertex/column layout; Q.xrow == Q.xcol
-    double* H;              // values of H (Q's pattern)
-    const int* qdiag;       // per vertex: arc of the diagonal block in Q/H, -1 if none
-    const int64_t* hpos;    // per Q/H arc: offset in F of the block's (0,0) entry, -1 if the block is upper
-    const int* hld;         // per Q/H arc: leading dimension of its front
+    const int* xcol;        // nvtx+1: columns of each vertex
+    const int* colvtx;      // n: vertex of each column
+    const int* cfront;      // n: front owning each column
+    DevSp B, Q;
+    // dense diagonal blocks (nc x nc per vertex, column-major): Q's (working + pristine) and H's
+    const int64_t* hdoff;   // nvtx+1
+    double* Qd; const double* Qd0; double* Hd;
+    const int64_t* hdpos;   // per vertex: offset in F of its diagonal block's (0,0) entry
+    const int* hdld;        // per vertex: leading dimension of its front
+    // Q nonzeros outside the diagonal blocks, lower triangle: CSR position and F offset
+    int nqoff;
+    const int* qoffk; const int64_t* qoffpos;
     const int* kind;        // cone kind per vertex
     const double* kpar;     // cone parameter per vertex
     const int64_t* cxblk;   // cache offsets per vertex (nvtx+1)
@@ -67,34 +71,34 @@ struct DevInst {
     const int* fres0; const int* fnres; const int* fnsep; const int* fparent;
     const int64_t* fptr; const int* fsepp; const int* fsep; const int* frel;
     int64_t fsize;
-    // L = BᵀB in front layout, built on the device from B at set-up
-    double* Finit;          // fsize doubles
+    double* Finit;          // fsize doubles: lower part of BᵀB in front layout, built on the device
     void* F;                // fsize FT (double or float)
-    // pristine inputs (never written) and their working copies (equilibrated in place at init)
-    const double* Bval0; const double* Qval0; const double* f0; const double* g0;
-    const double* p0; const double* d0; const double* y0;
+    // pristine vectors and working copies
+    const double* f0; const double* g0; const double* p0; const double* d0; const double* y0;
     double* f; double* g;
     double* pscl; double* yscl;
-    // iterates and workspace
     double* p; double* d; double* y;
     double* vn;             // NVEC_N n-vectors
     double* vm;             // NVEC_M m-vectors
     double* vv;             // NVEC_V nvtx-vectors
     double* work;           // cone workspace (wsize per warp)
-    const int* vfront;      // per vertex: its front
     double* po; double* dout; double* yo;   // result iterates (user scaling, solver order)
     double* hist;           // max_iter+1 rows (ROW_DOUBLES each)
     double* uhist;          // refine_max_iter + 2
     double* cghist;         // newton_max_iter + 1
-    // outputs
-    int* status;            // [0] IPM status, [1] rows written, [2] factor retries, [3] error code
-    double* scal;           // mu, pres, dres, pobj, dobj, nf, ng, sf, sg, nB, plus spares
+    int* status;            // [0] IPM status, [1] rows written, [2] factor retries, [3] factorizations
+    double* scal;           // NSCAL: mu pres dres pobj dobj nf ng sf sg nB, timers, counters
 };
 
-constexpr int NVEC_N = 12;  // Df Qp wf Dpa Dda Dp Dd df dx cgw  tmp1 tmp2
+constexpr int NVEC_N = 12;  // Df Qp wf Dpa Dda Dp Dd df dx cgw  tmp1 tmp2 (tmp2 also: column maxima)
 constexpr int NVEC_M = 8;   // Dg Dya Dy dg dy cgp tmp1 tmp2
 constexpr int NVEC_V = 6;   // step spsd flag vscl vnrm vswp
-constexpr int NSCAL = 16;   // mu pres dres pobj dobj | nf ng sf sg nB
+constexpr int NSCAL = 32;   // mu pres dres pobj dobj | nf ng sf sg nB | section clocks (NSEC) | counters
+// section timers (SM clock cycles), the TimerOutputs sections of the reference plus set-up
+enum Section { SEC_EQUIL = 0, SEC_FINIT, SEC_SCALE, SEC_INITKKT, SEC_PRED, SEC_CORR, SEC_MAXSTEPS, SEC_TRSV, SEC_GEMV, NSEC };
+constexpr int SCAL_SEC = 10;        // scal[10 .. 10+NSEC)
+constexpr int SCAL_NTRSV = 20;      // triangular solve sweeps
+constexpr int SCAL_NGEMV = 21;      // block-sparse matvecs
 constexpr int NSTAT = 4;    // status, history rows, factor retries, error
 
 // kernel modes: a full solve, or the pieces used by the step-wise API

@@ -212,11 +212,15 @@ struct Ctx {
     double *Df, *Qp, *wf, *Dpa, *Dda, *Dp, *Dd, *df, *dx, *cgw, *tn;
     double *Dg, *Dya, *Dy, *dg, *dyv, *cgp, *tm1, *tm2;
     double *vstep, *vspsd, *vflag, *vscl, *vnrm, *vswp;
-    DevBSM Hb;              // H: Q's block pattern with the scaled Hessian values
     double delta;
     double nf, ng, sf, sg, nB;
     int nrow_hist;
     int nretry;
+    int nfact;              // numeric factorizations performed
+    long long tsec[NSEC];   // per-section SM clocks (thread 0)
+    long long ntrsv, ngemv;
+    __device__ long long tic() const { __syncthreads(); return clock64(); }
+    __device__ void toc(int sec, long long t0) { __syncthreads(); tsec[sec] += clock64() - t0; }
     __device__ Ctx(const DevInst& I_, const Settings& s_, Shared& sh_) : I(I_), set(s_), sh(sh_) {
         red = sh.red;
         F = reinterpret_cast<FT*>(I.F);
@@ -231,52 +235,58 @@ struct Ctx {
         double* z = I.vv;
         vstep = z; vspsd = z + nv; vflag = z + 2 * nv; vscl = z + 3 * nv; vnrm = z + 4 * nv; vswp = z + 5 * nv;
         delta = 1; nrow_hist = 0; nretry = 0;
-        Hb = I.Q; Hb.val = I.H;
         nf = I.scal[5]; ng = I.scal[6]; sf = I.scal[7]; sg = I.scal[8]; nB = I.scal[9];
-        nrow_hist = I.status[1]; nretry = I.status[2];
+        nrow_hist = I.status[1]; nretry = I.status[2]; nfact = I.status[3];
+        for (int k = 0; k < NSEC; ++k) tsec[k] = (long long)I.scal[SCAL_SEC + k];
+        ntrsv = (long long)I.scal[SCAL_NTRSV]; ngemv = (long long)I.scal[SCAL_NGEMV];
     }
     __device__ void save() {
         if (threadIdx.x == 0) {
             I.scal[5] = nf; I.scal[6] = ng; I.scal[7] = sf; I.scal[8] = sg; I.scal[9] = nB;
-            I.status[1] = nrow_hist; I.status[2] = nretry;
+            I.status[1] = nrow_hist; I.status[2] = nretry; I.status[3] = nfact;
+            for (int k = 0; k < NSEC; ++k) I.scal[SCAL_SEC + k] = (double)tsec[k];
+            I.scal[SCAL_NTRSV] = (double)ntrsv; I.scal[SCAL_NGEMV] = (double)ngemv;
         }
         __syncthreads();
     }
 
     // ---- set-up --------------------------------------------------------------------------
-    // Ruiz equilibration  (src/IPM/src/scaling/scaling.jl:52-184)
+    // Ruiz equilibration  (src/IPM/src/scaling/scaling.jl:52-184).  Q = blockdiag(Qd) + Qo.
     __device__ void equilibrate(int itmax, double tol) {
-        const DevBSM& B = I.B; const DevBSM& Q = I.Q;
-        const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-        double* rnrm = tm1; double* rswp = tm2;
+        const DevSp& B = I.B; const DevSp& Q = I.Q;
+        const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, gl = lane % G, sub = lane / G;
+        double* rnrm = tm1; double* rswp = tm2; double* cmax = tn;
         for (int v = tid; v < nv; v += NT) { vscl[v] = 1; vswp[v] = 1; }
         for (int i = tid; i < m; i += NT) { rswp[i] = 1; I.yscl[i] = 1; }
         __syncthreads();
         for (int it = 0; it < itmax; ++it) {
-            for (int i = tid; i < m; i += NT) {
-                int u = B.rowout[i]; int r = i - B.xrow[u], nr = B.xrow[u + 1] - B.xrow[u];
+            // infnorms!: row maxima of B; column maxima of B, Qo and the Qd blocks
+            for (int i0 = warp * GPW; i0 < m; i0 += NW * GPW) {
+                const int i = i0 + sub;
                 double mx = 0;
-                for (int k = B.rptr[u]; k < B.rptr[u + 1]; ++k) {
-                    int e = B.rarc[k], v = B.rvtx[k];
-                    int nc = B.xcol[v + 1] - B.xcol[v];
-                    const double* blk = B.val + B.xblk[e] + r;
-                    for (int j = 0; j < nc; ++j) mx = fmax(mx, fabs(blk[(int64_t)j * nr]));
-                }
-                rnrm[i] = mx;
+                if (i < m) for (int k = B.rptr[i] + gl; k < B.rptr[i + 1]; k += G) mx = fmax(mx, fabs(B.val[k]));
+                mx = group_reduce(mx, OpMax());
+                if (i < m && gl == 0) rnrm[i] = mx;
             }
-            for (int v = warp; v < nv; v += NW) {
+            for (int j0 = warp * GPW; j0 < n; j0 += NW * GPW) {
+                const int j = j0 + sub;
                 double mx = 0;
-                for (int e = Q.xsrc[v]; e < Q.xsrc[v + 1]; ++e)
-                    for (int64_t b = Q.xblk[e] + lane; b < Q.xblk[e + 1]; b += 32) mx = fmax(mx, fabs(Q.val[b]));
-                for (int e = B.xsrc[v]; e < B.xsrc[v + 1]; ++e)
-                    for (int64_t b = B.xblk[e] + lane; b < B.xblk[e + 1]; b += 32) mx = fmax(mx, fabs(B.val[b]));
-                mx = warp_max(mx);
-                if (lane == 0) vnrm[v] = mx;
+                if (j < n) {
+                    for (int k = B.cptr[j] + gl; k < B.cptr[j + 1]; k += G) mx = fmax(mx, fabs(B.val[B.cpos[k]]));
+                    for (int k = Q.cptr[j] + gl; k < Q.cptr[j + 1]; k += G) mx = fmax(mx, fabs(Q.val[Q.cpos[k]]));
+                    int v = I.colvtx[j], c0 = I.xcol[v], nc = I.xcol[v + 1] - c0;
+                    const double* qd = I.Qd + I.hdoff[v] + (int64_t)(j - c0) * nc;
+                    for (int r = gl; r < nc; r += G) mx = fmax(mx, fabs(qd[r]));
+                }
+                mx = group_reduce(mx, OpMax());
+                if (j < n && gl == 0) cmax[j] = mx;
             }
             __syncthreads();
             double dd = 0;
             for (int v = tid; v < nv; v += NT) {
-                double nn = sqrt(vnrm[v]);
+                double mx = 0;
+                for (int j = I.xcol[v]; j < I.xcol[v + 1]; ++j) mx = fmax(mx, cmax[j]);
+                double nn = sqrt(mx);
                 dd = fmax(dd, fabs(1.0 - nn));
                 if (nn != 0) { vswp[v] = 1.0 / nn; vscl[v] *= vswp[v]; }
             }
@@ -287,23 +297,27 @@ struct Ctx {
             }
             dd = block_reduce(dd, red, OpMax(), 0.0);
             // applyscaling!: B ← E B D, Q ← D Q D
-            for (int v = warp; v < nv; v += NW) {
-                double sv = vswp[v];
-                int nc = B.xcol[v + 1] - B.xcol[v];
-                for (int e = B.xsrc[v]; e < B.xsrc[v + 1]; ++e) {
-                    int u = B.tgt[e], r0 = B.xrow[u], nr = B.xrow[u + 1] - r0;
-                    double* blk = B.val + B.xblk[e];
-                    for (int t = lane; t < nr * nc; t += 32) blk[t] *= rswp[r0 + t % nr] * sv;
+            for (int i0 = warp * GPW; i0 < m; i0 += NW * GPW) {
+                const int i = i0 + sub;
+                if (i < m) for (int k = B.rptr[i] + gl; k < B.rptr[i + 1]; k += G) B.val[k] *= rswp[i] * vswp[I.colvtx[B.cidx[k]]];
+            }
+            for (int i0 = warp * GPW; i0 < n; i0 += NW * GPW) {
+                const int i = i0 + sub;
+                if (i < n) {
+                    double su = vswp[I.colvtx[i]];
+                    for (int k = Q.rptr[i] + gl; k < Q.rptr[i + 1]; k += G) Q.val[k] *= su * vswp[I.colvtx[Q.cidx[k]]];
                 }
-                for (int e = Q.xsrc[v]; e < Q.xsrc[v + 1]; ++e) {
-                    double sc = vswp[Q.tgt[e]] * sv;
-                    for (int64_t b = Q.xblk[e] + lane; b < Q.xblk[e + 1]; b += 32) Q.val[b] *= sc;
-                }
+            }
+            for (int v = 0; v < nv; ++v) {
+                int nc = I.xcol[v + 1] - I.xcol[v];
+                double sc = vswp[v] * vswp[v];
+                double* qd = I.Qd + I.hdoff[v];
+                for (int t = tid; t < nc * nc; t += NT) qd[t] *= sc;
             }
             __syncthreads();
             if (dd < tol) break;
         }
-        for (int j = tid; j < n; j += NT) { I.pscl[j] = vscl[B.colvtx[j]]; I.f[j] *= I.pscl[j]; }
+        for (int j = tid; j < n; j += NT) { I.pscl[j] = vscl[I.colvtx[j]]; I.f[j] *= I.pscl[j]; }
         for (int i = tid; i < m; i += NT) I.g[i] *= I.yscl[i];
         __syncthreads();
     }
@@ -316,64 +330,64 @@ struct Ctx {
         while (lo < hi) { int md = (lo + hi) >> 1; if (I.fsep[md] < s) lo = md + 1; else hi = md; }
         return nres + (lo - I.fsepp[f]);
     }
+    __device__ int64_t fpos(int i, int j) const {   // offset in F of entry (i, j), i >= j
+        int f = I.cfront[j];
+        int nfr = I.fnres[f] + I.fnsep[f];
+        return I.fptr[f] + rowpos(f, i) + (int64_t)(j - I.fres0[f]) * nfr;
+    }
 
-    // Finit ← lower part of BᵀB in front layout  (uzawa.jl:29 `B' * B`; gemm.jl:48-82;
-    // chordal.jl:1-80 scatter).  Row blocks are accumulated one after another so the sum order is
-    // fixed; within a row block every entry pair is owned by one thread.
+    // Finit ← lower part of BᵀB in front layout  (uzawa.jl:29 `B' * B`; gemm.jl:48-82; chordal.jl:1-80).
+    // Rows of B are accumulated one after another (fixed summation order); within a row every
+    // nonzero pair (a >= b) is owned by one thread.
     __device__ void build_finit() {
-        const int* vfront = I.vfront;
-        const DevBSM& B = I.B;
+        const DevSp& B = I.B;
         const int tid = threadIdx.x;
         for (int64_t i = tid; i < I.fsize; i += NT) I.Finit[i] = 0;
         __syncthreads();
-        int* koff = reinterpret_cast<int*>(tn);    // prefix column offsets of the arcs of u (<= nvtx+1 <= 2n ints)
-        for (int u = 0; u < B.nout; ++u) {
-            const int k0 = B.rptr[u], k1 = B.rptr[u + 1], deg = k1 - k0;
-            const int r0u = B.xrow[u], nr = B.xrow[u + 1] - r0u;
-            if (tid == 0) {
-                int acc = 0;
-                for (int k = 0; k < deg; ++k) { koff[k] = acc; int v = B.rvtx[k0 + k]; acc += B.xcol[v + 1] - B.xcol[v]; }
-                koff[deg] = acc;
+        for (int r = 0; r < m; ++r) {
+            const int k0 = B.rptr[r], nz = B.rptr[r + 1] - k0;
+            const int np = nz * (nz + 1) / 2;
+            for (int t = tid; t < np; t += NT) {
+                int a = (int)((sqrt(8.0 * t + 1.0) - 1.0) * 0.5);
+                while ((a + 1) * (a + 2) / 2 <= t) ++a;
+                while (a * (a + 1) / 2 > t) --a;
+                int b = t - a * (a + 1) / 2;
+                int ca = B.cidx[k0 + a], cb = B.cidx[k0 + b];
+                I.Finit[fpos(ca, cb)] += B.val[k0 + a] * B.val[k0 + b];
             }
-            __syncthreads();
-            const int cu = koff[deg];
-            const int64_t npair = (int64_t)cu * cu;
-            for (int64_t t = tid; t < npair; t += NT) {
-                int x = (int)(t % cu), y = (int)(t / cu);
-                if (x < y) continue;
-                int lo = 0, hi = deg;   // arc of x: last k with koff[k] <= x
-                while (hi - lo > 1) { int md = (lo + hi) >> 1; if (koff[md] <= x) lo = md; else hi = md; }
-                int kx = lo;
-                lo = 0; hi = deg;
-                while (hi - lo > 1) { int md = (lo + hi) >> 1; if (koff[md] <= y) lo = md; else hi = md; }
-                int ky = lo;
-                int ex = B.rarc[k0 + kx], vx = B.rvtx[k0 + kx], ey = B.rarc[k0 + ky], vy = B.rvtx[k0 + ky];
-                int xl = x - koff[kx], yl = y - koff[ky];
-                const double* bx = B.val + B.xblk[ex] + (int64_t)xl * nr;
-                const double* by = B.val + B.xblk[ey] + (int64_t)yl * nr;
-                double s = 0;
-                for (int r = 0; r < nr; ++r) s = fma(bx[r], by[r], s);
-                int sx = B.xcol[vx] + xl, sy = B.xcol[vy] + yl;
-                int f = vfront[vy];
-                int nfr = I.fnres[f] + I.fnsep[f];
-                int64_t pos = I.fptr[f] + rowpos(f, sx) + (int64_t)(sy - I.fres0[f]) * nfr;
-                I.Finit[pos] += s;
-            }
-            __syncthreads();
+            if (np) __syncthreads();
         }
     }
 
+    // y <- alpha (blockdiag(D) + Qo) x + beta y with D = Qd (the data Q) or Hd (the scaled H)
+    __device__ void amul(const double* Dblk, const double* x, double* y, double alpha, double beta) {
+        const DevSp& Q = I.Q;
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, gl = lane % G, sub = lane / G;
+        for (int i0 = warp * GPW; i0 < n; i0 += NW * GPW) {
+            const int i = i0 + sub;
+            double acc = 0;
+            if (i < n) {
+                int v = I.colvtx[i], c0 = I.xcol[v], nc = I.xcol[v + 1] - c0;
+                const double* row = Dblk + I.hdoff[v] + (int64_t)(i - c0) * nc;   // symmetric: row = column
+                for (int j = gl; j < nc; j += G) acc = fma(row[j], x[c0 + j], acc);
+                for (int k = Q.rptr[i] + gl; k < Q.rptr[i + 1]; k += G) acc = fma(Q.val[k], x[Q.cidx[k]], acc);
+            }
+            acc = group_reduce(acc, OpSum());
+            if (i < n && gl == 0) y[i] = beta == 0.0 ? alpha * acc : fma(alpha, acc, beta * y[i]);
+        }
+        __syncthreads();
+    }
+
     __device__ void startingpoint() {  // solver/ipm.jl:331-365
-        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+        const int warp = threadIdx.x >> 5;
         for (int v = warp; v < nv; v += NW) {
-            int c0 = I.B.xcol[v], nc = I.B.xcol[v + 1] - c0;
+            int c0 = I.xcol[v], nc = I.xcol[v + 1] - c0;
             w_identity(I.kind[v], nc, I.p + c0);
             w_identity(I.kind[v], nc, I.d + c0);
         }
-        (void)lane;
         __syncthreads();
-        bgemvN(I.B, I.p, tm1, 1, 0);
-        bgemvN(I.Q, I.p, tn, 1, 0);
+        spmv(I.B, I.p, tm1, 1, 0);
+        amul(I.Qd, I.p, tn, 1, 0);
         const double eps = 2.220446049250313e-16;
         double np = bnorm(I.p, n, red), nz = bnorm(tm1, m, red), nw = bnorm(tn, n, red);
         double sp = nz > eps * np ? fmax(1.0, bnorm(I.g, m, red) / nz) : 1.0;
@@ -384,30 +398,38 @@ struct Ctx {
 
     // ---- cone fan-outs  (cone/cone.jl:146-553) -------------------------------------------
     __device__ bool scale_all(double& spsd_sum) {
-        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+        const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+        // H_vv ← Q_vv for every cone block (cone.jl:146-174)
+        for (int v = 0; v < nv; ++v) {
+            if (I.kind[v] == CONE_FREE) continue;
+            int nc = I.xcol[v + 1] - I.xcol[v];
+            const double* q = I.Qd + I.hdoff[v];
+            double* h = I.Hd + I.hdoff[v];
+            for (int t = tid; t < nc * nc; t += NT) h[t] = q[t];
+        }
+        __syncthreads();
+        // per cone: scaling point and ⟨p*, d*⟩
         for (int v = warp; v < nv; v += NW) {
             int k = I.kind[v];
-            int c0 = I.B.xcol[v], nc = I.B.xcol[v + 1] - c0;
+            int c0 = I.xcol[v], nc = I.xcol[v + 1] - c0;
             double sp = 0; bool fl = true;
-            if (k != CONE_FREE) {
-                int e = I.qdiag[v];
-                if (e < 0) fl = false;
-                else {
-                    double* Hv = I.H + I.Q.xblk[e];
-                    const double* Qv = I.Q.val + I.Q.xblk[e];
-                    for (int t = lane; t < nc * nc; t += 32) Hv[t] = Qv[t];
-                    __syncwarp();
-                    const double* p = I.p + c0; const double* d = I.d + c0;
-                    if (k == CONE_POS) {   // pos.jl:75-84
-                        double s = 0;
-                        for (int i = lane; i < nc; i += 32) { Hv[i + (int64_t)i * nc] += d[i] / p[i]; s += 1.0 / (p[i] * d[i]); }
-                        sp = warp_sum(s);
-                    } else if (k == CONE_SOC) {
-                        fl = w_socscale(Hv, I.cache + I.cxblk[v], p, d, nc, sp);
-                    }
-                }
+            const double* p = I.p + c0; const double* d = I.d + c0;
+            if (k == CONE_POS) {   // pos.jl:75-84
+                double* Hv = I.Hd + I.hdoff[v];
+                double s = 0;
+                for (int i = lane; i < nc; i += 32) { Hv[i + (int64_t)i * nc] += d[i] / p[i]; s += 1.0 / (p[i] * d[i]); }
+                sp = warp_sum(s);
+            } else if (k == CONE_SOC) {
+                fl = w_socpoint(I.cache + I.cxblk[v], p, d, nc, sp);
             }
             if (lane == 0) { vflag[v] = fl ? 1.0 : 0.0; vspsd[v] = sp; }
+        }
+        __syncthreads();
+        // SOC Hessian blocks H = (2 (Jw)(Jw)ᵀ − J) / β² added in place (soc.jl:231-256)
+        for (int v = 0; v < nv; ++v) {
+            if (I.kind[v] != CONE_SOC || vflag[v] == 0.0) continue;
+            int nc = I.xcol[v + 1] - I.xcol[v];
+            b_sochess(I.Hd + I.hdoff[v], I.cache + I.cxblk[v], nc);
         }
         __syncthreads();
         double ok = 1, s = 0;
@@ -422,7 +444,7 @@ struct Ctx {
         double* work = I.work + (int64_t)warp * I.wsize;
         for (int v = warp; v < nv; v += NW) {
             int k = I.kind[v];
-            int c0 = I.B.xcol[v], nc = I.B.xcol[v + 1] - c0;
+            int c0 = I.xcol[v], nc = I.xcol[v + 1] - c0;
             if (k == CONE_POS) {   // pos.jl:107-120
                 for (int i = lane; i < nc; i += 32) fr[c0 + i] = (sm - Dpv[c0 + i] * Ddv[c0 + i]) / I.p[c0 + i] - I.d[c0 + i];
             } else if (k == CONE_SOC) {
@@ -438,7 +460,7 @@ struct Ctx {
         const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
         for (int v = warp; v < nv; v += NW) {
             int k = I.kind[v];
-            int c0 = I.B.xcol[v], nc = I.B.xcol[v + 1] - c0;
+            int c0 = I.xcol[v], nc = I.xcol[v + 1] - c0;
             if (k == CONE_POS) {   // pos.jl:126-137
                 for (int i = lane; i < nc; i += 32) fr[c0 + i] = sm / I.p[c0 + i] - I.d[c0 + i];
             } else if (k == CONE_SOC) {
@@ -454,7 +476,7 @@ struct Ctx {
         const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
         for (int v = warp; v < nv; v += NW) {
             int k = I.kind[v];
-            int c0 = I.B.xcol[v], nc = I.B.xcol[v + 1] - c0;
+            int c0 = I.xcol[v], nc = I.xcol[v + 1] - c0;
             double tp = 1, td = 1;
             if (k == CONE_POS) {
                 tp = w_posmaxstep(I.p + c0, Dpv + c0, nc);
@@ -477,28 +499,32 @@ struct Ctx {
     __device__ void zerofree(double* x) {
         for (int v = threadIdx.x >> 5; v < nv; v += NW)
             if (I.kind[v] == CONE_FREE)
-                for (int j = I.B.xcol[v] + (threadIdx.x & 31); j < I.B.xcol[v + 1]; j += 32) x[j] = 0;
+                for (int j = I.xcol[v] + (threadIdx.x & 31); j < I.xcol[v + 1]; j += 32) x[j] = 0;
         __syncthreads();
     }
 
     // ---- factor  (kkt/uzawa.jl:73-115) ----------------------------------------------------
     __device__ void assemble(double dl, double rho) {
-        const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+        const int tid = threadIdx.x;
         for (int64_t i = tid; i < I.fsize; i += NT) F[i] = (FT)I.Finit[i];
         __syncthreads();
-        for (int v = warp; v < nv; v += NW) {
-            int nc = I.Q.xcol[v + 1] - I.Q.xcol[v];
-            for (int e = I.Q.xsrc[v]; e < I.Q.xsrc[v + 1]; ++e) {
-                int64_t pos = I.hpos[e];
-                if (pos < 0) continue;
-                int u = I.Q.tgt[e], nr = I.Q.xrow[u + 1] - I.Q.xrow[u], ld = I.hld[e];
-                const double* h = I.H + I.Q.xblk[e];
-                for (int t = lane; t < nr * nc; t += 32) {
-                    int i = t % nr, j = t / nr;
-                    int64_t q = pos + i + (int64_t)j * ld;
+        // + δ H: diagonal blocks (lower part) and the off-diagonal nonzeros of Q (chordal.jl:1-80)
+        for (int v = 0; v < nv; ++v) {
+            int nc = I.xcol[v + 1] - I.xcol[v];
+            int64_t base = I.hdpos[v];
+            int ld = I.hdld[v];
+            const double* h = I.Hd + I.hdoff[v];
+            for (int t = tid; t < nc * nc; t += NT) {
+                int r = t % nc, c = t / nc;
+                if (r >= c) {
+                    int64_t q = base + r + (int64_t)c * ld;
                     F[q] = (FT)(I.Finit[q] + dl * h[t]);
                 }
             }
+        }
+        for (int t = tid; t < I.nqoff; t += NT) {
+            int64_t q = I.qoffpos[t];
+            F[q] = (FT)(I.Finit[q] + dl * I.Q.val[I.qoffk[t]]);
         }
         __syncthreads();
         if (rho != 0) {
@@ -549,24 +575,36 @@ struct Ctx {
         delta = dl;
         assemble(dl, 0.0);
         int info = numeric_factor();
+        nfact++;
         rho = 0;
         if (info != 0) {
             assemble(dl, 0.0);
             rho = 2.220446049250313e-16 * factor_lower_norm();
             assemble(dl, rho);
             info = numeric_factor();
+            nfact++;
             nretry++;
         }
         return info == 0;
     }
 
     __device__ void Lsolve(double* x) {
+        long long t0 = tic(); ntrsv++;
+        Lsolve_(x);
+        toc(SEC_TRSV, t0);
+    }
+    __device__ void Usolve(double* x) {
+        long long t0 = tic(); ntrsv++;
+        Usolve_(x);
+        toc(SEC_TRSV, t0);
+    }
+    __device__ void Lsolve_(double* x) {
         for (int f = 0; f < I.nfront; ++f) {
             int nres = I.fnres[f], nfr = nres + I.fnsep[f];
             front_lsolve<FT>(F + I.fptr[f], nfr, nres, I.fres0[f], I.fsep + I.fsepp[f], x, sh);
         }
     }
-    __device__ void Usolve(double* x) {
+    __device__ void Usolve_(double* x) {
         for (int f = I.nfront - 1; f >= 0; --f) {
             int nres = I.fnres[f], nfr = nres + I.fnsep[f];
             front_usolve<FT>(F + I.fptr[f], nfr, nres, I.fres0[f], I.fsep + I.fsepp[f], x, sh);
@@ -574,10 +612,12 @@ struct Ctx {
     }
 
     // ---- KKT solve  (kkt/kkt.jl:9-21; kkt/cg.jl:69-167; kkt/uzawa.jl:199-227, 319-507) -------
-    __device__ void mulkkt(double* u, double* v, const DevBSM& A, const double* x, const double* yv) {
-        bgemvN(A, x, u, 1, 0);
-        bgemvT(I.B, yv, u, -1, 1);
-        bgemvN(I.B, x, v, 1, 0);
+    __device__ void mulkkt(double* u, double* v, const double* Ablk, const double* x, const double* yv) {
+        long long t0 = tic(); ngemv += 3;
+        amul(Ablk, x, u, 1, 0);
+        spmvT(I.B, yv, u, -1, 1);
+        spmv(I.B, x, v, 1, 0);
+        toc(SEC_GEMV, t0);
     }
 
     __device__ int cg(int stopmode, double* x, double* yv, double* u, double atol, int itmax, int& niter) {
@@ -597,7 +637,7 @@ struct Ctx {
                 status = CG_CONTINUE;
                 while (status == CG_CONTINUE) {
                     niter += 1;
-                    bgemvT(I.B, cgp, cgw, 1, 0);
+                    spmvT(I.B, cgp, cgw, 1, 0);
                     Lsolve(cgw);
                     double ep2 = bdot(cgw, cgw, n, red);
                     if (ep2 <= eps * np2) status = CG_NUMERICAL_FAILURE;
@@ -607,7 +647,7 @@ struct Ctx {
                         for (int i = threadIdx.x; i < m; i += NT) yv[i] = fma(a, cgp[i], yv[i]);
                         for (int i = threadIdx.x; i < n; i += NT) x[i] = fma(a, cgw[i], x[i]);
                         __syncthreads();
-                        bgemvN(I.B, cgw, u, -a, 1);
+                        spmv(I.B, cgw, u, -a, 1);
                         double pnu2 = nu2;
                         nu2 = bdot(u, u, m, red); nu = sqrt(nu2);
                         if (threadIdx.x == 0 && niter <= set.newton_max_iter) I.cghist[niter] = nu;
@@ -650,7 +690,7 @@ struct Ctx {
     }
 
     // stopmode 1 = solveexact!'s fstop/gstop on the scaled residual norms (solver/ipm.jl:278-315)
-    __device__ KKTOut solvekkt(int stopmode, double* x, double* yv, const DevBSM& A, const double* fv,
+    __device__ KKTOut solvekkt(int stopmode, double* x, double* yv, const double* A, const double* fv,
                                const double* gv, bool warm, double ftol, double gtol, int irmin) {
         const double stall = set.refine_stall_tol;
         const int irmax = set.refine_max_iter, cgmax = set.newton_max_iter;
@@ -677,10 +717,10 @@ struct Ctx {
             nir += 1;
             for (int i = threadIdx.x; i < n; i += NT) dx[i] = df[i] * dl;
             __syncthreads();
-            bgemvT(I.B, dg, dx, 1, 1);
+            spmvT(I.B, dg, dx, 1, 1);
             Lsolve(dx);
             Usolve(dx);
-            bgemvN(I.B, dx, dg, -1, 1);
+            spmv(I.B, dx, dg, -1, 1);
             for (int i = threadIdx.x; i < n; i += NT) x[i] += dx[i];
             for (int i = threadIdx.x; i < m; i += NT) yv[i] = fma(alpha, dg[i], yv[i]);
             __syncthreads();
@@ -713,7 +753,7 @@ struct Ctx {
 
     // ---- the iteration  (solver/ipm.jl:86-99, 502-571, 577-774; solver/solver.jl:20-52) ------
     __device__ void residuals() {
-        mulkkt(Df, Dg, I.Q, I.p, I.y);
+        mulkkt(Df, Dg, I.Qd, I.p, I.y);
         for (int i = threadIdx.x; i < n; i += NT) Df[i] = I.d[i] + I.f[i] - Df[i];
         for (int i = threadIdx.x; i < m; i += NT) Dg[i] = I.g[i] - Dg[i];
         __syncthreads();
@@ -734,7 +774,7 @@ struct Ctx {
             double nQp = bnorm(Qp, n, red);
             for (int i = threadIdx.x; i < n; i += NT) wf[i] = Qp[i] - I.d[i];
             __syncthreads();
-            bgemvT(I.B, I.y, wf, -1, 1);
+            spmvT(I.B, I.y, wf, -1, 1);
             double nwf = bnorm(wf, n, red), nd = bnorm(I.d, n, red);
             fl = fmax(nQp, nwf) < rtol * gy * (1 + nd / ny);
         }
@@ -744,7 +784,7 @@ struct Ctx {
         double fp = bdot(I.f, I.p, n, red), np = bnorm(I.p, n, red);
         bool fl = fp > atol * np * (1 + nf);
         if (fl) {
-            bgemvN(I.B, I.p, Dya, 1, 0);
+            spmv(I.B, I.p, Dya, 1, 0);
             double a = bnorm(Dya, m, red), b = bnorm(Qp, n, red);
             fl = fmax(a, b) < rtol * fabs(fp);
         }
@@ -775,7 +815,8 @@ struct Ctx {
     }
     __device__ double getaug() {
         double s = 0;
-        for (int64_t i = threadIdx.x; i < I.Q.xblk[I.Q.narc]; i += NT) s += I.H[i] * I.H[i];
+        for (int64_t i = threadIdx.x; i < I.hdoff[nv]; i += NT) s += I.Hd[i] * I.Hd[i];
+        for (int k = threadIdx.x; k < I.Q.nnz; k += NT) s += I.Q.val[k] * I.Q.val[k];
         double nH = sqrt(block_reduce(s, red, OpSum(), 0.0));
         if (nB == 0 || nH == 0) return 1.0;
         if (nrow_hist == 0) return set.aug_tol * nB * nB / nH;
@@ -797,7 +838,9 @@ struct Ctx {
         double dl = getaug();
         double pd = bdot(I.p, I.d, n, red);
         double spsd = 0;
+        long long t0 = tic();
         bool ok = scale_all(spsd);
+        toc(SEC_SCALE, t0);
         if (!ok) {
             status = NUMERICAL_FAILURE;
         } else {
@@ -806,7 +849,7 @@ struct Ctx {
             double mu = pd / nuf, mus = spsd / nuf, chi = mu * mus - 1;
             double pres = bscalenorm(Dg, I.yscl, m, red) / (1 + sg);
             double dres = bscalenorm(Df, I.pscl, n, red) / (1 + sf);
-            bgemvN(I.Q, I.p, Qp, 1, 0);
+            amul(I.Qd, I.p, Qp, 1, 0);
             double pQp = bdot(I.p, Qp, n, red);
             double pobj = pQp / 2 - bdot(I.f, I.p, n, red);
             double dobj = bdot(I.g, I.y, m, red) - pQp / 2;
@@ -823,7 +866,7 @@ struct Ctx {
                 if (!iok) status = nearstatus(NUMERICAL_FAILURE, mu, mus, pobj, dobj, pres, dres);
                 else {
                     const double eps = 2.220446049250313e-16;
-                    KKTOut o = solvekkt(1, Dpa, Dya, Hb, Df, Dg, false, eps, eps, 0);
+                    KKTOut o = solvekkt(1, Dpa, Dya, I.Hd, Df, Dg, false, eps, eps, 0);
                     row.piter = o.ncg; row.ppass = o.nir; row.pstat = o.status; row.dmin = o.dmin; row.dmax = o.dmax;
                     for (int i = threadIdx.x; i < n; i += NT) I.p[i] += Dpa[i];
                     for (int i = threadIdx.x; i < m; i += NT) I.y[i] += Dya[i];
@@ -833,7 +876,9 @@ struct Ctx {
                 status = nearstatus(NUMERICAL_FAILURE, mu, mus, pobj, dobj, pres, dres);
             } else {
                 double rho;
+                long long t1 = tic();
                 bool iok = initkkt(dl, rho);
+                toc(SEC_INITKKT, t1);
                 row.rho = rho;
                 if (!iok) status = nearstatus(NUMERICAL_FAILURE, mu, mus, pobj, dobj, pres, dres);
                 else {
@@ -843,17 +888,22 @@ struct Ctx {
                     else tol = 0.1 * mu / mu1;
                     double ftol = tol * (1 + nf), gtol = tol * (1 + ng);
                     // predictor  (solver/ipm.jl:119-163)
+                    long long t2 = tic();
                     if (I.mut > 0) initpredictor(wf, I.mut);
                     else { for (int i = threadIdx.x; i < n; i += NT) wf[i] = -I.d[i]; __syncthreads(); }
                     baxpy(1.0, Df, wf, n);
-                    KKTOut po = solvekkt(0, Dpa, Dya, Hb, wf, Dg, false, ftol, gtol, 1);
+                    KKTOut po = solvekkt(0, Dpa, Dya, I.Hd, wf, Dg, false, ftol, gtol, 1);
                     bcopy(Dda, Df, n);
-                    bgemvT(I.B, Dya, Dda, -1, -1);
-                    bgemvN(I.Q, Dpa, Dda, 1, 1);
+                    spmvT(I.B, Dya, Dda, -1, -1);
+                    amul(I.Qd, Dpa, Dda, 1, 1);
                     row.piter = po.ncg; row.ppass = po.nir; row.pstat = po.status; row.dmin = po.dmin; row.dmax = po.dmax;
                     zerofree(Dda);
+                    toc(SEC_PRED, t2);
                     // corrector  (solver/ipm.jl:181-272)
+                    long long t3 = tic();
                     double taua = maxsteps(Dpa, Dda, 1.0);
+                    toc(SEC_MAXSTEPS, t3);
+                    t3 = tic();
                     double sm = 0;
                     for (int j = threadIdx.x; j < n; j += NT) sm += (I.p[j] + taua * Dpa[j]) * (I.d[j] + taua * Dda[j]);
                     sm = block_reduce(sm, red, OpSum(), 0.0);
@@ -872,16 +922,19 @@ struct Ctx {
                     baxpy(1.0, Df, wf, n);
                     bcopy(Dp, Dpa, n);
                     bcopy(Dy, Dya, m);
-                    KKTOut co = solvekkt(0, Dp, Dy, Hb, wf, Dg, true, ftol, gtol, 1);
+                    KKTOut co = solvekkt(0, Dp, Dy, I.Hd, wf, Dg, true, ftol, gtol, 1);
                     bcopy(Dd, Df, n);
-                    bgemvT(I.B, Dy, Dd, -1, -1);
-                    bgemvN(I.Q, Dp, Dd, 1, 1);
+                    spmvT(I.B, Dy, Dd, -1, -1);
+                    amul(I.Qd, Dp, Dd, 1, 1);
                     row.citer = co.ncg; row.cpass = co.nir; row.cstat = co.status;
                     zerofree(Dd);
+                    toc(SEC_CORR, t3);
                     if (po.status != KKT_SOLVED || co.status != KKT_SOLVED) {
                         status = nearstatus(NUMERICAL_FAILURE, mu, mus, pobj, dobj, pres, dres);
                     } else {
+                        long long t4 = tic();
                         double st = maxsteps(Dp, Dd, set.step_frac);
+                        toc(SEC_MAXSTEPS, t4);
                         row.step = st;
                         for (int i = threadIdx.x; i < n; i += NT) { I.p[i] = fma(st, Dp[i], I.p[i]); I.d[i] = fma(st, Dd[i], I.d[i]); }
                         for (int i = threadIdx.x; i < m; i += NT) I.y[i] = fma(st, Dy[i], I.y[i]);
@@ -906,17 +959,18 @@ struct Ctx {
                       status == DUAL_INFEASIBLE || status == NEAR_DUAL_INFEASIBLE;
         if (!(infeas || nrow_hist == 0)) {
             residuals();
-            double pQp = bbdot(I.Q, I.p, I.p, red);
+            amul(I.Qd, I.p, Qp, 1, 0);
+            double pQp = bdot(I.p, Qp, n, red);
             pobj = pQp / 2 - bdot(I.f, I.p, n, red);
             dobj = bdot(I.g, I.y, m, red) - pQp / 2;
             mu = I.nu == 0 ? NaN : bdot(I.p, I.d, n, red) / (double)I.nu;
             pres = bscalenorm(Dg, I.yscl, m, red) / (1 + sg);
             dres = bscalenorm(Df, I.pscl, n, red) / (1 + sf);
         }
+        save();
         if (threadIdx.x == 0) {
             I.scal[0] = mu; I.scal[1] = pres; I.scal[2] = dres; I.scal[3] = pobj; I.scal[4] = dobj;
-            I.scal[5] = nf; I.scal[6] = ng; I.scal[7] = sf; I.scal[8] = sg; I.scal[9] = nB;
-            I.status[0] = status; I.status[1] = nrow_hist; I.status[2] = nretry;
+            I.status[0] = status;
         }
         for (int i = threadIdx.x; i < n; i += NT) { I.po[i] = I.p[i] * I.pscl[i]; I.dout[i] = I.d[i] / I.pscl[i]; }
         for (int i = threadIdx.x; i < m; i += NT) I.yo[i] = I.y[i] * I.yscl[i];
@@ -936,23 +990,30 @@ __device__ void solve_instance(const DevInst& I, const Settings& set, Shared& sh
     Ctx<FT> c(I, set, sh);
     if (mode == MODE_SOLVE || mode == MODE_INIT) {
         // working copies of the inputs: a solve never modifies the uploaded problem
-        for (int64_t i = threadIdx.x; i < I.B.xblk[I.B.narc]; i += NT) I.B.val[i] = I.Bval0[i];
-        for (int64_t i = threadIdx.x; i < I.Q.xblk[I.Q.narc]; i += NT) I.Q.val[i] = I.Qval0[i];
+        for (int i = threadIdx.x; i < I.B.nnz; i += NT) I.B.val[i] = I.B.val0[i];
+        for (int i = threadIdx.x; i < I.Q.nnz; i += NT) I.Q.val[i] = I.Q.val0[i];
+        for (int64_t i = threadIdx.x; i < I.hdoff[I.nvtx]; i += NT) I.Qd[i] = I.Qd0[i];
         for (int i = threadIdx.x; i < n; i += NT) { I.f[i] = I.f0[i]; I.p[i] = I.p0[i]; I.d[i] = I.d0[i]; }
         for (int i = threadIdx.x; i < m; i += NT) { I.g[i] = I.g0[i]; I.y[i] = I.y0[i]; }
         __syncthreads();
         // H = copy(Q) happens after equilibration (IPMSolver constructor order)
+        for (int k = threadIdx.x; k < NSCAL; k += NT) I.scal[k] = 0;
+        for (int k = 0; k < NSEC; ++k) c.tsec[k] = 0;
+        c.ntrsv = 0; c.ngemv = 0;
+        long long t0 = c.tic();
         if (set.scale_max_iter > 0) c.equilibrate(set.scale_max_iter, 1e-3);
         else {
             for (int j = threadIdx.x; j < n; j += NT) I.pscl[j] = 1;
             for (int i = threadIdx.x; i < m; i += NT) I.yscl[i] = 1;
             __syncthreads();
         }
+        c.toc(SEC_EQUIL, t0);
+        t0 = c.tic();
         c.build_finit();
-        int64_t nq = I.Q.xblk[I.Q.narc];
-        for (int64_t i = threadIdx.x; i < nq; i += NT) I.H[i] = I.Q.val[i];
+        c.toc(SEC_FINIT, t0);
+        for (int64_t i = threadIdx.x; i < I.hdoff[I.nvtx]; i += NT) I.Hd[i] = I.Qd[i];   // H = copy(Q)
         double s = 0;
-        for (int64_t i = threadIdx.x; i < I.B.xblk[I.B.narc]; i += NT) s += I.B.val[i] * I.B.val[i];
+        for (int i = threadIdx.x; i < I.B.nnz; i += NT) s += I.B.val[i] * I.B.val[i];
         c.nB = sqrt(block_reduce(s, c.red, OpSum(), 0.0));
         c.nf = bnorm(I.f, n, c.red);
         c.ng = bnorm(I.g, m, c.red);
@@ -967,7 +1028,7 @@ __device__ void solve_instance(const DevInst& I, const Settings& set, Shared& sh
             const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
             if (!(I.has_p0 && I.has_d0)) {
                 for (int v = warp; v < I.nvtx; v += NW) {   // dualshadow! / primalshadow!
-                    int k = I.kind[v], c0 = I.B.xcol[v], nc = I.B.xcol[v + 1] - c0;
+                    int k = I.kind[v], c0 = I.xcol[v], nc = I.xcol[v + 1] - c0;
                     double* dst = !I.has_d0 ? I.d + c0 : I.p + c0;
                     const double* src = !I.has_d0 ? I.p + c0 : I.d + c0;
                     if (k == CONE_POS) { for (int i = lane; i < nc; i += 32) dst[i] = 1.0 / src[i]; }

@@ -35,7 +35,8 @@ class mb_csc(C.Structure):
 
 class mb_result(C.Structure):
     _fields_ = [("status", I32), ("niter", I32), ("nsolve", I32), ("nfactor_retry", I32),
-                ("mu", F64), ("pres", F64), ("dres", F64), ("pobj", F64), ("dobj", F64)]
+                ("nfactor", I32), ("reserved", I32),
+                ("mu", F64), ("pres", F64), ("dres", F64), ("pobj", F64), ("dobj", F64), ("factor_flops", F64)]
 
 
 ROW_FIELDS = ["pres", "dres", "pobj", "dobj", "step", "piter", "ppass", "pstat", "citer", "cpass",
@@ -76,6 +77,7 @@ SIGNATURES = {
     "mb_batch_run": (I32, [C.c_void_p, I32, C.POINTER(F32)]),
     "mb_batch_fetch": (I32, [C.c_void_p, C.POINTER(PF64), C.POINTER(PF64), C.POINTER(PF64), C.POINTER(mb_result)]),
     "mb_batch_stats": (I32, [C.c_void_p, PI64]),
+    "mb_batch_timers": (I32, [C.c_void_p, PF64, I64]),
     "mb_batch_destroy": (I32, [C.c_void_p]),
 }
 

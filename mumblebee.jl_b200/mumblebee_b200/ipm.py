@@ -331,6 +331,8 @@ class IPMResult:
     pobj: float
     dobj: float
     nfactor_retry: int = 0
+    nfactor: int = 0
+    factor_flops: float = 0.0
 
 
 class IPMSolver:
@@ -374,7 +376,7 @@ class IPMSolver:
         check(self.L.mb_solver_result(self.h, _p(p, C.c_double), _p(d, C.c_double), _p(y, C.c_double), C.byref(r)),
               self.prob.ctx.h, "result")
         return IPMResult(p, d, y, IPMStatus(r.status), r.niter, r.nsolve, self.history(), r.mu, r.pres, r.dres,
-                         r.pobj, r.dobj, r.nfactor_retry)
+                         r.pobj, r.dobj, r.nfactor_retry, r.nfactor, r.factor_flops)
 
     def __del__(self):
         if getattr(self, "h", None):
@@ -438,8 +440,18 @@ class Batch:
         for i in range(k):
             r = res[i]
             out.append(IPMResult(ps[i], ds[i], ys[i], IPMStatus(r.status), r.niter, r.nsolve, IPMHistory(), r.mu,
-                                 r.pres, r.dres, r.pobj, r.dobj, r.nfactor_retry))
+                                 r.pres, r.dres, r.pobj, r.dobj, r.nfactor_retry, r.nfactor, r.factor_flops))
         return out
+
+    SECTIONS = ["equilibrate", "BtB", "scale", "initkkt", "predictor", "corrector", "maxsteps", "trsv", "gemv",
+                "ntrsv", "ngemv"]
+
+    def timers(self):
+        """Per-instance section clocks (after fetch): array (ninst, 11), columns SECTIONS."""
+        W = len(self.SECTIONS)
+        a = np.zeros(len(self.probs) * W)
+        check(self.L.mb_batch_timers(self.h, _p(a, C.c_double), a.size), self.ctx.h, "timers")
+        return a.reshape(len(self.probs), W)
 
     def stats(self):
         a = np.zeros(8, np.int64)

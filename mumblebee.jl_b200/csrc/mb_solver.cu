@@ -21,17 +21,128 @@
 namespace mb {
 
 constexpr int TS = 64;   // trailing-update tile
+constexpr int TLD = 36;  // tile row stride (doubles): 8-byte fragment loads of 8 rows x 4 columns hit 32 distinct banks
 
 struct Shared {
     double red[NW + 2];
     double diag[32 * 33];
     double xs[32];
     double acc[32];
-    double ta[TS * 33];
-    double tb[TS * 33];
+    double ta[TS * TLD];
+    double tb[TS * TLD];
     int flag;
     int ibuf[8];
 };
+
+// D += A·B on the FP64 tensor path (mma.m8n8k4, fragments: A[g][t], B[t][g], C[g][2t+i] with
+// g = lane/4, t = lane%4)
+__device__ __forceinline__ void dmma(double& c0, double& c1, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+                 : "+d"(c0), "+d"(c1) : "d"(a), "d"(b));
+}
+
+// Trailing update M[j0:, j0:] -= L21 L21ᵀ (lower part) for the panel columns [k0, k0+kb), kb <= 32.
+// Row blocks of 64 are staged once per sweep; each of the 16 warps owns a 16x16 piece of the
+// 64x64 output tile.  FP64: tensor-path DMMA.  FP32: FFMA register tiles.
+template <class FT>
+__device__ void syrk_update(FT* M, int nf, int k0, int kb, int j0, Shared& sh);
+
+template <>
+__device__ void syrk_update<double>(double* M, int nf, int k0, int kb, int j0, Shared& sh) {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int g = lane >> 2, t = lane & 3;
+    const int wr = warp >> 2, wc = warp & 3;
+    const int nrem = nf - j0, nt = (nrem + TS - 1) / TS;
+    const int kb4 = (kb + 3) & ~3;
+    double* ta = sh.ta;
+    double* tb = sh.tb;
+    for (int ti = 0; ti < nt; ++ti) {
+        const int rb = j0 + ti * TS;
+        for (int idx = tid; idx < TS * 32; idx += NT) {
+            int r = idx % TS, c = idx / TS;
+            ta[r * TLD + c] = (c < kb && rb + r < nf) ? M[(rb + r) + (int64_t)(k0 + c) * nf] : 0.0;
+        }
+        for (int tj = 0; tj <= ti; ++tj) {
+            const int cb = j0 + tj * TS;
+            for (int idx = tid; idx < TS * 32; idx += NT) {
+                int r = idx % TS, c = idx / TS;
+                tb[r * TLD + c] = (c < kb && cb + r < nf) ? M[(cb + r) + (int64_t)(k0 + c) * nf] : 0.0;
+            }
+            __syncthreads();
+            const bool skip = (ti == tj) && (wr < wc);   // strictly upper warp tiles of a diagonal tile
+            if (!skip) {
+                double acc[2][2][2];
+#pragma unroll
+                for (int a = 0; a < 2; ++a)
+#pragma unroll
+                    for (int b = 0; b < 2; ++b) { acc[a][b][0] = 0; acc[a][b][1] = 0; }
+                for (int k = 0; k < kb4; k += 4) {
+                    double a0 = ta[(wr * 16 + g) * TLD + k + t], a1 = ta[(wr * 16 + 8 + g) * TLD + k + t];
+                    double b0 = tb[(wc * 16 + g) * TLD + k + t], b1 = tb[(wc * 16 + 8 + g) * TLD + k + t];
+                    dmma(acc[0][0][0], acc[0][0][1], a0, b0);
+                    dmma(acc[0][1][0], acc[0][1][1], a0, b1);
+                    dmma(acc[1][0][0], acc[1][0][1], a1, b0);
+                    dmma(acc[1][1][0], acc[1][1][1], a1, b1);
+                }
+#pragma unroll
+                for (int a = 0; a < 2; ++a)
+#pragma unroll
+                    for (int b = 0; b < 2; ++b)
+#pragma unroll
+                        for (int q = 0; q < 2; ++q) {
+                            int row = rb + wr * 16 + a * 8 + g;
+                            int col = cb + wc * 16 + b * 8 + 2 * t + q;
+                            if (row < nf && col < nf && row >= col) M[row + (int64_t)col * nf] -= acc[a][b][q];
+                        }
+            }
+            __syncthreads();
+        }
+    }
+}
+
+template <>
+__device__ void syrk_update<float>(float* M, int nf, int k0, int kb, int j0, Shared& sh) {
+    const int tid = threadIdx.x;
+    const int nrem = nf - j0, nt = (nrem + TS - 1) / TS;
+    float* ta = reinterpret_cast<float*>(sh.ta);
+    float* tb = reinterpret_cast<float*>(sh.tb);
+    const int tr = tid & 15, tc = tid >> 4;   // rows tr + 16a, columns tc*2 + b
+    for (int ti = 0; ti < nt; ++ti) {
+        const int rb = j0 + ti * TS;
+        for (int idx = tid; idx < TS * 32; idx += NT) {
+            int r = idx % TS, c = idx / TS;
+            ta[c * (TS + 1) + r] = (c < kb && rb + r < nf) ? M[(rb + r) + (int64_t)(k0 + c) * nf] : 0.0f;
+        }
+        for (int tj = 0; tj <= ti; ++tj) {
+            const int cb = j0 + tj * TS;
+            for (int idx = tid; idx < TS * 32; idx += NT) {
+                int r = idx % TS, c = idx / TS;
+                tb[c * (TS + 1) + r] = (c < kb && cb + r < nf) ? M[(cb + r) + (int64_t)(k0 + c) * nf] : 0.0f;
+            }
+            __syncthreads();
+            float acc[4][2];
+#pragma unroll
+            for (int a = 0; a < 4; ++a) { acc[a][0] = 0; acc[a][1] = 0; }
+            for (int c = 0; c < kb; ++c) {
+                float bv0 = tb[c * (TS + 1) + tc * 2], bv1 = tb[c * (TS + 1) + tc * 2 + 1];
+#pragma unroll
+                for (int a = 0; a < 4; ++a) {
+                    float av = ta[c * (TS + 1) + tr + 16 * a];
+                    acc[a][0] = fmaf(av, bv0, acc[a][0]);
+                    acc[a][1] = fmaf(av, bv1, acc[a][1]);
+                }
+            }
+#pragma unroll
+            for (int a = 0; a < 4; ++a)
+#pragma unroll
+                for (int b = 0; b < 2; ++b) {
+                    int row = rb + tr + 16 * a, col = cb + tc * 2 + b;
+                    if (row < nf && col < nf && row >= col) M[row + (int64_t)col * nf] -= acc[a][b];
+                }
+            __syncthreads();
+        }
+    }
+}
 
 // ---------------------------------------------------------------------------------------------
 // dense kernels on one front (column-major, leading dimension nf)
@@ -96,47 +207,8 @@ __device__ int front_chol(FT* M, int nf, int nres, Shared& sh) {
             for (int c = 0; c < 32; ++c) if (c < kb) M[i + (int64_t)(k0 + c) * nf] = x[c];
         }
         __syncthreads();
-        // trailing update: M[j0:, j0:] -= L21 L21ᵀ (lower), 64x64 tiles
-        const int nrem = nf - j0;
-        if (nrem <= 0) continue;
-        const int nt = (nrem + TS - 1) / TS;
-        const int tr = tid & 15, tc = tid >> 4;   // 16 x 32 thread grid, 4x2 outputs each
-        for (int tj = 0; tj < nt; ++tj) {
-            for (int ti = tj; ti < nt; ++ti) {
-                const int rb = j0 + ti * TS, cb = j0 + tj * TS;
-                for (int idx = tid; idx < TS * 32; idx += NT) {
-                    int r = idx % TS, c = idx / TS;
-                    FT a = 0, b = 0;
-                    if (c < kb) {
-                        if (rb + r < nf) a = M[(rb + r) + (int64_t)(k0 + c) * nf];
-                        if (cb + r < nf) b = M[(cb + r) + (int64_t)(k0 + c) * nf];
-                    }
-                    ta[r * 33 + c] = a;
-                    tb[r * 33 + c] = b;
-                }
-                __syncthreads();
-                FT acc[4][2];
-#pragma unroll
-                for (int a = 0; a < 4; ++a) { acc[a][0] = 0; acc[a][1] = 0; }
-                for (int c = 0; c < kb; ++c) {
-                    FT bv0 = tb[(tc * 2 + 0) * 33 + c], bv1 = tb[(tc * 2 + 1) * 33 + c];
-#pragma unroll
-                    for (int a = 0; a < 4; ++a) {
-                        FT av = ta[(tr * 4 + a) * 33 + c];
-                        acc[a][0] += av * bv0;
-                        acc[a][1] += av * bv1;
-                    }
-                }
-#pragma unroll
-                for (int a = 0; a < 4; ++a)
-#pragma unroll
-                    for (int b = 0; b < 2; ++b) {
-                        int row = rb + tr * 4 + a, col = cb + tc * 2 + b;
-                        if (row < nf && col < nf && row >= col) M[row + (int64_t)col * nf] -= acc[a][b];
-                    }
-                __syncthreads();
-            }
-        }
+        // trailing update: M[j0:, j0:] -= L21 L21ᵀ (lower)
+        if (nf - j0 > 0) syrk_update<FT>(M, nf, k0, kb, j0, sh);
     }
     return 0;
 }
@@ -145,15 +217,20 @@ __device__ int front_chol(FT* M, int nf, int nres, Shared& sh) {
 template <class FT>
 __device__ void front_lsolve(const FT* M, int nf, int nres, int r0, const int* sep, double* x, Shared& sh) {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    double* T = sh.diag;   // the 32x32 diagonal triangle, T[c*33 + r] = L[k0+r, k0+c]
     for (int k0 = 0; k0 < nres; k0 += 32) {
         const int kb = min(32, nres - k0);
+        for (int idx = tid; idx < 32 * 32; idx += NT) {
+            int r = idx & 31, c = idx >> 5;
+            if (r < kb && c < kb && r >= c) T[c * 33 + r] = (double)M[(k0 + r) + (int64_t)(k0 + c) * nf];
+        }
+        __syncthreads();
         if (warp == 0) {
             double xv = lane < kb ? x[r0 + k0 + lane] : 0.0;
             for (int c = 0; c < kb; ++c) {
-                double xc = 0;
-                if (lane == c) { xv = xv / (double)M[(k0 + c) + (int64_t)(k0 + c) * nf]; }
-                xc = __shfl_sync(0xffffffffu, xv, c);
-                if (lane > c && lane < kb) xv -= (double)M[(k0 + lane) + (int64_t)(k0 + c) * nf] * xc;
+                if (lane == c) xv = xv / T[c * 33 + c];
+                double xc = __shfl_sync(0xffffffffu, xv, c);
+                if (lane > c && lane < kb) xv -= T[c * 33 + lane] * xc;
             }
             if (lane < kb) { x[r0 + k0 + lane] = xv; sh.xs[lane] = xv; }
         }
@@ -173,8 +250,13 @@ template <class FT>
 __device__ void front_usolve(const FT* M, int nf, int nres, int r0, const int* sep, double* x, Shared& sh) {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int nblk = (nres + 31) / 32;
+    double* T = sh.diag;   // T[c*33 + r] = L[k0+r, k0+c]
     for (int bk = nblk - 1; bk >= 0; --bk) {
         const int k0 = bk * 32, kb = min(32, nres - k0);
+        for (int idx = tid; idx < 32 * 32; idx += NT) {
+            int r = idx & 31, c = idx >> 5;
+            if (r < kb && c < kb && r >= c) T[c * 33 + r] = (double)M[(k0 + r) + (int64_t)(k0 + c) * nf];
+        }
         for (int c = warp; c < kb; c += NW) {
             double t = 0;
             for (int i = k0 + kb + lane; i < nf; i += 32) {
@@ -188,9 +270,9 @@ __device__ void front_usolve(const FT* M, int nf, int nres, int r0, const int* s
         if (warp == 0) {
             double yv = lane < kb ? x[r0 + k0 + lane] - sh.acc[lane] : 0.0;
             for (int c = kb - 1; c >= 0; --c) {
-                if (lane == c) yv = yv / (double)M[(k0 + c) + (int64_t)(k0 + c) * nf];
+                if (lane == c) yv = yv / T[c * 33 + c];
                 double xc = __shfl_sync(0xffffffffu, yv, c);
-                if (lane < c) yv -= (double)M[(k0 + c) + (int64_t)(k0 + lane) * nf] * xc;
+                if (lane < c) yv -= T[lane * 33 + c] * xc;
             }
             if (lane < kb) x[r0 + k0 + lane] = yv;
         }

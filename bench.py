@@ -43,7 +43,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--count", type=int, default=4096, help="instances per step per GPU")
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32", "mixed"])
     ap.add_argument("--seed", type=int, default=0)
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="bounded CPU-baseline sample length")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -264,7 +264,7 @@ def main():
     # roofline of the solver kernel: algorithmic factorization flops per launch / launch time
     flops = float(sum(r.nfactor * r.factor_flops for r in res))
     peaks = measure_peaks()
-    peak_key = "tf32" if args.precision == "fp32" else "fp64"
+    peak_key = "tf32" if args.precision in ("fp32", "mixed") else "fp64"
     achieved = flops / (ms / 1e3) / 1e12
     roofline = {"bound": "tensor", "achieved": achieved, "peak": peaks[peak_key], "unit": "TFLOP/s",
                 "frac": achieved / peaks[peak_key], "traffic": None,

@@ -54,6 +54,8 @@ enum mb_status {
 /* factor precision */
 #define MB_PREC_FP64 0     /* FP64 factor */
 #define MB_PREC_FP32 1     /* FP32 factor, FP64 refinement, residuals and termination tests */
+#define MB_PREC_MIXED 2    /* FP32 factor until a KKT solve misses its tolerance; that iteration is
+                              redone with the FP64 factor, which is kept for the rest of the solve */
 
 /* IPMSettings (settings/ipm.jl:2-17) + precision.  Integer fields first, then doubles. */
 typedef struct mb_settings {
@@ -102,6 +104,8 @@ typedef struct mb_result {
     int32_t nsolve;
     int32_t nfactor_retry;   /* ρ-regularized refactorizations (uzawa.jl:97-112) */
     int32_t nfactor;         /* numeric factorizations performed (including retries) */
+    int32_t nfp32;           /* iterations accepted with the FP32 factor (MB_PREC_MIXED / _FP32) */
+    int32_t nfallback;       /* iterations redone with the FP64 factor (MB_PREC_MIXED) */
     int32_t reserved;
     double mu, pres, dres, pobj, dobj;
     double factor_flops;     /* algorithmic flops of one factorization: Σ_fronts r³/3 + r²s + rs² */

@@ -9,7 +9,7 @@
 
 namespace mb {
 
-constexpr int NT = 512;          // threads per CTA
+constexpr int NT = CTA_THREADS;  // threads per CTA
 constexpr int NW = NT / 32;      // warps per CTA
 
 struct Shared;                   // defined in mb_solver.cu

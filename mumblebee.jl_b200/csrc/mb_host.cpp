@@ -125,7 +125,7 @@ struct InstPlan {
     // double in
     size_t Bval, Qval, Qd, f, g, kpar, p, d, y;
     // work
-    size_t wBval, wQval, wQd, Hd, Finit, pscl, yscl, vn, vm, vv, work, uhist, cghist, cache, wf, wg, wp, wd, wy;
+    size_t wBval, wQval, wQd, Hd, Finit, pscl, yscl, vn, vm, vv, work, uhist, cghist, cache, cache2, wf, wg, wp, wd, wy;
     // factor (bytes)
     size_t F;
     // out
@@ -306,12 +306,12 @@ static int plan_instance(const mb_problem* P, const mb_settings& set, const doub
     ip.wBval = pk.work.take(Bval.size()); ip.wQval = pk.work.take(Qval.size()); ip.wQd = pk.work.take(Qd.size());
     ip.Hd = pk.work.take(Qd.size()); ip.Finit = pk.work.take(fr.fsize);
     ip.pscl = pk.work.take(n); ip.yscl = pk.work.take(m);
-    ip.vn = pk.work.take((size_t)mb::NVEC_N * n); ip.vm = pk.work.take((size_t)mb::NVEC_M * m);
-    ip.vv = pk.work.take((size_t)mb::NVEC_V * nv); ip.work = pk.work.take((size_t)(512 / 32) * wmax);
+    ip.vn = pk.work.take((size_t)(mb::NVEC_N + 2) * n); ip.vm = pk.work.take((size_t)(mb::NVEC_M + 1) * m);
+    ip.vv = pk.work.take((size_t)mb::NVEC_V * nv); ip.work = pk.work.take((size_t)(mb::CTA_THREADS / 32) * wmax);
     ip.uhist = pk.work.take(set.refine_max_iter + 2); ip.cghist = pk.work.take(set.newton_max_iter + 1);
-    ip.cache = pk.work.take(std::max<i64>(cx[nv], 1));
+    ip.cache = pk.work.take(std::max<i64>(cx[nv], 1)); ip.cache2 = pk.work.take(std::max<i64>(cx[nv], 1));
     ip.wf = pk.work.take(n); ip.wg = pk.work.take(m); ip.wp = pk.work.take(n); ip.wd = pk.work.take(n); ip.wy = pk.work.take(m);
-    size_t esz = set.precision == MB_PREC_FP32 ? 4 : 8;
+    size_t esz = set.precision == MB_PREC_FP32 ? 4 : 8;   // mixed needs room for the FP64 factor
     ip.F = (pk.fbytes + 255) / 256 * 256;
     pk.fbytes = ip.F + fr.fsize * esz;
     ip.po = pk.out.take(n); ip.dout = pk.out.take(n); ip.yo = pk.out.take(m);
@@ -338,7 +338,7 @@ static void merge(Packed& dst, Packed& src) {
     for (size_t* f : {&ip.hdoff, &ip.hdpos, &ip.qoffpos, &ip.cxblk, &ip.fptr}) *f += b64;
     for (size_t* f : {&ip.Bval, &ip.Qval, &ip.Qd, &ip.f, &ip.g, &ip.kpar, &ip.p, &ip.d, &ip.y}) *f += bin;
     for (size_t* f : {&ip.wBval, &ip.wQval, &ip.wQd, &ip.Hd, &ip.Finit, &ip.pscl, &ip.yscl, &ip.vn, &ip.vm, &ip.vv,
-                      &ip.work, &ip.uhist, &ip.cghist, &ip.cache, &ip.wf, &ip.wg, &ip.wp, &ip.wd, &ip.wy}) *f += bw;
+                      &ip.work, &ip.uhist, &ip.cghist, &ip.cache, &ip.cache2, &ip.wf, &ip.wg, &ip.wp, &ip.wd, &ip.wy}) *f += bw;
     for (size_t* f : {&ip.po, &ip.dout, &ip.yo, &ip.scal, &ip.hist}) *f += bo;
     ip.status += bs;
     size_t fb = (dst.fbytes + 255) / 256 * 256;
@@ -417,6 +417,7 @@ static int upload(mb_batch* b) {
         I.hdpos = (const int64_t*)(q64 + p.hdpos); I.hdld = i32 + p.hdld;
         I.nqoff = (int)p.nqoff; I.qoffk = i32 + p.qoffk; I.qoffpos = (const int64_t*)(q64 + p.qoffpos);
         I.kind = i32 + p.kind; I.kpar = dn + p.kpar; I.cxblk = (const int64_t*)(q64 + p.cxblk); I.cache = wk + p.cache;
+        I.cache2 = wk + p.cache2;
         I.wsize = p.wsize;
         I.fres0 = i32 + p.fres0; I.fnres = i32 + p.fnres; I.fnsep = i32 + p.fnsep; I.fparent = i32 + p.fparent;
         I.fptr = (const int64_t*)(q64 + p.fptr); I.fsepp = i32 + p.fsepp; I.fsep = i32 + p.fsep; I.frel = i32 + p.frel;
@@ -445,6 +446,7 @@ static int make_batch(mb_ctx* ctx, mb_problem* const* probs, int32_t nprob, cons
     if (set) s = *set; else mb_settings_default(&s);
     if (s.stable) return fail(ctx, MB_E_UNSUPPORTED, "stable=true (StableUzawaSolver) is not available");
     if (s.max_iter < 0 || s.refine_max_iter < 0 || s.newton_max_iter < 0) return fail(ctx, MB_E_ARG, "negative iteration limit");
+    if (s.precision < 0 || s.precision > 2) return fail(ctx, MB_E_ARG, "precision must be 0 (FP64), 1 (FP32) or 2 (mixed)");
     auto b = std::make_unique<mb_batch>();
     b->ctx = ctx; b->set = s;
     CUDA_TRY(ctx, cudaSetDevice(ctx->device));
@@ -481,7 +483,7 @@ static int run_batch(mb_batch* b, int mode, int32_t grid, float* ms) {
     mb_ctx* ctx = b->ctx;
     int ninst = (int)b->pk.plans.size();
     if (ninst == 0) { if (ms) *ms = 0; return MB_OK; }
-    int g = grid > 0 ? grid : ctx->nsm;
+    int g = grid > 0 ? grid : ctx->nsm * mb::CTA_PER_SM;
     g = std::min(g, ninst);
     mb::Settings s;
     static_assert(sizeof(mb::Settings) == sizeof(mb_settings), "settings layout");
@@ -513,7 +515,8 @@ static void unpack_one(const mb_batch* b, size_t k, double* p, double* d, double
     if (y) for (i64 i = 0; i < ip.m; ++i) y[ip.rowmap[i]] = o[ip.yo + i];
     if (r) {
         const int32_t* st = b->h_i32 + ip.status;
-        r->status = st[0]; r->niter = st[1]; r->nfactor_retry = st[2]; r->nfactor = st[3]; r->reserved = 0;
+        r->status = st[0]; r->niter = st[1]; r->nfactor_retry = st[2]; r->nfactor = st[3];
+        r->nfp32 = st[4]; r->nfallback = st[5];
         r->factor_flops = ip.fflops;
         const double* sc = o + ip.scal;
         r->mu = sc[0]; r->pres = sc[1]; r->dres = sc[2]; r->pobj = sc[3]; r->dobj = sc[4];

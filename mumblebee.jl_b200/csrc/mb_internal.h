@@ -6,6 +6,11 @@
 
 namespace mb {
 
+// launch shape of the batched solver: CTA_THREADS threads per instance, CTA_PER_SM instances
+// resident per SM (the kernel is latency-bound; a second resident instance hides latency)
+constexpr int CTA_THREADS = 256;
+constexpr int CTA_PER_SM = 2;
+
 enum ConeKind { CONE_FREE = 0, CONE_POS = 1, CONE_SOC = 2, CONE_SDP = 3, CONE_EXP = 4, CONE_POW = 5 };
 
 // IPMStatus (src/IPM/src/ipm/ipm.jl:1), KKTStatus (kkt/kkt.jl:1), CGStatus (kkt/cg.jl:1-6)
@@ -64,6 +69,7 @@ struct DevInst {
     const double* kpar;     // cone parameter per vertex
     const int64_t* cxblk;   // cache offsets per vertex (nvtx+1)
     double* cache;
+    double* cache2;         // saved cache (mixed-precision redo)
     int wsize;              // per-cone workspace length (max over cones)
     // fronts (multifrontal): front f owns scalar columns [fres0[f], fres0[f]+fnres[f]) and the
     // separator rows fsep[fsepp[f] .. fsepp[f+1]); its (nres+nsep)^2 column-major storage starts at
@@ -86,20 +92,23 @@ struct DevInst {
     double* hist;           // max_iter+1 rows (ROW_DOUBLES each)
     double* uhist;          // refine_max_iter + 2
     double* cghist;         // newton_max_iter + 1
-    int* status;            // [0] IPM status, [1] rows written, [2] factor retries, [3] factorizations
+    int* status;            // [0] IPM status, [1] rows written, [2] factor retries, [3] factorizations,
+                            // [4] FP32 iterations, [5] FP64 redos (mixed precision)
     double* scal;           // NSCAL: mu pres dres pobj dobj nf ng sf sg nB, timers, counters
 };
 
 constexpr int NVEC_N = 12;  // Df Qp wf Dpa Dda Dp Dd df dx cgw  tmp1 tmp2 (tmp2 also: column maxima)
 constexpr int NVEC_M = 8;   // Dg Dya Dy dg dy cgp tmp1 tmp2
+// two more n-vectors and one m-vector follow the above (saved p, d, y of a mixed-precision redo)
 constexpr int NVEC_V = 6;   // step spsd flag vscl vnrm vswp
 constexpr int NSCAL = 32;   // mu pres dres pobj dobj | nf ng sf sg nB | section clocks (NSEC) | counters
 // section timers (SM clock cycles), the TimerOutputs sections of the reference plus set-up
-enum Section { SEC_EQUIL = 0, SEC_FINIT, SEC_SCALE, SEC_INITKKT, SEC_PRED, SEC_CORR, SEC_MAXSTEPS, SEC_TRSV, SEC_GEMV, NSEC };
+enum Section { SEC_EQUIL = 0, SEC_FINIT, SEC_SCALE, SEC_INITKKT, SEC_PRED, SEC_CORR, SEC_MAXSTEPS, SEC_TRSV, SEC_GEMV,
+               SEC_ASSEMBLE, SEC_RESID, SEC_AUG, NSEC };
 constexpr int SCAL_SEC = 10;        // scal[10 .. 10+NSEC)
-constexpr int SCAL_NTRSV = 20;      // triangular solve sweeps
-constexpr int SCAL_NGEMV = 21;      // block-sparse matvecs
-constexpr int NSTAT = 4;    // status, history rows, factor retries, error
+constexpr int SCAL_NTRSV = 22;      // triangular solve sweeps
+constexpr int SCAL_NGEMV = 23;      // block-sparse matvecs
+constexpr int NSTAT = 8;    // status, history rows, factor retries, factorizations, FP32 iterations, FP64 redos
 
 // kernel modes: a full solve, or the pieces used by the step-wise API
 enum Mode { MODE_SOLVE = 0, MODE_INIT = 1, MODE_STEP = 2, MODE_RESULT = 3 };

@@ -49,6 +49,8 @@ __device__ void syrk_update(FT* M, int nf, int k0, int kb, int j0, Shared& sh);
 
 template <>
 __device__ void syrk_update<double>(double* M, int nf, int k0, int kb, int j0, Shared& sh) {
+    // warps tile the 64x64 output as (NW/4) x 4; each warp owns RW x 16 (RW/8 x 2 DMMA tiles)
+    constexpr int WRN = NW / 4, RW = TS / WRN, MR = RW / 8;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int g = lane >> 2, t = lane & 3;
     const int wr = warp >> 2, wc = warp & 3;
@@ -69,28 +71,29 @@ __device__ void syrk_update<double>(double* M, int nf, int k0, int kb, int j0, S
                 tb[r * TLD + c] = (c < kb && cb + r < nf) ? M[(cb + r) + (int64_t)(k0 + c) * nf] : 0.0;
             }
             __syncthreads();
-            const bool skip = (ti == tj) && (wr < wc);   // strictly upper warp tiles of a diagonal tile
+            const bool skip = (ti == tj) && (wr * RW + RW - 1 < wc * 16);   // strictly upper warp tile
             if (!skip) {
-                double acc[2][2][2];
+                double acc[MR][2][2];
 #pragma unroll
-                for (int a = 0; a < 2; ++a)
+                for (int a = 0; a < MR; ++a)
 #pragma unroll
                     for (int b = 0; b < 2; ++b) { acc[a][b][0] = 0; acc[a][b][1] = 0; }
                 for (int k = 0; k < kb4; k += 4) {
-                    double a0 = ta[(wr * 16 + g) * TLD + k + t], a1 = ta[(wr * 16 + 8 + g) * TLD + k + t];
                     double b0 = tb[(wc * 16 + g) * TLD + k + t], b1 = tb[(wc * 16 + 8 + g) * TLD + k + t];
-                    dmma(acc[0][0][0], acc[0][0][1], a0, b0);
-                    dmma(acc[0][1][0], acc[0][1][1], a0, b1);
-                    dmma(acc[1][0][0], acc[1][0][1], a1, b0);
-                    dmma(acc[1][1][0], acc[1][1][1], a1, b1);
+#pragma unroll
+                    for (int a = 0; a < MR; ++a) {
+                        double av = ta[(wr * RW + a * 8 + g) * TLD + k + t];
+                        dmma(acc[a][0][0], acc[a][0][1], av, b0);
+                        dmma(acc[a][1][0], acc[a][1][1], av, b1);
+                    }
                 }
 #pragma unroll
-                for (int a = 0; a < 2; ++a)
+                for (int a = 0; a < MR; ++a)
 #pragma unroll
                     for (int b = 0; b < 2; ++b)
 #pragma unroll
                         for (int q = 0; q < 2; ++q) {
-                            int row = rb + wr * 16 + a * 8 + g;
+                            int row = rb + wr * RW + a * 8 + g;
                             int col = cb + wc * 16 + b * 8 + 2 * t + q;
                             if (row < nf && col < nf && row >= col) M[row + (int64_t)col * nf] -= acc[a][b][q];
                         }
@@ -102,11 +105,13 @@ __device__ void syrk_update<double>(double* M, int nf, int k0, int kb, int j0, S
 
 template <>
 __device__ void syrk_update<float>(float* M, int nf, int k0, int kb, int j0, Shared& sh) {
+    // each thread owns rows tr + 16a (a < 4) and columns tc*CW + b of the 64x64 tile
+    constexpr int CW = TS / (NT / 16);
     const int tid = threadIdx.x;
     const int nrem = nf - j0, nt = (nrem + TS - 1) / TS;
     float* ta = reinterpret_cast<float*>(sh.ta);
     float* tb = reinterpret_cast<float*>(sh.tb);
-    const int tr = tid & 15, tc = tid >> 4;   // rows tr + 16a, columns tc*2 + b
+    const int tr = tid & 15, tc = tid >> 4;
     for (int ti = 0; ti < nt; ++ti) {
         const int rb = j0 + ti * TS;
         for (int idx = tid; idx < TS * 32; idx += NT) {
@@ -120,23 +125,27 @@ __device__ void syrk_update<float>(float* M, int nf, int k0, int kb, int j0, Sha
                 tb[c * (TS + 1) + r] = (c < kb && cb + r < nf) ? M[(cb + r) + (int64_t)(k0 + c) * nf] : 0.0f;
             }
             __syncthreads();
-            float acc[4][2];
+            float acc[4][CW];
 #pragma unroll
-            for (int a = 0; a < 4; ++a) { acc[a][0] = 0; acc[a][1] = 0; }
+            for (int a = 0; a < 4; ++a)
+#pragma unroll
+                for (int b = 0; b < CW; ++b) acc[a][b] = 0;
             for (int c = 0; c < kb; ++c) {
-                float bv0 = tb[c * (TS + 1) + tc * 2], bv1 = tb[c * (TS + 1) + tc * 2 + 1];
+                float bv[CW];
+#pragma unroll
+                for (int b = 0; b < CW; ++b) bv[b] = tb[c * (TS + 1) + tc * CW + b];
 #pragma unroll
                 for (int a = 0; a < 4; ++a) {
                     float av = ta[c * (TS + 1) + tr + 16 * a];
-                    acc[a][0] = fmaf(av, bv0, acc[a][0]);
-                    acc[a][1] = fmaf(av, bv1, acc[a][1]);
+#pragma unroll
+                    for (int b = 0; b < CW; ++b) acc[a][b] = fmaf(av, bv[b], acc[a][b]);
                 }
             }
 #pragma unroll
             for (int a = 0; a < 4; ++a)
 #pragma unroll
-                for (int b = 0; b < 2; ++b) {
-                    int row = rb + tr + 16 * a, col = cb + tc * 2 + b;
+                for (int b = 0; b < CW; ++b) {
+                    int row = rb + tr + 16 * a, col = cb + tc * CW + b;
                     if (row < nf && col < nf && row >= col) M[row + (int64_t)col * nf] -= acc[a][b];
                 }
             __syncthreads();
@@ -144,13 +153,6 @@ __device__ void syrk_update<float>(float* M, int nf, int k0, int kb, int j0, Sha
     }
 }
 
-// ---------------------------------------------------------------------------------------------
-// dense kernels on one front (column-major, leading dimension nf)
-// ---------------------------------------------------------------------------------------------
-
-// Partial Cholesky of a front: factor the leading nres columns of the (nf x nf) lower matrix and
-// update the trailing (nf-nres) block to the Schur complement.  Returns 0 or the 1-based local
-// column whose pivot was not positive (cholesky!(…; check=false) info).
 template <class FT>
 __device__ int front_chol(FT* M, int nf, int nres, Shared& sh) {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -283,13 +285,17 @@ __device__ void front_usolve(const FT* M, int nf, int nres, int r0, const int* s
 // ---------------------------------------------------------------------------------------------
 // the per-instance solver
 // ---------------------------------------------------------------------------------------------
-template <class FT>
 struct Ctx {
     const DevInst& I;
     Settings set;
     Shared& sh;
     double* red;
-    FT* F;
+    double* F64;            // the factor storage viewed as FP64 ...
+    float* F32;             // ... or as FP32 (same buffer)
+    bool use32;             // this iteration factors in FP32
+    bool fellback;          // mixed precision: the FP64 factor is in use for good
+    int nfp32, nfallback;   // iterations accepted with the FP32 factor; FP64 redos
+    bool kktfail;           // the last iteration's factorization or a KKT solve failed
     int n, m, nv;
     double *Df, *Qp, *wf, *Dpa, *Dda, *Dp, *Dd, *df, *dx, *cgw, *tn;
     double *Dg, *Dya, *Dy, *dg, *dyv, *cgp, *tm1, *tm2;
@@ -305,7 +311,11 @@ struct Ctx {
     __device__ void toc(int sec, long long t0) { __syncthreads(); tsec[sec] += clock64() - t0; }
     __device__ Ctx(const DevInst& I_, const Settings& s_, Shared& sh_) : I(I_), set(s_), sh(sh_) {
         red = sh.red;
-        F = reinterpret_cast<FT*>(I.F);
+        F64 = reinterpret_cast<double*>(I.F);
+        F32 = reinterpret_cast<float*>(I.F);
+        use32 = set.precision == 1 || (set.precision == 2 && I.status[5] == 0);
+        fellback = I.status[5] != 0;
+        nfp32 = I.status[4]; nfallback = I.status[5];
         n = I.n; m = I.m; nv = I.nvtx;
         double* v = I.vn;
         Df = v; Qp = v + n; wf = v + 2 * (int64_t)n; Dpa = v + 3 * (int64_t)n; Dda = v + 4 * (int64_t)n;
@@ -326,6 +336,7 @@ struct Ctx {
         if (threadIdx.x == 0) {
             I.scal[5] = nf; I.scal[6] = ng; I.scal[7] = sf; I.scal[8] = sg; I.scal[9] = nB;
             I.status[1] = nrow_hist; I.status[2] = nretry; I.status[3] = nfact;
+            I.status[4] = nfp32; I.status[5] = nfallback;
             for (int k = 0; k < NSEC; ++k) I.scal[SCAL_SEC + k] = (double)tsec[k];
             I.scal[SCAL_NTRSV] = (double)ntrsv; I.scal[SCAL_NGEMV] = (double)ngemv;
         }
@@ -587,6 +598,10 @@ struct Ctx {
 
     // ---- factor  (kkt/uzawa.jl:73-115) ----------------------------------------------------
     __device__ void assemble(double dl, double rho) {
+        if (use32) assemble_t<float>(F32, dl, rho); else assemble_t<double>(F64, dl, rho);
+    }
+    template <class FT>
+    __device__ void assemble_t(FT* F, double dl, double rho) {
         const int tid = threadIdx.x;
         for (int64_t i = tid; i < I.fsize; i += NT) F[i] = (FT)I.Finit[i];
         __syncthreads();
@@ -620,6 +635,10 @@ struct Ctx {
     }
 
     __device__ double factor_lower_norm() {
+        return use32 ? factor_lower_norm_t<float>(F32) : factor_lower_norm_t<double>(F64);
+    }
+    template <class FT>
+    __device__ double factor_lower_norm_t(const FT* F) {
         double s = 0;
         for (int f = 0; f < I.nfront; ++f) {
             int nres = I.fnres[f], nfr = nres + I.fnsep[f];
@@ -633,6 +652,10 @@ struct Ctx {
     }
 
     __device__ int numeric_factor() {
+        return use32 ? numeric_factor_t<float>(F32) : numeric_factor_t<double>(F64);
+    }
+    template <class FT>
+    __device__ int numeric_factor_t(FT* F) {
         for (int f = 0; f < I.nfront; ++f) {
             int nres = I.fnres[f], nsep = I.fnsep[f], nfr = nres + nsep;
             FT* M = F + I.fptr[f];
@@ -655,7 +678,9 @@ struct Ctx {
 
     __device__ bool initkkt(double dl, double& rho) {
         delta = dl;
+        long long ta = tic();
         assemble(dl, 0.0);
+        toc(SEC_ASSEMBLE, ta);
         int info = numeric_factor();
         nfact++;
         rho = 0;
@@ -680,13 +705,17 @@ struct Ctx {
         Usolve_(x);
         toc(SEC_TRSV, t0);
     }
-    __device__ void Lsolve_(double* x) {
+    __device__ void Lsolve_(double* x) { if (use32) Lsolve_t<float>(F32, x); else Lsolve_t<double>(F64, x); }
+    __device__ void Usolve_(double* x) { if (use32) Usolve_t<float>(F32, x); else Usolve_t<double>(F64, x); }
+    template <class FT>
+    __device__ void Lsolve_t(const FT* F, double* x) {
         for (int f = 0; f < I.nfront; ++f) {
             int nres = I.fnres[f], nfr = nres + I.fnsep[f];
             front_lsolve<FT>(F + I.fptr[f], nfr, nres, I.fres0[f], I.fsep + I.fsepp[f], x, sh);
         }
     }
-    __device__ void Usolve_(double* x) {
+    template <class FT>
+    __device__ void Usolve_t(const FT* F, double* x) {
         for (int f = I.nfront - 1; f >= 0; --f) {
             int nres = I.fnres[f], nfr = nres + I.fnsep[f];
             front_usolve<FT>(F + I.fptr[f], nfr, nres, I.fres0[f], I.fsep + I.fsepp[f], x, sh);
@@ -913,11 +942,38 @@ struct Ctx {
         return dl;
     }
 
+    // One iteration.  Mixed precision (settings.precision == 2): the iteration runs with the FP32
+    // factor; if a KKT solve misses its tolerance it is redone from the saved iterate with the FP64
+    // factor, which stays in use for the rest of the solve.
     __device__ int step() {
+        if (set.precision != 2 || fellback) { use32 = set.precision == 1; return step_(); }
+        double* sp = I.vn + (int64_t)NVEC_N * n; double* sd = sp + n; double* sy = I.vm + (int64_t)NVEC_M * m;
+        for (int i = threadIdx.x; i < n; i += NT) { sp[i] = I.p[i]; sd[i] = I.d[i]; }
+        for (int i = threadIdx.x; i < m; i += NT) sy[i] = I.y[i];
+        for (int64_t i = threadIdx.x; i < I.cxblk[nv]; i += NT) I.cache2[i] = I.cache[i];
+        __syncthreads();
+        use32 = true;
+        int st = step_();
+        const Row& r = hrow(nrow_hist - 1);
+        (void)r;
+        if (!kktfail) { nfp32++; return st; }
+        for (int i = threadIdx.x; i < n; i += NT) { I.p[i] = sp[i]; I.d[i] = sd[i]; }
+        for (int i = threadIdx.x; i < m; i += NT) I.y[i] = sy[i];
+        for (int64_t i = threadIdx.x; i < I.cxblk[nv]; i += NT) I.cache[i] = I.cache2[i];
+        __syncthreads();
+        nrow_hist--;
+        fellback = true; use32 = false; nfallback++;
+        return step_();
+    }
+
+    __device__ int step_() {
         const double NaN = __longlong_as_double(0x7ff8000000000000LL);
+        kktfail = false;
         int status = CONTINUE;
         Row row{NaN, NaN, NaN, NaN, 0.0, 0, 0, (double)KKT_SOLVED, 0, 0, (double)KKT_SOLVED, NaN, NaN, NaN, 0.0, NaN, NaN};
+        long long tg = tic();
         double dl = getaug();
+        toc(SEC_AUG, tg);
         double pd = bdot(I.p, I.d, n, red);
         double spsd = 0;
         long long t0 = tic();
@@ -926,6 +982,7 @@ struct Ctx {
         if (!ok) {
             status = NUMERICAL_FAILURE;
         } else {
+            long long tr = tic();
             residuals();
             double nuf = (double)max(I.nu, 1);
             double mu = pd / nuf, mus = spsd / nuf, chi = mu * mus - 1;
@@ -936,6 +993,7 @@ struct Ctx {
             double pobj = pQp / 2 - bdot(I.f, I.p, n, red);
             double dobj = bdot(I.g, I.y, m, red) - pQp / 2;
             row.mu = mu; row.chi = chi; row.pres = pres; row.dres = dres; row.pobj = pobj; row.dobj = dobj;
+            toc(SEC_RESID, tr);
             if (isopt(mu, mus, I.mut, pobj, dobj, pres, dres, I.nu, set.gap_tol, set.feas_tol)) status = OPTIMAL;
             else if (isprimalinfeasible(set.infeas_rel, set.infeas_abs)) status = PRIMAL_INFEASIBLE;
             else if (isdualinfeasible(set.infeas_rel, set.infeas_abs)) status = DUAL_INFEASIBLE;
@@ -962,7 +1020,7 @@ struct Ctx {
                 bool iok = initkkt(dl, rho);
                 toc(SEC_INITKKT, t1);
                 row.rho = rho;
-                if (!iok) status = nearstatus(NUMERICAL_FAILURE, mu, mus, pobj, dobj, pres, dres);
+                if (!iok) { kktfail = true; status = nearstatus(NUMERICAL_FAILURE, mu, mus, pobj, dobj, pres, dres); }
                 else {
                     double mu1 = nrow_hist == 0 ? mu : hrow(0).mu;
                     double tol;
@@ -1012,6 +1070,7 @@ struct Ctx {
                     zerofree(Dd);
                     toc(SEC_CORR, t3);
                     if (po.status != KKT_SOLVED || co.status != KKT_SOLVED) {
+                        kktfail = true;
                         status = nearstatus(NUMERICAL_FAILURE, mu, mus, pobj, dobj, pres, dres);
                     } else {
                         long long t4 = tic();
@@ -1062,14 +1121,13 @@ struct Ctx {
 
 // init (solver/ipm.jl:431-478 and reinit! :375-429), then the solve_impl! loop
 // (solver/solver.jl:119-145) and result, or one of those pieces (mode)
-template <class FT>
 __device__ void solve_instance(const DevInst& I, const Settings& set, Shared& sh, int mode) {
     const int n = I.n, m = I.m;
     if (mode == MODE_SOLVE || mode == MODE_INIT) {
         if (threadIdx.x == 0) { for (int k = 0; k < NSTAT; ++k) I.status[k] = 0; }
         __syncthreads();
     }
-    Ctx<FT> c(I, set, sh);
+    Ctx c(I, set, sh);
     if (mode == MODE_SOLVE || mode == MODE_INIT) {
         // working copies of the inputs: a solve never modifies the uploaded problem
         for (int i = threadIdx.x; i < I.B.nnz; i += NT) I.B.val[i] = I.B.val0[i];
@@ -1150,8 +1208,7 @@ struct BatchArgs {
     int* counter;     // work queue head
 };
 
-template <class FT>
-__global__ void __launch_bounds__(NT, 1) ipm_batch_kernel(BatchArgs a) {
+__global__ void __launch_bounds__(NT, CTA_PER_SM) ipm_batch_kernel(BatchArgs a) {
     __shared__ Shared sh;
     __shared__ int next;
     for (;;) {
@@ -1160,7 +1217,7 @@ __global__ void __launch_bounds__(NT, 1) ipm_batch_kernel(BatchArgs a) {
         int k = next;
         __syncthreads();
         if (k >= a.ninst) break;
-        solve_instance<FT>(a.inst[k], a.set, sh, a.mode);
+        solve_instance(a.inst[k], a.set, sh, a.mode);
     }
 }
 
@@ -1175,8 +1232,8 @@ extern "C" int mb_launch_batch(const mb::DevInst* d_inst, int ninst, int mode, c
     a.inst = d_inst; a.ninst = ninst; a.mode = mode; a.set = *set; a.counter = d_counter;
     cudaError_t e = cudaMemsetAsync(d_counter, 0, sizeof(int), stream);
     if (e != cudaSuccess) return -1;
-    if (fp32) mb::ipm_batch_kernel<float><<<grid, mb::NT, 0, stream>>>(a);
-    else mb::ipm_batch_kernel<double><<<grid, mb::NT, 0, stream>>>(a);
+    (void)fp32;
+    mb::ipm_batch_kernel<<<grid, mb::NT, 0, stream>>>(a);
     e = cudaGetLastError();
     return e == cudaSuccess ? 0 : -2;
 }

@@ -35,7 +35,7 @@ class mb_csc(C.Structure):
 
 class mb_result(C.Structure):
     _fields_ = [("status", I32), ("niter", I32), ("nsolve", I32), ("nfactor_retry", I32),
-                ("nfactor", I32), ("reserved", I32),
+                ("nfactor", I32), ("nfp32", I32), ("nfallback", I32), ("reserved", I32),
                 ("mu", F64), ("pres", F64), ("dres", F64), ("pobj", F64), ("dobj", F64), ("factor_flops", F64)]
 
 

@@ -105,13 +105,13 @@ class IPMSettings:
     stable: bool = False
     infeas_abs: float = 1e-8
     infeas_rel: float = 1e-8
-    precision: str = "fp64"          # "fp64" or "fp32" (factor precision; refinement stays FP64)
+    precision: str = "fp64"          # "fp64", "fp32" or "mixed" (factor precision; refinement stays FP64)
 
     def to_c(self) -> mb_settings:
         s = mb_settings()
         for f in fields(self):
             if f.name == "precision":
-                s.precision = {"fp64": 0, "fp32": 1}[self.precision]
+                s.precision = {"fp64": 0, "fp32": 1, "mixed": 2}[self.precision]
             elif f.name == "stable":
                 s.stable = int(self.stable)
             else:
@@ -333,6 +333,8 @@ class IPMResult:
     nfactor_retry: int = 0
     nfactor: int = 0
     factor_flops: float = 0.0
+    nfp32: int = 0
+    nfallback: int = 0
 
 
 class IPMSolver:
@@ -376,7 +378,7 @@ class IPMSolver:
         check(self.L.mb_solver_result(self.h, _p(p, C.c_double), _p(d, C.c_double), _p(y, C.c_double), C.byref(r)),
               self.prob.ctx.h, "result")
         return IPMResult(p, d, y, IPMStatus(r.status), r.niter, r.nsolve, self.history(), r.mu, r.pres, r.dres,
-                         r.pobj, r.dobj, r.nfactor_retry, r.nfactor, r.factor_flops)
+                         r.pobj, r.dobj, r.nfactor_retry, r.nfactor, r.factor_flops, r.nfp32, r.nfallback)
 
     def __del__(self):
         if getattr(self, "h", None):
@@ -440,11 +442,11 @@ class Batch:
         for i in range(k):
             r = res[i]
             out.append(IPMResult(ps[i], ds[i], ys[i], IPMStatus(r.status), r.niter, r.nsolve, IPMHistory(), r.mu,
-                                 r.pres, r.dres, r.pobj, r.dobj, r.nfactor_retry, r.nfactor, r.factor_flops))
+                                 r.pres, r.dres, r.pobj, r.dobj, r.nfactor_retry, r.nfactor, r.factor_flops, r.nfp32, r.nfallback))
         return out
 
     SECTIONS = ["equilibrate", "BtB", "scale", "initkkt", "predictor", "corrector", "maxsteps", "trsv", "gemv",
-                "ntrsv", "ngemv"]
+                "assemble", "residual", "getaug", "ntrsv", "ngemv"]
 
     def timers(self):
         """Per-instance section clocks (after fetch): array (ninst, 11), columns SECTIONS."""

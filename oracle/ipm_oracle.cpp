@@ -688,6 +688,8 @@ struct Solver {
     i64 n = 0, m = 0;
     Timers tm;
     i64 nfactor_retry = 0;
+    i64 nfallback = 0;      // iterations redone with the FP64 factor (precision 2)
+    i64 nfp32 = 0;          // iterations accepted with the FP32 factor
 };
 
 // --------------------------------------------------------------------------------------------
@@ -1007,7 +1009,27 @@ static double getaug(const Solver& s) {
 
 static const double FORCING_FRAC = 0.1;
 
+static int step_(Solver& s);
+
+// precision 2 (mixed): iterate with an FP32 factor until a KKT solve misses its tolerance; that
+// iteration is redone from the saved iterate with the FP64 factor, which is kept from then on
 static int step(Solver& s) {
+    if (s.set.precision != 2 || s.nfallback > 0) { if (s.set.precision == 2) s.F.fp32 = false; return step_(s); }
+    std::vector<double> p0 = s.p, d0 = s.d, y0 = s.y;
+    std::vector<double> c0 = s.cache;
+    s.F.fp32 = true;
+    int st = step_(s);
+    const ob_row& r = s.hist.back();
+    bool kktfail = (r.pstat != KKT_SOLVED || r.cstat != KKT_SOLVED) && !std::isnan(r.rho);
+    if (!kktfail) { s.nfp32++; return st; }
+    s.hist.pop_back();
+    s.p = p0; s.d = d0; s.y = y0; s.cache = c0;
+    s.F.fp32 = false;
+    s.nfallback++;
+    return step_(s);
+}
+
+static int step_(Solver& s) {
     const double NaN = std::numeric_limits<double>::quiet_NaN();
     int status = CONTINUE;
     ob_row row{NaN, NaN, NaN, NaN, 0.0, 0, 0, (double)KKT_SOLVED, 0, 0, (double)KKT_SOLVED,
@@ -1301,7 +1323,7 @@ void* oracle_create(const ob_bsm* Qc, const ob_bsm* Bc, const double* f, const d
     }
     s->F.S = &s->S;
     s->F.val.assign(s->S.fsize, 0.0);
-    s->F.fp32 = s->set.precision == 1;
+    s->F.fp32 = s->set.precision >= 1;
     s->H = s->Q;
     // caches (cone.jl:46-65) and workspaces
     s->cxblk.assign(nv + 1, 0);
@@ -1406,6 +1428,8 @@ int oracle_symbolic(void* h, int64_t* nfront, int64_t* res0, int64_t* nres, int6
 }
 
 int64_t oracle_nfactor_retry(void* h) { return ((Solver*)h)->nfactor_retry; }
+int64_t oracle_nfallback(void* h) { return ((Solver*)h)->nfallback; }
+int64_t oracle_nfp32(void* h) { return ((Solver*)h)->nfp32; }
 
 void oracle_destroy(void* h) { delete (Solver*)h; }
 

@@ -109,6 +109,9 @@ def lib(threads: int = 1):
         L.oracle_nfactor_retry.argtypes = [C.c_void_p]
         L.oracle_nfactor_retry.restype = C.c_int64
         L.oracle_destroy.argtypes = [C.c_void_p]
+        for nm in ("oracle_nfallback", "oracle_nfp32"):
+            getattr(L, nm).argtypes = [C.c_void_p]
+            getattr(L, nm).restype = C.c_int64
         L.oracle_set_blas.argtypes = [C.c_char_p, C.c_int]
         L.oracle_set_threads.argtypes = [C.c_int]
         path = find_openblas()
@@ -183,6 +186,9 @@ class OracleSolver:
         self.L.oracle_symbolic(self.h, C.byref(nf), *[_p64(x) for x in a], cap)
         k = nf.value
         return dict(nfront=k, res0=a[0][:k], nres=a[1][:k], nsep=a[2][:k], parent=a[3][:k])
+
+    def mixed_counts(self):
+        return self.L.oracle_nfp32(self.h), self.L.oracle_nfallback(self.h)
 
     def nfactor_retry(self):
         return self.L.oracle_nfactor_retry(self.h)

@@ -83,3 +83,19 @@ def test_batch_equals_alone():
         assert ra.status == rm.status and ra.niter == rm.niter
         np.testing.assert_array_equal(ra.p, rm.p)
         np.testing.assert_array_equal(ra.y, rm.y)
+
+
+@pytest.mark.parametrize("name", ["socp_small", "port_small", "port_mid"])
+def test_mixed_precision_matches_fp64_oracle(name):
+    """Mixed precision (FP32 factor, FP64 refinement, FP64 redo on a missed KKT tolerance) reaches
+    the same optimum as the FP64 oracle within the stopping tolerance: objective within 1e-7
+    relative, residuals below feas_tol."""
+    ref = block_problem(SMALL[name]())
+    prob = _gpu_problem(ref)
+    _, o = oracle_solve(ref, vperm=prob.symbolic()["vperm"])
+    r = solve(prob, IPMSettings(precision="mixed"))
+    assert r.status == IPMStatus.OPTIMAL
+    assert r.pres < 1e-8 and r.dres < 1e-8
+    assert _rel(r.pobj, o["pobj"]) < 1e-7 and _rel(r.dobj, o["dobj"]) < 1e-7
+    assert r.nfp32 + r.nfallback >= 1 and r.nfp32 >= 1
+    assert np.linalg.norm(r.p - o["p"]) <= 1e-4 * max(1.0, np.linalg.norm(o["p"]))

@@ -153,9 +153,14 @@ struct Packed {
     }
 };
 
-static int64_t cone_cachesize(int k, i64 n) { return k == MB_CONE_SOC ? 5 + n : 0; }
+// cachesize / workspacesize / degree  (soc.jl:116-134, tdc.jl:122-143, pos.jl:21-31, noc.jl:20-28)
+static int64_t cone_cachesize(int k, i64 n) {
+    return k == MB_CONE_SOC ? 5 + n : ((k == MB_CONE_EXP || k == MB_CONE_POW) ? 19 : 0);
+}
 static int64_t cone_workspacesize(int k, i64 n) { return k == MB_CONE_SOC ? 2 * n : 0; }
-static int64_t cone_degree(int k, i64 n) { return k == MB_CONE_POS ? n : (k == MB_CONE_SOC ? 2 : 0); }
+static int64_t cone_degree(int k, i64 n) {
+    return k == MB_CONE_POS ? n : (k == MB_CONE_SOC ? 2 : ((k == MB_CONE_EXP || k == MB_CONE_POW) ? 3 : 0));
+}
 
 // Build one instance into its own (local) Packed: symbkkt (kkt/kkt.jl:23-53) with the host ordering,
 // the device index structures, the front placement of H and every arena offset.  Thread-safe: the
@@ -173,7 +178,9 @@ static int plan_instance(const mb_problem* P, const mb_settings& set, const doub
     ip.mut = P->mu;
     for (i64 v = 0; v < nv; ++v) {
         int k = P->kind[vp[v]];
-        if (k != MB_CONE_FREE && k != MB_CONE_POS && k != MB_CONE_SOC) { err = "cone kind not supported by this build"; return MB_E_UNSUPPORTED; }
+        if (k == MB_CONE_SDP) { err = "cone kind not supported by this build"; return MB_E_UNSUPPORTED; }
+        if ((k == MB_CONE_EXP || k == MB_CONE_POW) && B.ncols(v) != 3) { err = "exponential/power cones have dimension 3"; return MB_E_ARG; }
+        if (k == MB_CONE_POW && !(P->param[vp[v]] > 0 && P->param[vp[v]] < 1)) { err = "PowerCone needs 0 < α < 1"; return MB_E_ARG; }
     }
     // column map: solver column -> problem column -> user column
     std::vector<i64> cperm;

@@ -17,6 +17,7 @@
 #include "mb_internal.h"
 #include "mb_device.cuh"
 #include "mb_cones.cuh"
+#include "mb_tdc.cuh"
 
 namespace mb {
 
@@ -474,9 +475,15 @@ struct Ctx {
     __device__ void startingpoint() {  // solver/ipm.jl:331-365
         const int warp = threadIdx.x >> 5;
         for (int v = warp; v < nv; v += NW) {
+            int k = I.kind[v];
             int c0 = I.xcol[v], nc = I.xcol[v + 1] - c0;
-            w_identity(I.kind[v], nc, I.p + c0);
-            w_identity(I.kind[v], nc, I.d + c0);
+            if (k == CONE_EXP || k == CONE_POW) {
+                if ((threadIdx.x & 31) == 0) { tdidentity(TD{k, I.kpar[v]}, I.p + c0); tdidentity(TD{k, I.kpar[v]}, I.d + c0); }
+                __syncwarp();
+                continue;
+            }
+            w_identity(k, nc, I.p + c0);
+            w_identity(k, nc, I.d + c0);
         }
         __syncthreads();
         spmv(I.B, I.p, tm1, 1, 0);
@@ -514,8 +521,19 @@ struct Ctx {
                 sp = warp_sum(s);
             } else if (k == CONE_SOC) {
                 fl = w_socpoint(I.cache + I.cxblk[v], p, d, nc, sp);
+            } else if (k == CONE_EXP || k == CONE_POW) {
+                continue;
             }
             if (lane == 0) { vflag[v] = fl ? 1.0 : 0.0; vspsd[v] = sp; }
+        }
+        // exponential / power cones: one thread per cone (tdc.jl:186-294)
+        for (int v = tid; v < nv; v += NT) {
+            int k = I.kind[v];
+            if (k != CONE_EXP && k != CONE_POW) continue;
+            int c0 = I.xcol[v];
+            double sp = 0;
+            bool fl = tdscale(TD{k, I.kpar[v]}, I.Hd + I.hdoff[v], I.p + c0, I.d + c0, I.cache + I.cxblk[v], sp);
+            vflag[v] = fl ? 1.0 : 0.0; vspsd[v] = sp;
         }
         __syncthreads();
         // SOC Hessian blocks H = (2 (Jw)(Jw)ᵀ − J) / β² added in place (soc.jl:231-256)
@@ -542,9 +560,15 @@ struct Ctx {
                 for (int i = lane; i < nc; i += 32) fr[c0 + i] = (sm - Dpv[c0 + i] * Ddv[c0 + i]) / I.p[c0 + i] - I.d[c0 + i];
             } else if (k == CONE_SOC) {
                 w_soccorr(fr + c0, I.cache + I.cxblk[v], I.p + c0, Dpv + c0, Ddv + c0, sm, nc, work);
-            } else {
+            } else if (k == CONE_FREE) {
                 for (int i = lane; i < nc; i += 32) fr[c0 + i] = 0;
             }
+        }
+        for (int v = threadIdx.x; v < nv; v += NT) {   // tdc.jl:394-438
+            int k = I.kind[v];
+            if (k != CONE_EXP && k != CONE_POW) continue;
+            int c0 = I.xcol[v];
+            tdcorr(TD{k, I.kpar[v]}, fr + c0, I.p + c0, I.d + c0, Dpv + c0, Ddv + c0, sm, I.cache + I.cxblk[v]);
         }
         __syncthreads();
     }
@@ -558,9 +582,15 @@ struct Ctx {
                 for (int i = lane; i < nc; i += 32) fr[c0 + i] = sm / I.p[c0 + i] - I.d[c0 + i];
             } else if (k == CONE_SOC) {
                 w_soccorr0(fr + c0, I.cache + I.cxblk[v], I.p + c0, sm, nc);
-            } else {
+            } else if (k == CONE_FREE) {
                 for (int i = lane; i < nc; i += 32) fr[c0 + i] = 0;
             }
+        }
+        for (int v = threadIdx.x; v < nv; v += NT) {   // tdc.jl:446-450
+            int k = I.kind[v];
+            if (k != CONE_EXP && k != CONE_POW) continue;
+            int c0 = I.xcol[v];
+            tdcorr0(fr + c0, I.d + c0, sm, I.cache + I.cxblk[v]);
         }
         __syncthreads();
     }
@@ -579,8 +609,17 @@ struct Ctx {
                 tp = w_socmaxstep(I.p + c0, Dpv + c0, c[1], c[3], nc);
                 td = w_socmaxstep(I.d + c0, Ddv + c0, c[2], c[4], nc);
             }
+            if (k == CONE_EXP || k == CONE_POW) continue;
             if (k != CONE_FREE) { tp *= step_frac; td *= step_frac; }
             if (lane == 0) vstep[v] = jmin(tp, td);
+        }
+        for (int v = threadIdx.x; v < nv; v += NT) {   // tdc.jl:463-483 (certified nflog3 steps)
+            int k = I.kind[v];
+            if (k != CONE_EXP && k != CONE_POW) continue;
+            int c0 = I.xcol[v];
+            double tp = 1, td = 1;
+            tdmaxsteps(TD{k, I.kpar[v]}, I.p + c0, Dpv + c0, I.d + c0, Ddv + c0, I.cache + I.cxblk[v], tp, td);
+            vstep[v] = jmin(tp * step_frac, td * step_frac);
         }
         __syncthreads();
         double mn = __longlong_as_double(0x7ff0000000000000LL);
@@ -1173,6 +1212,14 @@ __device__ void solve_instance(const DevInst& I, const Settings& set, Shared& sh
                     const double* src = !I.has_d0 ? I.p + c0 : I.d + c0;
                     if (k == CONE_POS) { for (int i = lane; i < nc; i += 32) dst[i] = 1.0 / src[i]; }
                     else if (k == CONE_SOC) w_socshadow(dst, src, nc);
+                    else if (k == CONE_EXP || k == CONE_POW) {
+                        if (lane == 0) {
+                            double* C = I.cache + I.cxblk[v];
+                            if (!I.has_d0) tddualshadow(TD{k, I.kpar[v]}, dst, src, C);
+                            else tdprimalshadow(TD{k, I.kpar[v]}, dst, src, C);
+                        }
+                        __syncwarp();
+                    }
                     else { for (int i = lane; i < nc; i += 32) dst[i] = 0; }
                 }
             }
@@ -1182,6 +1229,9 @@ __device__ void solve_instance(const DevInst& I, const Settings& set, Shared& sh
             for (int i = threadIdx.x; i < m; i += NT) I.y[i] /= I.yscl[i];
             __syncthreads();
         }
+        for (int v = threadIdx.x; v < I.nvtx; v += NT)   // initcache! (exp.jl:22-25, pow.jl:35-38)
+            if (I.kind[v] == CONE_EXP || I.kind[v] == CONE_POW) tdinitcache(TD{I.kind[v], I.kpar[v]}, I.cache + I.cxblk[v]);
+        __syncthreads();
         c.save();
         if (threadIdx.x == 0) I.status[0] = CONTINUE;
         __syncthreads();

@@ -96,3 +96,61 @@ def portfolio_batch(count=4096, nmin=50, nmax=400, nfac=10, seed=0):
     rng = np.random.default_rng(seed)
     sizes = rng.integers(nmin, nmax + 1, size=count)
     return [portfolio(int(s), nfac=nfac, rng=np.random.default_rng([seed, i])) for i, s in enumerate(sizes)]
+
+
+def _exp_interior(rng):
+    x1, x2 = rng.uniform(0.5, 2.0, 2)
+    return [x1, x2, x2 * np.log(x1 / x2) - rng.uniform(0.1, 1.0)]
+
+
+def _exp_dual_interior(rng):
+    z1, mz3 = rng.uniform(0.5, 2.0, 2)
+    z2 = mz3 * (np.log(mz3 / z1) - 1.0) + rng.uniform(0.1, 1.0)
+    return [z1, z2, -mz3]
+
+
+def _pow_interior(rng, a):
+    x1, x2 = rng.uniform(0.5, 2.0, 2)
+    return [x1, x2, rng.uniform(-0.9, 0.9) * x1 ** a * x2 ** (1 - a)]
+
+
+def _pow_dual_interior(rng, a):
+    s1, s2 = rng.uniform(0.5, 2.0, 2)
+    return [s1, s2, rng.uniform(-0.9, 0.9) * (s1 / a) ** a * (s2 / (1 - a)) ** (1 - a)]
+
+
+def exppow(nexp=3000, npow=1000, nfree=4000, npos=4000, m=5000, density=0.001, seed=0):
+    """Exponential / power cone problem (configuration 4 shape): ``nexp`` exponential cones and
+    ``npow`` 3-d power cones with α ~ U(0.2, 0.8), plus free and nonnegative columns (the
+    log-sum-exp / relative-entropy epigraph variables), A sparse N(0,1) at the given density.
+    Feasible by construction: x0 in the cone interior, s0 in the dual-cone interior (0 on free
+    columns), y0 ~ U(-1, 1), b = A x0, c = Aᵀ y0 + s0."""
+    rng = np.random.default_rng(seed)
+    alphas = rng.uniform(0.2, 0.8, npow)
+    kinds, sizes, params, x0, s0 = [], [], [], [], []
+    for _ in range(nexp):
+        kinds.append(CONE_EXP); sizes.append(3); params.append(0.0)
+        x0 += _exp_interior(rng); s0 += _exp_dual_interior(rng)
+    for a in alphas:
+        kinds.append(CONE_POW); sizes.append(3); params.append(float(a))
+        x0 += _pow_interior(rng, a); s0 += _pow_dual_interior(rng, a)
+    if nfree:
+        kinds.append(CONE_FREE); sizes.append(nfree); params.append(0.0)
+        x0 += list(rng.uniform(-1, 1, nfree)); s0 += [0.0] * nfree
+    if npos:
+        kinds.append(CONE_POS); sizes.append(npos); params.append(0.0)
+        x0 += list(rng.uniform(0.5, 2.0, npos)); s0 += list(rng.uniform(0.5, 2.0, npos))
+    n = len(x0)
+    A = sp.random(m, n, density=density, format="csc", random_state=rng, data_rvs=lambda s: rng.standard_normal(s))
+    # every column carries at least one entry so that no variable is unconstrained
+    A = sp.lil_matrix(A)
+    empty = np.where(np.diff(sp.csc_matrix(A).indptr) == 0)[0]
+    for j in empty:
+        A[int(rng.integers(m)), j] = rng.standard_normal()
+    A = sp.csc_matrix(A)
+    x0 = np.array(x0); s0 = np.array(s0)
+    y0 = rng.uniform(-1, 1, m)
+    b = A @ x0
+    c = A.T @ y0 + s0
+    return dict(Q=sp.csc_matrix((n, n)), B=A, f=-c, g=b, mu=0.0, kinds=kinds, sizes=sizes, params=params,
+                name=f"exppow nexp={nexp} npow={npow} n={n} m={m} density={density} seed={seed}")

@@ -1353,8 +1353,9 @@ void* oracle_create(const ob_bsm* Qc, const ob_bsm* Bc, const double* f, const d
         if (d0) for (i64 i = 0; i < n; ++i) s->d[i] = d0[s->P2[i]];
         for (i64 v = 0; v < nv; ++v) {
             i64 c0 = s->B.xcol[v], nc = s->B.ncols(v);
-            if (!d0) cone_shadow(s->K[v], s->Kp[v], nc, s->d.data() + c0, s->p.data() + c0, s->cwork.data());
-            else if (!p0) cone_pshadow(s->K[v], s->Kp[v], nc, s->p.data() + c0, s->d.data() + c0, s->cwork.data());
+            double* cv = s->cache.data() + s->cxblk[v];
+            if (!d0) cone_shadow(s->K[v], s->Kp[v], nc, s->d.data() + c0, s->p.data() + c0, cv);
+            else if (!p0) cone_pshadow(s->K[v], s->Kp[v], nc, s->p.data() + c0, s->d.data() + c0, cv);
         }
         if (y0) for (i64 i = 0; i < m; ++i) s->y[i] = y0[s->P1[i]];
         for (i64 i = 0; i < n; ++i) { s->p[i] /= s->pscl[i]; s->d[i] *= s->pscl[i]; }
@@ -1428,6 +1429,59 @@ int oracle_symbolic(void* h, int64_t* nfront, int64_t* res0, int64_t* nres, int6
 }
 
 int64_t oracle_nfactor_retry(void* h) { return ((Solver*)h)->nfactor_retry; }
+
+// TDC cone primitives at a point x (for the known-answer tests): out = [grad(3), hess(9, from the
+// pivoted factor), third(9, along u), dual shadow d*(3), primal shadow of d*(3), det chain d1..d4,
+// two-word log(x1/x2) (2)], returns the tdfact flag
+// Tunçel scaling block at (p, d) and the certified steps along (Δp, Δd): out = [M(9), p*(3), d*(3),
+// τp, τd], returns the scale flag
+int oracle_tdc_scale_step(int kind, double alpha, const double* p, const double* d, const double* Dp,
+                          const double* Dd, double* out) {
+    TD c{kind, alpha};
+    double C[19] = {0};
+    tdinitcache(c, C);
+    double H[9] = {0}, spsd = 0;
+    bool ok = tdscale(c, H, p, d, C, spsd);
+    for (int i = 0; i < 9; ++i) out[i] = H[i];
+    double sp[3], C2[19] = {0};
+    tdprimalshadow(c, sp, d, C2);
+    for (int i = 0; i < 3; ++i) { out[9 + i] = sp[i]; out[12 + i] = C[TD_SD + i]; }
+    double tp, td;
+    tdmaxsteps(c, p, Dp, d, Dd, C, tp, td);
+    out[15] = tp; out[16] = td;
+    return ok ? 1 : 0;
+}
+
+int oracle_tdc_eval(int kind, double alpha, const double* x, const double* u, double* out) {
+    TD c{kind, alpha};
+    double C[19] = {0};
+    tdinitcache(c, C);
+    tddet(c, C, x);
+    double g[3];
+    tdbarrgrad(c, g, x, C);
+    bool ok = tdfact(c, C + TD_L, x, C);
+    double H[9];
+    for (int j = 0; j < 3; ++j) {
+        double e[3] = {0, 0, 0}, col[3];
+        e[j] = 1;
+        tdhessmul(col, C + TD_L, e);
+        for (int i = 0; i < 3; ++i) H[i + 3 * j] = col[i];
+    }
+    double D[9];
+    tdbarrthird(c, D, x, u, C);
+    double sd[3], sp[3];
+    tddualshadow(c, sd, x, C);
+    double C2[19] = {0};
+    tdprimalshadow(c, sp, sd, C2);
+    for (int i = 0; i < 3; ++i) out[i] = g[i];
+    for (int i = 0; i < 9; ++i) out[3 + i] = H[i];
+    for (int i = 0; i < 9; ++i) out[12 + i] = D[i];
+    for (int i = 0; i < 3; ++i) { out[21 + i] = sd[i]; out[24 + i] = sp[i]; }
+    out[27] = C[TD_D1]; out[28] = C[TD_D2]; out[29] = C[TD_D3]; out[30] = C[TD_D4];
+    DD l = twolograt(x[0], x[1]);
+    out[31] = l.h; out[32] = l.l;
+    return ok ? 1 : 0;
+}
 int64_t oracle_nfallback(void* h) { return ((Solver*)h)->nfallback; }
 int64_t oracle_nfp32(void* h) { return ((Solver*)h)->nfp32; }
 

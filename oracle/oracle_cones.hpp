@@ -191,37 +191,48 @@ static inline double posmaxstep(const double* x, const double* Dx, int64_t n) { 
     return tau;
 }
 
+}  // namespace orc
+
+#include "oracle_tdc.hpp"
+
+namespace orc {
+
 // ---------------------------------------------------------------- dispatch
 static inline int64_t cone_degree(int k, int64_t n) {
     switch (k) {
         case CONE_POS: return n;           // pos.jl:21-23
         case CONE_SOC: return 2;           // soc.jl:116-118
         case CONE_FREE: return 0;          // noc.jl:20-22
+        case CONE_EXP: case CONE_POW: return 3;   // tdc.jl:131-134
         default: return 0;
     }
 }
 static inline int64_t cone_cachesize(int k, int64_t n) {
     switch (k) {
         case CONE_SOC: return 5 + n;       // soc.jl:124-126
+        case CONE_EXP: case CONE_POW: return 19;  // tdc.jl:140-143
         default: return 0;
     }
 }
 static inline int64_t cone_workspacesize(int k, int64_t n) {
     switch (k) {
         case CONE_SOC: return 2 * n;       // soc.jl:132-134
+        case CONE_EXP: case CONE_POW: return 15;  // tdc.jl:122-125
         default: return 0;
     }
 }
-static inline void cone_identity(int k, double, int64_t n, double* x) {
+static inline void cone_identity(int k, double kp, int64_t n, double* x) {
     switch (k) {
+        case CONE_EXP: case CONE_POW: tdidentity(TD{k, kp}, x); break;
         case CONE_POS: for (int64_t i = 0; i < n; ++i) x[i] = 1.0; break;      // pos.jl:43-50
         case CONE_SOC: for (int64_t i = 0; i < n; ++i) x[i] = 0.0; if (n > 0) x[0] = std::sqrt(2.0); break;  // soc.jl:163-167
         default: for (int64_t i = 0; i < n; ++i) x[i] = 0.0; break;             // noc.jl:38-41
     }
 }
-static inline bool cone_scale(int k, double, int64_t n, double* H, const double* p, const double* d, double* c,
+static inline bool cone_scale(int k, double kp, int64_t n, double* H, const double* p, const double* d, double* c,
                               double*, double* spsd) {
     switch (k) {
+        case CONE_EXP: case CONE_POW: return tdscale(TD{k, kp}, H, p, d, c, *spsd);
         case CONE_POS: {  // pos.jl:75-84
             double s = 0;
             for (int64_t i = 0; i < n; ++i) { H[i + i * n] += d[i] / p[i]; s += 1.0 / (p[i] * d[i]); }
@@ -232,9 +243,10 @@ static inline bool cone_scale(int k, double, int64_t n, double* H, const double*
         default: *spsd = 0; return true;
     }
 }
-static inline void cone_corr(int k, double, int64_t n, double* r, const double* p, const double* d,
+static inline void cone_corr(int k, double kp, int64_t n, double* r, const double* p, const double* d,
                              const double* Dp, const double* Dd, double sm, double* c, double* work) {
     switch (k) {
+        case CONE_EXP: case CONE_POW: tdcorr(TD{k, kp}, r, p, d, Dp, Dd, sm, c); break;
         case CONE_POS: for (int64_t i = 0; i < n; ++i) r[i] = (sm - Dp[i] * Dd[i]) / p[i] - d[i]; break;  // pos.jl:107-120
         case CONE_SOC: soccorr(r, c, p, Dp, Dd, sm, n, work); break;
         default: for (int64_t i = 0; i < n; ++i) r[i] = 0.0; break;   // noc.jl:63-77
@@ -243,31 +255,37 @@ static inline void cone_corr(int k, double, int64_t n, double* r, const double* 
 static inline void cone_corr0(int k, double, int64_t n, double* r, const double* p, const double* d, double sm,
                               double* c, double*) {
     switch (k) {
+        case CONE_EXP: case CONE_POW: tdcorr0(r, d, sm, c); break;
         case CONE_POS: for (int64_t i = 0; i < n; ++i) r[i] = sm / p[i] - d[i]; break;  // pos.jl:126-137
         case CONE_SOC: soccorr0(r, c, p, sm, n); break;
         default: for (int64_t i = 0; i < n; ++i) r[i] = 0.0; break;
     }
 }
-static inline void cone_maxsteps(int k, double, int64_t n, const double* p, const double* Dp, const double* d,
+static inline void cone_maxsteps(int k, double kp, int64_t n, const double* p, const double* Dp, const double* d,
                                  const double* Dd, double* c, double*, double* tp, double* td) {
     switch (k) {
+        case CONE_EXP: case CONE_POW: tdmaxsteps(TD{k, kp}, p, Dp, d, Dd, c, *tp, *td); break;
         case CONE_POS: *tp = posmaxstep(p, Dp, n); *td = posmaxstep(d, Dd, n); break;
         case CONE_SOC: *tp = socmaxstep(p, Dp, c[1], c[3], n); *td = socmaxstep(d, Dd, c[2], c[4], n); break;
         default: *tp = 1.0; *td = 1.0; break;
     }
 }
 // dual shadow d* = -f'(p)
-static inline bool cone_shadow(int k, double, int64_t n, double* s, const double* x, double*) {
+static inline bool cone_shadow(int k, double kp, int64_t n, double* s, const double* x, double* c) {
     switch (k) {
+        case CONE_EXP: case CONE_POW: return tddualshadow(TD{k, kp}, s, x, c);
         case CONE_POS: for (int64_t i = 0; i < n; ++i) s[i] = 1.0 / x[i]; return true;  // pos.jl:198-204
         case CONE_SOC: return socshadow(s, x, n);
         default: for (int64_t i = 0; i < n; ++i) s[i] = 0.0; return true;
     }
 }
 // primal shadow p*: -f'(p*) = d
-static inline bool cone_pshadow(int k, double kp, int64_t n, double* s, const double* x, double* w) {
-    return cone_shadow(k, kp, n, s, x, w);
+static inline bool cone_pshadow(int k, double kp, int64_t n, double* s, const double* x, double* c) {
+    if (k == CONE_EXP || k == CONE_POW) return tdprimalshadow(TD{k, kp}, s, x, c);
+    return cone_shadow(k, kp, n, s, x, c);
 }
-static inline void cone_initcache(int, double, int64_t, double*) {}
+static inline void cone_initcache(int k, double kp, int64_t, double* c) {
+    if (k == CONE_EXP || k == CONE_POW) tdinitcache(TD{k, kp}, c);
+}
 
 }  // namespace orc

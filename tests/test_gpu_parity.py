@@ -99,3 +99,16 @@ def test_mixed_precision_matches_fp64_oracle(name):
     assert _rel(r.pobj, o["pobj"]) < 1e-7 and _rel(r.dobj, o["dobj"]) < 1e-7
     assert r.nfp32 + r.nfallback >= 1 and r.nfp32 >= 1
     assert np.linalg.norm(r.p - o["p"]) <= 1e-4 * max(1.0, np.linalg.norm(o["p"]))
+
+
+@pytest.mark.parametrize("name", ["exp_small", "pow_small", "exppow_mix"])
+def test_exp_pow_matches_oracle(name):
+    from helpers import TDC, TDC_TOL
+    ref = block_problem(TDC[name]())
+    prob = _gpu_problem(ref)
+    _, o = oracle_solve(ref, vperm=prob.symbolic()["vperm"], **TDC_TOL)
+    r = solve(prob, IPMSettings(**TDC_TOL))
+    assert o["status"] == "OPTIMAL" and r.status == IPMStatus.OPTIMAL
+    assert abs(r.niter - o["niter"]) <= 2
+    assert _rel(r.pobj, o["pobj"]) < 1e-7 and _rel(r.dobj, o["dobj"]) < 1e-7
+    assert r.pres < 1e-7 and r.dres < 1e-7

@@ -190,6 +190,26 @@ int mb_batch_stats(mb_batch* b, int64_t* stats8);   /* bytes: input, workspace, 
 int mb_batch_timers(mb_batch* b, double* out, int64_t cap);
 int mb_batch_destroy(mb_batch* b);
 
+/* mb_batch_solve without any device allocation: every device array of the batch is placed in one
+ * fixed, file-scope device scratch of MB_STATIC_SCRATCH_BYTES.  No counterpart in the reference
+ * (Mumblebee.jl allocates its solver state per solve).  It is for callers that may not allocate
+ * device memory during service: a process that reserved its HBM budget up front (a cudaMalloc
+ * could fail or take it past the budget mid-service), and a process whose other streams run
+ * latency-critical work (cudaFree, and cudaMalloc when it grows the heap, synchronise the whole
+ * device).  It calls no cudaMalloc, cudaMallocHost or cudaFree and no allocating library routine;
+ * the host-side symbolic planning still uses ordinary heap memory.
+ * Limit: all instances together (their mb_problem_footprint bytes plus a few KB of alignment) must
+ * fit in MB_STATIC_SCRATCH_BYTES (32 MiB, e.g. two 400-asset portfolio instances); larger inputs
+ * return MB_E_NOMEM before any device work, with the needed size in mb_last_error.
+ * The scratch is one per device and per process: calls that overlap in time on one device (two
+ * host threads, or two contexts on the same device) race on it and corrupt each other's results.
+ * The first call on a device does the set-up (looks up the scratch address, which may load the
+ * module); make it before any stream capture begins.  Arguments and outputs as mb_batch_solve. */
+#define MB_STATIC_SCRATCH_BYTES (32u << 20)
+int mb_batch_solve_static(mb_ctx* ctx, mb_problem* const* probs, int32_t nprob, const mb_settings* settings,
+                          int32_t grid, double* const* p_out, double* const* d_out, double* const* y_out,
+                          mb_result* results);
+
 #ifdef __cplusplus
 }
 #endif

@@ -972,3 +972,163 @@ int mb_batch_solve(mb_ctx* ctx, mb_problem* const* probs, int32_t nprob, const m
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------------------------
+// mb_batch_solve_static: the batched solve from the fixed device scratch of mb_solver.cu, for
+// callers that may not allocate device memory during service (a process that reserved its HBM
+// budget up front, or one whose other streams cannot absorb the device-wide synchronisation of
+// cudaFree / a growing cudaMalloc).  No counterpart in the reference.  Same planning, DevInst
+// layout and kernel as mb_batch_solve; only the placement of the device arrays differs, and no
+// cudaMalloc, cudaMallocHost or cudaFree is called.  Calls that overlap on one device race on
+// the scratch; the first call per device looks its address up and should precede stream capture.
+// ---------------------------------------------------------------------------------------------
+extern "C" int mb_static_scratch(int device, void** ptr, size_t* bytes);
+
+namespace {
+
+// byte offsets of the batch's arrays inside the scratch, each rounded up to 256 bytes
+struct StaticLayout {
+    size_t inst, counter, ost, i32, i64a, din, work, out, F, total;
+    StaticLayout(const Packed& pk) {
+        size_t off = 0;
+        auto region = [&](size_t bytes) { size_t o = off; off += (std::max<size_t>(bytes, 1) + 255) / 256 * 256; return o; };
+        inst = region(pk.plans.size() * sizeof(mb::DevInst));
+        counter = region(sizeof(int));
+        ost = region(pk.ost.size() * sizeof(int32_t));
+        i32 = region(pk.i32.size() * sizeof(int32_t));
+        i64a = region(pk.i64a.size() * sizeof(i64));
+        din = region(pk.din.size() * sizeof(double));
+        work = region(pk.work.size() * sizeof(double));
+        out = region(pk.out.size() * sizeof(double));
+        F = region(pk.fbytes);
+        total = off;
+    }
+};
+
+// DevInst of plan p over arrays based at the given device pointers (the layout upload() builds)
+mb::DevInst static_devinst(const InstPlan& p, int32_t* i32, i64* q64, double* dn, double* wk, double* ot,
+                           int32_t* ost, char* F) {
+    mb::DevInst I{};
+    I.n = (int)p.n; I.m = (int)p.m; I.nvtx = (int)p.nvtx; I.nfront = (int)p.nfront; I.nu = (int)p.nu;
+    I.has_p0 = p.has_p0; I.has_d0 = p.has_d0; I.has_y0 = p.has_y0; I.mut = p.mut;
+    I.xcol = i32 + p.xcol; I.colvtx = i32 + p.colvtx; I.cfront = i32 + p.cfront;
+    auto fillsp = [&](mb::DevSp& A, i64 nrow, i64 ncol, i64 nnz, size_t rptr, size_t cidx, size_t wval, size_t val0,
+                      size_t cptr, size_t ridx, size_t cpos) {
+        A.nrow = (int)nrow; A.ncol = (int)ncol; A.nnz = (int)nnz;
+        A.rptr = i32 + rptr; A.cidx = i32 + cidx; A.val = wk + wval; A.val0 = dn + val0;
+        A.cptr = i32 + cptr; A.ridx = i32 + ridx; A.cpos = i32 + cpos;
+    };
+    fillsp(I.B, p.m, p.n, p.Bnnz, p.Brptr, p.Bcidx, p.wBval, p.Bval, p.Bcptr, p.Bridx, p.Bcpos);
+    fillsp(I.Q, p.n, p.n, p.Qnnz, p.Qrptr, p.Qcidx, p.wQval, p.Qval, p.Qcptr, p.Qridx, p.Qcpos);
+    I.hdoff = (const int64_t*)(q64 + p.hdoff); I.Qd = wk + p.wQd; I.Qd0 = dn + p.Qd; I.Hd = wk + p.Hd;
+    I.hdpos = (const int64_t*)(q64 + p.hdpos); I.hdld = i32 + p.hdld;
+    I.nqoff = (int)p.nqoff; I.qoffk = i32 + p.qoffk; I.qoffpos = (const int64_t*)(q64 + p.qoffpos);
+    I.kind = i32 + p.kind; I.kpar = dn + p.kpar; I.cxblk = (const int64_t*)(q64 + p.cxblk); I.cache = wk + p.cache;
+    I.cache2 = wk + p.cache2;
+    I.wsize = p.wsize;
+    I.fres0 = i32 + p.fres0; I.fnres = i32 + p.fnres; I.fnsep = i32 + p.fnsep; I.fparent = i32 + p.fparent;
+    I.fptr = (const int64_t*)(q64 + p.fptr); I.fsepp = i32 + p.fsepp; I.fsep = i32 + p.fsep; I.frel = i32 + p.frel;
+    I.fsize = p.fsize;
+    I.Finit = wk + p.Finit; I.F = F + p.F;
+    I.f0 = dn + p.f; I.g0 = dn + p.g; I.p0 = dn + p.p; I.d0 = dn + p.d; I.y0 = dn + p.y;
+    I.f = wk + p.wf; I.g = wk + p.wg; I.pscl = wk + p.pscl; I.yscl = wk + p.yscl;
+    I.p = wk + p.wp; I.d = wk + p.wd; I.y = wk + p.wy;
+    I.vn = wk + p.vn; I.vm = wk + p.vm; I.vv = wk + p.vv; I.work = wk + p.work;
+    I.po = ot + p.po; I.dout = ot + p.dout; I.yo = ot + p.yo;
+    I.hist = ot + p.hist; I.uhist = wk + p.uhist; I.cghist = wk + p.cghist;
+    I.status = ost + p.status; I.scal = ot + p.scal;
+    return I;
+}
+
+// results of plan ip from host copies of the output and status arrays (what unpack_one reads)
+void static_unpack(const InstPlan& ip, const double* o, const int32_t* st, int max_iter, double* p, double* d,
+                   double* y, mb_result* r) {
+    if (p) for (i64 i = 0; i < ip.n; ++i) p[ip.colmap[i]] = o[ip.po + i];
+    if (d) for (i64 i = 0; i < ip.n; ++i) d[ip.colmap[i]] = o[ip.dout + i];
+    if (y) for (i64 i = 0; i < ip.m; ++i) y[ip.rowmap[i]] = o[ip.yo + i];
+    if (!r) return;
+    st += ip.status;
+    r->status = st[0]; r->niter = st[1]; r->nfactor_retry = st[2]; r->nfactor = st[3];
+    r->nfp32 = st[4]; r->nfallback = st[5];
+    r->factor_flops = ip.fflops;
+    const double* sc = o + ip.scal;
+    r->mu = sc[0]; r->pres = sc[1]; r->dres = sc[2]; r->pobj = sc[3]; r->dobj = sc[4];
+    int ns = 0, nr = std::min<int>(st[1], max_iter + 1);
+    for (int i = 0; i < nr; ++i) {
+        const double* row = o + ip.hist + (size_t)i * mb::ROW_DOUBLES;
+        ns += (int)(row[5] + row[6] + row[8] + row[9]);
+    }
+    r->nsolve = ns;
+}
+
+}  // namespace
+
+extern "C" int mb_batch_solve_static(mb_ctx* ctx, mb_problem* const* probs, int32_t nprob, const mb_settings* settings,
+                                     int32_t grid, double* const* p_out, double* const* d_out, double* const* y_out,
+                                     mb_result* results) {
+    if (!ctx || nprob < 0 || (nprob > 0 && !probs)) return fail(ctx, MB_E_ARG, "bad arguments");
+    mb_settings s;
+    if (settings) s = *settings; else mb_settings_default(&s);
+    if (s.stable) return fail(ctx, MB_E_UNSUPPORTED, "stable=true (StableUzawaSolver) is not available");
+    if (s.max_iter < 0 || s.refine_max_iter < 0 || s.newton_max_iter < 0) return fail(ctx, MB_E_ARG, "negative iteration limit");
+    if (s.precision < 0 || s.precision > 2) return fail(ctx, MB_E_ARG, "precision must be 0 (FP64), 1 (FP32) or 2 (mixed)");
+    for (int32_t k = 0; k < nprob; ++k) if (!probs[k]) return fail(ctx, MB_E_ARG, "null problem");
+    if (nprob == 0) return MB_OK;
+    // plan on the host, then check the fit before touching the device
+    Packed pk;
+    for (int32_t k = 0; k < nprob; ++k) {
+        Packed one;
+        std::string err;
+        int rc = plan_instance(probs[k], s, nullptr, nullptr, nullptr, one, err);
+        if (rc) return fail(ctx, rc, err);
+        merge(pk, one);
+    }
+    const StaticLayout L(pk);
+    if (L.total > (size_t)MB_STATIC_SCRATCH_BYTES)
+        return fail(ctx, MB_E_NOMEM, "mb_batch_solve_static: the batch needs " + std::to_string(L.total) +
+                                     " bytes of device scratch but the static scratch holds " +
+                                     std::to_string((size_t)MB_STATIC_SCRATCH_BYTES) +
+                                     " (MB_STATIC_SCRATCH_BYTES); solve fewer or smaller problems per call, or use mb_batch_solve");
+    CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+    void* scratch = nullptr;
+    size_t cap = 0;
+    int e = mb_static_scratch(ctx->device, &scratch, &cap);
+    if (e != 0) return fail(ctx, MB_E_CUDA, std::string("static scratch lookup: ") + cudaGetErrorString((cudaError_t)e));
+    if (L.total > cap) return fail(ctx, MB_E_NOMEM, "mb_batch_solve_static: the static scratch is smaller than its declared size");
+    char* base = (char*)scratch;
+    int32_t* s_i32 = (int32_t*)(base + L.i32);
+    i64* s_i64 = (i64*)(base + L.i64a);
+    double* s_din = (double*)(base + L.din);
+    double* s_work = (double*)(base + L.work);
+    double* s_out = (double*)(base + L.out);
+    int32_t* s_ost = (int32_t*)(base + L.ost);
+    mb::DevInst* s_inst = (mb::DevInst*)(base + L.inst);
+    int* s_counter = (int*)(base + L.counter);
+    std::vector<mb::DevInst> hi;
+    hi.reserve(pk.plans.size());
+    for (const InstPlan& p : pk.plans)
+        hi.push_back(static_devinst(p, s_i32, s_i64, s_din, s_work, s_out, s_ost, base + L.F));
+    cudaStream_t st = ctx->stream;
+    if (pk.i32.size()) CUDA_TRY(ctx, cudaMemcpyAsync(s_i32, pk.i32.h.data(), pk.i32.size() * sizeof(int32_t), cudaMemcpyHostToDevice, st));
+    if (pk.i64a.size()) CUDA_TRY(ctx, cudaMemcpyAsync(s_i64, pk.i64a.h.data(), pk.i64a.size() * sizeof(i64), cudaMemcpyHostToDevice, st));
+    if (pk.din.size()) CUDA_TRY(ctx, cudaMemcpyAsync(s_din, pk.din.h.data(), pk.din.size() * sizeof(double), cudaMemcpyHostToDevice, st));
+    CUDA_TRY(ctx, cudaMemcpyAsync(s_inst, hi.data(), hi.size() * sizeof(mb::DevInst), cudaMemcpyHostToDevice, st));
+    // the status words start at zero (mb_batch_solve clears its fresh array the same way); the
+    // work counter is cleared by mb_launch_batch
+    CUDA_TRY(ctx, cudaMemsetAsync(s_ost, 0, std::max<size_t>(pk.ost.size(), 1) * sizeof(int32_t), st));
+    int ninst = (int)pk.plans.size();
+    int g = std::min(grid > 0 ? grid : ctx->nsm * mb::CTA_PER_SM, ninst);
+    mb::Settings ds;
+    std::memcpy(&ds, &s, sizeof(ds));
+    if (mb_launch_batch(s_inst, ninst, mb::MODE_SOLVE, &ds, s_counter, g, s.precision == MB_PREC_FP32, st))
+        return fail(ctx, MB_E_CUDA, std::string("launch failed: ") + cudaGetErrorString(cudaGetLastError()));
+    std::vector<double> h_out(std::max<size_t>(pk.out.size(), 1));
+    std::vector<int32_t> h_ost(std::max<size_t>(pk.ost.size(), 1));
+    CUDA_TRY(ctx, cudaMemcpyAsync(h_out.data(), s_out, h_out.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(ctx, cudaMemcpyAsync(h_ost.data(), s_ost, h_ost.size() * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(ctx, cudaStreamSynchronize(st));
+    for (size_t k = 0; k < pk.plans.size(); ++k)
+        static_unpack(pk.plans[k], h_out.data(), h_ost.data(), s.max_iter, p_out ? p_out[k] : nullptr,
+                      d_out ? d_out[k] : nullptr, y_out ? y_out[k] : nullptr, results ? &results[k] : nullptr);
+    return MB_OK;
+}

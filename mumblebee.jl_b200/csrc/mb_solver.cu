@@ -1287,3 +1287,46 @@ extern "C" int mb_launch_batch(const mb::DevInst* d_inst, int ninst, int mode, c
     e = cudaGetLastError();
     return e == cudaSuccess ? 0 : -2;
 }
+
+// ---------------------------------------------------------------------------------------------
+// Fixed device scratch for mb_batch_solve_static (no counterpart in the reference).
+//
+// Some callers may not allocate device memory during service: a process that reserved its HBM
+// budget up front (a cudaMalloc could fail, or take it past the budget, mid-service), and a
+// process whose other streams run latency-critical work (cudaFree, and cudaMalloc when it has to
+// grow the heap, synchronise the whole device).  For them the batched solve can run from this
+// file-scope array, which the driver places when it loads this module.  It is one per device and
+// per process: calls that overlap in time on one device race on it.
+// ---------------------------------------------------------------------------------------------
+#include <mutex>
+#include "../../include/mumblebee_gpu.h"
+
+static __device__ __align__(256) unsigned char mb_static_scratch_buf[MB_STATIC_SCRATCH_BYTES];
+
+// Device address and size of the scratch on `device`.  The address is looked up once per device
+// with that device current (cudaGetSymbolAddress, which may load the module) and cached; the
+// previously current device is restored.  Returns a cudaError_t value (0 on success).
+extern "C" int mb_static_scratch(int device, void** ptr, size_t* bytes) {
+    constexpr int MAXDEV = 64;
+    static std::mutex mu;
+    static void* addr[MAXDEV] = {};
+    if (!ptr || !bytes || device < 0 || device >= MAXDEV) return (int)cudaErrorInvalidValue;
+    std::lock_guard<std::mutex> lock(mu);
+    if (!addr[device]) {
+        int cur = -1;
+        cudaError_t e = cudaGetDevice(&cur);
+        if (e != cudaSuccess) return (int)e;
+        if (cur != device && (e = cudaSetDevice(device)) != cudaSuccess) return (int)e;
+        void* p = nullptr;
+        e = cudaGetSymbolAddress(&p, mb_static_scratch_buf);
+        if (cur != device) {
+            cudaError_t r = cudaSetDevice(cur);
+            if (e == cudaSuccess) e = r;
+        }
+        if (e != cudaSuccess) return (int)e;
+        addr[device] = p;
+    }
+    *ptr = addr[device];
+    *bytes = sizeof(mb_static_scratch_buf);
+    return (int)cudaSuccess;
+}

@@ -2,8 +2,10 @@
 """Benchmark: batched interior-point solves per second on B200.
 
 Workload (one "step"): one batch of synthetic portfolio QP/SOCP instances solved to the 1e-8 gap
-(n_assets ~ U[50, 400], factor model F (n x 10), D ~ U(0.1, 1), budget
-equality, long-only cone, SOC risk bound), all instances in one persistent launch.
+(4096 per GPU by default: n_assets ~ U[50, 400], factor model F (n x 10), D ~ U(0.1, 1), budget
+equality, long-only cone, SOC risk bound), all instances in one persistent launch.  Both factor
+precisions are timed (FP64 and mixed FP32/FP64), with per-instance p50/p99 latency from the
+device's global timer.
 
   value  — solves/s with every input resident in HBM (device time, CUDA events on the launching
            stream, max over ranks)
@@ -31,9 +33,14 @@ sys.path.insert(0, os.path.join(ROOT, "mumblebee.jl_b200"))
 
 import numpy as np  # noqa: E402
 
-WORKLOAD = ("batched portfolio QP/SOCP (configuration 3): n_assets~U[50,400], F n x 10 N(0,1), D~U(0.1,1), "
+WORKLOAD = ("batched portfolio QP/SOCP: n_assets~U[50,400], F n x 10 N(0,1), D~U(0.1,1), "
             "budget equality, long-only cone, SOC risk bound; solve to 1e-8 gap")
 METRIC = "IPM solves/s & p50/p99 latency at 1e-8 gap: mixed vs FP64 GPU; factor TC%"
+# DRAM bytes (read + write) of one ipm_batch_kernel launch per instance of this workload, FP64
+# factor: an ncu capture of a smaller launch of the same instance distribution, divided by its
+# instance count (profiles/ipm_batch_kernel_portfolio_fp64.txt gives the command and the figures)
+TRAFFIC_BYTES_PER_INSTANCE_FP64 = None
+TRAFFIC_SOURCE = None
 
 
 def parse():
@@ -48,6 +55,7 @@ def parse():
     ap.add_argument("--cpu-seconds", type=float, default=15.0, help="bounded CPU-baseline sample length")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-compare", action="store_true", help="skip the other precision's arm")
     return ap.parse_args()
 
 
@@ -230,6 +238,38 @@ def run_reference(args, ws, rank):
     print(json.dumps(line), flush=True)
 
 
+def timed_arm(probs, precision, args, pg, local, ws, ctx):
+    """Prepare a batch at `precision`, warm up, time `steps` persistent launches (CUDA events on the
+    launching stream, max over ranks) and read back statuses, iterations and latencies."""
+    from mumblebee_b200.ipm import Batch, IPMSettings
+    settings = IPMSettings(precision=precision)
+    t0 = time.time()
+    batch = Batch(probs, settings, ctx=ctx)
+    t_prep = time.time() - t0
+    st = batch.stats()
+    for _ in range(args.warmup):
+        batch.run()
+    barrier(pg, local)
+    clk = Clocks(local)
+    ms_steps = [batch.run() for _ in range(args.steps)]
+    clocks = clk.stop()
+    ms = sum(ms_steps) / len(ms_steps)
+    ms_max = allreduce_max(pg, ms, local)
+    res = batch.fetch(want_vectors=False)          # results of the last timed launch
+    lat, svc = batch.latencies_ms()
+    out = {"precision": precision, "ms": ms, "ms_max": ms_max, "ms_steps": ms_steps, "clocks": clocks,
+           "value": args.count * ws / (ms_max / 1e3), "res": res, "stats": st, "prepare_s": t_prep,
+           "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                          "max": float(lat.max())},
+           "solve_ms": {"p50": float(np.percentile(svc, 50)), "p99": float(np.percentile(svc, 99))},
+           "optimal": sum(1 for r in res if r.status.name == "OPTIMAL"),
+           "near_optimal": sum(1 for r in res if r.status.name == "NEAR_OPTIMAL"),
+           "iters_mean": float(np.mean([r.niter for r in res])),
+           "flops": float(sum(r.nfactor * r.factor_flops for r in res))}
+    del batch
+    return out
+
+
 def main():
     args = parse()
     ws, rank, local, pg = dist_setup(args)
@@ -238,41 +278,32 @@ def main():
         if pg is not None:
             pg.destroy_process_group()
         return
-    from mumblebee_b200.ipm import Batch, Context, IPMSettings, batch_solve
+    from mumblebee_b200.ipm import Context, IPMSettings, batch_solve
     ctx = Context.default(local)
-    settings = IPMSettings(precision=args.precision)
     t0 = time.time()
     probs, sizes = make_problems(args.count, args.seed, rank, ctx)
     t_gen = time.time() - t0
-    t0 = time.time()
-    batch = Batch(probs, settings, ctx=ctx)
-    t_prep = time.time() - t0
-    st = batch.stats()
-    for _ in range(args.warmup):
-        batch.run()
-    res = batch.fetch(want_vectors=False)
-    nok = sum(1 for r in res if r.status.name in ("OPTIMAL",))
-    iters = [r.niter for r in res]
-    # timed region: device time of K persistent launches (CUDA events on the launching stream)
-    barrier(pg, local)
-    clk = Clocks(local)
-    ms_steps = [batch.run() for _ in range(args.steps)]
-    clocks = clk.stop()
-    ms = sum(ms_steps) / len(ms_steps)
-    ms_max = allreduce_max(pg, ms, local)
-    value = args.count * ws / (ms_max / 1e3)
+    main_arm = timed_arm(probs, args.precision, args, pg, local, ws, ctx)
+    other = None
+    if not args.no_compare:
+        other = timed_arm(probs, "mixed" if args.precision == "fp64" else "fp64", args, pg, local, ws, ctx)
     # roofline of the solver kernel: algorithmic factorization flops per launch / launch time
-    flops = float(sum(r.nfactor * r.factor_flops for r in res))
     peaks = measure_peaks()
     peak_key = "tf32" if args.precision in ("fp32", "mixed") else "fp64"
-    achieved = flops / (ms / 1e3) / 1e12
+    achieved = main_arm["flops"] / (main_arm["ms"] / 1e3) / 1e12
+    traffic = None
+    if args.precision == "fp64" and TRAFFIC_BYTES_PER_INSTANCE_FP64 is not None:
+        traffic = TRAFFIC_BYTES_PER_INSTANCE_FP64 * args.count
     roofline = {"bound": "tensor", "achieved": achieved, "peak": peaks[peak_key], "unit": "TFLOP/s",
-                "frac": achieved / peaks[peak_key], "traffic": None,
+                "frac": achieved / peaks[peak_key], "traffic": traffic,
                 "peak_source": f"measured live: torch {peak_key} GEMM 8192^3 best of 5 on this GPU",
-                "kernel": "ipm_batch_kernel", "flops_per_launch": flops}
+                "kernel": "ipm_batch_kernel", "flops_per_launch": main_arm["flops"]}
+    if traffic is not None:
+        roofline["traffic_source"] = TRAFFIC_SOURCE
     # end to end through the C ABI: host problems in, host results out
     e2e = None
     if not args.no_e2e:
+        settings = IPMSettings(precision=args.precision)
         batch_solve(probs, settings)          # warm-up
         barrier(pg, local)
         t = time.perf_counter()
@@ -280,6 +311,7 @@ def main():
             batch_solve(probs, settings)
         dt = (time.perf_counter() - t) / max(1, min(args.steps, 2))
         dt = allreduce_max(pg, dt, local)
+        st = main_arm["stats"]
         e2e = {"value": args.count * ws / dt, "unit": "solves/s", "h2d_bytes_per_step": st["input_bytes"],
                "d2h_bytes_per_step": st["output_bytes"]}
     cpu = None
@@ -290,17 +322,28 @@ def main():
                "sample": f"{done} instances of the same distribution, FP64 oracle, {cores} processes x 1 thread, "
                          f"{args.cpu_seconds:.0f} s"}
     if rank == 0:
-        line = {"metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": ws, "steps": args.steps,
-                "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
-                "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        st = main_arm["stats"]
+        arms = {a["precision"]: {"solves_per_s": a["value"], "ms_per_step": a["ms_max"],
+                                 "latency_ms": a["latency_ms"], "solve_ms": a["solve_ms"],
+                                 "optimal": f"{a['optimal']}/{args.count}", "near_optimal": a["near_optimal"],
+                                 "iters_mean": a["iters_mean"]}
+                for a in (main_arm, other) if a is not None}
+        if "mixed" in arms and "fp64" in arms:
+            arms["mixed_over_fp64"] = arms["mixed"]["solves_per_s"] / arms["fp64"]["solves_per_s"]
+        line = {"metric": METRIC, "value": main_arm["value"], "unit": "solves/s", "n_gpus": ws,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": main_arm["ms_max"],
+                "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+                "data": "synthetic",
                 "config": {"workload": WORKLOAD, "instances_per_gpu": args.count, "precision": args.precision,
                            "parallelism": f"instances sharded over {ws} GPU(s), one persistent launch per step",
                            "l2": f"inputs larger than L2: {st['input_bytes'] / 1e9:.2f} GB uploaded + "
                                  f"{(st['work_bytes'] + st['factor_bytes']) / 1e9:.2f} GB workspace per step",
-                           "optimal": f"{nok}/{len(res)}", "iters_mean": float(np.mean(iters)),
-                           "setup_s": {"generate": round(t_gen, 2), "prepare": round(t_prep, 2)}},
+                           "optimal": f"{main_arm['optimal']}/{args.count}", "iters_mean": main_arm["iters_mean"],
+                           "setup_s": {"generate": round(t_gen, 2), "prepare": round(main_arm["prepare_s"], 2)}},
+                "latency_ms": main_arm["latency_ms"], "solve_ms": main_arm["solve_ms"],
+                "precisions": arms,
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": args.steps,
-                "clocks": clocks, "step_ms": ms_steps}
+                "clocks": main_arm["clocks"], "step_ms": main_arm["ms_steps"]}
         print(json.dumps(line), flush=True)
     if pg is not None:
         pg.destroy_process_group()

@@ -188,6 +188,10 @@ int mb_batch_stats(mb_batch* b, int64_t* stats8);   /* bytes: input, workspace, 
  * then the number of triangular-solve sweeps and of matvecs (the TimerOutputs sections of the
  * reference, solver/ipm.jl:137-755) */
 int mb_batch_timers(mb_batch* b, double* out, int64_t cap);
+/* per-instance device timestamps after mb_batch_fetch, 2 int64 each: the GPU global timer (ns)
+ * when a CTA took the instance from the work queue and when its solve finished.  Latency of an
+ * instance submitted with the launch = finish − the launch's earliest take. */
+int mb_batch_times(mb_batch* b, int64_t* out, int64_t cap);
 int mb_batch_destroy(mb_batch* b);
 
 /* mb_batch_solve without any device allocation: every device array of the batch is placed in one

@@ -954,6 +954,16 @@ int mb_batch_timers(mb_batch* b, double* out, int64_t cap) {
     return MB_OK;
 }
 
+int mb_batch_times(mb_batch* b, int64_t* out, int64_t cap) {
+    if (!b || !out) return MB_E_ARG;
+    for (size_t k = 0; k < b->pk.plans.size() && (int64_t)(2 * k + 2) <= cap; ++k) {
+        const double* sc = b->h_out + b->pk.plans[k].scal;
+        std::memcpy(&out[2 * k], &sc[mb::SCAL_T0], sizeof(int64_t));
+        std::memcpy(&out[2 * k + 1], &sc[mb::SCAL_T1], sizeof(int64_t));
+    }
+    return MB_OK;
+}
+
 int mb_batch_destroy(mb_batch* b) {
     if (!b) return MB_E_ARG;
     delete b;

@@ -108,6 +108,8 @@ enum Section { SEC_EQUIL = 0, SEC_FINIT, SEC_SCALE, SEC_INITKKT, SEC_PRED, SEC_C
 constexpr int SCAL_SEC = 10;        // scal[10 .. 10+NSEC)
 constexpr int SCAL_NTRSV = 22;      // triangular solve sweeps
 constexpr int SCAL_NGEMV = 23;      // block-sparse matvecs
+constexpr int SCAL_T0 = 24;         // %globaltimer (ns, bit pattern) when a CTA took the instance
+constexpr int SCAL_T1 = 25;         // %globaltimer (ns, bit pattern) when its solve finished
 constexpr int NSTAT = 8;    // status, history rows, factor retries, factorizations, FP32 iterations, FP64 redos
 
 // kernel modes: a full solve, or the pieces used by the step-wise API

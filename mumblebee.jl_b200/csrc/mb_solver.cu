@@ -1250,6 +1250,12 @@ __device__ void solve_instance(const DevInst& I, const Settings& set, Shared& sh
     }
 }
 
+__device__ __forceinline__ unsigned long long globaltimer() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
 struct BatchArgs {
     const DevInst* inst;
     int ninst;
@@ -1267,7 +1273,12 @@ __global__ void __launch_bounds__(NT, CTA_PER_SM) ipm_batch_kernel(BatchArgs a) 
         int k = next;
         __syncthreads();
         if (k >= a.ninst) break;
+        unsigned long long t0 = globaltimer();
         solve_instance(a.inst[k], a.set, sh, a.mode);
+        if (threadIdx.x == 0) {
+            a.inst[k].scal[SCAL_T0] = __longlong_as_double((long long)t0);
+            a.inst[k].scal[SCAL_T1] = __longlong_as_double((long long)globaltimer());
+        }
     }
 }
 

@@ -78,6 +78,7 @@ SIGNATURES = {
     "mb_batch_fetch": (I32, [C.c_void_p, C.POINTER(PF64), C.POINTER(PF64), C.POINTER(PF64), C.POINTER(mb_result)]),
     "mb_batch_stats": (I32, [C.c_void_p, PI64]),
     "mb_batch_timers": (I32, [C.c_void_p, PF64, I64]),
+    "mb_batch_times": (I32, [C.c_void_p, PI64, I64]),
     "mb_batch_destroy": (I32, [C.c_void_p]),
     "mb_batch_solve_static": (I32, [C.c_void_p, C.POINTER(C.c_void_p), I32, C.POINTER(mb_settings), I32,
                                     C.POINTER(PF64), C.POINTER(PF64), C.POINTER(PF64), C.POINTER(mb_result)]),

@@ -120,7 +120,7 @@ def _pow_dual_interior(rng, a):
 
 
 def exppow(nexp=3000, npow=1000, nfree=4000, npos=4000, m=5000, density=0.001, seed=0):
-    """Exponential / power cone problem (configuration 4 shape): ``nexp`` exponential cones and
+    """Exponential / power cone problem (defaults: n = 20000, m = 5000): ``nexp`` exponential cones and
     ``npow`` 3-d power cones with α ~ U(0.2, 0.8), plus free and nonnegative columns (the
     log-sum-exp / relative-entropy epigraph variables), A sparse N(0,1) at the given density.
     Feasible by construction: x0 in the cone interior, s0 in the dual-cone interior (0 on free

@@ -455,6 +455,19 @@ class Batch:
         check(self.L.mb_batch_timers(self.h, _p(a, C.c_double), a.size), self.ctx.h, "timers")
         return a.reshape(len(self.probs), W)
 
+    def times(self):
+        """Per-instance GPU global-timer stamps (after fetch), int64 ns, array (ninst, 2): when a CTA
+        took the instance and when its solve finished."""
+        a = np.zeros(2 * len(self.probs), np.int64)
+        check(self.L.mb_batch_times(self.h, _p(a, C.c_int64), a.size), self.ctx.h, "times")
+        return a.reshape(len(self.probs), 2)
+
+    def latencies_ms(self):
+        """Latency of each instance of the last run, all submitted with the launch: finish time minus
+        the launch's earliest take (ms); and its solve time on its CTA (ms)."""
+        t = self.times()
+        return (t[:, 1] - t[:, 0].min()) / 1e6, (t[:, 1] - t[:, 0]) / 1e6
+
     def stats(self):
         a = np.zeros(8, np.int64)
         self.L.mb_batch_stats(self.h, _p(a, C.c_int64))

@@ -1354,8 +1354,8 @@ void* oracle_create(const ob_bsm* Qc, const ob_bsm* Bc, const double* f, const d
         for (i64 v = 0; v < nv; ++v) {
             i64 c0 = s->B.xcol[v], nc = s->B.ncols(v);
             double* cv = s->cache.data() + s->cxblk[v];
-            if (!d0) cone_shadow(s->K[v], s->Kp[v], nc, s->d.data() + c0, s->p.data() + c0, cv);
-            else if (!p0) cone_pshadow(s->K[v], s->Kp[v], nc, s->p.data() + c0, s->d.data() + c0, cv);
+            if (!d0) cone_shadow(s->K[v], s->Kp[v], nc, s->d.data() + c0, s->p.data() + c0, cv, s->cwork.data());
+            else if (!p0) cone_pshadow(s->K[v], s->Kp[v], nc, s->p.data() + c0, s->d.data() + c0, cv, s->cwork.data());
         }
         if (y0) for (i64 i = 0; i < m; ++i) s->y[i] = y0[s->P1[i]];
         for (i64 i = 0; i < n; ++i) { s->p[i] /= s->pscl[i]; s->d[i] *= s->pscl[i]; }
@@ -1482,6 +1482,37 @@ int oracle_tdc_eval(int kind, double alpha, const double* x, const double* u, do
     out[31] = l.h; out[32] = l.l;
     return ok ? 1 : 0;
 }
+// Semidefinite cone primitives on svec vectors of length n = d(d+1)/2 (known-answer tests):
+// H (n×n) += W ⊗ₛ W and the cache [R | S | s] at (p, d), ⟨p*, d*⟩, the corrector along (Δp, Δd)
+// and the zero corrector at σμ, the steps τp/τd, and the shadow X⁻¹ of p.  Returns bit 0 = scale
+// succeeded, bit 1 = shadow succeeded.
+int oracle_sdp_probe(int64_t n, const double* p, const double* d, const double* Dp, const double* Dd, double sm,
+                     double* H, double* cache, double* spsd, double* r, double* r0, double* steps, double* shp) {
+    std::vector<double> work(std::max<int64_t>(sdp_workspacesize(n), 1));
+    bool ok = sdp_scale(H, n, cache, p, d, work.data(), *spsd);
+    int flags = ok ? 1 : 0;
+    if (ok) {
+        sdp_corr(r, cache, Dp, Dd, sm, n, work.data());
+        sdp_corr0(r0, cache, sm, n, work.data());
+        double tp, td;
+        cone_maxsteps(CONE_SDP, 0.0, n, p, Dp, d, Dd, cache, work.data(), &tp, &td);
+        steps[0] = tp; steps[1] = td;
+    }
+    if (sdp_shadow(shp, p, n, work.data())) flags |= 2;
+    return flags;
+}
+
+// smallest eigenvalue of the symmetric d×d M (column-major): out[0] through the tridiagonal
+// Laguerre path capped at lmax, out[1] through the analytic path (d ≤ 3 only); and the Jacobi SVD
+// of A: U (d×d), s (d); returns the SVD's convergence flag
+int oracle_sdp_eig(int d, const double* M, double lmax, const double* A, double* out, double* U, double* sv) {
+    std::vector<double> W(M, M + (size_t)d * d), a(d), b(std::max(d, 1));
+    out[0] = sdp_eigminsturm(W.data(), a.data(), b.data(), d, lmax);
+    out[1] = d <= 3 ? sdp_eigmin_small(M, d) : NAN;
+    std::copy(A, A + (size_t)d * d, U);
+    return sdp_svdjacobi(U, sv, d) ? 1 : 0;
+}
+
 int64_t oracle_nfallback(void* h) { return ((Solver*)h)->nfallback; }
 int64_t oracle_nfp32(void* h) { return ((Solver*)h)->nfp32; }
 

@@ -112,6 +112,11 @@ def lib(threads: int = 1):
         for nm in ("oracle_nfallback", "oracle_nfp32"):
             getattr(L, nm).argtypes = [C.c_void_p]
             getattr(L, nm).restype = C.c_int64
+        PD = C.POINTER(C.c_double)
+        L.oracle_sdp_probe.argtypes = [C.c_int64, PD, PD, PD, PD, C.c_double, PD, PD, PD, PD, PD, PD, PD]
+        L.oracle_sdp_probe.restype = C.c_int
+        L.oracle_sdp_eig.argtypes = [C.c_int, PD, C.c_double, PD, PD, PD, PD]
+        L.oracle_sdp_eig.restype = C.c_int
         L.oracle_set_blas.argtypes = [C.c_char_p, C.c_int]
         L.oracle_set_threads.argtypes = [C.c_int]
         path = find_openblas()
@@ -202,3 +207,30 @@ class OracleSolver:
 def solve(prob, settings=None, vperm=None, **kw):
     s = OracleSolver(prob, settings, vperm, **kw)
     return s.solve()
+
+
+def sdp_probe(p, d, Dp, Dd, sm):
+    """Semidefinite-cone primitives at svec points (p, d): the added Hessian block H, the cache
+    [R | S | s], ⟨p*, d*⟩, corrector along (Δp, Δd), zero corrector, steps (τp, τd), shadow p⁻¹."""
+    n = len(p)
+    k = int((np.sqrt(1 + 8 * n) - 1) // 2)
+    arr = lambda x: np.ascontiguousarray(x, dtype=np.float64)
+    p, d, Dp, Dd = arr(p), arr(d), arr(Dp), arr(Dd)
+    H = np.zeros(n * n); cache = np.zeros(2 * k * k + k); spsd = np.zeros(1)
+    r = np.zeros(n); r0 = np.zeros(n); steps = np.zeros(2); shp = np.zeros(n)
+    flags = lib().oracle_sdp_probe(n, _pd(p), _pd(d), _pd(Dp), _pd(Dd), sm, _pd(H), _pd(cache), _pd(spsd), _pd(r),
+                                   _pd(r0), _pd(steps), _pd(shp))
+    R = cache[:k * k].reshape(k, k, order="F"); S = cache[k * k:2 * k * k].reshape(k, k, order="F")
+    return dict(ok=bool(flags & 1), shadow_ok=bool(flags & 2), H=H.reshape(n, n, order="F"), R=R, S=S,
+                s=cache[2 * k * k:], spsd=spsd[0], corr=r, corr0=r0, tp=steps[0], td=steps[1], shadow=shp)
+
+
+def sdp_eig(M, lmax, A):
+    """eigmin of M by the Laguerre/Sturm path (capped at lmax) and the analytic path (d ≤ 3), and the
+    one-sided Jacobi SVD of A (U, s, converged)."""
+    d = M.shape[0]
+    Mf = np.asfortranarray(M, dtype=np.float64).ravel(order="F")
+    Af = np.asfortranarray(A, dtype=np.float64).ravel(order="F")
+    out = np.zeros(2); U = np.zeros(d * d); sv = np.zeros(d)
+    ok = lib().oracle_sdp_eig(d, _pd(Mf), lmax, _pd(Af), _pd(out), _pd(U), _pd(sv))
+    return out[0], out[1], U.reshape(d, d, order="F"), sv, bool(ok)

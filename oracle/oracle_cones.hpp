@@ -194,6 +194,7 @@ static inline double posmaxstep(const double* x, const double* Dx, int64_t n) { 
 }  // namespace orc
 
 #include "oracle_tdc.hpp"
+#include "oracle_sdp.hpp"
 
 namespace orc {
 
@@ -204,6 +205,7 @@ static inline int64_t cone_degree(int k, int64_t n) {
         case CONE_SOC: return 2;           // soc.jl:116-118
         case CONE_FREE: return 0;          // noc.jl:20-22
         case CONE_EXP: case CONE_POW: return 3;   // tdc.jl:131-134
+        case CONE_SDP: return triroot(n);  // sdp.jl:41-43
         default: return 0;
     }
 }
@@ -211,6 +213,7 @@ static inline int64_t cone_cachesize(int k, int64_t n) {
     switch (k) {
         case CONE_SOC: return 5 + n;       // soc.jl:124-126
         case CONE_EXP: case CONE_POW: return 19;  // tdc.jl:140-143
+        case CONE_SDP: return sdp_cachesize(n);
         default: return 0;
     }
 }
@@ -218,6 +221,7 @@ static inline int64_t cone_workspacesize(int k, int64_t n) {
     switch (k) {
         case CONE_SOC: return 2 * n;       // soc.jl:132-134
         case CONE_EXP: case CONE_POW: return 15;  // tdc.jl:122-125
+        case CONE_SDP: return sdp_workspacesize(n);
         default: return 0;
     }
 }
@@ -226,12 +230,14 @@ static inline void cone_identity(int k, double kp, int64_t n, double* x) {
         case CONE_EXP: case CONE_POW: tdidentity(TD{k, kp}, x); break;
         case CONE_POS: for (int64_t i = 0; i < n; ++i) x[i] = 1.0; break;      // pos.jl:43-50
         case CONE_SOC: for (int64_t i = 0; i < n; ++i) x[i] = 0.0; if (n > 0) x[0] = std::sqrt(2.0); break;  // soc.jl:163-167
+        case CONE_SDP: sdp_identity(x, n); break;
         default: for (int64_t i = 0; i < n; ++i) x[i] = 0.0; break;             // noc.jl:38-41
     }
 }
 static inline bool cone_scale(int k, double kp, int64_t n, double* H, const double* p, const double* d, double* c,
-                              double*, double* spsd) {
+                              double* work, double* spsd) {
     switch (k) {
+        case CONE_SDP: return sdp_scale(H, n, c, p, d, work, *spsd);
         case CONE_EXP: case CONE_POW: return tdscale(TD{k, kp}, H, p, d, c, *spsd);
         case CONE_POS: {  // pos.jl:75-84
             double s = 0;
@@ -249,21 +255,29 @@ static inline void cone_corr(int k, double kp, int64_t n, double* r, const doubl
         case CONE_EXP: case CONE_POW: tdcorr(TD{k, kp}, r, p, d, Dp, Dd, sm, c); break;
         case CONE_POS: for (int64_t i = 0; i < n; ++i) r[i] = (sm - Dp[i] * Dd[i]) / p[i] - d[i]; break;  // pos.jl:107-120
         case CONE_SOC: soccorr(r, c, p, Dp, Dd, sm, n, work); break;
+        case CONE_SDP: sdp_corr(r, c, Dp, Dd, sm, n, work); break;
         default: for (int64_t i = 0; i < n; ++i) r[i] = 0.0; break;   // noc.jl:63-77
     }
 }
 static inline void cone_corr0(int k, double, int64_t n, double* r, const double* p, const double* d, double sm,
-                              double* c, double*) {
+                              double* c, double* work) {
     switch (k) {
         case CONE_EXP: case CONE_POW: tdcorr0(r, d, sm, c); break;
+        case CONE_SDP: sdp_corr0(r, c, sm, n, work); break;
         case CONE_POS: for (int64_t i = 0; i < n; ++i) r[i] = sm / p[i] - d[i]; break;  // pos.jl:126-137
         case CONE_SOC: soccorr0(r, c, p, sm, n); break;
         default: for (int64_t i = 0; i < n; ++i) r[i] = 0.0; break;
     }
 }
 static inline void cone_maxsteps(int k, double kp, int64_t n, const double* p, const double* Dp, const double* d,
-                                 const double* Dd, double* c, double*, double* tp, double* td) {
+                                 const double* Dd, double* c, double* work, double* tp, double* td) {
     switch (k) {
+        case CONE_SDP: {   // sdp.jl:516-519: τp through R, τd through S scaled by Σ
+            int64_t dd = triroot(n);
+            *tp = sdp_maxstep(c, Dp, nullptr, n, work);
+            *td = sdp_maxstep(c + dd * dd, Dd, c + 2 * dd * dd, n, work);
+            break;
+        }
         case CONE_EXP: case CONE_POW: tdmaxsteps(TD{k, kp}, p, Dp, d, Dd, c, *tp, *td); break;
         case CONE_POS: *tp = posmaxstep(p, Dp, n); *td = posmaxstep(d, Dd, n); break;
         case CONE_SOC: *tp = socmaxstep(p, Dp, c[1], c[3], n); *td = socmaxstep(d, Dd, c[2], c[4], n); break;
@@ -271,8 +285,9 @@ static inline void cone_maxsteps(int k, double kp, int64_t n, const double* p, c
     }
 }
 // dual shadow d* = -f'(p)
-static inline bool cone_shadow(int k, double kp, int64_t n, double* s, const double* x, double* c) {
+static inline bool cone_shadow(int k, double kp, int64_t n, double* s, const double* x, double* c, double* work) {
     switch (k) {
+        case CONE_SDP: return sdp_shadow(s, x, n, work);
         case CONE_EXP: case CONE_POW: return tddualshadow(TD{k, kp}, s, x, c);
         case CONE_POS: for (int64_t i = 0; i < n; ++i) s[i] = 1.0 / x[i]; return true;  // pos.jl:198-204
         case CONE_SOC: return socshadow(s, x, n);
@@ -280,9 +295,9 @@ static inline bool cone_shadow(int k, double kp, int64_t n, double* s, const dou
     }
 }
 // primal shadow p*: -f'(p*) = d
-static inline bool cone_pshadow(int k, double kp, int64_t n, double* s, const double* x, double* c) {
+static inline bool cone_pshadow(int k, double kp, int64_t n, double* s, const double* x, double* c, double* work) {
     if (k == CONE_EXP || k == CONE_POW) return tdprimalshadow(TD{k, kp}, s, x, c);
-    return cone_shadow(k, kp, n, s, x, c);
+    return cone_shadow(k, kp, n, s, x, c, work);
 }
 static inline void cone_initcache(int k, double kp, int64_t, double* c) {
     if (k == CONE_EXP || k == CONE_POW) tdinitcache(TD{k, kp}, c);

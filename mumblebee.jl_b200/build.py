@@ -22,7 +22,7 @@ COMMON = ["-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-lineinfo"]
 
 SOURCES_CU = ["mb_solver.cu"]
 SOURCES_CPP = ["mb_host.cpp"]
-HEADERS = ["mb_internal.h", "mb_device.cuh", "mb_cones.cuh", "mb_tdc.cuh", "mb_symbolic.hpp"]
+HEADERS = ["mb_internal.h", "mb_device.cuh", "mb_cones.cuh", "mb_tdc.cuh", "mb_sdp.cuh", "mb_symbolic.hpp"]
 
 
 def _newer(target, deps):

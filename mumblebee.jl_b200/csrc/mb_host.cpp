@@ -153,12 +153,25 @@ struct Packed {
     }
 };
 
-// cachesize / workspacesize / degree  (soc.jl:116-134, tdc.jl:122-143, pos.jl:21-31, noc.jl:20-28)
+// cachesize / workspacesize / degree  (soc.jl:116-134, tdc.jl:122-143, pos.jl:21-31, noc.jl:20-28,
+// sdp.jl:41-70: an SDP block of svec length n has order d = triroot(n), cache R | S | s = 2d² + d,
+// workspace max(3d², 2d² + 2d))
+static int64_t triroot(i64 n) {
+    int64_t t = 1 + 8 * n, r = (int64_t)std::sqrt((double)t);
+    while (r * r > t) --r;
+    while ((r + 1) * (r + 1) <= t) ++r;
+    return (r - 1) / 2;
+}
 static int64_t cone_cachesize(int k, i64 n) {
+    if (k == MB_CONE_SDP) { int64_t d = triroot(n); return 2 * d * d + d; }
     return k == MB_CONE_SOC ? 5 + n : ((k == MB_CONE_EXP || k == MB_CONE_POW) ? 19 : 0);
 }
-static int64_t cone_workspacesize(int k, i64 n) { return k == MB_CONE_SOC ? 2 * n : 0; }
+static int64_t cone_workspacesize(int k, i64 n) {
+    if (k == MB_CONE_SDP) { int64_t d = triroot(n); return std::max<int64_t>(3 * d * d, 2 * d * d + 2 * d); }
+    return k == MB_CONE_SOC ? 2 * n : 0;
+}
 static int64_t cone_degree(int k, i64 n) {
+    if (k == MB_CONE_SDP) return triroot(n);
     return k == MB_CONE_POS ? n : (k == MB_CONE_SOC ? 2 : ((k == MB_CONE_EXP || k == MB_CONE_POW) ? 3 : 0));
 }
 
@@ -178,7 +191,9 @@ static int plan_instance(const mb_problem* P, const mb_settings& set, const doub
     ip.mut = P->mu;
     for (i64 v = 0; v < nv; ++v) {
         int k = P->kind[vp[v]];
-        if (k == MB_CONE_SDP) { err = "cone kind not supported by this build"; return MB_E_UNSUPPORTED; }
+        if (k == MB_CONE_SDP && triroot(B.ncols(v)) * (triroot(B.ncols(v)) + 1) / 2 != B.ncols(v)) {
+            err = "a semidefinite cone's dimension must be d(d+1)/2"; return MB_E_ARG;
+        }
         if ((k == MB_CONE_EXP || k == MB_CONE_POW) && B.ncols(v) != 3) { err = "exponential/power cones have dimension 3"; return MB_E_ARG; }
         if (k == MB_CONE_POW && !(P->param[vp[v]] > 0 && P->param[vp[v]] < 1)) { err = "PowerCone needs 0 < α < 1"; return MB_E_ARG; }
     }
@@ -1142,3 +1157,378 @@ extern "C" int mb_batch_solve_static(mb_ctx* ctx, mb_problem* const* probs, int3
                       d_out ? d_out[k] : nullptr, y_out ? y_out[k] : nullptr, results ? &results[k] : nullptr);
     return MB_OK;
 }
+
+// ---------------------------------------------------------------------------------------------
+// Serving loop: continuous batching of independent requests (no counterpart in the reference,
+// which solves one problem per call).  One device arena and one descriptor ring are allocated at
+// creation; requests are planned by a pool of host threads, admitted in arrival order while
+// their footprint fits the arena and a ring slot is free, published to the persistent serve
+// kernel (ipm_serve_kernel) on a copy stream, and collected as their done stamps appear, while
+// other requests keep running on the device.
+// ---------------------------------------------------------------------------------------------
+#include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <map>
+#include <mutex>
+#include <unordered_map>
+
+extern "C" int mb_launch_serve(const mb::ServeArgs* a, int grid, cudaStream_t stream);
+
+namespace {
+
+// first-fit allocator over [0, cap) in 256-byte granules, coalescing on release
+struct RangeAlloc {
+    std::map<size_t, size_t> fr;   // offset -> length
+    size_t cap = 0, used = 0;
+    void init(size_t c) { cap = c; fr.clear(); fr[0] = c; used = 0; }
+    static size_t round(size_t n) { return (std::max<size_t>(n, 1) + 255) / 256 * 256; }
+    bool alloc(size_t n, size_t& off) {
+        n = round(n);
+        for (auto it = fr.begin(); it != fr.end(); ++it)
+            if (it->second >= n) {
+                off = it->first;
+                size_t rest = it->second - n;
+                fr.erase(it);
+                if (rest) fr[off + n] = rest;
+                used += n;
+                return true;
+            }
+        return false;
+    }
+    void release(size_t off, size_t n) {
+        n = round(n);
+        used -= n;
+        auto it = fr.emplace(off, n).first;
+        auto nx = std::next(it);
+        if (nx != fr.end() && it->first + it->second == nx->first) { it->second += nx->second; fr.erase(nx); }
+        if (it != fr.begin()) {
+            auto pv = std::prev(it);
+            if (pv->first + pv->second == it->first) { pv->second += it->second; fr.erase(it); }
+        }
+    }
+};
+
+double now_s() {
+    using namespace std::chrono;
+    return duration<double>(steady_clock::now().time_since_epoch()).count();
+}
+
+enum ReqState { RQ_QUEUED = 0, RQ_PLANNED = 1, RQ_RUNNING = 2, RQ_DONE = 3, RQ_FAILED = 4 };
+
+struct Request {
+    int64_t ticket = 0;
+    mb_problem* prob = nullptr;
+    int state = RQ_QUEUED;
+    int rc = MB_OK;
+    std::string err;
+    Packed pk;
+    size_t bytes = 0, off = 0;
+    uint64_t seq = 0;
+    double t_submit = 0, t_admit = 0, t_done = 0;
+    std::vector<double> p, d, y;
+    mb_result res{};
+    int64_t dev_t0 = 0, dev_t1 = 0;
+};
+
+}  // namespace
+
+struct mb_server {
+    mb_ctx* ctx = nullptr;
+    mb_settings set{};
+    cudaStream_t kstream = nullptr, cstream = nullptr;
+    cudaEvent_t kevent = nullptr;
+    bool krunning = false;
+    int grid = 0;
+    char* d_arena = nullptr;
+    RangeAlloc arena;
+    mb::DevInst* d_ring = nullptr;
+    unsigned long long* d_ctrl = nullptr;
+    unsigned long long* h_done = nullptr;   // mapped
+    unsigned long long* dv_done = nullptr;  // its device alias
+    int cap = 0;
+    long long idle_ns = 0;
+    uint64_t next_seq = 0;
+    std::map<uint64_t, Request*> inflight;   // by seq
+    std::unordered_map<int64_t, std::unique_ptr<Request>> reqs;
+    std::deque<Request*> queued, planned;
+    int64_t next_ticket = 1;
+    int64_t nlaunch = 0, ncomplete = 0, nfail = 0;
+    double t0 = 0;
+    std::mutex mu;
+    std::condition_variable cv_plan, cv_done;
+    bool quit = false;
+    std::string fatal;
+    std::vector<std::thread> planners;
+    std::thread loop;
+
+    ~mb_server() {
+        {
+            std::lock_guard<std::mutex> lk(mu);
+            quit = true;
+        }
+        cv_plan.notify_all();
+        for (auto& t : planners) if (t.joinable()) t.join();
+        if (loop.joinable()) loop.join();
+        if (d_ctrl && cstream) {
+            unsigned long long one = 1;
+            cudaMemcpyAsync(d_ctrl + 2, &one, sizeof(one), cudaMemcpyHostToDevice, cstream);
+            cudaStreamSynchronize(cstream);
+        }
+        if (kstream) cudaStreamSynchronize(kstream);
+        cudaFree(d_arena); cudaFree(d_ring); cudaFree(d_ctrl);
+        if (h_done) cudaFreeHost(h_done);
+        if (kevent) cudaEventDestroy(kevent);
+        if (kstream) cudaStreamDestroy(kstream);
+        if (cstream) cudaStreamDestroy(cstream);
+    }
+
+    void plan_worker() {
+        for (;;) {
+            Request* r = nullptr;
+            {
+                std::unique_lock<std::mutex> lk(mu);
+                cv_plan.wait(lk, [&] { return quit || !queued.empty(); });
+                if (quit) return;
+                r = queued.front();
+                queued.pop_front();
+            }
+            std::string err;
+            Packed pk;
+            int rc = plan_instance(r->prob, set, nullptr, nullptr, nullptr, pk, err);
+            size_t bytes = rc ? 0 : StaticLayout(pk).total;
+            std::lock_guard<std::mutex> lk(mu);
+            if (rc) { r->rc = rc; r->err = err; r->state = RQ_FAILED; r->t_done = now_s() - t0; ++nfail; cv_done.notify_all(); continue; }
+            if (bytes > arena.cap) {
+                r->rc = MB_E_NOMEM; r->err = "request footprint exceeds the server arena"; r->state = RQ_FAILED;
+                r->t_done = now_s() - t0; ++nfail; cv_done.notify_all(); continue;
+            }
+            r->pk = std::move(pk);
+            r->bytes = bytes;
+            r->state = RQ_PLANNED;
+            planned.push_back(r);
+        }
+    }
+
+    // copy one planned request into the arena and publish it (caller holds mu)
+    int admit(Request* r) {
+        const StaticLayout L(r->pk);
+        char* base = d_arena + r->off;
+        int32_t* s_i32 = (int32_t*)(base + L.i32);
+        i64* s_i64 = (i64*)(base + L.i64a);
+        double* s_din = (double*)(base + L.din);
+        int32_t* s_ost = (int32_t*)(base + L.ost);
+        const InstPlan& ip = r->pk.plans[0];
+        mb::DevInst I = static_devinst(ip, s_i32, s_i64, s_din, (double*)(base + L.work), (double*)(base + L.out),
+                                       s_ost, base + L.F);
+        const Packed& pk = r->pk;
+        cudaError_t e = cudaSuccess;
+        if (pk.i32.size() && !e) e = cudaMemcpyAsync(s_i32, pk.i32.h.data(), pk.i32.size() * 4, cudaMemcpyHostToDevice, cstream);
+        if (pk.i64a.size() && !e) e = cudaMemcpyAsync(s_i64, pk.i64a.h.data(), pk.i64a.size() * 8, cudaMemcpyHostToDevice, cstream);
+        if (pk.din.size() && !e) e = cudaMemcpyAsync(s_din, pk.din.h.data(), pk.din.size() * 8, cudaMemcpyHostToDevice, cstream);
+        if (!e) e = cudaMemsetAsync(s_ost, 0, std::max<size_t>(pk.ost.size(), 1) * 4, cstream);
+        r->seq = next_seq;
+        if (!e) e = cudaMemcpyAsync(d_ring + r->seq % cap, &I, sizeof(I), cudaMemcpyHostToDevice, cstream);
+        unsigned long long tail = r->seq + 1;
+        if (!e) e = cudaMemcpyAsync(d_ctrl + 1, &tail, sizeof(tail), cudaMemcpyHostToDevice, cstream);
+        if (e) { fatal = std::string("serve publish: ") + cudaGetErrorString(e); return MB_E_CUDA; }
+        ++next_seq;
+        r->state = RQ_RUNNING;
+        r->t_admit = now_s() - t0;
+        inflight[r->seq] = r;
+        return MB_OK;
+    }
+
+    // copy one finished request's outputs back and release its arena (caller holds mu)
+    void collect(Request* r) {
+        const StaticLayout L(r->pk);
+        char* base = d_arena + r->off;
+        const Packed& pk = r->pk;
+        std::vector<double> h_out(std::max<size_t>(pk.out.size(), 1));
+        std::vector<int32_t> h_ost(std::max<size_t>(pk.ost.size(), 1));
+        cudaError_t e = cudaMemcpyAsync(h_out.data(), base + L.out, h_out.size() * 8, cudaMemcpyDeviceToHost, cstream);
+        if (!e) e = cudaMemcpyAsync(h_ost.data(), base + L.ost, h_ost.size() * 4, cudaMemcpyDeviceToHost, cstream);
+        if (!e) e = cudaStreamSynchronize(cstream);
+        const InstPlan& ip = pk.plans[0];
+        if (e) { r->rc = MB_E_CUDA; r->err = cudaGetErrorString(e); r->state = RQ_FAILED; ++nfail; }
+        else {
+            r->p.assign(ip.n, 0.0); r->d.assign(ip.n, 0.0); r->y.assign(ip.m, 0.0);
+            static_unpack(ip, h_out.data(), h_ost.data(), set.max_iter, r->p.data(), r->d.data(), r->y.data(), &r->res);
+            std::memcpy(&r->dev_t0, &h_out[ip.scal + mb::SCAL_T0], 8);
+            std::memcpy(&r->dev_t1, &h_out[ip.scal + mb::SCAL_T1], 8);
+            r->state = RQ_DONE;
+            ++ncomplete;
+        }
+        r->t_done = now_s() - t0;
+        arena.release(r->off, r->bytes);
+        r->pk = Packed();
+    }
+
+    void run_loop() {
+        cudaSetDevice(ctx->device);
+        for (;;) {
+            bool busy = false;
+            {
+                std::lock_guard<std::mutex> lk(mu);
+                if (quit && inflight.empty()) return;
+                // admit in planning order while the arena and the ring have room
+                while (!planned.empty() && fatal.empty()) {
+                    Request* r = planned.front();
+                    uint64_t oldest = inflight.empty() ? next_seq : inflight.begin()->first;
+                    if (next_seq - oldest >= (uint64_t)cap) break;
+                    if (!arena.alloc(r->bytes, r->off)) break;
+                    planned.pop_front();
+                    if (admit(r)) { arena.release(r->off, r->bytes); r->state = RQ_FAILED; r->rc = MB_E_CUDA; r->err = fatal; ++nfail; }
+                    busy = true;
+                }
+                // collect finished requests (any order)
+                for (auto it = inflight.begin(); it != inflight.end();) {
+                    Request* r = it->second;
+                    volatile unsigned long long* dn = h_done + r->seq % cap;
+                    if (*dn == r->seq + 1) {
+                        collect(r);
+                        it = inflight.erase(it);
+                        busy = true;
+                        cv_done.notify_all();
+                    } else ++it;
+                }
+                // (re)launch the persistent grid when work is published and the grid has exited
+                if (krunning && cudaEventQuery(kevent) != cudaErrorNotReady) {
+                    cudaError_t e = cudaEventQuery(kevent);
+                    krunning = false;
+                    if (e != cudaSuccess) fatal = std::string("serve kernel: ") + cudaGetErrorString(e);
+                }
+                if (!krunning && !inflight.empty() && fatal.empty()) {
+                    // the launch is ordered after the publishing copies so the first poll sees them
+                    cudaEvent_t pub;
+                    cudaEventCreateWithFlags(&pub, cudaEventDisableTiming);
+                    cudaEventRecord(pub, cstream);
+                    cudaStreamWaitEvent(kstream, pub, 0);
+                    cudaEventDestroy(pub);
+                    mb::ServeArgs a;
+                    a.ring = d_ring; a.ctrl = d_ctrl; a.done = dv_done; a.cap = cap; a.idle_ns = idle_ns;
+                    std::memcpy(&a.set, &set, sizeof(a.set));
+                    if (mb_launch_serve(&a, grid, kstream)) fatal = "serve kernel launch failed";
+                    else { cudaEventRecord(kevent, kstream); krunning = true; ++nlaunch; }
+                }
+                if (!fatal.empty()) {   // fail everything outstanding
+                    for (auto& kv : inflight) { kv.second->state = RQ_FAILED; kv.second->rc = MB_E_CUDA; kv.second->err = fatal; ++nfail; }
+                    inflight.clear();
+                    for (Request* r : planned) { r->state = RQ_FAILED; r->rc = MB_E_CUDA; r->err = fatal; ++nfail; }
+                    planned.clear();
+                    cv_done.notify_all();
+                    if (quit) return;
+                }
+            }
+            if (!busy) std::this_thread::sleep_for(std::chrono::microseconds(20));
+        }
+    }
+};
+
+extern "C" {
+
+int mb_server_create(mb_ctx* ctx, const mb_settings* settings, int64_t arena_bytes, int32_t capacity,
+                     int32_t nplanners, mb_server** out) {
+    if (!ctx || !out || arena_bytes <= 0 || capacity <= 0) return fail(ctx, MB_E_ARG, "bad arguments");
+    mb_settings s;
+    if (settings) s = *settings; else mb_settings_default(&s);
+    if (s.stable) return fail(ctx, MB_E_UNSUPPORTED, "stable=true (StableUzawaSolver) is not available");
+    if (s.precision < 0 || s.precision > 2) return fail(ctx, MB_E_ARG, "precision must be 0, 1 or 2");
+    auto sv = std::make_unique<mb_server>();
+    sv->ctx = ctx; sv->set = s; sv->cap = capacity; sv->idle_ns = 20000000;   // 20 ms
+    sv->grid = ctx->nsm * mb::CTA_PER_SM;
+    sv->t0 = now_s();
+    CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+    CUDA_TRY(ctx, cudaStreamCreateWithFlags(&sv->kstream, cudaStreamNonBlocking));
+    CUDA_TRY(ctx, cudaStreamCreateWithFlags(&sv->cstream, cudaStreamNonBlocking));
+    CUDA_TRY(ctx, cudaEventCreateWithFlags(&sv->kevent, cudaEventDisableTiming));
+    CUDA_TRY(ctx, cudaMalloc((void**)&sv->d_arena, (size_t)arena_bytes));
+    CUDA_TRY(ctx, cudaMalloc((void**)&sv->d_ring, sizeof(mb::DevInst) * capacity));
+    CUDA_TRY(ctx, cudaMalloc((void**)&sv->d_ctrl, 4 * sizeof(unsigned long long)));
+    CUDA_TRY(ctx, cudaMemset(sv->d_ctrl, 0, 4 * sizeof(unsigned long long)));
+    CUDA_TRY(ctx, cudaHostAlloc((void**)&sv->h_done, sizeof(unsigned long long) * capacity, cudaHostAllocMapped));
+    std::memset(sv->h_done, 0, sizeof(unsigned long long) * capacity);
+    CUDA_TRY(ctx, cudaHostGetDevicePointer((void**)&sv->dv_done, sv->h_done, 0));
+    sv->arena.init((size_t)arena_bytes);
+    int np = nplanners > 0 ? nplanners : (int)std::max(1u, std::thread::hardware_concurrency() / 2);
+    mb_server* raw = sv.get();
+    for (int t = 0; t < np; ++t) sv->planners.emplace_back([raw] { raw->plan_worker(); });
+    sv->loop = std::thread([raw] { raw->run_loop(); });
+    *out = sv.release();
+    return MB_OK;
+}
+
+int mb_server_submit(mb_server* s, mb_problem* prob, int64_t* ticket) {
+    if (!s || !prob || !ticket) return MB_E_ARG;
+    auto r = std::make_unique<Request>();
+    r->prob = prob;
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (!s->fatal.empty()) return fail(s->ctx, MB_E_CUDA, s->fatal);
+    r->ticket = s->next_ticket++;
+    r->t_submit = now_s() - s->t0;
+    *ticket = r->ticket;
+    s->queued.push_back(r.get());
+    s->reqs[r->ticket] = std::move(r);
+    s->cv_plan.notify_one();
+    return MB_OK;
+}
+
+int mb_server_poll(mb_server* s, int64_t ticket, int32_t* state) {
+    if (!s || !state) return MB_E_ARG;
+    std::lock_guard<std::mutex> lk(s->mu);
+    auto it = s->reqs.find(ticket);
+    if (it == s->reqs.end()) return MB_E_ARG;
+    *state = it->second->state;
+    return MB_OK;
+}
+
+int mb_server_wait(mb_server* s, int64_t ticket, double timeout_s, int32_t* state) {
+    if (!s || !state) return MB_E_ARG;
+    std::unique_lock<std::mutex> lk(s->mu);
+    auto it = s->reqs.find(ticket);
+    if (it == s->reqs.end()) return MB_E_ARG;
+    Request* r = it->second.get();
+    s->cv_done.wait_for(lk, std::chrono::duration<double>(std::max(0.0, timeout_s)),
+                        [&] { return r->state == RQ_DONE || r->state == RQ_FAILED; });
+    *state = r->state;
+    return MB_OK;
+}
+
+int mb_server_result(mb_server* s, int64_t ticket, double* p, double* d, double* y, mb_result* res, double* times5) {
+    if (!s) return MB_E_ARG;
+    std::unique_ptr<Request> r;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        auto it = s->reqs.find(ticket);
+        if (it == s->reqs.end()) return MB_E_ARG;
+        if (it->second->state != RQ_DONE && it->second->state != RQ_FAILED) return fail(s->ctx, MB_E_STATE, "request not finished");
+        r = std::move(it->second);
+        s->reqs.erase(it);
+    }
+    if (times5) {
+        times5[0] = r->t_submit; times5[1] = r->t_admit; times5[2] = r->t_done;
+        times5[3] = (double)r->dev_t0; times5[4] = (double)r->dev_t1;
+    }
+    if (r->state == RQ_FAILED) return fail(s->ctx, r->rc, r->err);
+    if (p) std::copy(r->p.begin(), r->p.end(), p);
+    if (d) std::copy(r->d.begin(), r->d.end(), d);
+    if (y) std::copy(r->y.begin(), r->y.end(), y);
+    if (res) *res = r->res;
+    return MB_OK;
+}
+
+int mb_server_stats(mb_server* s, int64_t* st) {
+    if (!s || !st) return MB_E_ARG;
+    std::lock_guard<std::mutex> lk(s->mu);
+    st[0] = (int64_t)s->queued.size(); st[1] = (int64_t)s->planned.size(); st[2] = (int64_t)s->inflight.size();
+    st[3] = s->ncomplete; st[4] = s->nfail; st[5] = s->nlaunch; st[6] = (int64_t)s->arena.used; st[7] = (int64_t)s->arena.cap;
+    return MB_OK;
+}
+
+int mb_server_destroy(mb_server* s) {
+    if (!s) return MB_E_ARG;
+    delete s;
+    return MB_OK;
+}
+
+}  // extern "C"

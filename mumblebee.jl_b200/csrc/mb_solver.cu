@@ -18,6 +18,7 @@
 #include "mb_device.cuh"
 #include "mb_cones.cuh"
 #include "mb_tdc.cuh"
+#include "mb_sdp.cuh"
 
 namespace mb {
 
@@ -482,6 +483,7 @@ struct Ctx {
                 __syncwarp();
                 continue;
             }
+            if (k == CONE_SDP) { w_sdpidentity(I.p + c0, nc); w_sdpidentity(I.d + c0, nc); continue; }
             w_identity(k, nc, I.p + c0);
             w_identity(k, nc, I.d + c0);
         }
@@ -521,7 +523,7 @@ struct Ctx {
                 sp = warp_sum(s);
             } else if (k == CONE_SOC) {
                 fl = w_socpoint(I.cache + I.cxblk[v], p, d, nc, sp);
-            } else if (k == CONE_EXP || k == CONE_POW) {
+            } else if (k == CONE_EXP || k == CONE_POW || k == CONE_SDP) {
                 continue;
             }
             if (lane == 0) { vflag[v] = fl ? 1.0 : 0.0; vspsd[v] = sp; }
@@ -534,6 +536,16 @@ struct Ctx {
             double sp = 0;
             bool fl = tdscale(TD{k, I.kpar[v]}, I.Hd + I.hdoff[v], I.p + c0, I.d + c0, I.cache + I.cxblk[v], sp);
             vflag[v] = fl ? 1.0 : 0.0; vspsd[v] = sp;
+        }
+        __syncthreads();
+        // semidefinite cones: the whole block per cone (sdp.jl:121-263)
+        for (int v = 0; v < nv; ++v) {
+            if (I.kind[v] != CONE_SDP) continue;
+            int c0 = I.xcol[v], nc = I.xcol[v + 1] - c0;
+            double sp = 0;
+            bool fl = b_sdpscale(I.Hd + I.hdoff[v], nc, I.cache + I.cxblk[v], I.p + c0, I.d + c0, I.work, sp,
+                                 SdpSh{red, &sh.flag});
+            if (threadIdx.x == 0) { vflag[v] = fl ? 1.0 : 0.0; vspsd[v] = sp; }
         }
         __syncthreads();
         // SOC Hessian blocks H = (2 (Jw)(Jw)ᵀ − J) / β² added in place (soc.jl:231-256)
@@ -571,6 +583,11 @@ struct Ctx {
             tdcorr(TD{k, I.kpar[v]}, fr + c0, I.p + c0, I.d + c0, Dpv + c0, Ddv + c0, sm, I.cache + I.cxblk[v]);
         }
         __syncthreads();
+        for (int v = 0; v < nv; ++v) {   // sdp.jl:293-431, the whole block per cone
+            if (I.kind[v] != CONE_SDP) continue;
+            int c0 = I.xcol[v], nc = I.xcol[v + 1] - c0;
+            b_sdpcorr(fr + c0, I.cache + I.cxblk[v], Dpv + c0, Ddv + c0, sm, nc, I.work);
+        }
     }
 
     __device__ void initpredictor(double* fr, double sm) {
@@ -593,6 +610,11 @@ struct Ctx {
             tdcorr0(fr + c0, I.d + c0, sm, I.cache + I.cxblk[v]);
         }
         __syncthreads();
+        for (int v = 0; v < nv; ++v) {   // sdp.jl:437-510
+            if (I.kind[v] != CONE_SDP) continue;
+            int c0 = I.xcol[v], nc = I.xcol[v + 1] - c0;
+            b_sdpcorr0(fr + c0, I.cache + I.cxblk[v], sm, nc, I.work);
+        }
     }
 
     __device__ double maxsteps(const double* Dpv, const double* Ddv, double step_frac) {
@@ -609,7 +631,7 @@ struct Ctx {
                 tp = w_socmaxstep(I.p + c0, Dpv + c0, c[1], c[3], nc);
                 td = w_socmaxstep(I.d + c0, Ddv + c0, c[2], c[4], nc);
             }
-            if (k == CONE_EXP || k == CONE_POW) continue;
+            if (k == CONE_EXP || k == CONE_POW || k == CONE_SDP) continue;
             if (k != CONE_FREE) { tp *= step_frac; td *= step_frac; }
             if (lane == 0) vstep[v] = jmin(tp, td);
         }
@@ -620,6 +642,16 @@ struct Ctx {
             double tp = 1, td = 1;
             tdmaxsteps(TD{k, I.kpar[v]}, I.p + c0, Dpv + c0, I.d + c0, Ddv + c0, I.cache + I.cxblk[v], tp, td);
             vstep[v] = jmin(tp * step_frac, td * step_frac);
+        }
+        __syncthreads();
+        for (int v = 0; v < nv; ++v) {   // sdp.jl:516-519: τp through R, τd through S and Σ
+            if (I.kind[v] != CONE_SDP) continue;
+            int c0 = I.xcol[v], nc = I.xcol[v + 1] - c0;
+            const double* c = I.cache + I.cxblk[v];
+            const int64_t dd = sdp_triroot(nc);
+            double tp = b_sdpmaxstep(c, Dpv + c0, nullptr, nc, I.work, SdpSh{red, &sh.flag});
+            double td = b_sdpmaxstep(c + dd * dd, Ddv + c0, c + 2 * dd * dd, nc, I.work, SdpSh{red, &sh.flag});
+            if (threadIdx.x == 0) vstep[v] = jmin(tp * step_frac, td * step_frac);
         }
         __syncthreads();
         double mn = __longlong_as_double(0x7ff0000000000000LL);
@@ -1220,7 +1252,16 @@ __device__ void solve_instance(const DevInst& I, const Settings& set, Shared& sh
                         }
                         __syncwarp();
                     }
+                    else if (k == CONE_SDP) {}
                     else { for (int i = lane; i < nc; i += 32) dst[i] = 0; }
+                }
+                __syncthreads();
+                for (int v = 0; v < I.nvtx; ++v) {   // sdpshadow! for either side (sdp.jl:640-705)
+                    if (I.kind[v] != CONE_SDP) continue;
+                    int c0 = I.xcol[v], nc = I.xcol[v + 1] - c0;
+                    double* dst = !I.has_d0 ? I.d + c0 : I.p + c0;
+                    const double* src = !I.has_d0 ? I.p + c0 : I.d + c0;
+                    b_sdpshadow(dst, src, nc, I.work, SdpSh{c.red, &sh.flag});
                 }
             }
             __syncthreads();
@@ -1282,7 +1323,59 @@ __global__ void __launch_bounds__(NT, CTA_PER_SM) ipm_batch_kernel(BatchArgs a) 
     }
 }
 
+// ---- serving loop (see ServeArgs) ----------------------------------------------------------
+__device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long* p) {
+    unsigned long long v;
+    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+constexpr long long SERVE_MAX_POLLS = 50000000;   // hard bound on one idle wait (≈ 100 s at 2 µs)
+
+__global__ void __launch_bounds__(NT, CTA_PER_SM) ipm_serve_kernel(ServeArgs a) {
+    __shared__ Shared sh;
+    __shared__ long long next;
+    for (;;) {
+        if (threadIdx.x == 0) {
+            long long got = -1;
+            const unsigned long long t_idle = globaltimer();
+            for (long long it = 0; it < SERVE_MAX_POLLS; ++it) {
+                unsigned long long t = ld_acquire_u64(&a.ctrl[1]);
+                unsigned long long h = ld_acquire_u64(&a.ctrl[0]);
+                if (h < t) {
+                    if (atomicCAS(&a.ctrl[0], h, h + 1) == h) { got = (long long)h; break; }
+                    continue;
+                }
+                if (ld_acquire_u64(&a.ctrl[2]) != 0) break;
+                if ((long long)(globaltimer() - t_idle) > a.idle_ns) break;
+                __nanosleep(2000);
+            }
+            __threadfence();
+            next = got;
+        }
+        __syncthreads();
+        const long long k = next;
+        __syncthreads();
+        if (k < 0) break;
+        const DevInst& I = a.ring[k % a.cap];
+        unsigned long long t0 = globaltimer();
+        solve_instance(I, a.set, sh, MODE_SOLVE);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            I.scal[SCAL_T0] = __longlong_as_double((long long)t0);
+            I.scal[SCAL_T1] = __longlong_as_double((long long)globaltimer());
+            __threadfence_system();
+            *(volatile unsigned long long*)&a.done[k % a.cap] = (unsigned long long)k + 1;
+        }
+        __syncthreads();
+    }
+}
+
 }  // namespace mb
+
+extern "C" int mb_launch_serve(const mb::ServeArgs* a, int grid, cudaStream_t stream) {
+    mb::ipm_serve_kernel<<<grid, mb::NT, 0, stream>>>(*a);
+    return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
 
 // ---------------------------------------------------------------------------------------------
 // launch entry used by the host runtime

@@ -80,6 +80,13 @@ SIGNATURES = {
     "mb_batch_timers": (I32, [C.c_void_p, PF64, I64]),
     "mb_batch_times": (I32, [C.c_void_p, PI64, I64]),
     "mb_batch_destroy": (I32, [C.c_void_p]),
+    "mb_server_create": (I32, [C.c_void_p, C.POINTER(mb_settings), I64, I32, I32, C.POINTER(C.c_void_p)]),
+    "mb_server_submit": (I32, [C.c_void_p, C.c_void_p, PI64]),
+    "mb_server_poll": (I32, [C.c_void_p, I64, PI32]),
+    "mb_server_wait": (I32, [C.c_void_p, I64, C.c_double, PI32]),
+    "mb_server_result": (I32, [C.c_void_p, I64, PF64, PF64, PF64, C.POINTER(mb_result), PF64]),
+    "mb_server_stats": (I32, [C.c_void_p, PI64]),
+    "mb_server_destroy": (I32, [C.c_void_p]),
     "mb_batch_solve_static": (I32, [C.c_void_p, C.POINTER(C.c_void_p), I32, C.POINTER(mb_settings), I32,
                                     C.POINTER(PF64), C.POINTER(PF64), C.POINTER(PF64), C.POINTER(mb_result)]),
 }

@@ -154,3 +154,76 @@ def exppow(nexp=3000, npow=1000, nfree=4000, npos=4000, m=5000, density=0.001, s
     c = A.T @ y0 + s0
     return dict(Q=sp.csc_matrix((n, n)), B=A, f=-c, g=b, mu=0.0, kinds=kinds, sizes=sizes, params=params,
                 name=f"exppow nexp={nexp} npow={npow} n={n} m={m} density={density} seed={seed}")
+
+
+def _svec(M):
+    d = M.shape[0]
+    r2 = np.sqrt(2.0)
+    return np.concatenate([[M[j, j]] + [r2 * M[i, j] for i in range(j + 1, d)] for j in range(d)])
+
+
+def _spd(rng, d):
+    A = rng.standard_normal((d, d))
+    return A @ A.T / d + np.eye(d)
+
+
+def sdp(nblocks=3, d=4, m=10, density=0.3, npos=0, seed=0):
+    """Random SDP with ``nblocks`` PSD blocks of order ``d`` (svec coordinates: column-major lower
+    triangle, off-diagonals scaled by √2, as SemidefiniteCone stores them) and ``npos`` nonnegative
+    columns; A sparse N(0,1) at the given density with every column covered.  Feasible by
+    construction: x0, s0 positive definite (A Aᵀ/d + I), y0 ~ N(0,1), b = A x0, c = Aᵀ y0 + s0."""
+    rng = np.random.default_rng(seed)
+    k = d * (d + 1) // 2
+    x0, s0, kinds, sizes = [], [], [], []
+    for _ in range(nblocks):
+        x0.append(_svec(_spd(rng, d))); s0.append(_svec(_spd(rng, d)))
+        kinds.append(CONE_SDP); sizes.append(k)
+    if npos:
+        x0.append(rng.uniform(0.5, 2.0, npos)); s0.append(rng.uniform(0.5, 2.0, npos))
+        kinds.append(CONE_POS); sizes.append(npos)
+    x0 = np.concatenate(x0); s0 = np.concatenate(s0)
+    n = len(x0)
+    A = sp.lil_matrix(sp.random(m, n, density=density, format="csc", random_state=rng,
+                                data_rvs=lambda s: rng.standard_normal(s)))
+    for j in np.where(np.diff(sp.csc_matrix(A).indptr) == 0)[0]:
+        A[int(rng.integers(m)), j] = rng.standard_normal()
+    A = sp.csc_matrix(A)
+    y0 = rng.standard_normal(m)
+    b = A @ x0
+    c = A.T @ y0 + s0
+    return dict(Q=sp.csc_matrix((n, n)), B=A, f=-c, g=b, mu=0.0, kinds=kinds, sizes=sizes,
+                params=[0.0] * len(kinds), name=f"sdp {nblocks}x PSD({d}) npos={npos} m={m} seed={seed}")
+
+
+def sdp_eigmin(d=5, seed=0):
+    """min ⟨C, X⟩ s.t. tr X = 1, X ⪰ 0: the optimum is λmin(C) (C symmetric N(0,1)); returns the
+    problem and that value."""
+    rng = np.random.default_rng(seed)
+    Cm = rng.standard_normal((d, d)); Cm = (Cm + Cm.T) / 2
+    k = d * (d + 1) // 2
+    B = sp.csc_matrix(_svec(np.eye(d)).reshape(1, k))
+    pb = dict(Q=sp.csc_matrix((k, k)), B=B, f=-_svec(Cm), g=np.array([1.0]), mu=0.0, kinds=[CONE_SDP], sizes=[k],
+              params=[0.0], name=f"sdp eigmin d={d} seed={seed}")
+    return pb, float(np.linalg.eigvalsh(Cm).min())
+
+
+def maxcut(nodes=12, extra=6, band=2, seed=0):
+    """Max-cut relaxation on a band graph (bandwidth ``band``) plus ``extra`` random edges, weights
+    U(0,1): max ¼⟨L, X⟩ s.t. diag(X) = 1, X ⪰ 0, written as min ⟨−L/4, X⟩ with one PSD block."""
+    rng = np.random.default_rng(seed)
+    W = np.zeros((nodes, nodes))
+    for i in range(nodes):
+        for j in range(i + 1, min(nodes, i + band + 1)):
+            W[i, j] = W[j, i] = rng.uniform()
+    for _ in range(extra):
+        i, j = rng.choice(nodes, 2, replace=False)
+        W[i, j] = W[j, i] = rng.uniform()
+    L = np.diag(W.sum(1)) - W
+    k = nodes * (nodes + 1) // 2
+    rows = []
+    for i in range(nodes):
+        E = np.zeros((nodes, nodes)); E[i, i] = 1.0
+        rows.append(_svec(E))
+    B = sp.csc_matrix(np.array(rows))
+    return dict(Q=sp.csc_matrix((k, k)), B=B, f=_svec(L / 4), g=np.ones(nodes), mu=0.0, kinds=[CONE_SDP],
+                sizes=[k], params=[0.0], name=f"maxcut nodes={nodes} band={band} extra={extra} seed={seed}")

@@ -508,3 +508,71 @@ def batch_solve_static(probs, settings: IPMSettings | None = None, grid: int = 0
     return [IPMResult(ps[i], ds[i], ys[i], IPMStatus(res[i].status), res[i].niter, res[i].nsolve, IPMHistory(),
                       res[i].mu, res[i].pres, res[i].dres, res[i].pobj, res[i].dobj, res[i].nfactor_retry,
                       res[i].nfactor, res[i].factor_flops, res[i].nfp32, res[i].nfallback) for i in range(k)]
+
+
+# ---------------------------------------------------------------------------------------- serving
+class Server:
+    """Continuous-batching request loop (mb_server_*): one device arena of ``arena_bytes`` and a ring
+    of ``capacity`` request slots feed a persistent solver grid; requests submitted while others are
+    on the device are admitted as memory and slots free up.  Keep each problem alive until its
+    result has been read."""
+
+    QUEUED, PLANNED, RUNNING, DONE, FAILED = range(5)
+
+    def __init__(self, settings: IPMSettings | None = None, arena_bytes: int = 8 << 30, capacity: int = 4096,
+                 planners: int = 0, ctx: Context | None = None):
+        self.ctx = ctx or Context.default()
+        self.L = self.ctx.L
+        self.settings = settings or IPMSettings()
+        self._cs = self.settings.to_c()
+        h = C.c_void_p()
+        check(self.L.mb_server_create(self.ctx.h, C.byref(self._cs), int(arena_bytes), int(capacity), int(planners),
+                                      C.byref(h)), self.ctx.h, "server create")
+        self.h = h
+        self._probs = {}
+
+    def submit(self, prob: IPMProblem) -> int:
+        t = C.c_int64()
+        check(self.L.mb_server_submit(self.h, prob.h, C.byref(t)), self.ctx.h, "server submit")
+        self._probs[t.value] = prob
+        return t.value
+
+    def state(self, ticket: int) -> int:
+        s = C.c_int32()
+        check(self.L.mb_server_poll(self.h, ticket, C.byref(s)), self.ctx.h, "server poll")
+        return s.value
+
+    def wait(self, ticket: int, timeout: float = 60.0) -> int:
+        s = C.c_int32()
+        check(self.L.mb_server_wait(self.h, ticket, float(timeout), C.byref(s)), self.ctx.h, "server wait")
+        return s.value
+
+    def result(self, ticket: int):
+        """IPMResult of a finished ticket and its times: (result, [submitted, admitted, finished] in
+        host seconds, (device start, device end) in ns).  Raises MBError for a failed request."""
+        prob = self._probs[ticket]
+        info = prob.info()
+        p, d, y = np.zeros(info["n"]), np.zeros(info["n"]), np.zeros(info["m"])
+        r = mb_result()
+        t = np.zeros(5)
+        rc = self.L.mb_server_result(self.h, ticket, _p(p, C.c_double), _p(d, C.c_double), _p(y, C.c_double),
+                                     C.byref(r), _p(t, C.c_double))
+        self._probs.pop(ticket, None)
+        check(rc, self.ctx.h, "server result")
+        res = IPMResult(p, d, y, IPMStatus(r.status), r.niter, r.nsolve, IPMHistory(), r.mu, r.pres, r.dres, r.pobj,
+                        r.dobj, r.nfactor_retry, r.nfactor, r.factor_flops, r.nfp32, r.nfallback)
+        return res, t[:3].tolist(), (int(t[3]), int(t[4]))
+
+    def stats(self):
+        a = np.zeros(8, np.int64)
+        check(self.L.mb_server_stats(self.h, _p(a, C.c_int64)), self.ctx.h, "server stats")
+        return dict(queued=int(a[0]), planned=int(a[1]), running=int(a[2]), completed=int(a[3]), failed=int(a[4]),
+                    launches=int(a[5]), arena_used=int(a[6]), arena_bytes=int(a[7]))
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.mb_server_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()

@@ -47,3 +47,11 @@ TDC = {
 # exponential / power cones stall in the certified line-search band just above a 1e-8 gap (the
 # reference's own power-cone examples run at 1e-5..1e-6); their parity runs use 1e-7
 TDC_TOL = dict(feas_tol=1e-7, gap_tol=1e-7)
+
+SDP = {
+    "sdp3x4": lambda: G.sdp(3, 4, 10, 0.3, 0, 0),
+    "sdp2x6_pos": lambda: G.sdp(2, 6, 15, 0.3, 5, 1),
+    "sdp4x3": lambda: G.sdp(4, 3, 12, 0.2, 0, 2),
+    "sdp1x10": lambda: G.sdp(1, 10, 20, 0.2, 0, 3),
+    "maxcut12": lambda: G.maxcut(12, 6, 2, 0),
+}

@@ -112,3 +112,39 @@ def test_exp_pow_matches_oracle(name):
     assert abs(r.niter - o["niter"]) <= 2
     assert _rel(r.pobj, o["pobj"]) < 1e-7 and _rel(r.dobj, o["dobj"]) < 1e-7
     assert r.pres < 1e-7 and r.dres < 1e-7
+
+
+@pytest.mark.parametrize("name", ["sdp3x4", "sdp2x6_pos", "sdp4x3", "sdp1x10", "maxcut12"])
+def test_sdp_matches_oracle(name):
+    """Semidefinite cones (sdp.jl): same status and iteration count as the oracle, objectives to
+    1e-9 relative, iterates to 1e-6 relative."""
+    from helpers import SDP
+    ref = block_problem(SDP[name]())
+    prob = _gpu_problem(ref)
+    _, o = oracle_solve(ref, vperm=prob.symbolic()["vperm"])
+    r = solve(prob, IPMSettings())
+    assert o["status"] == "OPTIMAL" and r.status == IPMStatus.OPTIMAL
+    assert r.niter == o["niter"]
+    assert _rel(r.pobj, o["pobj"]) < 1e-9 and _rel(r.dobj, o["dobj"]) < 1e-9
+    assert r.pres < 1e-8 and r.dres < 1e-8
+    for k in ("p", "d", "y"):
+        a, b = getattr(r, k), o[k]
+        assert np.linalg.norm(a - b) <= 1e-6 * max(1.0, np.linalg.norm(b)), k
+
+
+@pytest.mark.parametrize("d,seed", [(3, 0), (6, 1), (12, 2)])
+def test_sdp_eigmin_known_answer_on_device(d, seed):
+    pb, lam = G.sdp_eigmin(d, seed)
+    r = solve(_gpu_problem(block_problem(pb)), IPMSettings())
+    assert r.status == IPMStatus.OPTIMAL
+    assert abs(r.pobj - lam) <= 1e-7 * max(1.0, abs(lam))
+
+
+def test_sdp_batch_equals_alone():
+    from helpers import SDP
+    probs = [_gpu_problem(block_problem(SDP[k]())) for k in ("sdp3x4", "sdp2x6_pos", "maxcut12")]
+    alone = [solve(p, IPMSettings()) for p in probs]
+    many = batch_solve(probs, IPMSettings())
+    for a, b in zip(alone, many):
+        assert a.niter == b.niter and a.pobj == b.pobj
+        assert np.array_equal(a.p, b.p)

@@ -110,3 +110,32 @@ def test_eigmin_and_jacobi_svd(d):
     np.testing.assert_allclose(np.sort(sv), np.sort(np.linalg.svd(A, compute_uv=False)), rtol=1e-12)
     np.testing.assert_allclose(U.T @ U, np.eye(d), atol=1e-12)
     np.testing.assert_allclose(U.T @ A @ A.T @ U, np.diag(sv ** 2), atol=1e-10 * np.abs(A).max() ** 2 * d)
+
+
+# ----------------------------------------------------------------------------- whole solves
+from helpers import block_problem, oracle_solve          # noqa: E402
+from mumblebee_b200 import generators as G               # noqa: E402
+
+
+@pytest.mark.parametrize("d,seed", [(2, 0), (5, 1), (9, 2)])
+def test_oracle_sdp_eigmin_known_answer(d, seed):
+    pb, lam = G.sdp_eigmin(d, seed)
+    _, r = oracle_solve(block_problem(pb))
+    assert r["status"] == "OPTIMAL"
+    assert abs(r["pobj"] - lam) <= 1e-7 * max(1.0, abs(lam))
+
+
+@pytest.mark.parametrize("pb", [G.sdp(3, 4, 10, 0.3, 0, 0), G.sdp(2, 6, 15, 0.3, 5, 1), G.maxcut(12, 6, 2, 0)],
+                         ids=["sdp3x4", "sdp2x6_pos", "maxcut12"])
+def test_oracle_sdp_solves_to_optimal_psd_iterates(pb):
+    prob = block_problem(pb)
+    s, r = oracle_solve(prob)
+    assert r["status"] == "OPTIMAL"
+    assert r["pres"] < 1e-8 and r["dres"] < 1e-8
+    assert abs(r["pobj"] - r["dobj"]) <= 1e-8 * max(1.0, abs(r["pobj"]))
+    off = 0
+    for k, n in zip(pb["kinds"], pb["sizes"]):
+        if k == G.CONE_SDP:
+            for v in (r["p"], r["d"]):
+                assert np.linalg.eigvalsh(smat(v[off:off + n])).min() > -1e-8
+        off += n

@@ -57,6 +57,12 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-compare", action="store_true", help="skip the other precision's arm")
+    ap.add_argument("--no-serve", action="store_true", help="skip the serving arm")
+    ap.add_argument("--serve-rate", type=float, default=2000.0, help="offered requests per second")
+    ap.add_argument("--serve-seconds", type=float, default=1.0, help="length of the arrival window")
+    ap.add_argument("--serve-nmin", type=int, default=100)
+    ap.add_argument("--serve-nmax", type=int, default=2000)
+    ap.add_argument("--serve-arena-gb", type=int, default=32)
     return ap.parse_args()
 
 
@@ -271,6 +277,57 @@ def timed_arm(probs, precision, args, pg, local, ws, ctx):
     return out
 
 
+def serve_arm(args, ctx):
+    """Serving workload: distinct requests from the seeded SOCP / portfolio QP / max-cut SDP mix
+    (target n log-uniform in [serve_nmin, serve_nmax]) submitted to the continuous-batching server
+    on a Poisson schedule at the offered rate.  Latency = results ready − submitted, on the server's
+    host clock; solves/s = completed ÷ (last finish − first submit)."""
+    from mumblebee_b200 import generators as G
+    from mumblebee_b200.ipm import IPMProblem, IPMSettings, Server, _CONES
+    nreq = max(1, int(args.serve_rate * args.serve_seconds))
+    mix = G.serving_mix(nreq + 6, seed=args.seed + 7, nmin=args.serve_nmin, nmax=args.serve_nmax)
+    probs = [IPMProblem(pb["Q"], pb["B"], pb["f"], pb["g"], pb["mu"], [_CONES[k]() for k in pb["kinds"]],
+                        pb["sizes"], ctx=ctx) for _, pb in mix]
+    kinds = [k for k, _ in mix]
+    srv = Server(IPMSettings(precision=args.precision), arena_bytes=args.serve_arena_gb << 30, capacity=8192,
+                 planners=os.cpu_count() or 1, ctx=ctx)
+    for t in [srv.submit(p) for p in probs[nreq:]]:      # warm-up: module load, first launch
+        srv.wait(t, 600.0)
+        srv.result(t)
+    rng = np.random.default_rng(args.seed + 11)
+    arrivals = np.cumsum(rng.exponential(1.0 / args.serve_rate, nreq))
+    t0 = time.perf_counter()
+    tickets = []
+    for i in range(nreq):
+        while True:
+            dt = arrivals[i] - (time.perf_counter() - t0)
+            if dt <= 0:
+                break
+            if dt > 2e-3:
+                time.sleep(dt - 1e-3)
+        tickets.append(srv.submit(probs[i]))
+    lat, queue, ok, fin, sub = [], [], 0, [], []
+    for t, k in zip(tickets, kinds):
+        srv.wait(t, 3600.0)
+        r, tm, _ = srv.result(t)
+        lat.append(tm[2] - tm[0]); queue.append(tm[1] - tm[0]); fin.append(tm[2]); sub.append(tm[0])
+        ok += r.status.name == "OPTIMAL"
+    st = srv.stats()
+    srv.close()
+    lat = np.array(lat) * 1e3; queue = np.array(queue) * 1e3
+    span = max(fin) - min(sub)
+    sizes = [p.info()["n"] for p in probs[:nreq]]
+    return {"offered_req_per_s": args.serve_rate, "requests": nreq, "solves_per_s": nreq / span,
+            "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
+                           "max": float(lat.max())},
+            "admission_wait_ms": {"p50": float(np.percentile(queue, 50)), "p99": float(np.percentile(queue, 99))},
+            "optimal": f"{ok}/{nreq}", "grid_launches": st["launches"],
+            "mix": "equal shares SOCP (SOC(20) blocks, m = 0.4 n), portfolio QP, max-cut SDP (one PSD block)",
+            "sizes": f"target n log-uniform in [{args.serve_nmin}, {args.serve_nmax}], realised n in "
+                     f"[{min(sizes)}, {max(sizes)}], mean {float(np.mean(sizes)):.0f}",
+            "arena_gb": args.serve_arena_gb, "precision": args.precision}
+
+
 def main():
     args = parse()
     ws, rank, local, pg = dist_setup(args)
@@ -315,6 +372,9 @@ def main():
         st = main_arm["stats"]
         e2e = {"value": args.count * ws / dt, "unit": "solves/s", "h2d_bytes_per_step": st["input_bytes"],
                "d2h_bytes_per_step": st["output_bytes"]}
+    serve = None
+    if not args.no_serve:
+        serve = serve_arm(args, ctx)
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         cores = os.cpu_count() or 1
@@ -342,7 +402,7 @@ def main():
                            "optimal": f"{main_arm['optimal']}/{args.count}", "iters_mean": main_arm["iters_mean"],
                            "setup_s": {"generate": round(t_gen, 2), "prepare": round(main_arm["prepare_s"], 2)}},
                 "latency_ms": main_arm["latency_ms"], "solve_ms": main_arm["solve_ms"],
-                "precisions": arms,
+                "precisions": arms, "serving": serve,
                 "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": args.steps,
                 "clocks": main_arm["clocks"], "step_ms": main_arm["ms_steps"]}
         print(json.dumps(line), flush=True)

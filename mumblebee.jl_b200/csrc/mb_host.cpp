@@ -182,8 +182,18 @@ static int plan_instance(const mb_problem* P, const mb_settings& set, const doub
                          const double* y0, Packed& pk, std::string& err) {
     Sym sym = do_symbolic(P);
     const auto& vp = sym.vperm;
-    mbh::BSM B = mbh::selectvtxs(P->B, vp);
-    mbh::BSM Q = mbh::halfselectvtxs(mbh::halfselectvtxs(P->Q, vp), vp);
+    // with the identity order, selectvtxs is a copy, and the double transpose of halfselectvtxs
+    // returns Q itself when each column's arcs are already in ascending target order: skip them
+    bool ident = true;
+    for (size_t k = 0; k < vp.size() && ident; ++k) ident = vp[k] == (i64)k;
+    bool qsorted = ident;
+    for (i64 v = 0; v < P->Q.nvtx && qsorted; ++v)
+        for (i64 e = P->Q.xsrc[v] + 1; e < P->Q.xsrc[v + 1] && qsorted; ++e) qsorted = P->Q.tgt[e - 1] < P->Q.tgt[e];
+    mbh::BSM Bp, Qp;
+    if (!ident) Bp = mbh::selectvtxs(P->B, vp);
+    if (!qsorted) Qp = mbh::halfselectvtxs(mbh::halfselectvtxs(P->Q, vp), vp);
+    const mbh::BSM& B = ident ? P->B : Bp;
+    const mbh::BSM& Q = qsorted ? P->Q : Qp;
     const mbh::Fronts& fr = sym.fr;
     InstPlan ip;
     const i64 n = B.ncol, m = B.nrow, nv = B.nvtx;

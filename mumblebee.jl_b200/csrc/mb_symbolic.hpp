@@ -282,6 +282,28 @@ inline BSM halfselectvtxs(const BSM& A, const std::vector<i64>& sel) {
 // vertex adjacency: pattern of Q ∪ BᵀB  (IPM/src/utils.jl:135-145 weightedgraph), sorted lists
 inline std::vector<std::vector<i64>> vertex_graph(const BSM& B, const BSM& Q) {
     i64 nv = B.nvtx;
+    if (nv > 0 && nv <= 8192) {
+        // bitset form: a vertex's neighbours are the union of its rows' vertex sets
+        const i64 W = (nv + 63) / 64;
+        std::vector<uint64_t> rb((size_t)B.nout * W, 0), ab((size_t)W);
+        for (i64 v = 0; v < nv; ++v)
+            for (i64 e = B.xsrc[v]; e < B.xsrc[v + 1]; ++e) rb[(size_t)B.tgt[e] * W + (v >> 6)] |= 1ull << (v & 63);
+        std::vector<std::vector<i64>> adj(nv);
+        for (i64 v = 0; v < nv; ++v) {
+            std::fill(ab.begin(), ab.end(), 0ull);
+            for (i64 e = B.xsrc[v]; e < B.xsrc[v + 1]; ++e) {
+                const uint64_t* r = rb.data() + (size_t)B.tgt[e] * W;
+                for (i64 q = 0; q < W; ++q) ab[q] |= r[q];
+            }
+            ab[v >> 6] |= 1ull << (v & 63);
+            for (i64 e = Q.xsrc[v]; e < Q.xsrc[v + 1]; ++e) { i64 u = Q.tgt[e]; ab[u >> 6] |= 1ull << (u & 63); }
+            for (i64 q = 0; q < W; ++q) { uint64_t x = ab[q]; while (x) { int b = __builtin_ctzll(x); x &= x - 1; adj[v].push_back(q * 64 + b); } }
+        }
+        for (i64 v = 0; v < nv; ++v)   // Q pattern is used symmetrically
+            for (i64 e = Q.xsrc[v]; e < Q.xsrc[v + 1]; ++e) { i64 u = Q.tgt[e]; if (u != v) adj[u].push_back(v); }
+        for (auto& a : adj) { std::sort(a.begin(), a.end()); a.erase(std::unique(a.begin(), a.end()), a.end()); }
+        return adj;
+    }
     std::vector<std::vector<i64>> rows(B.nout), adj(nv);
     for (i64 v = 0; v < nv; ++v) for (i64 e = B.xsrc[v]; e < B.xsrc[v + 1]; ++e) rows[B.tgt[e]].push_back(v);
     std::vector<i64> mark(nv, -1);

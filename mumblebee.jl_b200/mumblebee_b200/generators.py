@@ -227,3 +227,28 @@ def maxcut(nodes=12, extra=6, band=2, seed=0):
     B = sp.csc_matrix(np.array(rows))
     return dict(Q=sp.csc_matrix((k, k)), B=B, f=_svec(L / 4), g=np.ones(nodes), mu=0.0, kinds=[CONE_SDP],
                 sizes=[k], params=[0.0], name=f"maxcut nodes={nodes} band={band} extra={extra} seed={seed}")
+
+
+def serving_mix(count, seed=0, nmin=100, nmax=2000):
+    """Request stream of the serving workload: ``count`` problems, in equal shares SOCP (``socp``,
+    SOC(20) blocks, m = 0.4 n, about 25 nonzeros per row), portfolio QP (``portfolio``) and max-cut
+    SDP (``maxcut``, one PSD block), each with a target size n log-uniform in [nmin, nmax]; every
+    request is a distinct seeded instance.  Returns (kind, problem) pairs."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(count):
+        n = float(np.exp(rng.uniform(np.log(nmin), np.log(nmax))))
+        kind = ("socp", "qp", "sdp")[i % 3]
+        s = int(rng.integers(1 << 31))
+        if kind == "socp":
+            ncone = max(1, int(round(n / 20)))
+            nn = 20 * ncone
+            m = max(4, int(0.4 * nn))
+            pb = socp(nn, m, ncone, density=min(0.5, 25.0 / nn), seed=s)
+        elif kind == "qp":
+            pb = portfolio(max(10, int(round((n - 21) / 2))), seed=s)
+        else:
+            nodes = max(4, int(round((np.sqrt(1 + 8 * n) - 1) / 2)))
+            pb = maxcut(nodes, extra=nodes // 2, band=2, seed=s)
+        out.append((kind, pb))
+    return out

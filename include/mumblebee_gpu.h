@@ -215,12 +215,13 @@ int mb_batch_solve_static(mb_ctx* ctx, mb_problem* const* probs, int32_t nprob, 
                           mb_result* results);
 
 /* Serving loop (continuous batching).  No counterpart in the reference, which solves one problem
- * per call: a server owns one device arena of `arena_bytes`, a ring of `capacity` request slots
- * and a persistent solver grid.  Requests are planned on `nplanners` host threads (0 = half the
- * cores), admitted in arrival order while their footprint (mb_problem_footprint plus alignment)
- * fits the arena and a slot is free, solved while other requests are on the device, and copied
- * back as they finish; results equal those of mb_batch_solve for the same problem.  The problem
- * must stay alive until its ticket has finished.  States: 0 queued, 1 planned, 2 running,
+ * per call: a server owns one device arena of `arena_bytes` and a ring of `capacity` request
+ * slots.  Requests are planned on `nplanners` host threads (0 = half the cores), admitted in
+ * arrival order while their footprint (mb_problem_footprint plus alignment) fits the arena and a
+ * slot is free, and launched in admission waves on a pool of streams, so they start on SMs as
+ * earlier requests' CTAs retire while those keep running; each is copied back as it finishes.
+ * Results equal those of mb_batch_solve for the same problem.  The problem must stay alive until
+ * its ticket has finished.  States: 0 queued, 1 planned, 2 running,
  * 3 done, 4 failed (mb_server_result returns the failure's code and message). */
 typedef struct mb_server mb_server;
 int mb_server_create(mb_ctx* ctx, const mb_settings* settings, int64_t arena_bytes, int32_t capacity,
@@ -233,7 +234,7 @@ int mb_server_wait(mb_server* s, int64_t ticket, double timeout_s, int32_t* stat
  * the ticket. */
 int mb_server_result(mb_server* s, int64_t ticket, double* p, double* d, double* y, mb_result* res,
                      double* times5);
-/* queued, planned, running, completed, failed, grid launches, arena bytes in use, arena bytes */
+/* queued, planned, running, completed, failed, kernel launches, arena bytes in use, arena bytes */
 int mb_server_stats(mb_server* s, int64_t* stats8);
 int mb_server_destroy(mb_server* s);
 

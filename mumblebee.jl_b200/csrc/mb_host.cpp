@@ -1171,10 +1171,11 @@ extern "C" int mb_batch_solve_static(mb_ctx* ctx, mb_problem* const* probs, int3
 // ---------------------------------------------------------------------------------------------
 // Serving loop: continuous batching of independent requests (no counterpart in the reference,
 // which solves one problem per call).  One device arena and one descriptor ring are allocated at
-// creation; requests are planned by a pool of host threads, admitted in arrival order while
-// their footprint fits the arena and a ring slot is free, published to the persistent serve
-// kernel (ipm_serve_kernel) on a copy stream, and collected as their done stamps appear, while
-// other requests keep running on the device.
+// creation; requests are planned by a pool of host threads, admitted in arrival order while their
+// footprint fits the arena and a ring slot is free, and launched in admission waves, each on an
+// idle stream of a pool, so that new requests start on SMs as soon as earlier requests' CTAs
+// retire while those keep running.  Each instance stamps its completion into mapped host memory;
+// results are copied back as the stamps appear.  No kernel waits on the host or on another kernel.
 // ---------------------------------------------------------------------------------------------
 #include <chrono>
 #include <condition_variable>
@@ -1183,7 +1184,8 @@ extern "C" int mb_batch_solve_static(mb_ctx* ctx, mb_problem* const* probs, int3
 #include <mutex>
 #include <unordered_map>
 
-extern "C" int mb_launch_serve(const mb::ServeArgs* a, int grid, cudaStream_t stream);
+extern "C" int mb_launch_wave(const mb::DevInst* d_inst, int ninst, const mb::Settings* set, int* d_counter, int grid,
+                              unsigned long long* done, long long seq0, int cap, cudaStream_t stream);
 
 namespace {
 
@@ -1241,23 +1243,27 @@ struct Request {
     int64_t dev_t0 = 0, dev_t1 = 0;
 };
 
+constexpr int SERVE_STREAMS = 64;
+
 }  // namespace
 
 struct mb_server {
     mb_ctx* ctx = nullptr;
     mb_settings set{};
-    cudaStream_t kstream = nullptr, cstream = nullptr;
-    cudaEvent_t kevent = nullptr;
-    bool krunning = false;
-    int grid = 0;
+    cudaStream_t cstream = nullptr;
+    cudaStream_t ks[SERVE_STREAMS] = {};
+    cudaEvent_t klast[SERVE_STREAMS] = {};   // last launch on each stream
+    bool kused[SERVE_STREAMS] = {};
+    cudaEvent_t evpub = nullptr;
+    int rr = 0;
+    int grid_max = 0;
     char* d_arena = nullptr;
     RangeAlloc arena;
     mb::DevInst* d_ring = nullptr;
-    unsigned long long* d_ctrl = nullptr;
-    unsigned long long* h_done = nullptr;   // mapped
-    unsigned long long* dv_done = nullptr;  // its device alias
+    int* d_cnt = nullptr;                    // one work counter per stream
+    unsigned long long* h_done = nullptr;    // mapped
+    unsigned long long* dv_done = nullptr;   // its device alias
     int cap = 0;
-    long long idle_ns = 0;
     uint64_t next_seq = 0;
     std::map<uint64_t, Request*> inflight;   // by seq
     std::unordered_map<int64_t, std::unique_ptr<Request>> reqs;
@@ -1280,16 +1286,15 @@ struct mb_server {
         cv_plan.notify_all();
         for (auto& t : planners) if (t.joinable()) t.join();
         if (loop.joinable()) loop.join();
-        if (d_ctrl && cstream) {
-            unsigned long long one = 1;
-            cudaMemcpyAsync(d_ctrl + 2, &one, sizeof(one), cudaMemcpyHostToDevice, cstream);
-            cudaStreamSynchronize(cstream);
-        }
-        if (kstream) cudaStreamSynchronize(kstream);
-        cudaFree(d_arena); cudaFree(d_ring); cudaFree(d_ctrl);
+        for (int i = 0; i < SERVE_STREAMS; ++i) if (ks[i]) cudaStreamSynchronize(ks[i]);
+        if (cstream) cudaStreamSynchronize(cstream);
+        cudaFree(d_arena); cudaFree(d_ring); cudaFree(d_cnt);
         if (h_done) cudaFreeHost(h_done);
-        if (kevent) cudaEventDestroy(kevent);
-        if (kstream) cudaStreamDestroy(kstream);
+        for (int i = 0; i < SERVE_STREAMS; ++i) {
+            if (klast[i]) cudaEventDestroy(klast[i]);
+            if (ks[i]) cudaStreamDestroy(ks[i]);
+        }
+        if (evpub) cudaEventDestroy(evpub);
         if (cstream) cudaStreamDestroy(cstream);
     }
 
@@ -1320,17 +1325,16 @@ struct mb_server {
         }
     }
 
-    // copy one planned request into the arena and publish it (caller holds mu)
-    int admit(Request* r) {
+    // copy one planned request into the arena and its ring slot (caller holds mu)
+    int stage(Request* r) {
         const StaticLayout L(r->pk);
         char* base = d_arena + r->off;
         int32_t* s_i32 = (int32_t*)(base + L.i32);
         i64* s_i64 = (i64*)(base + L.i64a);
         double* s_din = (double*)(base + L.din);
         int32_t* s_ost = (int32_t*)(base + L.ost);
-        const InstPlan& ip = r->pk.plans[0];
-        mb::DevInst I = static_devinst(ip, s_i32, s_i64, s_din, (double*)(base + L.work), (double*)(base + L.out),
-                                       s_ost, base + L.F);
+        mb::DevInst I = static_devinst(r->pk.plans[0], s_i32, s_i64, s_din, (double*)(base + L.work),
+                                       (double*)(base + L.out), s_ost, base + L.F);
         const Packed& pk = r->pk;
         cudaError_t e = cudaSuccess;
         if (pk.i32.size() && !e) e = cudaMemcpyAsync(s_i32, pk.i32.h.data(), pk.i32.size() * 4, cudaMemcpyHostToDevice, cstream);
@@ -1339,14 +1343,40 @@ struct mb_server {
         if (!e) e = cudaMemsetAsync(s_ost, 0, std::max<size_t>(pk.ost.size(), 1) * 4, cstream);
         r->seq = next_seq;
         if (!e) e = cudaMemcpyAsync(d_ring + r->seq % cap, &I, sizeof(I), cudaMemcpyHostToDevice, cstream);
-        unsigned long long tail = r->seq + 1;
-        if (!e) e = cudaMemcpyAsync(d_ctrl + 1, &tail, sizeof(tail), cudaMemcpyHostToDevice, cstream);
-        if (e) { fatal = std::string("serve publish: ") + cudaGetErrorString(e); return MB_E_CUDA; }
+        if (e) { fatal = std::string("serve staging: ") + cudaGetErrorString(e); return MB_E_CUDA; }
         ++next_seq;
         r->state = RQ_RUNNING;
         r->t_admit = now_s() - t0;
         inflight[r->seq] = r;
         return MB_OK;
+    }
+
+    // launch ring slots [s0, s1) on an idle stream after the staging copies (caller holds mu)
+    void launch(uint64_t s0, uint64_t s1) {
+        if (cudaEventRecord(evpub, cstream) != cudaSuccess) { fatal = "serve: event record failed"; return; }
+        int k = -1;
+        for (int t = 0; t < SERVE_STREAMS && k < 0; ++t) {
+            int i = (rr + t) % SERVE_STREAMS;
+            if (!kused[i] || cudaEventQuery(klast[i]) == cudaSuccess) k = i;
+        }
+        if (k < 0) k = rr % SERVE_STREAMS;   // every stream busy: queue behind the oldest choice
+        rr = (k + 1) % SERVE_STREAMS;
+        cudaStreamWaitEvent(ks[k], evpub, 0);
+        mb::Settings ds;
+        std::memcpy(&ds, &set, sizeof(ds));
+        while (s0 < s1) {   // one launch per contiguous run of ring slots
+            uint64_t end = std::min<uint64_t>(s1, (s0 / cap + 1) * (uint64_t)cap);
+            int n = (int)(end - s0);
+            int g = std::min(n, grid_max);
+            if (mb_launch_wave(d_ring + s0 % cap, n, &ds, d_cnt + k, g, dv_done, (long long)s0, cap, ks[k])) {
+                fatal = std::string("serve launch: ") + cudaGetErrorString(cudaGetLastError());
+                return;
+            }
+            ++nlaunch;
+            s0 = end;
+        }
+        cudaEventRecord(klast[k], ks[k]);
+        kused[k] = true;
     }
 
     // copy one finished request's outputs back and release its arena (caller holds mu)
@@ -1380,17 +1410,7 @@ struct mb_server {
             bool busy = false;
             {
                 std::lock_guard<std::mutex> lk(mu);
-                if (quit && inflight.empty()) return;
-                // admit in planning order while the arena and the ring have room
-                while (!planned.empty() && fatal.empty()) {
-                    Request* r = planned.front();
-                    uint64_t oldest = inflight.empty() ? next_seq : inflight.begin()->first;
-                    if (next_seq - oldest >= (uint64_t)cap) break;
-                    if (!arena.alloc(r->bytes, r->off)) break;
-                    planned.pop_front();
-                    if (admit(r)) { arena.release(r->off, r->bytes); r->state = RQ_FAILED; r->rc = MB_E_CUDA; r->err = fatal; ++nfail; }
-                    busy = true;
-                }
+                if (quit && inflight.empty() && planned.empty()) return;
                 // collect finished requests (any order)
                 for (auto it = inflight.begin(); it != inflight.end();) {
                     Request* r = it->second;
@@ -1402,25 +1422,24 @@ struct mb_server {
                         cv_done.notify_all();
                     } else ++it;
                 }
-                // (re)launch the persistent grid when work is published and the grid has exited
-                if (krunning && cudaEventQuery(kevent) != cudaErrorNotReady) {
-                    cudaError_t e = cudaEventQuery(kevent);
-                    krunning = false;
-                    if (e != cudaSuccess) fatal = std::string("serve kernel: ") + cudaGetErrorString(e);
+                // a failed launch shows up as an error on its stream's event
+                for (int i = 0; i < SERVE_STREAMS && fatal.empty(); ++i)
+                    if (kused[i]) {
+                        cudaError_t e = cudaEventQuery(klast[i]);
+                        if (e != cudaSuccess && e != cudaErrorNotReady) fatal = std::string("serve kernel: ") + cudaGetErrorString(e);
+                    }
+                // admit in planning order while the arena and the ring have room, then launch the wave
+                uint64_t s0 = next_seq;
+                while (!planned.empty() && fatal.empty()) {
+                    Request* r = planned.front();
+                    uint64_t oldest = inflight.empty() ? next_seq : inflight.begin()->first;
+                    if (next_seq - oldest >= (uint64_t)cap) break;
+                    if (!arena.alloc(r->bytes, r->off)) break;
+                    planned.pop_front();
+                    if (stage(r)) { arena.release(r->off, r->bytes); r->state = RQ_FAILED; r->rc = MB_E_CUDA; r->err = fatal; ++nfail; }
+                    busy = true;
                 }
-                if (!krunning && !inflight.empty() && fatal.empty()) {
-                    // the launch is ordered after the publishing copies so the first poll sees them
-                    cudaEvent_t pub;
-                    cudaEventCreateWithFlags(&pub, cudaEventDisableTiming);
-                    cudaEventRecord(pub, cstream);
-                    cudaStreamWaitEvent(kstream, pub, 0);
-                    cudaEventDestroy(pub);
-                    mb::ServeArgs a;
-                    a.ring = d_ring; a.ctrl = d_ctrl; a.done = dv_done; a.cap = cap; a.idle_ns = idle_ns;
-                    std::memcpy(&a.set, &set, sizeof(a.set));
-                    if (mb_launch_serve(&a, grid, kstream)) fatal = "serve kernel launch failed";
-                    else { cudaEventRecord(kevent, kstream); krunning = true; ++nlaunch; }
-                }
+                if (next_seq > s0 && fatal.empty()) launch(s0, next_seq);
                 if (!fatal.empty()) {   // fail everything outstanding
                     for (auto& kv : inflight) { kv.second->state = RQ_FAILED; kv.second->rc = MB_E_CUDA; kv.second->err = fatal; ++nfail; }
                     inflight.clear();
@@ -1445,17 +1464,19 @@ int mb_server_create(mb_ctx* ctx, const mb_settings* settings, int64_t arena_byt
     if (s.stable) return fail(ctx, MB_E_UNSUPPORTED, "stable=true (StableUzawaSolver) is not available");
     if (s.precision < 0 || s.precision > 2) return fail(ctx, MB_E_ARG, "precision must be 0, 1 or 2");
     auto sv = std::make_unique<mb_server>();
-    sv->ctx = ctx; sv->set = s; sv->cap = capacity; sv->idle_ns = 20000000;   // 20 ms
-    sv->grid = ctx->nsm * mb::CTA_PER_SM;
+    sv->ctx = ctx; sv->set = s; sv->cap = capacity;
+    sv->grid_max = ctx->nsm * mb::CTA_PER_SM;
     sv->t0 = now_s();
     CUDA_TRY(ctx, cudaSetDevice(ctx->device));
-    CUDA_TRY(ctx, cudaStreamCreateWithFlags(&sv->kstream, cudaStreamNonBlocking));
     CUDA_TRY(ctx, cudaStreamCreateWithFlags(&sv->cstream, cudaStreamNonBlocking));
-    CUDA_TRY(ctx, cudaEventCreateWithFlags(&sv->kevent, cudaEventDisableTiming));
+    for (int i = 0; i < SERVE_STREAMS; ++i) {
+        CUDA_TRY(ctx, cudaStreamCreateWithFlags(&sv->ks[i], cudaStreamNonBlocking));
+        CUDA_TRY(ctx, cudaEventCreateWithFlags(&sv->klast[i], cudaEventDisableTiming));
+    }
+    CUDA_TRY(ctx, cudaEventCreateWithFlags(&sv->evpub, cudaEventDisableTiming));
     CUDA_TRY(ctx, cudaMalloc((void**)&sv->d_arena, (size_t)arena_bytes));
     CUDA_TRY(ctx, cudaMalloc((void**)&sv->d_ring, sizeof(mb::DevInst) * capacity));
-    CUDA_TRY(ctx, cudaMalloc((void**)&sv->d_ctrl, 4 * sizeof(unsigned long long)));
-    CUDA_TRY(ctx, cudaMemset(sv->d_ctrl, 0, 4 * sizeof(unsigned long long)));
+    CUDA_TRY(ctx, cudaMalloc((void**)&sv->d_cnt, sizeof(int) * SERVE_STREAMS));
     CUDA_TRY(ctx, cudaHostAlloc((void**)&sv->h_done, sizeof(unsigned long long) * capacity, cudaHostAllocMapped));
     std::memset(sv->h_done, 0, sizeof(unsigned long long) * capacity);
     CUDA_TRY(ctx, cudaHostGetDevicePointer((void**)&sv->dv_done, sv->h_done, 0));

@@ -115,19 +115,5 @@ constexpr int NSTAT = 8;    // status, history rows, factor retries, factorizati
 // kernel modes: a full solve, or the pieces used by the step-wise API
 enum Mode { MODE_SOLVE = 0, MODE_INIT = 1, MODE_STEP = 2, MODE_RESULT = 3 };
 
-// Serving loop (continuous batching): a persistent grid claims published requests from a ring of
-// descriptors.  The host publishes request `seq` by copying its arrays and ring[seq % cap], then
-// the new count `tail`, on one copy stream (stream order makes the data visible first).  A CTA
-// claims with a CAS on `head`, solves, and writes seq + 1 to done[seq % cap] (mapped host memory)
-// after a system-scope fence.  An idle CTA waits at most idle_ns (and a fixed number of polls),
-// then exits; the host relaunches the grid when work is published and the grid has exited.
-struct ServeArgs {
-    const DevInst* ring;              // cap descriptors (device memory)
-    unsigned long long* ctrl;         // device: [0] head (claimed count), [1] tail (published), [2] stop
-    unsigned long long* done;         // mapped host memory, cap entries
-    int cap;
-    long long idle_ns;
-    Settings set;
-};
 
 }  // namespace mb

@@ -1303,6 +1303,11 @@ struct BatchArgs {
     int mode;
     Settings set;
     int* counter;     // work queue head
+    // optional per-instance completion stamps (serving loop): done[(seq0 + k) % cap] = seq0 + k + 1,
+    // written to mapped host memory after a system-scope fence
+    unsigned long long* done;
+    long long seq0;
+    int cap;
 };
 
 __global__ void __launch_bounds__(NT, CTA_PER_SM) ipm_batch_kernel(BatchArgs a) {
@@ -1319,63 +1324,16 @@ __global__ void __launch_bounds__(NT, CTA_PER_SM) ipm_batch_kernel(BatchArgs a) 
         if (threadIdx.x == 0) {
             a.inst[k].scal[SCAL_T0] = __longlong_as_double((long long)t0);
             a.inst[k].scal[SCAL_T1] = __longlong_as_double((long long)globaltimer());
-        }
-    }
-}
-
-// ---- serving loop (see ServeArgs) ----------------------------------------------------------
-__device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long* p) {
-    unsigned long long v;
-    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
-    return v;
-}
-constexpr long long SERVE_MAX_POLLS = 50000000;   // hard bound on one idle wait (≈ 100 s at 2 µs)
-
-__global__ void __launch_bounds__(NT, CTA_PER_SM) ipm_serve_kernel(ServeArgs a) {
-    __shared__ Shared sh;
-    __shared__ long long next;
-    for (;;) {
-        if (threadIdx.x == 0) {
-            long long got = -1;
-            const unsigned long long t_idle = globaltimer();
-            for (long long it = 0; it < SERVE_MAX_POLLS; ++it) {
-                unsigned long long t = ld_acquire_u64(&a.ctrl[1]);
-                unsigned long long h = ld_acquire_u64(&a.ctrl[0]);
-                if (h < t) {
-                    if (atomicCAS(&a.ctrl[0], h, h + 1) == h) { got = (long long)h; break; }
-                    continue;
-                }
-                if (ld_acquire_u64(&a.ctrl[2]) != 0) break;
-                if ((long long)(globaltimer() - t_idle) > a.idle_ns) break;
-                __nanosleep(2000);
+            if (a.done) {
+                __threadfence_system();
+                const long long seq = a.seq0 + k;
+                *(volatile unsigned long long*)&a.done[seq % a.cap] = (unsigned long long)seq + 1;
             }
-            __threadfence();
-            next = got;
         }
-        __syncthreads();
-        const long long k = next;
-        __syncthreads();
-        if (k < 0) break;
-        const DevInst& I = a.ring[k % a.cap];
-        unsigned long long t0 = globaltimer();
-        solve_instance(I, a.set, sh, MODE_SOLVE);
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            I.scal[SCAL_T0] = __longlong_as_double((long long)t0);
-            I.scal[SCAL_T1] = __longlong_as_double((long long)globaltimer());
-            __threadfence_system();
-            *(volatile unsigned long long*)&a.done[k % a.cap] = (unsigned long long)k + 1;
-        }
-        __syncthreads();
     }
 }
 
 }  // namespace mb
-
-extern "C" int mb_launch_serve(const mb::ServeArgs* a, int grid, cudaStream_t stream) {
-    mb::ipm_serve_kernel<<<grid, mb::NT, 0, stream>>>(*a);
-    return cudaGetLastError() == cudaSuccess ? 0 : -2;
-}
 
 // ---------------------------------------------------------------------------------------------
 // launch entry used by the host runtime
@@ -1384,6 +1342,7 @@ extern "C" int mb_launch_batch(const mb::DevInst* d_inst, int ninst, int mode, c
                                int* d_counter, int grid, int fp32, cudaStream_t stream) {
     mb::BatchArgs a;
     a.inst = d_inst; a.ninst = ninst; a.mode = mode; a.set = *set; a.counter = d_counter;
+    a.done = nullptr; a.seq0 = 0; a.cap = 1;
     cudaError_t e = cudaMemsetAsync(d_counter, 0, sizeof(int), stream);
     if (e != cudaSuccess) return -1;
     (void)fp32;
@@ -1433,4 +1392,17 @@ extern "C" int mb_static_scratch(int device, void** ptr, size_t* bytes) {
     *ptr = addr[device];
     *bytes = sizeof(mb_static_scratch_buf);
     return (int)cudaSuccess;
+}
+
+// the serving loop's launch: one admission wave of ring slots [seq0, seq0 + ninst), each instance
+// stamping done[(seq0 + k) % cap] when it finishes
+extern "C" int mb_launch_wave(const mb::DevInst* d_inst, int ninst, const mb::Settings* set, int* d_counter, int grid,
+                              unsigned long long* done, long long seq0, int cap, cudaStream_t stream) {
+    mb::BatchArgs a;
+    a.inst = d_inst; a.ninst = ninst; a.mode = mb::MODE_SOLVE; a.set = *set; a.counter = d_counter;
+    a.done = done; a.seq0 = seq0; a.cap = cap;
+    cudaError_t e = cudaMemsetAsync(d_counter, 0, sizeof(int), stream);
+    if (e != cudaSuccess) return -1;
+    mb::ipm_batch_kernel<<<grid, mb::NT, 0, stream>>>(a);
+    return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }

@@ -83,7 +83,7 @@ def test_oversize_request_fails_and_server_goes_on():
     srv.close()
 
 
-def test_idle_grid_exits_and_is_relaunched():
+def test_requests_after_a_lull_are_served():
     ctx = Context.default(0)
     p = product_problem(TDC["exp_small"](), ctx=ctx)
     s = IPMSettings(**TDC_TOL)
@@ -91,7 +91,7 @@ def test_idle_grid_exits_and_is_relaunched():
     t1 = srv.submit(p)
     assert srv.wait(t1, 60.0) == Server.DONE
     r1 = srv.result(t1)[0]
-    time.sleep(0.2)                           # longer than the grid's idle limit
+    time.sleep(0.2)                           # nothing on the device in between
     t2 = srv.submit(p)
     assert srv.wait(t2, 60.0) == Server.DONE
     r2 = srv.result(t2)[0]

@@ -25,6 +25,8 @@ namespace mb {
 constexpr int TS = 64;   // trailing-update tile
 constexpr int TLD = 36;  // tile row stride (doubles): 8-byte fragment loads of 8 rows x 4 columns hit 32 distinct banks
 
+// Block-shared scratch (dynamic shared memory: it exceeds the 48 KB static limit).  ta/tb and
+// ta2/tb2 are the two stages of the double-buffered tiles of the FP64 front update.
 struct Shared {
     double red[NW + 2];
     double diag[32 * 33];
@@ -32,6 +34,8 @@ struct Shared {
     double acc[32];
     double ta[TS * TLD];
     double tb[TS * TLD];
+    double ta2[TS * TLD];
+    double tb2[TS * TLD];
     int flag;
     int ibuf[8];
 };
@@ -155,14 +159,13 @@ __device__ void syrk_update<float>(float* M, int nf, int k0, int kb, int j0, Sha
     }
 }
 
+// Factor the kb x kb diagonal block at k0 (warp 0) and solve the panel below it:
+// L21 = A21 L11^{-T} for rows [k0 + kb, nf).  Returns the failing pivot (1-based in the front) or 0.
 template <class FT>
-__device__ int front_chol(FT* M, int nf, int nres, Shared& sh) {
+__device__ int diag_panel(FT* M, int nf, int k0, int kb, Shared& sh) {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     FT* S = reinterpret_cast<FT*>(sh.diag);
-    FT* ta = reinterpret_cast<FT*>(sh.ta);
-    FT* tb = reinterpret_cast<FT*>(sh.tb);
-    for (int k0 = 0; k0 < nres; k0 += 32) {
-        const int kb = min(32, nres - k0);
+    {
         if (warp == 0) {
             if (lane < kb)
                 for (int c = 0; c <= lane; ++c) S[lane * 33 + c] = M[(k0 + lane) + (int64_t)(k0 + c) * nf];
@@ -211,9 +214,132 @@ __device__ int front_chol(FT* M, int nf, int nres, Shared& sh) {
             for (int c = 0; c < 32; ++c) if (c < kb) M[i + (int64_t)(k0 + c) * nf] = x[c];
         }
         __syncthreads();
-        // trailing update: M[j0:, j0:] -= L21 L21ᵀ (lower)
+    }
+    return 0;
+}
+
+// Right-looking front factorization (FP32 path): per 32-column panel, diagonal block + panel,
+// then the trailing update M[j0:, j0:] -= L21 L21ᵀ (lower).
+template <class FT>
+__device__ int front_chol(FT* M, int nf, int nres, Shared& sh) {
+    for (int k0 = 0; k0 < nres; k0 += 32) {
+        const int kb = min(32, nres - k0);
+        int info = diag_panel<FT>(M, nf, k0, kb, sh);
+        if (info) return info;
+        const int j0 = k0 + kb;
         if (nf - j0 > 0) syrk_update<FT>(M, nf, k0, kb, j0, sh);
     }
+    return 0;
+}
+
+// ---- FP64 left-looking front factorization ---------------------------------------------------
+__device__ __forceinline__ void cp_async8(void* sdst, const void* gsrc, bool valid) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(sdst);
+    const int sz = valid ? 8 : 0;   // 0: write zeros, read nothing
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sa), "l"(gsrc), "r"(sz) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+// Stage rows [r0, r0 + 64) x columns [k0, k0 + 32) of the column-major M (leading dimension nf)
+// as buf[r * TLD + c], zero where the row is >= rmax or the column >= kmax.  A warp copies 8 rows x
+// 4 columns per instruction: 64-byte runs in global memory, conflict-free 16-lane phases in
+// shared memory.
+__device__ __forceinline__ void stage_tile_f64(double* buf, const double* M, int nf, int r0, int rmax, int k0,
+                                               int kmax) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int rl = lane >> 2, cl = lane & 3;
+    for (int i = warp; i < 64; i += NW) {
+        const int r = (i & 7) * 8 + rl, c = (i >> 3) * 4 + cl;
+        const int gr = r0 + r, gc = k0 + c;
+        const bool v = gr < rmax && gc < kmax;
+        cp_async8(buf + r * TLD + c, v ? M + gr + (int64_t)gc * nf : M, v);
+    }
+}
+
+// M[r, c] -= Σ_{k in [K0, K1)} M[r, k] M[c, k] for c in [J0, J0 + nb) (nb <= 64), r in [J0, nf),
+// r >= c: each 64-row tile accumulates over K in registers (FP64 DMMA) from double-buffered
+// asynchronous copies and is written back once.  Requires K1 <= J0 (the K columns are final).
+__device__ void update_cols_f64(double* M, int nf, int J0, int nb, int K0, int K1, Shared& sh) {
+    if (K1 <= K0 || nb <= 0) return;
+    constexpr int WRN = NW / 4, RW = TS / WRN, MR = RW / 8;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int g = lane >> 2, t = lane & 3;
+    const int wr = warp >> 2, wc = warp & 3;
+    const int nk = (K1 - K0 + 31) / 32;
+    const int cmax = min(nf, J0 + nb);
+    double* A[2] = {sh.ta, sh.ta2};
+    double* B[2] = {sh.tb, sh.tb2};
+    for (int rb = J0; rb < nf; rb += TS) {
+        const bool skip = wc * 16 >= nb || (rb == J0 && wr * RW + RW - 1 < wc * 16);
+        double acc[MR][2][2];
+#pragma unroll
+        for (int a = 0; a < MR; ++a)
+#pragma unroll
+            for (int b = 0; b < 2; ++b) { acc[a][b][0] = 0; acc[a][b][1] = 0; }
+        stage_tile_f64(A[0], M, nf, rb, nf, K0, K1);
+        stage_tile_f64(B[0], M, nf, J0, cmax, K0, K1);
+        cp_async_commit();
+        for (int q = 0; q < nk; ++q) {
+            const int cur = q & 1;
+            if (q + 1 < nk) {
+                stage_tile_f64(A[cur ^ 1], M, nf, rb, nf, K0 + 32 * (q + 1), K1);
+                stage_tile_f64(B[cur ^ 1], M, nf, J0, cmax, K0 + 32 * (q + 1), K1);
+                cp_async_commit();
+                cp_async_wait<1>();
+            } else {
+                cp_async_wait<0>();
+            }
+            __syncthreads();
+            if (!skip) {
+                const double* ta = A[cur];
+                const double* tb = B[cur];
+                const int kb4 = (min(32, K1 - K0 - 32 * q) + 3) & ~3;
+                for (int k = 0; k < kb4; k += 4) {
+                    double b0 = tb[(wc * 16 + g) * TLD + k + t], b1 = tb[(wc * 16 + 8 + g) * TLD + k + t];
+#pragma unroll
+                    for (int a = 0; a < MR; ++a) {
+                        double av = ta[(wr * RW + a * 8 + g) * TLD + k + t];
+                        dmma(acc[a][0][0], acc[a][0][1], av, b0);
+                        dmma(acc[a][1][0], acc[a][1][1], av, b1);
+                    }
+                }
+            }
+            __syncthreads();
+        }
+        if (!skip) {
+#pragma unroll
+            for (int a = 0; a < MR; ++a)
+#pragma unroll
+                for (int b = 0; b < 2; ++b)
+#pragma unroll
+                    for (int q = 0; q < 2; ++q) {
+                        const int row = rb + wr * RW + a * 8 + g;
+                        const int col = J0 + wc * 16 + b * 8 + 2 * t + q;
+                        if (row < nf && col < cmax && row >= col) M[row + (int64_t)col * nf] -= acc[a][b][q];
+                    }
+        }
+    }
+    __syncthreads();
+}
+
+// FP64 front: left-looking over 64-column blocks (each column updated once, from final L columns),
+// 32-column diagonal/panel steps inside a block, then the separator's Schur complement (the update
+// matrix handed to the parent by extend-add).
+template <>
+__device__ int front_chol<double>(double* M, int nf, int nres, Shared& sh) {
+    for (int J = 0; J < nres; J += 64) {
+        const int nb = min(64, nres - J);
+        update_cols_f64(M, nf, J, nb, 0, J, sh);
+        for (int h = 0; h < nb; h += 32) {
+            const int k0 = J + h, kb = min(32, nb - h);
+            if (h > 0) update_cols_f64(M, nf, k0, kb, J, J + 32, sh);
+            int info = diag_panel<double>(M, nf, k0, kb, sh);
+            if (info) return info;
+        }
+    }
+    for (int J = nres; J < nf; J += 64) update_cols_f64(M, nf, J, min(64, nf - J), 0, nres, sh);
     return 0;
 }
 
@@ -1311,7 +1437,8 @@ struct BatchArgs {
 };
 
 __global__ void __launch_bounds__(NT, CTA_PER_SM) ipm_batch_kernel(BatchArgs a) {
-    __shared__ Shared sh;
+    extern __shared__ __align__(16) unsigned char mb_dsmem[];
+    Shared& sh = *reinterpret_cast<Shared*>(mb_dsmem);
     __shared__ int next;
     for (;;) {
         if (threadIdx.x == 0) next = atomicAdd(a.counter, 1);
@@ -1346,7 +1473,9 @@ extern "C" int mb_launch_batch(const mb::DevInst* d_inst, int ninst, int mode, c
     cudaError_t e = cudaMemsetAsync(d_counter, 0, sizeof(int), stream);
     if (e != cudaSuccess) return -1;
     (void)fp32;
-    mb::ipm_batch_kernel<<<grid, mb::NT, 0, stream>>>(a);
+    e = cudaFuncSetAttribute(mb::ipm_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(mb::Shared));
+    if (e != cudaSuccess) return -1;
+    mb::ipm_batch_kernel<<<grid, mb::NT, sizeof(mb::Shared), stream>>>(a);
     e = cudaGetLastError();
     return e == cudaSuccess ? 0 : -2;
 }
@@ -1403,6 +1532,8 @@ extern "C" int mb_launch_wave(const mb::DevInst* d_inst, int ninst, const mb::Se
     a.done = done; a.seq0 = seq0; a.cap = cap;
     cudaError_t e = cudaMemsetAsync(d_counter, 0, sizeof(int), stream);
     if (e != cudaSuccess) return -1;
-    mb::ipm_batch_kernel<<<grid, mb::NT, 0, stream>>>(a);
+    e = cudaFuncSetAttribute(mb::ipm_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(mb::Shared));
+    if (e != cudaSuccess) return -1;
+    mb::ipm_batch_kernel<<<grid, mb::NT, sizeof(mb::Shared), stream>>>(a);
     return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }

@@ -23,6 +23,7 @@
 namespace mb {
 
 constexpr int TS = 64;   // trailing-update tile
+constexpr double MIXED_MAX_SOLVES = 4;   // KKT solves (IR passes + CG steps) an FP32 iteration may take
 constexpr int TLD = 36;  // tile row stride (doubles): 8-byte fragment loads of 8 rows x 4 columns hit 32 distinct banks
 
 // Block-shared scratch (dynamic shared memory: it exceeds the 48 KB static limit).  ta/tb and
@@ -324,6 +325,98 @@ __device__ void update_cols_f64(double* M, int nf, int J0, int nb, int K0, int K
     __syncthreads();
 }
 
+__device__ __forceinline__ void cp_async4(void* sdst, const void* gsrc, bool valid) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(sdst);
+    const int sz = valid ? 4 : 0;
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(sa), "l"(gsrc), "r"(sz) : "memory");
+}
+
+// FP32 stage: rows [r0, r0 + 64) x columns [k0, k0 + 32) of M as buf[c * 68 + r] (k-major, so a
+// thread reads its 4 rows as one float4), zero where the row is >= rmax or the column >= kmax
+constexpr int T32LD = 68;
+__device__ __forceinline__ void stage_tile_f32(float* buf, const float* M, int nf, int r0, int rmax, int k0, int kmax) {
+    for (int i = threadIdx.x; i < 64 * 32; i += NT) {
+        const int r = i & 63, c = i >> 6;
+        const int gr = r0 + r, gc = k0 + c;
+        const bool v = gr < rmax && gc < kmax;
+        cp_async4(buf + c * T32LD + r, v ? M + gr + (int64_t)gc * nf : M, v);
+    }
+}
+
+// FP32 twin of update_cols_f64: each thread owns a 4 x 4 block of the 64 x 64 tile (FFMA)
+__device__ void update_cols_f32(float* M, int nf, int J0, int nb, int K0, int K1, Shared& sh) {
+    if (K1 <= K0 || nb <= 0) return;
+    const int tr = threadIdx.x & 15, tc = threadIdx.x >> 4;
+    const int nk = (K1 - K0 + 31) / 32;
+    const int cmax = min(nf, J0 + nb);
+    float* A[2] = {reinterpret_cast<float*>(sh.ta), reinterpret_cast<float*>(sh.ta2)};
+    float* B[2] = {reinterpret_cast<float*>(sh.tb), reinterpret_cast<float*>(sh.tb2)};
+    for (int rb = J0; rb < nf; rb += TS) {
+        const bool skip = tc * 4 >= nb || (rb == J0 && tr * 4 + 3 < tc * 4);
+        float acc[4][4];
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+            for (int b = 0; b < 4; ++b) acc[a][b] = 0.f;
+        stage_tile_f32(A[0], M, nf, rb, nf, K0, K1);
+        stage_tile_f32(B[0], M, nf, J0, cmax, K0, K1);
+        cp_async_commit();
+        for (int q = 0; q < nk; ++q) {
+            const int cur = q & 1;
+            if (q + 1 < nk) {
+                stage_tile_f32(A[cur ^ 1], M, nf, rb, nf, K0 + 32 * (q + 1), K1);
+                stage_tile_f32(B[cur ^ 1], M, nf, J0, cmax, K0 + 32 * (q + 1), K1);
+                cp_async_commit();
+                cp_async_wait<1>();
+            } else {
+                cp_async_wait<0>();
+            }
+            __syncthreads();
+            if (!skip) {
+                const float* ta = A[cur];
+                const float* tb = B[cur];
+                const int kb = min(32, K1 - K0 - 32 * q);
+                for (int k = 0; k < kb; ++k) {
+                    const float4 av = *reinterpret_cast<const float4*>(ta + k * T32LD + tr * 4);
+                    const float4 bv = *reinterpret_cast<const float4*>(tb + k * T32LD + tc * 4);
+                    const float ar[4] = {av.x, av.y, av.z, av.w}, br[4] = {bv.x, bv.y, bv.z, bv.w};
+#pragma unroll
+                    for (int a = 0; a < 4; ++a)
+#pragma unroll
+                        for (int b = 0; b < 4; ++b) acc[a][b] = fmaf(ar[a], br[b], acc[a][b]);
+                }
+            }
+            __syncthreads();
+        }
+        if (!skip) {
+#pragma unroll
+            for (int b = 0; b < 4; ++b)
+#pragma unroll
+                for (int a = 0; a < 4; ++a) {
+                    const int row = rb + tr * 4 + a, col = J0 + tc * 4 + b;
+                    if (row < nf && col < cmax && row >= col) M[row + (int64_t)col * nf] -= acc[a][b];
+                }
+        }
+    }
+    __syncthreads();
+}
+
+template <>
+__device__ int front_chol<float>(float* M, int nf, int nres, Shared& sh) {
+    for (int J = 0; J < nres; J += 64) {
+        const int nb = min(64, nres - J);
+        update_cols_f32(M, nf, J, nb, 0, J, sh);
+        for (int h = 0; h < nb; h += 32) {
+            const int k0 = J + h, kb = min(32, nb - h);
+            if (h > 0) update_cols_f32(M, nf, k0, kb, J, J + 32, sh);
+            int info = diag_panel<float>(M, nf, k0, kb, sh);
+            if (info) return info;
+        }
+    }
+    for (int J = nres; J < nf; J += 64) update_cols_f32(M, nf, J, min(64, nf - J), 0, nres, sh);
+    return 0;
+}
+
 // FP64 front: left-looking over 64-column blocks (each column updated once, from final L columns),
 // 32-column diagonal/panel steps inside a block, then the separator's Schur complement (the update
 // matrix handed to the parent by extend-add).
@@ -422,6 +515,7 @@ struct Ctx {
     float* F32;             // ... or as FP32 (same buffer)
     bool use32;             // this iteration factors in FP32
     bool fellback;          // mixed precision: the FP64 factor is in use for good
+    int switched;           // mixed precision: moved to FP64 after a solve-heavy FP32 iteration
     int nfp32, nfallback;   // iterations accepted with the FP32 factor; FP64 redos
     bool kktfail;           // the last iteration's factorization or a KKT solve failed
     int n, m, nv;
@@ -441,8 +535,9 @@ struct Ctx {
         red = sh.red;
         F64 = reinterpret_cast<double*>(I.F);
         F32 = reinterpret_cast<float*>(I.F);
-        use32 = set.precision == 1 || (set.precision == 2 && I.status[5] == 0);
-        fellback = I.status[5] != 0;
+        use32 = set.precision == 1 || (set.precision == 2 && I.status[5] == 0 && I.status[6] == 0);
+        fellback = I.status[5] != 0 || I.status[6] != 0;
+        switched = I.status[6];
         nfp32 = I.status[4]; nfallback = I.status[5];
         n = I.n; m = I.m; nv = I.nvtx;
         double* v = I.vn;
@@ -464,7 +559,7 @@ struct Ctx {
         if (threadIdx.x == 0) {
             I.scal[5] = nf; I.scal[6] = ng; I.scal[7] = sf; I.scal[8] = sg; I.scal[9] = nB;
             I.status[1] = nrow_hist; I.status[2] = nretry; I.status[3] = nfact;
-            I.status[4] = nfp32; I.status[5] = nfallback;
+            I.status[4] = nfp32; I.status[5] = nfallback; I.status[6] = switched;
             for (int k = 0; k < NSEC; ++k) I.scal[SCAL_SEC + k] = (double)tsec[k];
             I.scal[SCAL_NTRSV] = (double)ntrsv; I.scal[SCAL_NGEMV] = (double)ngemv;
         }
@@ -1151,9 +1246,14 @@ struct Ctx {
         __syncthreads();
         use32 = true;
         int st = step_();
-        const Row& r = hrow(nrow_hist - 1);
-        (void)r;
-        if (!kktfail) { nfp32++; return st; }
+        if (!kktfail) {
+            nfp32++;
+            // an FP32 factor that needed more KKT solves than MIXED_MAX_SOLVES costs more in solves
+            // than it saved in the factorization: keep this iteration and factor in FP64 from now on
+            const Row& r = hrow(nrow_hist - 1);
+            if (r.piter + r.ppass + r.citer + r.cpass > MIXED_MAX_SOLVES) { fellback = true; switched = 1; }
+            return st;
+        }
         for (int i = threadIdx.x; i < n; i += NT) { I.p[i] = sp[i]; I.d[i] = sd[i]; }
         for (int i = threadIdx.x; i < m; i += NT) I.y[i] = sy[i];
         for (int64_t i = threadIdx.x; i < I.cxblk[nv]; i += NT) I.cache[i] = I.cache2[i];

@@ -689,6 +689,7 @@ struct Solver {
     Timers tm;
     i64 nfactor_retry = 0;
     i64 nfallback = 0;      // iterations redone with the FP64 factor (precision 2)
+    bool switched = false;  // moved to the FP64 factor after a solve-heavy FP32 iteration (precision 2)
     i64 nfp32 = 0;          // iterations accepted with the FP32 factor
 };
 
@@ -1012,16 +1013,23 @@ static const double FORCING_FRAC = 0.1;
 static int step_(Solver& s);
 
 // precision 2 (mixed): iterate with an FP32 factor until a KKT solve misses its tolerance; that
-// iteration is redone from the saved iterate with the FP64 factor, which is kept from then on
+// iteration is redone from the saved iterate with the FP64 factor, which is kept from then on.
+// An accepted FP32 iteration that needed more than MIXED_MAX_SOLVES KKT solves (IR passes + CG
+// steps) also moves the solve to the FP64 factor for the remaining iterations, without a redo.
+static const double MIXED_MAX_SOLVES = 4;
 static int step(Solver& s) {
-    if (s.set.precision != 2 || s.nfallback > 0) { if (s.set.precision == 2) s.F.fp32 = false; return step_(s); }
+    if (s.set.precision != 2 || s.nfallback > 0 || s.switched) { if (s.set.precision == 2) s.F.fp32 = false; return step_(s); }
     std::vector<double> p0 = s.p, d0 = s.d, y0 = s.y;
     std::vector<double> c0 = s.cache;
     s.F.fp32 = true;
     int st = step_(s);
     const ob_row& r = s.hist.back();
     bool kktfail = (r.pstat != KKT_SOLVED || r.cstat != KKT_SOLVED) && !std::isnan(r.rho);
-    if (!kktfail) { s.nfp32++; return st; }
+    if (!kktfail) {
+        s.nfp32++;
+        if (r.piter + r.ppass + r.citer + r.cpass > MIXED_MAX_SOLVES) s.switched = true;
+        return st;
+    }
     s.hist.pop_back();
     s.p = p0; s.d = d0; s.y = y0; s.cache = c0;
     s.F.fp32 = false;

@@ -459,8 +459,17 @@ __device__ void front_lsolve(const FT* M, int nf, int nres, int r0, const int* s
         }
         __syncthreads();
         for (int i = k0 + kb + tid; i < nf; i += NT) {
+            const FT* Mi = M + i + (int64_t)k0 * nf;
             double t = 0;
-            for (int c = 0; c < kb; ++c) t = fma((double)M[i + (int64_t)(k0 + c) * nf], sh.xs[c], t);
+            if (kb == 32) {   // all 32 loads in flight before the FMA chain
+                FT v[32];
+#pragma unroll
+                for (int c = 0; c < 32; ++c) v[c] = Mi[(int64_t)c * nf];
+#pragma unroll
+                for (int c = 0; c < 32; ++c) t = fma((double)v[c], sh.xs[c], t);
+            } else {
+                for (int c = 0; c < kb; ++c) t = fma((double)Mi[(int64_t)c * nf], sh.xs[c], t);
+            }
             int tg = i < nres ? r0 + i : sep[i - nres];
             x[tg] -= t;
         }
@@ -481,12 +490,22 @@ __device__ void front_usolve(const FT* M, int nf, int nres, int r0, const int* s
             if (r < kb && c < kb && r >= c) T[c * 33 + r] = (double)M[(k0 + r) + (int64_t)(k0 + c) * nf];
         }
         for (int c = warp; c < kb; c += NW) {
-            double t = 0;
-            for (int i = k0 + kb + lane; i < nf; i += 32) {
-                int src = i < nres ? r0 + i : sep[i - nres];
-                t = fma((double)M[i + (int64_t)(k0 + c) * nf], x[src], t);
+            const FT* Mc = M + (int64_t)(k0 + c) * nf;
+            double t0 = 0, t1 = 0, t2 = 0, t3 = 0;
+            int i = k0 + kb + lane;
+            for (; i + 96 < nf; i += 128) {   // four rows per lane in flight
+                int s0 = i < nres ? r0 + i : sep[i - nres];
+                int s1 = i + 32 < nres ? r0 + i + 32 : sep[i + 32 - nres];
+                int s2 = i + 64 < nres ? r0 + i + 64 : sep[i + 64 - nres];
+                int s3 = i + 96 < nres ? r0 + i + 96 : sep[i + 96 - nres];
+                double m0 = (double)Mc[i], m1 = (double)Mc[i + 32], m2 = (double)Mc[i + 64], m3 = (double)Mc[i + 96];
+                t0 = fma(m0, x[s0], t0); t1 = fma(m1, x[s1], t1); t2 = fma(m2, x[s2], t2); t3 = fma(m3, x[s3], t3);
             }
-            t = warp_sum(t);
+            for (; i < nf; i += 32) {
+                int src = i < nres ? r0 + i : sep[i - nres];
+                t0 = fma((double)Mc[i], x[src], t0);
+            }
+            double t = warp_sum((t0 + t1) + (t2 + t3));
             if (lane == 0) sh.acc[c] = t;
         }
         __syncthreads();
@@ -895,7 +914,14 @@ struct Ctx {
     template <class FT>
     __device__ void assemble_t(FT* F, double dl, double rho) {
         const int tid = threadIdx.x;
-        for (int64_t i = tid; i < I.fsize; i += NT) F[i] = (FT)I.Finit[i];
+        {
+            int64_t i = tid;
+            for (; i + 3 * NT < I.fsize; i += 4 * NT) {
+                double a0 = I.Finit[i], a1 = I.Finit[i + NT], a2 = I.Finit[i + 2 * NT], a3 = I.Finit[i + 3 * NT];
+                F[i] = (FT)a0; F[i + NT] = (FT)a1; F[i + 2 * NT] = (FT)a2; F[i + 3 * NT] = (FT)a3;
+            }
+            for (; i < I.fsize; i += NT) F[i] = (FT)I.Finit[i];
+        }
         __syncthreads();
         // + δ H: diagonal blocks (lower part) and the off-diagonal nonzeros of Q (chordal.jl:1-80)
         for (int v = 0; v < nv; ++v) {

@@ -450,14 +450,25 @@ inline Fronts analyze(const std::vector<std::vector<i64>>& adj0, const std::vect
     Fronts S;
     S.postperm = post;
     S.vfront.assign(n, -1);
-    // fundamental supernodes: v joins its only child v-1 when struct(v-1) = {v} ∪ struct(v)
-    // (the sizes decide it because struct(v) ⊇ struct(v-1) \ {v} always holds)
-    std::vector<i64> ssz(n);
-    for (i64 v = 0; v < n; ++v) ssz[v] = (i64)sv[v].size();
+    // relaxed supernodes: v joins the front of its child v-1 (its last child in postorder, so the
+    // columns stay contiguous) when the explicit zeros this adds to the front's columns stay within
+    // 5% of the merged front's lower-triangle entries; with no zero added this is the maximal
+    // supernode.  struct(v-1) ⊆ {v} ∪ struct(v) (etree property), so the merged front's rows hold
+    // every column's structure and the added entries are zeros of L.
+    std::vector<i64> ssw(n, 0);   // scalar rows of struct(v)
+    for (i64 v = 0; v < n; ++v) for (i64 u : sv[v]) ssw[v] += w[u];
+    i64 fcols = 0, fzeros = 0;    // the open front: scalar columns, zeros added so far
     for (i64 v = 0; v < n; ++v) {
-        bool merge = v > 0 && kids[v].size() == 1 && kids[v][0] == v - 1 && ssz[v - 1] == ssz[v] + 1;
+        bool merge = false;
+        if (v > 0 && par[v - 1] == v) {
+            const i64 add = fcols * (w[v] + ssw[v] - ssw[v - 1]);
+            const i64 cols = fcols + w[v], nfm = cols + ssw[v];
+            const double entries = (double)cols * (double)nfm - 0.5 * (double)cols * (double)(cols - 1);
+            merge = add == 0 || (double)(fzeros + add) <= 0.05 * entries;
+            if (merge) { fzeros += add; fcols = cols; }
+        }
         if (merge) S.vfront[v] = S.vfront[v - 1];
-        else { S.vfront[v] = S.nfront++; S.fvtx.push_back(v); }
+        else { S.vfront[v] = S.nfront++; S.fvtx.push_back(v); fcols = w[v]; fzeros = 0; }
     }
     S.fvtx.push_back(n);
     std::vector<i64> vcol(n + 1, 0);

@@ -413,17 +413,26 @@ static Symbolic analyze(const std::vector<std::vector<i64>>& adj0, const std::ve
             for (i64 u : sv[c]) if (u > v && mark[u] != v) { mark[u] = v; s.push_back(u); }
         std::sort(s.begin(), s.end());
     }
-    // fundamental supernodes: v joins child c when c is v's only child and
-    // struct(c) = {v} U struct(v)
+    // relaxed supernodes: v joins the front of its child v-1 (last child in postorder) when the
+    // explicit zeros added to the front's columns stay within 5% of the merged front's lower
+    // entries (CliqueTrees' own partition is not available here; the numeric factor does not
+    // depend on the partition, only the storage does)
     Symbolic S;
     S.postperm = post;
-    std::vector<i64> front(n, -1);
+    std::vector<i64> front(n, -1), ssw(n, 0);
+    for (i64 v = 0; v < n; ++v) for (i64 u : sv[v]) ssw[v] += w[u];
+    i64 fcols = 0, fzeros = 0;
     for (i64 v = 0; v < n; ++v) {
         bool merge = false;
-        if (v > 0 && kids[v].size() == 1 && kids[v][0] == v - 1 && sv[v - 1].size() == sv[v].size() + 1)
-            merge = true;
+        if (v > 0 && par[v - 1] == v) {
+            const i64 add = fcols * (w[v] + ssw[v] - ssw[v - 1]);
+            const i64 cols = fcols + w[v], nfm = cols + ssw[v];
+            const double entries = (double)cols * (double)nfm - 0.5 * (double)cols * (double)(cols - 1);
+            merge = add == 0 || (double)(fzeros + add) <= 0.05 * entries;
+            if (merge) { fzeros += add; fcols = cols; }
+        }
         if (merge) front[v] = front[v - 1];
-        else { front[v] = S.nfront++; S.fvtx.push_back(v); }
+        else { front[v] = S.nfront++; S.fvtx.push_back(v); fcols = w[v]; fzeros = 0; }
     }
     S.fvtx.push_back(n);
     // scalar columns of each vertex

@@ -51,6 +51,9 @@ enum mb_status {
     MB_NEAR_DUAL_INFEASIBLE, MB_NEAR_ILL_POSED
 };
 
+/* algorithmic flops of one factorization above which a lone instance runs grid-cooperatively */
+#define MB_LARGE_FLOPS 1.0e9
+
 /* factor precision */
 #define MB_PREC_FP64 0     /* FP64 factor */
 #define MB_PREC_FP32 1     /* FP32 factor, FP64 refinement, residuals and termination tests */
@@ -66,7 +69,9 @@ typedef struct mb_settings {
     int32_t newton_max_iter;   /* 100 CG iterations per KKT solve */
     int32_t stable;            /* 0   (StableUzawaSolver not available: must be 0) */
     int32_t precision;         /* MB_PREC_FP64 */
-    int32_t reserved;
+    int32_t large;             /* 0: a single instance whose factorization exceeds MB_LARGE_FLOPS runs
+                                  grid-cooperatively (all SMs help with its large fronts); 1: always
+                                  for a single instance; -1: never */
     double step_frac;          /* 0.99 */
     double feas_tol;           /* 1e-8 */
     double gap_tol;            /* 1e-8 */

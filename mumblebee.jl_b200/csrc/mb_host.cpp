@@ -22,6 +22,9 @@
 
 extern "C" int mb_launch_batch(const mb::DevInst* d_inst, int ninst, int mode, const mb::Settings* set,
                                int* d_counter, int grid, int fp32, cudaStream_t stream);
+extern "C" int mb_launch_coop(const mb::DevInst* d_inst, int mode, const mb::Settings* set, mb::CoopCtl* d_ctl,
+                              int grid, cudaStream_t stream);
+extern "C" int mb_coop_grid(int device, int nsm);
 
 using mbh::i64;
 
@@ -393,13 +396,14 @@ struct mb_batch {
     void* d_F = nullptr;
     mb::DevInst* d_inst = nullptr;
     int* d_counter = nullptr;
+    mb::CoopCtl* d_coop = nullptr;   // grid-cooperative mode control block (one large instance)
     int32_t* h_i32 = nullptr;   // pinned mirrors of the status words
     double* h_out = nullptr;    // pinned output staging
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     int64_t launches = 0;
     ~mb_batch() {
         cudaFree(d_i32); cudaFree(d_i64); cudaFree(d_din); cudaFree(d_work); cudaFree(d_out); cudaFree(d_F);
-        cudaFree(d_inst); cudaFree(d_counter); cudaFree(d_ost);
+        cudaFree(d_inst); cudaFree(d_counter); cudaFree(d_ost); cudaFree(d_coop);
         cudaFreeHost(h_i32); cudaFreeHost(h_out);
         if (e0) cudaEventDestroy(e0);
         if (e1) cudaEventDestroy(e1);
@@ -521,8 +525,12 @@ static int run_batch(mb_batch* b, int mode, int32_t grid, float* ms) {
     static_assert(sizeof(mb::Settings) == sizeof(mb_settings), "settings layout");
     std::memcpy(&s, &b->set, sizeof(s));
     CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+    // a lone large instance runs on the whole GPU (grid-cooperative mode)
+    const bool coop = ninst == 1 && (b->set.large == 1 || (b->set.large == 0 && b->pk.plans[0].fflops >= MB_LARGE_FLOPS));
+    if (coop && !b->d_coop) CUDA_TRY(ctx, cudaMalloc((void**)&b->d_coop, sizeof(mb::CoopCtl)));
     CUDA_TRY(ctx, cudaEventRecord(b->e0, ctx->stream));
-    int rc = mb_launch_batch(b->d_inst, ninst, mode, &s, b->d_counter, g, b->set.precision == MB_PREC_FP32, ctx->stream);
+    int rc = coop ? mb_launch_coop(b->d_inst, mode, &s, b->d_coop, mb_coop_grid(ctx->device, ctx->nsm), ctx->stream)
+                  : mb_launch_batch(b->d_inst, ninst, mode, &s, b->d_counter, g, b->set.precision == MB_PREC_FP32, ctx->stream);
     if (rc) return fail(ctx, MB_E_CUDA, std::string("launch failed: ") + cudaGetErrorString(cudaGetLastError()));
     b->launches++;
     CUDA_TRY(ctx, cudaEventRecord(b->e1, ctx->stream));
@@ -585,7 +593,7 @@ void mb_settings_default(mb_settings* s) {
     if (!s) return;
     std::memset(s, 0, sizeof(*s));
     s->verbose = 0; s->max_iter = 100; s->scale_max_iter = 10; s->refine_max_iter = 10; s->newton_max_iter = 100;
-    s->stable = 0; s->precision = MB_PREC_FP64;
+    s->stable = 0; s->precision = MB_PREC_FP64; s->large = 0;
     s->step_frac = 0.99; s->feas_tol = 1e-8; s->gap_tol = 1e-8; s->near_factor = 1000.0; s->stall_tol = 1e-3;
     s->refine_stall_tol = 0.5; s->aug_tol = 1e-7; s->infeas_abs = 1e-8; s->infeas_rel = 1e-8;
 }

@@ -22,7 +22,7 @@ enum CGStatus { CG_CONTINUE = 0, CG_SOLVED, CG_NUMERICAL_FAILURE, CG_ITMAX };
 
 // Settings, field order shared with mb_settings in include/mumblebee_gpu.h
 struct Settings {
-    int32_t verbose, max_iter, scale_max_iter, refine_max_iter, newton_max_iter, stable, precision, reserved;
+    int32_t verbose, max_iter, scale_max_iter, refine_max_iter, newton_max_iter, stable, precision, large;
     double step_frac, feas_tol, gap_tol, near_factor, stall_tol, refine_stall_tol, aug_tol, infeas_abs, infeas_rel;
 };
 
@@ -110,10 +110,28 @@ constexpr int SCAL_NTRSV = 22;      // triangular solve sweeps
 constexpr int SCAL_NGEMV = 23;      // block-sparse matvecs
 constexpr int SCAL_T0 = 24;         // %globaltimer (ns, bit pattern) when a CTA took the instance
 constexpr int SCAL_T1 = 25;         // %globaltimer (ns, bit pattern) when its solve finished
-constexpr int NSTAT = 8;    // status, history rows, factor retries, factorizations, FP32 iterations, FP64 redos
+constexpr int NSTAT = 8;    // status, history rows, factor retries, factorizations, FP32 iterations, FP64 redos,
+                            // switched-to-FP64 flag, grid-barrier timeout flag
 
 // kernel modes: a full solve, or the pieces used by the step-wise API
 enum Mode { MODE_SOLVE = 0, MODE_INIT = 1, MODE_STEP = 2, MODE_RESULT = 3 };
+
+// Grid-cooperative mode for one large instance: CTA 0 (the leader) runs the iteration; the other
+// CTAs of a cooperative launch help with the dense work of large fronts (assembly copy, factor
+// update tiles, panel rows, extend-add).  The leader posts a command here and meets the helpers at
+// a grid barrier; every wait is bounded (COOP_WAIT_NS), after which `abort` is set and every role
+// returns.  The host zeroes this block before each launch.
+struct CoopCtl {
+    unsigned int count;     // barrier arrivals
+    unsigned int gen;       // barrier generation
+    int abort;              // a barrier wait timed out
+    int cmd;                // command for the helpers
+    int ia[8];
+    long long la[4];
+    void* pa[4];
+};
+enum CoopCmd { COOP_NONE = 0, COOP_EXIT = 1, COOP_FILL = 2, COOP_COPY = 3, COOP_UPDATE = 4, COOP_PANEL = 5,
+               COOP_EXTEND = 6 };
 
 
 }  // namespace mb

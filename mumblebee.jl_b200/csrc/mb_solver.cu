@@ -48,123 +48,11 @@ __device__ __forceinline__ void dmma(double& c0, double& c1, double a, double b)
                  : "+d"(c0), "+d"(c1) : "d"(a), "d"(b));
 }
 
-// Trailing update M[j0:, j0:] -= L21 L21ᵀ (lower part) for the panel columns [k0, k0+kb), kb <= 32.
-// Row blocks of 64 are staged once per sweep; each of the 16 warps owns a 16x16 piece of the
-// 64x64 output tile.  FP64: tensor-path DMMA.  FP32: FFMA register tiles.
+// Factor the kb x kb diagonal block at k0 (warp 0; the factor is kept in sh.diag and written back
+// to M).  Returns the failing pivot (1-based in the front) or 0.
 template <class FT>
-__device__ void syrk_update(FT* M, int nf, int k0, int kb, int j0, Shared& sh);
-
-template <>
-__device__ void syrk_update<double>(double* M, int nf, int k0, int kb, int j0, Shared& sh) {
-    // warps tile the 64x64 output as (NW/4) x 4; each warp owns RW x 16 (RW/8 x 2 DMMA tiles)
-    constexpr int WRN = NW / 4, RW = TS / WRN, MR = RW / 8;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int g = lane >> 2, t = lane & 3;
-    const int wr = warp >> 2, wc = warp & 3;
-    const int nrem = nf - j0, nt = (nrem + TS - 1) / TS;
-    const int kb4 = (kb + 3) & ~3;
-    double* ta = sh.ta;
-    double* tb = sh.tb;
-    for (int ti = 0; ti < nt; ++ti) {
-        const int rb = j0 + ti * TS;
-        for (int idx = tid; idx < TS * 32; idx += NT) {
-            int r = idx % TS, c = idx / TS;
-            ta[r * TLD + c] = (c < kb && rb + r < nf) ? M[(rb + r) + (int64_t)(k0 + c) * nf] : 0.0;
-        }
-        for (int tj = 0; tj <= ti; ++tj) {
-            const int cb = j0 + tj * TS;
-            for (int idx = tid; idx < TS * 32; idx += NT) {
-                int r = idx % TS, c = idx / TS;
-                tb[r * TLD + c] = (c < kb && cb + r < nf) ? M[(cb + r) + (int64_t)(k0 + c) * nf] : 0.0;
-            }
-            __syncthreads();
-            const bool skip = (ti == tj) && (wr * RW + RW - 1 < wc * 16);   // strictly upper warp tile
-            if (!skip) {
-                double acc[MR][2][2];
-#pragma unroll
-                for (int a = 0; a < MR; ++a)
-#pragma unroll
-                    for (int b = 0; b < 2; ++b) { acc[a][b][0] = 0; acc[a][b][1] = 0; }
-                for (int k = 0; k < kb4; k += 4) {
-                    double b0 = tb[(wc * 16 + g) * TLD + k + t], b1 = tb[(wc * 16 + 8 + g) * TLD + k + t];
-#pragma unroll
-                    for (int a = 0; a < MR; ++a) {
-                        double av = ta[(wr * RW + a * 8 + g) * TLD + k + t];
-                        dmma(acc[a][0][0], acc[a][0][1], av, b0);
-                        dmma(acc[a][1][0], acc[a][1][1], av, b1);
-                    }
-                }
-#pragma unroll
-                for (int a = 0; a < MR; ++a)
-#pragma unroll
-                    for (int b = 0; b < 2; ++b)
-#pragma unroll
-                        for (int q = 0; q < 2; ++q) {
-                            int row = rb + wr * RW + a * 8 + g;
-                            int col = cb + wc * 16 + b * 8 + 2 * t + q;
-                            if (row < nf && col < nf && row >= col) M[row + (int64_t)col * nf] -= acc[a][b][q];
-                        }
-            }
-            __syncthreads();
-        }
-    }
-}
-
-template <>
-__device__ void syrk_update<float>(float* M, int nf, int k0, int kb, int j0, Shared& sh) {
-    // each thread owns rows tr + 16a (a < 4) and columns tc*CW + b of the 64x64 tile
-    constexpr int CW = TS / (NT / 16);
-    const int tid = threadIdx.x;
-    const int nrem = nf - j0, nt = (nrem + TS - 1) / TS;
-    float* ta = reinterpret_cast<float*>(sh.ta);
-    float* tb = reinterpret_cast<float*>(sh.tb);
-    const int tr = tid & 15, tc = tid >> 4;
-    for (int ti = 0; ti < nt; ++ti) {
-        const int rb = j0 + ti * TS;
-        for (int idx = tid; idx < TS * 32; idx += NT) {
-            int r = idx % TS, c = idx / TS;
-            ta[c * (TS + 1) + r] = (c < kb && rb + r < nf) ? M[(rb + r) + (int64_t)(k0 + c) * nf] : 0.0f;
-        }
-        for (int tj = 0; tj <= ti; ++tj) {
-            const int cb = j0 + tj * TS;
-            for (int idx = tid; idx < TS * 32; idx += NT) {
-                int r = idx % TS, c = idx / TS;
-                tb[c * (TS + 1) + r] = (c < kb && cb + r < nf) ? M[(cb + r) + (int64_t)(k0 + c) * nf] : 0.0f;
-            }
-            __syncthreads();
-            float acc[4][CW];
-#pragma unroll
-            for (int a = 0; a < 4; ++a)
-#pragma unroll
-                for (int b = 0; b < CW; ++b) acc[a][b] = 0;
-            for (int c = 0; c < kb; ++c) {
-                float bv[CW];
-#pragma unroll
-                for (int b = 0; b < CW; ++b) bv[b] = tb[c * (TS + 1) + tc * CW + b];
-#pragma unroll
-                for (int a = 0; a < 4; ++a) {
-                    float av = ta[c * (TS + 1) + tr + 16 * a];
-#pragma unroll
-                    for (int b = 0; b < CW; ++b) acc[a][b] = fmaf(av, bv[b], acc[a][b]);
-                }
-            }
-#pragma unroll
-            for (int a = 0; a < 4; ++a)
-#pragma unroll
-                for (int b = 0; b < CW; ++b) {
-                    int row = rb + tr + 16 * a, col = cb + tc * CW + b;
-                    if (row < nf && col < nf && row >= col) M[row + (int64_t)col * nf] -= acc[a][b];
-                }
-            __syncthreads();
-        }
-    }
-}
-
-// Factor the kb x kb diagonal block at k0 (warp 0) and solve the panel below it:
-// L21 = A21 L11^{-T} for rows [k0 + kb, nf).  Returns the failing pivot (1-based in the front) or 0.
-template <class FT>
-__device__ int diag_panel(FT* M, int nf, int k0, int kb, Shared& sh) {
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+__device__ int diag_factor(FT* M, int nf, int k0, int kb, Shared& sh) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     FT* S = reinterpret_cast<FT*>(sh.diag);
     {
         if (warp == 0) {
@@ -198,9 +86,27 @@ __device__ int diag_panel(FT* M, int nf, int k0, int kb, Shared& sh) {
         }
         __syncthreads();
         if (sh.flag) return sh.flag;
-        // panel: L21 = A21 L11^{-T}
+    }
+    return 0;
+}
+
+// Panel solve L21 = A21 L11^{-T} for the rows [k0 + kb, nf) owned by this rank (row blocks of NT
+// rows dealt round-robin over nranks CTAs).  With `load`, the factored diagonal block is first read
+// back from M into sh.diag (a helper CTA that did not factor it).
+template <class FT>
+__device__ void panel_rows(FT* M, int nf, int k0, int kb, Shared& sh, int rank, int nranks, bool load) {
+    const int tid = threadIdx.x;
+    FT* S = reinterpret_cast<FT*>(sh.diag);
+    if (load) {
+        for (int t = tid; t < 32 * 32; t += NT) {
+            const int r = t & 31, c = t >> 5;
+            if (r < kb && c <= r) S[r * 33 + c] = M[(k0 + r) + (int64_t)(k0 + c) * nf];
+        }
+        __syncthreads();
+    }
+    {
         const int j0 = k0 + kb;
-        for (int i = j0 + tid; i < nf; i += NT) {
+        for (int i = j0 + rank * NT + tid; i < nf; i += NT * nranks) {
             FT x[32];
 #pragma unroll
             for (int c = 0; c < 32; ++c) {
@@ -216,20 +122,13 @@ __device__ int diag_panel(FT* M, int nf, int k0, int kb, Shared& sh) {
         }
         __syncthreads();
     }
-    return 0;
 }
 
-// Right-looking front factorization (FP32 path): per 32-column panel, diagonal block + panel,
-// then the trailing update M[j0:, j0:] -= L21 L21ᵀ (lower).
 template <class FT>
-__device__ int front_chol(FT* M, int nf, int nres, Shared& sh) {
-    for (int k0 = 0; k0 < nres; k0 += 32) {
-        const int kb = min(32, nres - k0);
-        int info = diag_panel<FT>(M, nf, k0, kb, sh);
-        if (info) return info;
-        const int j0 = k0 + kb;
-        if (nf - j0 > 0) syrk_update<FT>(M, nf, k0, kb, j0, sh);
-    }
+__device__ int diag_panel(FT* M, int nf, int k0, int kb, Shared& sh) {
+    int info = diag_factor<FT>(M, nf, k0, kb, sh);
+    if (info) return info;
+    panel_rows<FT>(M, nf, k0, kb, sh, 0, 1, false);
     return 0;
 }
 
@@ -262,7 +161,8 @@ __device__ __forceinline__ void stage_tile_f64(double* buf, const double* M, int
 // M[r, c] -= Σ_{k in [K0, K1)} M[r, k] M[c, k] for c in [J0, J0 + nb) (nb <= 64), r in [J0, nf),
 // r >= c: each 64-row tile accumulates over K in registers (FP64 DMMA) from double-buffered
 // asynchronous copies and is written back once.  Requires K1 <= J0 (the K columns are final).
-__device__ void update_cols_f64(double* M, int nf, int J0, int nb, int K0, int K1, Shared& sh) {
+__device__ void update_cols_f64(double* M, int nf, int J0, int nb, int K0, int K1, Shared& sh, int rank = 0,
+                                int nranks = 1) {
     if (K1 <= K0 || nb <= 0) return;
     constexpr int WRN = NW / 4, RW = TS / WRN, MR = RW / 8;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -272,7 +172,7 @@ __device__ void update_cols_f64(double* M, int nf, int J0, int nb, int K0, int K
     const int cmax = min(nf, J0 + nb);
     double* A[2] = {sh.ta, sh.ta2};
     double* B[2] = {sh.tb, sh.tb2};
-    for (int rb = J0; rb < nf; rb += TS) {
+    for (int rb = J0 + TS * rank; rb < nf; rb += TS * nranks) {
         const bool skip = wc * 16 >= nb || (rb == J0 && wr * RW + RW - 1 < wc * 16);
         double acc[MR][2][2];
 #pragma unroll
@@ -344,14 +244,15 @@ __device__ __forceinline__ void stage_tile_f32(float* buf, const float* M, int n
 }
 
 // FP32 twin of update_cols_f64: each thread owns a 4 x 4 block of the 64 x 64 tile (FFMA)
-__device__ void update_cols_f32(float* M, int nf, int J0, int nb, int K0, int K1, Shared& sh) {
+__device__ void update_cols_f32(float* M, int nf, int J0, int nb, int K0, int K1, Shared& sh, int rank = 0,
+                                int nranks = 1) {
     if (K1 <= K0 || nb <= 0) return;
     const int tr = threadIdx.x & 15, tc = threadIdx.x >> 4;
     const int nk = (K1 - K0 + 31) / 32;
     const int cmax = min(nf, J0 + nb);
     float* A[2] = {reinterpret_cast<float*>(sh.ta), reinterpret_cast<float*>(sh.ta2)};
     float* B[2] = {reinterpret_cast<float*>(sh.tb), reinterpret_cast<float*>(sh.tb2)};
-    for (int rb = J0; rb < nf; rb += TS) {
+    for (int rb = J0 + TS * rank; rb < nf; rb += TS * nranks) {
         const bool skip = tc * 4 >= nb || (rb == J0 && tr * 4 + 3 < tc * 4);
         float acc[4][4];
 #pragma unroll
@@ -401,40 +302,7 @@ __device__ void update_cols_f32(float* M, int nf, int J0, int nb, int K0, int K1
     __syncthreads();
 }
 
-template <>
-__device__ int front_chol<float>(float* M, int nf, int nres, Shared& sh) {
-    for (int J = 0; J < nres; J += 64) {
-        const int nb = min(64, nres - J);
-        update_cols_f32(M, nf, J, nb, 0, J, sh);
-        for (int h = 0; h < nb; h += 32) {
-            const int k0 = J + h, kb = min(32, nb - h);
-            if (h > 0) update_cols_f32(M, nf, k0, kb, J, J + 32, sh);
-            int info = diag_panel<float>(M, nf, k0, kb, sh);
-            if (info) return info;
-        }
-    }
-    for (int J = nres; J < nf; J += 64) update_cols_f32(M, nf, J, min(64, nf - J), 0, nres, sh);
-    return 0;
-}
 
-// FP64 front: left-looking over 64-column blocks (each column updated once, from final L columns),
-// 32-column diagonal/panel steps inside a block, then the separator's Schur complement (the update
-// matrix handed to the parent by extend-add).
-template <>
-__device__ int front_chol<double>(double* M, int nf, int nres, Shared& sh) {
-    for (int J = 0; J < nres; J += 64) {
-        const int nb = min(64, nres - J);
-        update_cols_f64(M, nf, J, nb, 0, J, sh);
-        for (int h = 0; h < nb; h += 32) {
-            const int k0 = J + h, kb = min(32, nb - h);
-            if (h > 0) update_cols_f64(M, nf, k0, kb, J, J + 32, sh);
-            int info = diag_panel<double>(M, nf, k0, kb, sh);
-            if (info) return info;
-        }
-    }
-    for (int J = nres; J < nf; J += 64) update_cols_f64(M, nf, J, min(64, nf - J), 0, nres, sh);
-    return 0;
-}
 
 // forward solve with front f: x[res] <- D⁻¹ x[res]; x[sep] -= L_off x[res]
 template <class FT>
@@ -522,6 +390,169 @@ __device__ void front_usolve(const FT* M, int nf, int nres, int r0, const int* s
     }
 }
 
+// ---- grid-cooperative help for large fronts (CoopCtl) ----------------------------------------
+constexpr long long COOP_WAIT_NS = 60000000000LL;   // longest wait at a grid barrier (60 s)
+constexpr int COOP_MIN_FRONT = 192;                 // fronts from this order up use the helpers
+
+__device__ __forceinline__ unsigned int ld_acquire_u32(const unsigned int* p) {
+    unsigned int v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ int ld_volatile_i32(const int* p) { return *(const volatile int*)p; }
+__device__ __forceinline__ unsigned long long gtimer() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Grid barrier over all CTAs of the cooperative launch.  Returns false (on every thread) once any
+// wait has timed out; the barrier then no longer waits.
+__device__ bool coop_barrier(CoopCtl* c) {
+    __syncthreads();
+    if (threadIdx.x == 0 && ld_volatile_i32(&c->abort) == 0) {
+        const unsigned int g = ld_acquire_u32(&c->gen);
+        __threadfence();
+        const unsigned int prev = atomicAdd(&c->count, 1u);
+        if (prev + 1 == gridDim.x) {
+            atomicExch(&c->count, 0u);
+            __threadfence();
+            atomicAdd(&c->gen, 1u);
+        } else {
+            const unsigned long long t0 = gtimer();
+            unsigned int nap = 100;   // ns; backs off to 8 us so idle helpers poll the hot word rarely
+            while (ld_acquire_u32(&c->gen) == g) {
+                if (ld_volatile_i32(&c->abort) != 0) break;
+                if ((long long)(gtimer() - t0) > COOP_WAIT_NS) { atomicExch(&c->abort, 1); break; }
+                __nanosleep(nap);
+                if (nap < 8000) nap *= 2;
+            }
+        }
+    }
+    __syncthreads();
+    asm volatile("fence.acq_rel.gpu;" ::: "memory");
+    return ld_volatile_i32(&c->abort) == 0;
+}
+
+// one command's share for this rank (every CTA of the grid runs it between two barriers)
+__device__ void coop_exec(CoopCtl* c, Shared& sh, int rank, int nranks) {
+    if (threadIdx.x == 0) {
+        const volatile CoopCtl* vc = c;
+        sh.ibuf[0] = vc->cmd;
+        for (int k = 0; k < 7; ++k) sh.ibuf[1 + k] = vc->ia[k];
+    }
+    __syncthreads();
+    const int cmd = sh.ibuf[0];
+    const int* ia = sh.ibuf + 1;
+    const volatile CoopCtl* vc = c;
+    void* p0 = vc->pa[0];
+    void* p1 = vc->pa[1];
+    void* p2 = vc->pa[2];
+    const long long l0 = vc->la[0];
+    __syncthreads();
+    const int tid = threadIdx.x;
+    if (cmd == COOP_FILL) {                 // p0[0 .. l0) = 0 (doubles)
+        double* x = (double*)p0;
+        for (long long i = (long long)rank * NT + tid; i < l0; i += (long long)NT * nranks) x[i] = 0;
+    } else if (cmd == COOP_COPY) {          // (FT) p0[i] = p1[i], i < l0; ia[0] = FP32
+        const double* src = (const double*)p1;
+        if (ia[0]) { float* dst = (float*)p0; for (long long i = (long long)rank * NT + tid; i < l0; i += (long long)NT * nranks) dst[i] = (float)src[i]; }
+        else { double* dst = (double*)p0; for (long long i = (long long)rank * NT + tid; i < l0; i += (long long)NT * nranks) dst[i] = src[i]; }
+    } else if (cmd == COOP_UPDATE) {        // update_cols(p0, nf=ia1, J0=ia2, nb=ia3, K0=ia4, K1=ia5); ia0 = FP32
+        if (ia[0]) update_cols_f32((float*)p0, ia[1], ia[2], ia[3], ia[4], ia[5], sh, rank, nranks);
+        else update_cols_f64((double*)p0, ia[1], ia[2], ia[3], ia[4], ia[5], sh, rank, nranks);
+    } else if (cmd == COOP_PANEL) {         // panel_rows(p0, nf=ia1, k0=ia2, kb=ia3); ia0 = FP32
+        if (ia[0]) panel_rows<float>((float*)p0, ia[1], ia[2], ia[3], sh, rank, nranks, rank != 0);
+        else panel_rows<double>((double*)p0, ia[1], ia[2], ia[3], sh, rank, nranks, rank != 0);
+    } else if (cmd == COOP_EXTEND) {        // parent p1 += child p0's update block; ia: FP32, nfr, nres, nsep, np; p2 = rel
+        const int nfr = ia[1], nres = ia[2], nsep = ia[3], np = ia[4];
+        const int* rel = (const int*)p2;
+        for (long long t = (long long)rank * NT + tid; t < (long long)nsep * nsep; t += (long long)NT * nranks) {
+            const int i = (int)(t % nsep), j = (int)(t / nsep);
+            if (i < j) continue;
+            const long long dst = rel[i] + (long long)rel[j] * np, src = (nres + i) + (long long)(nres + j) * nfr;
+            if (ia[0]) ((float*)p1)[dst] += ((const float*)p0)[src];
+            else ((double*)p1)[dst] += ((const double*)p0)[src];
+        }
+    }
+    __syncthreads();
+}
+
+// leader: post a command (fields set by the caller's thread 0 through `post`) and run its share
+template <class Post>
+__device__ bool coop_call(CoopCtl* c, Shared& sh, Post post) {
+    if (threadIdx.x == 0) post(c);
+    if (!coop_barrier(c)) return false;
+    coop_exec(c, sh, 0, gridDim.x);
+    return coop_barrier(c);
+}
+
+// helpers: serve commands until COOP_EXIT or an abort
+__device__ void coop_helper(CoopCtl* c, Shared& sh) {
+    for (;;) {
+        if (!coop_barrier(c)) return;
+        if (threadIdx.x == 0) sh.ibuf[0] = ((const volatile CoopCtl*)c)->cmd;
+        __syncthreads();
+        const int cmd = sh.ibuf[0];
+        __syncthreads();
+        if (cmd == COOP_EXIT) return;
+        coop_exec(c, sh, blockIdx.x, gridDim.x);
+        if (!coop_barrier(c)) return;
+    }
+}
+
+template <class FT> struct IsF32 { static constexpr int v = 0; };
+template <> struct IsF32<float> { static constexpr int v = 1; };
+
+template <class FT>
+__device__ __forceinline__ void update_cols(FT* M, int nf, int J0, int nb, int K0, int K1, Shared& sh);
+template <>
+__device__ __forceinline__ void update_cols<double>(double* M, int nf, int J0, int nb, int K0, int K1, Shared& sh) {
+    update_cols_f64(M, nf, J0, nb, K0, K1, sh);
+}
+template <>
+__device__ __forceinline__ void update_cols<float>(float* M, int nf, int J0, int nb, int K0, int K1, Shared& sh) {
+    update_cols_f32(M, nf, J0, nb, K0, K1, sh);
+}
+
+constexpr int COOP_ABORTED = -1;   // front_chol result when the grid barrier timed out
+
+// Front factorization: left-looking over 64-column blocks (each column updated once, from final L
+// columns), 32-column diagonal/panel steps inside a block, then the separator's Schur complement
+// (the update matrix handed to the parent by extend-add).  With `coop` and a front of at least
+// COOP_MIN_FRONT, the update tiles and panel rows are shared with the helper CTAs.
+template <class FT>
+__device__ int front_chol_ll(FT* M, int nf, int nres, Shared& sh, CoopCtl* coop) {
+    const bool big = coop != nullptr && nf >= COOP_MIN_FRONT;
+    auto upd = [&](int J0, int nb, int K0, int K1) -> bool {
+        if (K1 <= K0 || nb <= 0) return true;
+        if (!big) { update_cols<FT>(M, nf, J0, nb, K0, K1, sh); return true; }
+        return coop_call(coop, sh, [&](CoopCtl* c) {
+            c->cmd = COOP_UPDATE; c->pa[0] = M;
+            c->ia[0] = IsF32<FT>::v; c->ia[1] = nf; c->ia[2] = J0; c->ia[3] = nb; c->ia[4] = K0; c->ia[5] = K1;
+        });
+    };
+    for (int J = 0; J < nres; J += 64) {
+        const int nb = min(64, nres - J);
+        if (!upd(J, nb, 0, J)) return COOP_ABORTED;
+        for (int h = 0; h < nb; h += 32) {
+            const int k0 = J + h, kb = min(32, nb - h);
+            if (h > 0 && !upd(k0, kb, J, J + 32)) return COOP_ABORTED;
+            const int info = diag_factor<FT>(M, nf, k0, kb, sh);
+            if (info) return info;
+            if (!big) panel_rows<FT>(M, nf, k0, kb, sh, 0, 1, false);
+            else if (!coop_call(coop, sh, [&](CoopCtl* c) {
+                         c->cmd = COOP_PANEL; c->pa[0] = M;
+                         c->ia[0] = IsF32<FT>::v; c->ia[1] = nf; c->ia[2] = k0; c->ia[3] = kb;
+                     }))
+                return COOP_ABORTED;
+        }
+    }
+    for (int J = nres; J < nf; J += 64)
+        if (!upd(J, min(64, nf - J), 0, nres)) return COOP_ABORTED;
+    return 0;
+}
+
 // ---------------------------------------------------------------------------------------------
 // the per-instance solver
 // ---------------------------------------------------------------------------------------------
@@ -529,6 +560,7 @@ struct Ctx {
     const DevInst& I;
     Settings set;
     Shared& sh;
+    CoopCtl* coop;          // grid-cooperative mode (one large instance), else null
     double* red;
     double* F64;            // the factor storage viewed as FP64 ...
     float* F32;             // ... or as FP32 (same buffer)
@@ -550,7 +582,8 @@ struct Ctx {
     long long ntrsv, ngemv;
     __device__ long long tic() const { __syncthreads(); return clock64(); }
     __device__ void toc(int sec, long long t0) { __syncthreads(); tsec[sec] += clock64() - t0; }
-    __device__ Ctx(const DevInst& I_, const Settings& s_, Shared& sh_) : I(I_), set(s_), sh(sh_) {
+    __device__ Ctx(const DevInst& I_, const Settings& s_, Shared& sh_, CoopCtl* coop_ = nullptr)
+        : I(I_), set(s_), sh(sh_), coop(coop_) {
         red = sh.red;
         F64 = reinterpret_cast<double*>(I.F);
         F32 = reinterpret_cast<float*>(I.F);
@@ -677,8 +710,12 @@ struct Ctx {
     __device__ void build_finit() {
         const DevSp& B = I.B;
         const int tid = threadIdx.x;
-        for (int64_t i = tid; i < I.fsize; i += NT) I.Finit[i] = 0;
-        __syncthreads();
+        if (coop && I.fsize >= ((int64_t)1 << 20)) {
+            coop_call(coop, sh, [&](CoopCtl* c) { c->cmd = COOP_FILL; c->pa[0] = I.Finit; c->la[0] = I.fsize; });
+        } else {
+            for (int64_t i = tid; i < I.fsize; i += NT) I.Finit[i] = 0;
+            __syncthreads();
+        }
         for (int r = 0; r < m; ++r) {
             const int k0 = B.rptr[r], nz = B.rptr[r + 1] - k0;
             const int np = nz * (nz + 1) / 2;
@@ -914,7 +951,11 @@ struct Ctx {
     template <class FT>
     __device__ void assemble_t(FT* F, double dl, double rho) {
         const int tid = threadIdx.x;
-        {
+        if (coop && I.fsize >= ((int64_t)1 << 20)) {   // the copy F <- Finit shared with the helpers
+            coop_call(coop, sh, [&](CoopCtl* c) {
+                c->cmd = COOP_COPY; c->pa[0] = F; c->pa[1] = I.Finit; c->la[0] = I.fsize; c->ia[0] = IsF32<FT>::v;
+            });
+        } else {
             int64_t i = tid;
             for (; i + 3 * NT < I.fsize; i += 4 * NT) {
                 double a0 = I.Finit[i], a1 = I.Finit[i + NT], a2 = I.Finit[i + 2 * NT], a3 = I.Finit[i + 3 * NT];
@@ -977,13 +1018,22 @@ struct Ctx {
         for (int f = 0; f < I.nfront; ++f) {
             int nres = I.fnres[f], nsep = I.fnsep[f], nfr = nres + nsep;
             FT* M = F + I.fptr[f];
-            int info = front_chol<FT>(M, nfr, nres, sh);
+            int info = front_chol_ll<FT>(M, nfr, nres, sh, coop);
+            if (info == COOP_ABORTED) return COOP_ABORTED;
             if (info) return I.fres0[f] + info;
             int p = I.fparent[f];
             if (p >= 0 && nsep > 0) {
                 int np = I.fnres[p] + I.fnsep[p];
                 FT* P = F + I.fptr[p];
                 const int* rel = I.frel + I.fsepp[f];
+                if (coop && nsep >= COOP_MIN_FRONT) {   // extend-add shared with the helpers
+                    if (!coop_call(coop, sh, [&](CoopCtl* c) {
+                            c->cmd = COOP_EXTEND; c->pa[0] = M; c->pa[1] = P; c->pa[2] = (void*)rel;
+                            c->ia[0] = IsF32<FT>::v; c->ia[1] = nfr; c->ia[2] = nres; c->ia[3] = nsep; c->ia[4] = np;
+                        }))
+                        return COOP_ABORTED;
+                    continue;
+                }
                 for (int64_t t = threadIdx.x; t < (int64_t)nsep * nsep; t += NT) {
                     int i = (int)(t % nsep), j = (int)(t / nsep);
                     if (i >= j) P[rel[i] + (int64_t)rel[j] * np] += M[(nres + i) + (int64_t)(nres + j) * nfr];
@@ -1444,13 +1494,13 @@ struct Ctx {
 
 // init (solver/ipm.jl:431-478 and reinit! :375-429), then the solve_impl! loop
 // (solver/solver.jl:119-145) and result, or one of those pieces (mode)
-__device__ void solve_instance(const DevInst& I, const Settings& set, Shared& sh, int mode) {
+__device__ void solve_instance(const DevInst& I, const Settings& set, Shared& sh, int mode, CoopCtl* coop = nullptr) {
     const int n = I.n, m = I.m;
     if (mode == MODE_SOLVE || mode == MODE_INIT) {
         if (threadIdx.x == 0) { for (int k = 0; k < NSTAT; ++k) I.status[k] = 0; }
         __syncthreads();
     }
-    Ctx c(I, set, sh);
+    Ctx c(I, set, sh, coop);
     if (mode == MODE_SOLVE || mode == MODE_INIT) {
         // working copies of the inputs: a solve never modifies the uploaded problem
         for (int i = threadIdx.x; i < I.B.nnz; i += NT) I.B.val[i] = I.B.val0[i];
@@ -1586,7 +1636,42 @@ __global__ void __launch_bounds__(NT, CTA_PER_SM) ipm_batch_kernel(BatchArgs a) 
     }
 }
 
+// One large instance on the whole GPU (cooperative launch): CTA 0 runs the solve and posts the
+// dense work of its large fronts to the other CTAs; COOP_EXIT releases them when it is done.
+__global__ void __launch_bounds__(NT, CTA_PER_SM) ipm_coop_kernel(BatchArgs a, CoopCtl* c) {
+    extern __shared__ __align__(16) unsigned char mb_dsmem[];
+    Shared& sh = *reinterpret_cast<Shared*>(mb_dsmem);
+    if (blockIdx.x != 0) { coop_helper(c, sh); return; }
+    const DevInst& I = a.inst[0];
+    const unsigned long long t0 = globaltimer();
+    solve_instance(I, a.set, sh, a.mode, c);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        I.scal[SCAL_T0] = __longlong_as_double((long long)t0);
+        I.scal[SCAL_T1] = __longlong_as_double((long long)globaltimer());
+        c->cmd = COOP_EXIT;
+    }
+    coop_barrier(c);
+    if (threadIdx.x == 0 && ld_volatile_i32(&c->abort) != 0) I.status[7] = 1;
+}
+
 }  // namespace mb
+
+// grid-cooperative launch of one instance: every CTA of the grid co-resident (grid <= 2 per SM)
+extern "C" int mb_launch_coop(const mb::DevInst* d_inst, int mode, const mb::Settings* set, mb::CoopCtl* d_ctl,
+                              int grid, cudaStream_t stream) {
+    cudaError_t e = cudaMemsetAsync(d_ctl, 0, sizeof(mb::CoopCtl), stream);
+    if (e != cudaSuccess) return -1;
+    e = cudaFuncSetAttribute(mb::ipm_coop_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(mb::Shared));
+    if (e != cudaSuccess) return -1;
+    mb::BatchArgs a;
+    a.inst = d_inst; a.ninst = 1; a.mode = mode; a.set = *set; a.counter = nullptr;
+    a.done = nullptr; a.seq0 = 0; a.cap = 1;
+    void* args[] = {(void*)&a, (void*)&d_ctl};
+    e = cudaLaunchCooperativeKernel((const void*)mb::ipm_coop_kernel, dim3(grid), dim3(mb::NT), args,
+                                    sizeof(mb::Shared), stream);
+    return e == cudaSuccess ? 0 : -2;
+}
 
 // ---------------------------------------------------------------------------------------------
 // launch entry used by the host runtime
@@ -1662,4 +1747,15 @@ extern "C" int mb_launch_wave(const mb::DevInst* d_inst, int ninst, const mb::Se
     if (e != cudaSuccess) return -1;
     mb::ipm_batch_kernel<<<grid, mb::NT, sizeof(mb::Shared), stream>>>(a);
     return cudaGetLastError() == cudaSuccess ? 0 : -2;
+}
+
+// CTAs of ipm_coop_kernel that can be co-resident (the grid of a cooperative launch)
+extern "C" int mb_coop_grid(int device, int nsm) {
+    (void)device;
+    int per_sm = 0;
+    if (cudaFuncSetAttribute(mb::ipm_coop_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(mb::Shared)) != cudaSuccess)
+        return nsm;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, mb::ipm_coop_kernel, mb::NT, sizeof(mb::Shared)) != cudaSuccess || per_sm < 1)
+        return nsm;
+    return nsm * (per_sm < mb::CTA_PER_SM ? per_sm : mb::CTA_PER_SM);
 }

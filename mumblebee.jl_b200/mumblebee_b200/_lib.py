@@ -18,7 +18,7 @@ PI64, PF64, PI32 = C.POINTER(I64), C.POINTER(F64), C.POINTER(I32)
 
 class mb_settings(C.Structure):
     _fields_ = [("verbose", I32), ("max_iter", I32), ("scale_max_iter", I32), ("refine_max_iter", I32),
-                ("newton_max_iter", I32), ("stable", I32), ("precision", I32), ("reserved", I32),
+                ("newton_max_iter", I32), ("stable", I32), ("precision", I32), ("large", I32),
                 ("step_frac", F64), ("feas_tol", F64), ("gap_tol", F64), ("near_factor", F64),
                 ("stall_tol", F64), ("refine_stall_tol", F64), ("aug_tol", F64), ("infeas_abs", F64),
                 ("infeas_rel", F64)]

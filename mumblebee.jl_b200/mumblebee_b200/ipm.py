@@ -106,6 +106,7 @@ class IPMSettings:
     infeas_abs: float = 1e-8
     infeas_rel: float = 1e-8
     precision: str = "fp64"          # "fp64", "fp32" or "mixed" (factor precision; refinement stays FP64)
+    large: int = 0                   # a lone large instance runs grid-cooperatively: 0 auto, 1 always, -1 never
 
     def to_c(self) -> mb_settings:
         s = mb_settings()

@@ -623,7 +623,7 @@ typedef struct {
     int32_t newton_max_iter;
     int32_t stable;
     int32_t precision;      // 0 = FP64 factor, 1 = FP32 factor (mixed)
-    int32_t reserved;
+    int32_t large;
     double step_frac;
     double feas_tol;
     double gap_tol;

@@ -29,7 +29,7 @@ class Settings(C.Structure):
     """IPMSettings (settings/ipm.jl:1-18) plus the precision knob; layout shared with mb_settings."""
     _fields_ = [("verbose", C.c_int32), ("max_iter", C.c_int32), ("scale_max_iter", C.c_int32),
                 ("refine_max_iter", C.c_int32), ("newton_max_iter", C.c_int32), ("stable", C.c_int32),
-                ("precision", C.c_int32), ("reserved", C.c_int32),
+                ("precision", C.c_int32), ("large", C.c_int32),
                 ("step_frac", C.c_double), ("feas_tol", C.c_double), ("gap_tol", C.c_double),
                 ("near_factor", C.c_double), ("stall_tol", C.c_double), ("refine_stall_tol", C.c_double),
                 ("aug_tol", C.c_double), ("infeas_abs", C.c_double), ("infeas_rel", C.c_double)]
@@ -37,7 +37,7 @@ class Settings(C.Structure):
 
 def default_settings(**kw) -> Settings:
     s = Settings(verbose=0, max_iter=100, scale_max_iter=10, refine_max_iter=10, newton_max_iter=100,
-                 stable=0, precision=0, reserved=0, step_frac=0.99, feas_tol=1e-8, gap_tol=1e-8,
+                 stable=0, precision=0, large=0, step_frac=0.99, feas_tol=1e-8, gap_tol=1e-8,
                  near_factor=1000.0, stall_tol=1e-3, refine_stall_tol=0.5, aug_tol=1e-7,
                  infeas_abs=1e-8, infeas_rel=1e-8)
     for k, v in kw.items():

@@ -1,0 +1,43 @@
+"""Grid-cooperative mode for one large instance (settings `large`): the leader CTA runs the solve and
+the helper CTAs take update tiles, panel rows, extend-adds and the assembly copy of its large
+fronts.  Each of those elements is still computed by exactly one CTA in the same order, so the
+result must equal the one-CTA path bit for bit."""
+import numpy as np
+import pytest
+
+from helpers import SDP, block_problem
+from mumblebee_b200 import generators as G
+from mumblebee_b200.ipm import Context, IPMProblem, IPMSettings, IPMStatus, solve
+
+pytestmark = pytest.mark.gpu
+
+CASES = {
+    "socp500": lambda: G.socp(500, 200, 25, 0.05, 0),                       # one front of 500
+    "port300": lambda: G.portfolio(300, seed=4),                            # one front of 621
+    "maxcut30": lambda: G.maxcut(30, 15, 2, 1),                             # SDP, one front of 465
+    "exppow_multi": lambda: G.exppow(nexp=150, npow=60, nfree=200, npos=200, m=400, density=0.01, seed=2),
+}
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_large_mode_equals_one_cta(name):
+    prob = IPMProblem.from_dict(block_problem(CASES[name]()), ctx=Context.default())
+    tol = dict(feas_tol=1e-7, gap_tol=1e-7) if name.startswith("exppow") else {}
+    a = solve(prob, IPMSettings(large=-1, **tol))
+    b = solve(prob, IPMSettings(large=1, **tol))
+    assert a.status == b.status and a.status in (IPMStatus.OPTIMAL, IPMStatus.NEAR_OPTIMAL)
+    assert a.niter == b.niter and a.nfactor == b.nfactor
+    assert a.pobj == b.pobj and a.dobj == b.dobj
+    for x, y in ((a.p, b.p), (a.d, b.d), (a.y, b.y)):
+        assert np.array_equal(x, y)
+
+
+def test_large_mode_sdp_and_step_api():
+    from mumblebee_b200.ipm import init
+    prob = IPMProblem.from_dict(block_problem(SDP["sdp1x10"]()), ctx=Context.default())
+    a = solve(prob, IPMSettings(large=-1))
+    s = init(prob, IPMSettings(large=1))
+    while s.step() == IPMStatus.CONTINUE:
+        pass
+    b = s.result()
+    assert a.niter == b.niter and a.pobj == b.pobj

@@ -22,7 +22,12 @@ COMMON = ["-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-lineinfo"]
 
 SOURCES_CU = ["mb_solver.cu"]
 SOURCES_CPP = ["mb_host.cpp"]
-HEADERS = ["mb_internal.h", "mb_device.cuh", "mb_cones.cuh", "mb_tdc.cuh", "mb_sdp.cuh", "mb_symbolic.hpp"]
+# headers each source includes (a change rebuilds only the sources that use it)
+DEPS = {
+    "mb_solver.cu": ["mb_internal.h", "mb_device.cuh", "mb_cones.cuh", "mb_tdc.cuh", "mb_sdp.cuh"],
+    "mb_host.cpp": ["mb_internal.h", "mb_symbolic.hpp"],
+}
+HEADERS = sorted({h for v in DEPS.values() for h in v})
 
 
 def _newer(target, deps):
@@ -36,12 +41,13 @@ def build(verbose: bool = False, force: bool = False) -> str:
     os.makedirs(LIBDIR, exist_ok=True)
     objdir = os.path.join(HERE, "_build")
     os.makedirs(objdir, exist_ok=True)
-    hdrs = [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(HERE, "..", "include", "mumblebee_gpu.h")]
+    api = os.path.join(HERE, "..", "include", "mumblebee_gpu.h")
     objs = []
     for src in SOURCES_CU + SOURCES_CPP:
         s = os.path.join(CSRC, src)
         o = os.path.join(objdir, src + ".o")
         objs.append(o)
+        hdrs = [os.path.join(CSRC, h) for h in DEPS[src]] + [api]
         if force or _newer(o, [s] + hdrs):
             cmd = [NVCC] + ARCH + COMMON + ["-c", s, "-o", o]
             if src.endswith(".cu"):

@@ -129,9 +129,10 @@ struct CoopCtl {
     int ia[8];
     long long la[4];
     void* pa[4];
+    double acc[32];         // backward-solve column dots gathered from the helpers
 };
 enum CoopCmd { COOP_NONE = 0, COOP_EXIT = 1, COOP_FILL = 2, COOP_COPY = 3, COOP_UPDATE = 4, COOP_PANEL = 5,
-               COOP_EXTEND = 6 };
+               COOP_EXTEND = 6, COOP_LROWS = 7, COOP_UDOTS = 8 };
 
 
 }  // namespace mb

@@ -304,95 +304,66 @@ __device__ void update_cols_f32(float* M, int nf, int J0, int nb, int K0, int K1
 
 
 
-// forward solve with front f: x[res] <- D⁻¹ x[res]; x[sep] -= L_off x[res]
+// forward-solve row update for the 32-column block at k0: x[row i] -= L[i, k0:k0+kb] xs for the rows
+// i >= k0 + kb of this rank (row blocks of NT dealt over nranks CTAs); xs = sh.xs, or with `load`
+// read back from x (a helper CTA)
 template <class FT>
-__device__ void front_lsolve(const FT* M, int nf, int nres, int r0, const int* sep, double* x, Shared& sh) {
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    double* T = sh.diag;   // the 32x32 diagonal triangle, T[c*33 + r] = L[k0+r, k0+c]
-    for (int k0 = 0; k0 < nres; k0 += 32) {
-        const int kb = min(32, nres - k0);
-        for (int idx = tid; idx < 32 * 32; idx += NT) {
-            int r = idx & 31, c = idx >> 5;
-            if (r < kb && c < kb && r >= c) T[c * 33 + r] = (double)M[(k0 + r) + (int64_t)(k0 + c) * nf];
-        }
-        __syncthreads();
-        if (warp == 0) {
-            double xv = lane < kb ? x[r0 + k0 + lane] : 0.0;
-            for (int c = 0; c < kb; ++c) {
-                if (lane == c) xv = xv / T[c * 33 + c];
-                double xc = __shfl_sync(0xffffffffu, xv, c);
-                if (lane > c && lane < kb) xv -= T[c * 33 + lane] * xc;
-            }
-            if (lane < kb) { x[r0 + k0 + lane] = xv; sh.xs[lane] = xv; }
-        }
-        __syncthreads();
-        for (int i = k0 + kb + tid; i < nf; i += NT) {
-            const FT* Mi = M + i + (int64_t)k0 * nf;
-            double t = 0;
-            if (kb == 32) {   // all 32 loads in flight before the FMA chain
-                FT v[32];
-#pragma unroll
-                for (int c = 0; c < 32; ++c) v[c] = Mi[(int64_t)c * nf];
-#pragma unroll
-                for (int c = 0; c < 32; ++c) t = fma((double)v[c], sh.xs[c], t);
-            } else {
-                for (int c = 0; c < kb; ++c) t = fma((double)Mi[(int64_t)c * nf], sh.xs[c], t);
-            }
-            int tg = i < nres ? r0 + i : sep[i - nres];
-            x[tg] -= t;
-        }
+__device__ void lsolve_rows(const FT* M, int nf, int nres, int r0, const int* sep, double* x, int k0, int kb,
+                            Shared& sh, int rank, int nranks, bool load) {
+    const int tid = threadIdx.x;
+    if (load) {
+        if (tid < kb) sh.xs[tid] = x[r0 + k0 + tid];
         __syncthreads();
     }
+    for (int i = k0 + kb + rank * NT + tid; i < nf; i += NT * nranks) {
+        const FT* Mi = M + i + (int64_t)k0 * nf;
+        double t = 0;
+        if (kb == 32) {   // all 32 loads in flight before the FMA chain
+            FT v[32];
+#pragma unroll
+            for (int c = 0; c < 32; ++c) v[c] = Mi[(int64_t)c * nf];
+#pragma unroll
+            for (int c = 0; c < 32; ++c) t = fma((double)v[c], sh.xs[c], t);
+        } else {
+            for (int c = 0; c < kb; ++c) t = fma((double)Mi[(int64_t)c * nf], sh.xs[c], t);
+        }
+        int tg = i < nres ? r0 + i : sep[i - nres];
+        x[tg] -= t;
+    }
+    __syncthreads();
 }
 
-// backward solve with front f: x[res] -= L_offᵀ x[sep]; x[res] <- D⁻ᵀ x[res]
+// backward-solve column dots for the 32-column block at k0: out[c] = L[k0+kb:, k0+c] · x[rows], one
+// warp per column, columns dealt over the gw-th of `gws` warps of the grid
 template <class FT>
-__device__ void front_usolve(const FT* M, int nf, int nres, int r0, const int* sep, double* x, Shared& sh) {
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int nblk = (nres + 31) / 32;
-    double* T = sh.diag;   // T[c*33 + r] = L[k0+r, k0+c]
-    for (int bk = nblk - 1; bk >= 0; --bk) {
-        const int k0 = bk * 32, kb = min(32, nres - k0);
-        for (int idx = tid; idx < 32 * 32; idx += NT) {
-            int r = idx & 31, c = idx >> 5;
-            if (r < kb && c < kb && r >= c) T[c * 33 + r] = (double)M[(k0 + r) + (int64_t)(k0 + c) * nf];
+__device__ void usolve_dots(const FT* M, int nf, int nres, int r0, const int* sep, const double* x, int k0, int kb,
+                            double* out, int gw, int gws) {
+    const int lane = threadIdx.x & 31;
+    for (int c = gw; c < kb; c += gws) {
+        const FT* Mc = M + (int64_t)(k0 + c) * nf;
+        double t0 = 0, t1 = 0, t2 = 0, t3 = 0;
+        int i = k0 + kb + lane;
+        for (; i + 96 < nf; i += 128) {   // four rows per lane in flight
+            int s0 = i < nres ? r0 + i : sep[i - nres];
+            int s1 = i + 32 < nres ? r0 + i + 32 : sep[i + 32 - nres];
+            int s2 = i + 64 < nres ? r0 + i + 64 : sep[i + 64 - nres];
+            int s3 = i + 96 < nres ? r0 + i + 96 : sep[i + 96 - nres];
+            double m0 = (double)Mc[i], m1 = (double)Mc[i + 32], m2 = (double)Mc[i + 64], m3 = (double)Mc[i + 96];
+            t0 = fma(m0, x[s0], t0); t1 = fma(m1, x[s1], t1); t2 = fma(m2, x[s2], t2); t3 = fma(m3, x[s3], t3);
         }
-        for (int c = warp; c < kb; c += NW) {
-            const FT* Mc = M + (int64_t)(k0 + c) * nf;
-            double t0 = 0, t1 = 0, t2 = 0, t3 = 0;
-            int i = k0 + kb + lane;
-            for (; i + 96 < nf; i += 128) {   // four rows per lane in flight
-                int s0 = i < nres ? r0 + i : sep[i - nres];
-                int s1 = i + 32 < nres ? r0 + i + 32 : sep[i + 32 - nres];
-                int s2 = i + 64 < nres ? r0 + i + 64 : sep[i + 64 - nres];
-                int s3 = i + 96 < nres ? r0 + i + 96 : sep[i + 96 - nres];
-                double m0 = (double)Mc[i], m1 = (double)Mc[i + 32], m2 = (double)Mc[i + 64], m3 = (double)Mc[i + 96];
-                t0 = fma(m0, x[s0], t0); t1 = fma(m1, x[s1], t1); t2 = fma(m2, x[s2], t2); t3 = fma(m3, x[s3], t3);
-            }
-            for (; i < nf; i += 32) {
-                int src = i < nres ? r0 + i : sep[i - nres];
-                t0 = fma((double)Mc[i], x[src], t0);
-            }
-            double t = warp_sum((t0 + t1) + (t2 + t3));
-            if (lane == 0) sh.acc[c] = t;
+        for (; i < nf; i += 32) {
+            int src = i < nres ? r0 + i : sep[i - nres];
+            t0 = fma((double)Mc[i], x[src], t0);
         }
-        __syncthreads();
-        if (warp == 0) {
-            double yv = lane < kb ? x[r0 + k0 + lane] - sh.acc[lane] : 0.0;
-            for (int c = kb - 1; c >= 0; --c) {
-                if (lane == c) yv = yv / T[c * 33 + c];
-                double xc = __shfl_sync(0xffffffffu, yv, c);
-                if (lane < c) yv -= T[lane * 33 + c] * xc;
-            }
-            if (lane < kb) x[r0 + k0 + lane] = yv;
-        }
-        __syncthreads();
+        double t = warp_sum((t0 + t1) + (t2 + t3));
+        if (lane == 0) out[c] = t;
     }
 }
 
 // ---- grid-cooperative help for large fronts (CoopCtl) ----------------------------------------
 constexpr long long COOP_WAIT_NS = 60000000000LL;   // longest wait at a grid barrier (60 s)
 constexpr int COOP_MIN_FRONT = 192;                 // fronts from this order up use the helpers
+constexpr int COOP_MIN_SOLVE = 2048;                // ... and in the triangular solves from this order up
 
 __device__ __forceinline__ unsigned int ld_acquire_u32(const unsigned int* p) {
     unsigned int v;
@@ -464,6 +435,13 @@ __device__ void coop_exec(CoopCtl* c, Shared& sh, int rank, int nranks) {
     } else if (cmd == COOP_PANEL) {         // panel_rows(p0, nf=ia1, k0=ia2, kb=ia3); ia0 = FP32
         if (ia[0]) panel_rows<float>((float*)p0, ia[1], ia[2], ia[3], sh, rank, nranks, rank != 0);
         else panel_rows<double>((double*)p0, ia[1], ia[2], ia[3], sh, rank, nranks, rank != 0);
+    } else if (cmd == COOP_LROWS) {         // lsolve_rows(p0, nf=ia1, nres=ia2, r0=ia3, sep=p1, x=p2, k0=ia4, kb=ia5)
+        if (ia[0]) lsolve_rows<float>((const float*)p0, ia[1], ia[2], ia[3], (const int*)p1, (double*)p2, ia[4], ia[5], sh, rank, nranks, true);
+        else lsolve_rows<double>((const double*)p0, ia[1], ia[2], ia[3], (const int*)p1, (double*)p2, ia[4], ia[5], sh, rank, nranks, true);
+    } else if (cmd == COOP_UDOTS) {         // usolve_dots(...) into c->acc, columns over all warps of the grid
+        const int gw = rank * NW + (threadIdx.x >> 5), gws = nranks * NW;
+        if (ia[0]) usolve_dots<float>((const float*)p0, ia[1], ia[2], ia[3], (const int*)p1, (const double*)p2, ia[4], ia[5], c->acc, gw, gws);
+        else usolve_dots<double>((const double*)p0, ia[1], ia[2], ia[3], (const int*)p1, (const double*)p2, ia[4], ia[5], c->acc, gw, gws);
     } else if (cmd == COOP_EXTEND) {        // parent p1 += child p0's update block; ia: FP32, nfr, nres, nsep, np; p2 = rel
         const int nfr = ia[1], nres = ia[2], nsep = ia[3], np = ia[4];
         const int* rel = (const int*)p2;
@@ -503,6 +481,78 @@ __device__ void coop_helper(CoopCtl* c, Shared& sh) {
 
 template <class FT> struct IsF32 { static constexpr int v = 0; };
 template <> struct IsF32<float> { static constexpr int v = 1; };
+
+// forward solve with front f: x[res] <- D⁻¹ x[res]; x[sep] -= L_off x[res]
+template <class FT>
+__device__ void front_lsolve(const FT* M, int nf, int nres, int r0, const int* sep, double* x, Shared& sh,
+                             CoopCtl* coop = nullptr) {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    double* T = sh.diag;   // the 32x32 diagonal triangle, T[c*33 + r] = L[k0+r, k0+c]
+    for (int k0 = 0; k0 < nres; k0 += 32) {
+        const int kb = min(32, nres - k0);
+        for (int idx = tid; idx < 32 * 32; idx += NT) {
+            int r = idx & 31, c = idx >> 5;
+            if (r < kb && c < kb && r >= c) T[c * 33 + r] = (double)M[(k0 + r) + (int64_t)(k0 + c) * nf];
+        }
+        __syncthreads();
+        if (warp == 0) {
+            double xv = lane < kb ? x[r0 + k0 + lane] : 0.0;
+            for (int c = 0; c < kb; ++c) {
+                if (lane == c) xv = xv / T[c * 33 + c];
+                double xc = __shfl_sync(0xffffffffu, xv, c);
+                if (lane > c && lane < kb) xv -= T[c * 33 + lane] * xc;
+            }
+            if (lane < kb) { x[r0 + k0 + lane] = xv; sh.xs[lane] = xv; }
+        }
+        __syncthreads();
+        if (!coop) {
+            lsolve_rows<FT>(M, nf, nres, r0, sep, x, k0, kb, sh, 0, 1, false);
+        } else if (!coop_call(coop, sh, [&](CoopCtl* c) {
+                       c->cmd = COOP_LROWS; c->pa[0] = (void*)M; c->pa[1] = (void*)sep; c->pa[2] = x;
+                       c->ia[0] = IsF32<FT>::v; c->ia[1] = nf; c->ia[2] = nres; c->ia[3] = r0; c->ia[4] = k0; c->ia[5] = kb;
+                   })) {
+            return;
+        }
+    }
+}
+
+// backward solve with front f: x[res] -= L_offᵀ x[sep]; x[res] <- D⁻ᵀ x[res]
+template <class FT>
+__device__ void front_usolve(const FT* M, int nf, int nres, int r0, const int* sep, double* x, Shared& sh,
+                             CoopCtl* coop = nullptr) {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int nblk = (nres + 31) / 32;
+    double* T = sh.diag;   // T[c*33 + r] = L[k0+r, k0+c]
+    for (int bk = nblk - 1; bk >= 0; --bk) {
+        const int k0 = bk * 32, kb = min(32, nres - k0);
+        for (int idx = tid; idx < 32 * 32; idx += NT) {
+            int r = idx & 31, c = idx >> 5;
+            if (r < kb && c < kb && r >= c) T[c * 33 + r] = (double)M[(k0 + r) + (int64_t)(k0 + c) * nf];
+        }
+        if (!coop) {
+            usolve_dots<FT>(M, nf, nres, r0, sep, x, k0, kb, sh.acc, warp, NW);
+        } else {
+            if (!coop_call(coop, sh, [&](CoopCtl* c) {
+                    c->cmd = COOP_UDOTS; c->pa[0] = (void*)M; c->pa[1] = (void*)sep; c->pa[2] = x;
+                    c->ia[0] = IsF32<FT>::v; c->ia[1] = nf; c->ia[2] = nres; c->ia[3] = r0; c->ia[4] = k0; c->ia[5] = kb;
+                }))
+                return;
+            if (threadIdx.x < kb) sh.acc[threadIdx.x] = ((const volatile CoopCtl*)coop)->acc[threadIdx.x];
+        }
+        __syncthreads();
+        if (warp == 0) {
+            double yv = lane < kb ? x[r0 + k0 + lane] - sh.acc[lane] : 0.0;
+            for (int c = kb - 1; c >= 0; --c) {
+                if (lane == c) yv = yv / T[c * 33 + c];
+                double xc = __shfl_sync(0xffffffffu, yv, c);
+                if (lane < c) yv -= T[lane * 33 + c] * xc;
+            }
+            if (lane < kb) x[r0 + k0 + lane] = yv;
+        }
+        __syncthreads();
+    }
+}
+
 
 template <class FT>
 __device__ __forceinline__ void update_cols(FT* M, int nf, int J0, int nb, int K0, int K1, Shared& sh);
@@ -1079,14 +1129,16 @@ struct Ctx {
     __device__ void Lsolve_t(const FT* F, double* x) {
         for (int f = 0; f < I.nfront; ++f) {
             int nres = I.fnres[f], nfr = nres + I.fnsep[f];
-            front_lsolve<FT>(F + I.fptr[f], nfr, nres, I.fres0[f], I.fsep + I.fsepp[f], x, sh);
+            front_lsolve<FT>(F + I.fptr[f], nfr, nres, I.fres0[f], I.fsep + I.fsepp[f], x, sh,
+                             nfr >= COOP_MIN_SOLVE ? coop : nullptr);
         }
     }
     template <class FT>
     __device__ void Usolve_t(const FT* F, double* x) {
         for (int f = I.nfront - 1; f >= 0; --f) {
             int nres = I.fnres[f], nfr = nres + I.fnsep[f];
-            front_usolve<FT>(F + I.fptr[f], nfr, nres, I.fres0[f], I.fsep + I.fsepp[f], x, sh);
+            front_usolve<FT>(F + I.fptr[f], nfr, nres, I.fres0[f], I.fsep + I.fsepp[f], x, sh,
+                             nfr >= COOP_MIN_SOLVE ? coop : nullptr);
         }
     }
 

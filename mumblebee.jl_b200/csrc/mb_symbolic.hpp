@@ -417,6 +417,20 @@ inline Fronts analyze(const std::vector<std::vector<i64>>& adj0, const std::vect
     std::vector<std::vector<i64>> ch(n);
     std::vector<i64> roots;
     for (i64 v = 0; v < n; ++v) { if (par0[v] < 0) roots.push_back(v); else ch[par0[v]].push_back(v); }
+    // children are visited in increasing size of their row structure (ties by index), so the child
+    // with the largest structure, the one a chain of supernodes continues through, comes last and
+    // can merge with its parent; any postorder of the etree gives the same factor
+    {
+        std::vector<i64> ssz0(n, 0), mk(n, -1);
+        std::vector<std::vector<i64>> s0(n);
+        for (i64 v = 0; v < n; ++v) {
+            for (i64 u : adj0[v]) if (u > v && mk[u] != v) { mk[u] = v; s0[v].push_back(u); }
+            for (i64 c : ch[v]) for (i64 u : s0[c]) if (u > v && mk[u] != v) { mk[u] = v; s0[v].push_back(u); }
+            ssz0[v] = (i64)s0[v].size();
+        }
+        for (i64 v = 0; v < n; ++v)
+            std::stable_sort(ch[v].begin(), ch[v].end(), [&](i64 a, i64 b) { return ssz0[a] < ssz0[b]; });
+    }
     std::vector<i64> post; post.reserve(n);
     std::vector<std::pair<i64, size_t>> st;
     for (i64 r : roots) {

@@ -16,6 +16,7 @@ CASES = {
     "port300": lambda: G.portfolio(300, seed=4),                            # one front of 621
     "maxcut30": lambda: G.maxcut(30, 15, 2, 1),                             # SDP, one front of 465
     "exppow_multi": lambda: G.exppow(nexp=150, npow=60, nfree=200, npos=200, m=400, density=0.01, seed=2),
+    "socp2100": lambda: G.socp(2100, 840, 105, 0.012, 5),                   # front >= 2048: shared solves too
 }
 
 

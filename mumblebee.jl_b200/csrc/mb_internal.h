@@ -132,7 +132,7 @@ struct CoopCtl {
     double acc[32];         // backward-solve column dots gathered from the helpers
 };
 enum CoopCmd { COOP_NONE = 0, COOP_EXIT = 1, COOP_FILL = 2, COOP_COPY = 3, COOP_UPDATE = 4, COOP_PANEL = 5,
-               COOP_EXTEND = 6, COOP_LROWS = 7, COOP_UDOTS = 8 };
+               COOP_EXTEND = 6, COOP_LROWS = 7, COOP_UDOTS = 8, COOP_SCHUR = 9 };
 
 
 }  // namespace mb

@@ -161,9 +161,8 @@ __device__ __forceinline__ void stage_tile_f64(double* buf, const double* M, int
 // M[r, c] -= Σ_{k in [K0, K1)} M[r, k] M[c, k] for c in [J0, J0 + nb) (nb <= 64), r in [J0, nf),
 // r >= c: each 64-row tile accumulates over K in registers (FP64 DMMA) from double-buffered
 // asynchronous copies and is written back once.  Requires K1 <= J0 (the K columns are final).
-__device__ void update_cols_f64(double* M, int nf, int J0, int nb, int K0, int K1, Shared& sh, int rank = 0,
-                                int nranks = 1) {
-    if (K1 <= K0 || nb <= 0) return;
+// one 64-row tile at rb of the column block [J0, J0 + nb): accumulate over K, write back once
+__device__ void tile_f64(double* M, int nf, int rb, int J0, int nb, int K0, int K1, Shared& sh) {
     constexpr int WRN = NW / 4, RW = TS / WRN, MR = RW / 8;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int g = lane >> 2, t = lane & 3;
@@ -172,7 +171,7 @@ __device__ void update_cols_f64(double* M, int nf, int J0, int nb, int K0, int K
     const int cmax = min(nf, J0 + nb);
     double* A[2] = {sh.ta, sh.ta2};
     double* B[2] = {sh.tb, sh.tb2};
-    for (int rb = J0 + TS * rank; rb < nf; rb += TS * nranks) {
+    {
         const bool skip = wc * 16 >= nb || (rb == J0 && wr * RW + RW - 1 < wc * 16);
         double acc[MR][2][2];
 #pragma unroll
@@ -225,6 +224,13 @@ __device__ void update_cols_f64(double* M, int nf, int J0, int nb, int K0, int K
     __syncthreads();
 }
 
+__device__ void update_cols_f64(double* M, int nf, int J0, int nb, int K0, int K1, Shared& sh, int rank = 0,
+                                int nranks = 1) {
+    if (K1 <= K0 || nb <= 0) return;
+    for (int rb = J0 + TS * rank; rb < nf; rb += TS * nranks) tile_f64(M, nf, rb, J0, nb, K0, K1, sh);
+    __syncthreads();
+}
+
 __device__ __forceinline__ void cp_async4(void* sdst, const void* gsrc, bool valid) {
     const unsigned sa = (unsigned)__cvta_generic_to_shared(sdst);
     const int sz = valid ? 4 : 0;
@@ -244,15 +250,13 @@ __device__ __forceinline__ void stage_tile_f32(float* buf, const float* M, int n
 }
 
 // FP32 twin of update_cols_f64: each thread owns a 4 x 4 block of the 64 x 64 tile (FFMA)
-__device__ void update_cols_f32(float* M, int nf, int J0, int nb, int K0, int K1, Shared& sh, int rank = 0,
-                                int nranks = 1) {
-    if (K1 <= K0 || nb <= 0) return;
+__device__ void tile_f32(float* M, int nf, int rb, int J0, int nb, int K0, int K1, Shared& sh) {
     const int tr = threadIdx.x & 15, tc = threadIdx.x >> 4;
     const int nk = (K1 - K0 + 31) / 32;
     const int cmax = min(nf, J0 + nb);
     float* A[2] = {reinterpret_cast<float*>(sh.ta), reinterpret_cast<float*>(sh.ta2)};
     float* B[2] = {reinterpret_cast<float*>(sh.tb), reinterpret_cast<float*>(sh.tb2)};
-    for (int rb = J0 + TS * rank; rb < nf; rb += TS * nranks) {
+    {
         const bool skip = tc * 4 >= nb || (rb == J0 && tr * 4 + 3 < tc * 4);
         float acc[4][4];
 #pragma unroll
@@ -299,6 +303,28 @@ __device__ void update_cols_f32(float* M, int nf, int J0, int nb, int K0, int K1
                 }
         }
     }
+    __syncthreads();
+}
+
+__device__ void update_cols_f32(float* M, int nf, int J0, int nb, int K0, int K1, Shared& sh, int rank = 0,
+                                int nranks = 1) {
+    if (K1 <= K0 || nb <= 0) return;
+    for (int rb = J0 + TS * rank; rb < nf; rb += TS * nranks) tile_f32(M, nf, rb, J0, nb, K0, K1, sh);
+    __syncthreads();
+}
+
+// Schur complement of a front's separator block, M[r, c] -= Σ_{k < K1} M[r, k] M[c, k] for
+// J0 <= c <= r < nf: every (row tile, 64-column block) pair, dealt round-robin over nranks CTAs
+template <class FT>
+__device__ void schur_tiles(FT* M, int nf, int J0, int K1, Shared& sh, int rank, int nranks) {
+    if (K1 <= 0) return;
+    int gi = 0;
+    for (int J = J0; J < nf; J += 64)
+        for (int rb = J; rb < nf; rb += TS, ++gi)
+            if (gi % nranks == rank) {
+                if constexpr (sizeof(FT) == 8) tile_f64((double*)M, nf, rb, J, min(64, nf - J), 0, K1, sh);
+                else tile_f32((float*)M, nf, rb, J, min(64, nf - J), 0, K1, sh);
+            }
     __syncthreads();
 }
 
@@ -435,6 +461,9 @@ __device__ void coop_exec(CoopCtl* c, Shared& sh, int rank, int nranks) {
     } else if (cmd == COOP_PANEL) {         // panel_rows(p0, nf=ia1, k0=ia2, kb=ia3); ia0 = FP32
         if (ia[0]) panel_rows<float>((float*)p0, ia[1], ia[2], ia[3], sh, rank, nranks, rank != 0);
         else panel_rows<double>((double*)p0, ia[1], ia[2], ia[3], sh, rank, nranks, rank != 0);
+    } else if (cmd == COOP_SCHUR) {         // schur_tiles(p0, nf=ia1, J0=ia2, K1=ia3)
+        if (ia[0]) schur_tiles<float>((float*)p0, ia[1], ia[2], ia[3], sh, rank, nranks);
+        else schur_tiles<double>((double*)p0, ia[1], ia[2], ia[3], sh, rank, nranks);
     } else if (cmd == COOP_LROWS) {         // lsolve_rows(p0, nf=ia1, nres=ia2, r0=ia3, sep=p1, x=p2, k0=ia4, kb=ia5)
         if (ia[0]) lsolve_rows<float>((const float*)p0, ia[1], ia[2], ia[3], (const int*)p1, (double*)p2, ia[4], ia[5], sh, rank, nranks, true);
         else lsolve_rows<double>((const double*)p0, ia[1], ia[2], ia[3], (const int*)p1, (double*)p2, ia[4], ia[5], sh, rank, nranks, true);
@@ -598,8 +627,15 @@ __device__ int front_chol_ll(FT* M, int nf, int nres, Shared& sh, CoopCtl* coop)
                 return COOP_ABORTED;
         }
     }
-    for (int J = nres; J < nf; J += 64)
-        if (!upd(J, min(64, nf - J), 0, nres)) return COOP_ABORTED;
+    if (!big) {
+        for (int J = nres; J < nf; J += 64) upd(J, min(64, nf - J), 0, nres);
+    } else if (nres > 0 && nf > nres &&
+               !coop_call(coop, sh, [&](CoopCtl* c) {   // the whole separator block in one command
+                   c->cmd = COOP_SCHUR; c->pa[0] = M;
+                   c->ia[0] = IsF32<FT>::v; c->ia[1] = nf; c->ia[2] = nres; c->ia[3] = nres;
+               })) {
+        return COOP_ABORTED;
+    }
     return 0;
 }
 

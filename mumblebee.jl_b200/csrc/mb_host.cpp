@@ -11,6 +11,10 @@
 #include <cstdio>
 #include <cstring>
 #include <atomic>
+#include <chrono>
+#include <cstdlib>
+#include <mutex>
+#include <unordered_map>
 #include <memory>
 #include <string>
 #include <thread>
@@ -63,7 +67,50 @@ struct Sym {
     mbh::Fronts fr;
 };
 
+static Sym do_symbolic_(const mb_problem* P);
+
+// The symbolic analysis depends only on the sparsity structure: the block-column layout and arc
+// pattern of B and Q and the vertex weights.  Batches and request streams repeat structures
+// (portfolio instances of the same size, re-solved models), so analyses are kept in a bounded
+// cache keyed by that structure; a hit is checked against the full key, never the hash alone.
+struct SymKey {
+    std::vector<i64> data;
+    uint64_t hash = 0;
+    bool operator==(const SymKey& o) const { return hash == o.hash && data == o.data; }
+};
+struct SymKeyHash { size_t operator()(const SymKey& k) const { return (size_t)k.hash; } };
+
+static SymKey sym_key(const mb_problem* P) {
+    SymKey k;
+    const mbh::BSM &B = P->B, &Q = P->Q;
+    auto add = [&](const std::vector<i64>& v) { k.data.push_back((i64)v.size()); k.data.insert(k.data.end(), v.begin(), v.end()); };
+    k.data.push_back(B.nvtx); k.data.push_back(B.nout);
+    add(B.xcol); add(B.xrow); add(B.xsrc); add(B.tgt); add(Q.xsrc); add(Q.tgt);
+    uint64_t h = 1469598103934665603ull;   // FNV-1a over the 64-bit words
+    for (i64 x : k.data) { h ^= (uint64_t)x; h *= 1099511628211ull; }
+    k.hash = h;
+    return k;
+}
+
+static std::mutex g_sym_mu;
+static std::unordered_map<SymKey, std::shared_ptr<const Sym>, SymKeyHash> g_sym_cache;
+constexpr size_t SYM_CACHE_MAX = 4096;
+
 static Sym do_symbolic(const mb_problem* P) {
+    SymKey key = sym_key(P);
+    {
+        std::lock_guard<std::mutex> lk(g_sym_mu);
+        auto it = g_sym_cache.find(key);
+        if (it != g_sym_cache.end()) return *it->second;
+    }
+    auto S = std::make_shared<const Sym>(do_symbolic_(P));
+    std::lock_guard<std::mutex> lk(g_sym_mu);
+    if (g_sym_cache.size() >= SYM_CACHE_MAX) g_sym_cache.clear();
+    g_sym_cache.emplace(std::move(key), S);
+    return *S;
+}
+
+static Sym do_symbolic_(const mb_problem* P) {
     Sym S;
     const mbh::BSM& B = P->B;
     i64 nv = B.nvtx;
@@ -89,9 +136,20 @@ static Sym do_symbolic(const mb_problem* P) {
 // ---------------------------------------------------------------------------------------------
 // packing instances into device arenas
 // ---------------------------------------------------------------------------------------------
+// vector storage whose resize leaves new elements uninitialised (arenas are filled by copies)
+template <class T>
+struct NoInitAlloc : std::allocator<T> {
+    using value_type = T;
+    NoInitAlloc() = default;
+    template <class U> NoInitAlloc(const NoInitAlloc<U>&) {}
+    template <class U> struct rebind { using other = NoInitAlloc<U>; };
+    template <class U> void construct(U* p) { ::new (static_cast<void*>(p)) U; }
+    template <class U, class... Args> void construct(U* p, Args&&... args) { ::new (static_cast<void*>(p)) U(std::forward<Args>(args)...); }
+};
+
 template <class T>
 struct Arena {
-    std::vector<T> h;
+    std::vector<T, NoInitAlloc<T>> h;
     size_t n = 0;                 // for device-only arenas (no host image)
     bool host = true;
     static size_t al(size_t x) { return (x + 31) / 32 * 32; }
@@ -475,6 +533,65 @@ static int upload(mb_batch* b) {
     return MB_OK;
 }
 
+static double host_time() {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+static bool trace_on() {   // MB_TRACE=1 prints the host phases of batch preparation to stderr
+    static const bool on = [] { const char* e = std::getenv("MB_TRACE"); return e && e[0] == '1'; }();
+    return on;
+}
+
+// Concatenate single-instance plans into the batch arenas: offsets first (the layout merge()
+// builds), one allocation per arena, then the instances copied in parallel.
+static void merge_all(Packed& dst, std::vector<Packed>& src, int nth) {
+    const size_t n = src.size();
+    std::vector<size_t> b32(n), b64(n), bin(n), bw(n), bo(n), bs(n), bf(n);
+    size_t t32 = dst.i32.size(), t64 = dst.i64a.size(), tin = dst.din.size(), tw = dst.work.size(),
+           to = dst.out.size(), ts = dst.ost.size(), tf = dst.fbytes;
+    auto al = [](size_t x) { return (x + 31) / 32 * 32; };
+    for (size_t k = 0; k < n; ++k) {
+        b32[k] = al(t32); t32 = b32[k] + src[k].i32.size();
+        b64[k] = al(t64); t64 = b64[k] + src[k].i64a.size();
+        bin[k] = al(tin); tin = bin[k] + src[k].din.size();
+        bw[k] = al(tw); tw = bw[k] + src[k].work.size();
+        bo[k] = al(to); to = bo[k] + src[k].out.size();
+        bs[k] = al(ts); ts = bs[k] + src[k].ost.size();
+        bf[k] = (tf + 255) / 256 * 256; tf = bf[k] + src[k].fbytes;
+    }
+    dst.i32.h.resize(t32); dst.i64a.h.resize(t64); dst.din.h.resize(tin);
+    dst.work.n = tw; dst.out.n = to; dst.ost.n = ts; dst.fbytes = tf;
+    const size_t p0 = dst.plans.size();
+    dst.plans.resize(p0 + n);
+    std::atomic<size_t> next{0};
+    auto worker = [&]() {
+        for (;;) {
+            const size_t k = next.fetch_add(1);
+            if (k >= n) break;
+            Packed& s = src[k];
+            if (s.i32.size()) std::memcpy(dst.i32.h.data() + b32[k], s.i32.h.data(), s.i32.size() * sizeof(int32_t));
+            if (s.i64a.size()) std::memcpy(dst.i64a.h.data() + b64[k], s.i64a.h.data(), s.i64a.size() * sizeof(i64));
+            if (s.din.size()) std::memcpy(dst.din.h.data() + bin[k], s.din.h.data(), s.din.size() * sizeof(double));
+            InstPlan ip = std::move(s.plans[0]);
+            for (size_t* f : {&ip.xcol, &ip.colvtx, &ip.cfront, &ip.Brptr, &ip.Bcidx, &ip.Bcptr, &ip.Bridx, &ip.Bcpos,
+                              &ip.Qrptr, &ip.Qcidx, &ip.Qcptr, &ip.Qridx, &ip.Qcpos, &ip.hdld, &ip.qoffk, &ip.kind,
+                              &ip.fres0, &ip.fnres, &ip.fnsep, &ip.fparent, &ip.fsepp, &ip.fsep, &ip.frel}) *f += b32[k];
+            for (size_t* f : {&ip.hdoff, &ip.hdpos, &ip.qoffpos, &ip.cxblk, &ip.fptr}) *f += b64[k];
+            for (size_t* f : {&ip.Bval, &ip.Qval, &ip.Qd, &ip.f, &ip.g, &ip.kpar, &ip.p, &ip.d, &ip.y}) *f += bin[k];
+            for (size_t* f : {&ip.wBval, &ip.wQval, &ip.wQd, &ip.Hd, &ip.Finit, &ip.pscl, &ip.yscl, &ip.vn, &ip.vm, &ip.vv,
+                              &ip.work, &ip.uhist, &ip.cghist, &ip.cache, &ip.cache2, &ip.wf, &ip.wg, &ip.wp, &ip.wd, &ip.wy}) *f += bw[k];
+            for (size_t* f : {&ip.po, &ip.dout, &ip.yo, &ip.scal, &ip.hist}) *f += bo[k];
+            ip.status += bs[k];
+            ip.F += bf[k];
+            dst.plans[p0 + k] = std::move(ip);
+            s = Packed();   // release this instance's staging early
+        }
+    };
+    std::vector<std::thread> th;
+    for (int t = 1; t < std::max(1, nth); ++t) th.emplace_back(worker);
+    worker();
+    for (auto& t : th) t.join();
+}
+
 static int make_batch(mb_ctx* ctx, mb_problem* const* probs, int32_t nprob, const mb_settings* set,
                       const double* p0, const double* d0, const double* y0, mb_batch** out) {
     if (!ctx || !out || nprob < 0 || (nprob > 0 && !probs)) return fail(ctx, MB_E_ARG, "bad arguments");
@@ -485,6 +602,7 @@ static int make_batch(mb_ctx* ctx, mb_problem* const* probs, int32_t nprob, cons
     if (s.precision < 0 || s.precision > 2) return fail(ctx, MB_E_ARG, "precision must be 0 (FP64), 1 (FP32) or 2 (mixed)");
     auto b = std::make_unique<mb_batch>();
     b->ctx = ctx; b->set = s;
+    const double t_start = host_time();
     CUDA_TRY(ctx, cudaSetDevice(ctx->device));
     for (int32_t k = 0; k < nprob; ++k) if (!probs[k]) return fail(ctx, MB_E_ARG, "null problem");
     std::vector<Packed> local(nprob);
@@ -503,14 +621,16 @@ static int make_batch(mb_ctx* ctx, mb_problem* const* probs, int32_t nprob, cons
     for (int t = 1; t < nth; ++t) th.emplace_back(worker);
     worker();
     for (auto& t : th) t.join();
-    for (int32_t k = 0; k < nprob; ++k) {
-        if (rcs[k]) return fail(ctx, rcs[k], errs[k]);
-        merge(b->pk, local[k]);
-        Packed().i32.h.swap(local[k].i32.h);
-        b->probs.push_back(probs[k]);
-    }
+    for (int32_t k = 0; k < nprob; ++k) if (rcs[k]) return fail(ctx, rcs[k], errs[k]);
+    const double t_plan = host_time();
+    merge_all(b->pk, local, nth);
+    for (int32_t k = 0; k < nprob; ++k) b->probs.push_back(probs[k]);
+    const double t_merge = host_time();
     int rc = upload(b.get());
     if (rc) return rc;
+    if (trace_on())
+        fprintf(stderr, "mb_batch: %d instances, plan %.1f ms, merge %.1f ms, upload %.1f ms (%d threads)\n", nprob,
+                1e3 * (t_plan - t_start), 1e3 * (t_merge - t_plan), 1e3 * (host_time() - t_merge), nth);
     *out = b.release();
     return MB_OK;
 }

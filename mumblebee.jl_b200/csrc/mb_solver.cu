@@ -512,7 +512,7 @@ template <class FT> struct IsF32 { static constexpr int v = 0; };
 template <> struct IsF32<float> { static constexpr int v = 1; };
 
 // forward solve with front f: x[res] <- D⁻¹ x[res]; x[sep] -= L_off x[res]
-template <class FT>
+template <class FT, bool COOP = false>
 __device__ void front_lsolve(const FT* M, int nf, int nres, int r0, const int* sep, double* x, Shared& sh,
                              CoopCtl* coop = nullptr) {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -534,7 +534,7 @@ __device__ void front_lsolve(const FT* M, int nf, int nres, int r0, const int* s
             if (lane < kb) { x[r0 + k0 + lane] = xv; sh.xs[lane] = xv; }
         }
         __syncthreads();
-        if (!coop) {
+        if (!COOP || !coop) {
             lsolve_rows<FT>(M, nf, nres, r0, sep, x, k0, kb, sh, 0, 1, false);
         } else if (!coop_call(coop, sh, [&](CoopCtl* c) {
                        c->cmd = COOP_LROWS; c->pa[0] = (void*)M; c->pa[1] = (void*)sep; c->pa[2] = x;
@@ -546,7 +546,7 @@ __device__ void front_lsolve(const FT* M, int nf, int nres, int r0, const int* s
 }
 
 // backward solve with front f: x[res] -= L_offᵀ x[sep]; x[res] <- D⁻ᵀ x[res]
-template <class FT>
+template <class FT, bool COOP = false>
 __device__ void front_usolve(const FT* M, int nf, int nres, int r0, const int* sep, double* x, Shared& sh,
                              CoopCtl* coop = nullptr) {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -558,7 +558,7 @@ __device__ void front_usolve(const FT* M, int nf, int nres, int r0, const int* s
             int r = idx & 31, c = idx >> 5;
             if (r < kb && c < kb && r >= c) T[c * 33 + r] = (double)M[(k0 + r) + (int64_t)(k0 + c) * nf];
         }
-        if (!coop) {
+        if (!COOP || !coop) {
             usolve_dots<FT>(M, nf, nres, r0, sep, x, k0, kb, sh.acc, warp, NW);
         } else {
             if (!coop_call(coop, sh, [&](CoopCtl* c) {
@@ -600,9 +600,9 @@ constexpr int COOP_ABORTED = -1;   // front_chol result when the grid barrier ti
 // columns), 32-column diagonal/panel steps inside a block, then the separator's Schur complement
 // (the update matrix handed to the parent by extend-add).  With `coop` and a front of at least
 // COOP_MIN_FRONT, the update tiles and panel rows are shared with the helper CTAs.
-template <class FT>
+template <class FT, bool COOP>
 __device__ int front_chol_ll(FT* M, int nf, int nres, Shared& sh, CoopCtl* coop) {
-    const bool big = coop != nullptr && nf >= COOP_MIN_FRONT;
+    const bool big = COOP && coop != nullptr && nf >= COOP_MIN_FRONT;
     auto upd = [&](int J0, int nb, int K0, int K1) -> bool {
         if (K1 <= K0 || nb <= 0) return true;
         if (!big) { update_cols<FT>(M, nf, J0, nb, K0, K1, sh); return true; }
@@ -642,6 +642,7 @@ __device__ int front_chol_ll(FT* M, int nf, int nres, Shared& sh, CoopCtl* coop)
 // ---------------------------------------------------------------------------------------------
 // the per-instance solver
 // ---------------------------------------------------------------------------------------------
+template <bool COOP>   // COOP: the leader of a grid-cooperative launch (else no cooperative code is built)
 struct Ctx {
     const DevInst& I;
     Settings set;
@@ -796,7 +797,7 @@ struct Ctx {
     __device__ void build_finit() {
         const DevSp& B = I.B;
         const int tid = threadIdx.x;
-        if (coop && I.fsize >= ((int64_t)1 << 20)) {
+        if (COOP && coop && I.fsize >= ((int64_t)1 << 20)) {
             coop_call(coop, sh, [&](CoopCtl* c) { c->cmd = COOP_FILL; c->pa[0] = I.Finit; c->la[0] = I.fsize; });
         } else {
             for (int64_t i = tid; i < I.fsize; i += NT) I.Finit[i] = 0;
@@ -1037,7 +1038,7 @@ struct Ctx {
     template <class FT>
     __device__ void assemble_t(FT* F, double dl, double rho) {
         const int tid = threadIdx.x;
-        if (coop && I.fsize >= ((int64_t)1 << 20)) {   // the copy F <- Finit shared with the helpers
+        if (COOP && coop && I.fsize >= ((int64_t)1 << 20)) {   // the copy F <- Finit shared with the helpers
             coop_call(coop, sh, [&](CoopCtl* c) {
                 c->cmd = COOP_COPY; c->pa[0] = F; c->pa[1] = I.Finit; c->la[0] = I.fsize; c->ia[0] = IsF32<FT>::v;
             });
@@ -1104,7 +1105,7 @@ struct Ctx {
         for (int f = 0; f < I.nfront; ++f) {
             int nres = I.fnres[f], nsep = I.fnsep[f], nfr = nres + nsep;
             FT* M = F + I.fptr[f];
-            int info = front_chol_ll<FT>(M, nfr, nres, sh, coop);
+            int info = front_chol_ll<FT, COOP>(M, nfr, nres, sh, coop);
             if (info == COOP_ABORTED) return COOP_ABORTED;
             if (info) return I.fres0[f] + info;
             int p = I.fparent[f];
@@ -1112,7 +1113,7 @@ struct Ctx {
                 int np = I.fnres[p] + I.fnsep[p];
                 FT* P = F + I.fptr[p];
                 const int* rel = I.frel + I.fsepp[f];
-                if (coop && nsep >= COOP_MIN_FRONT) {   // extend-add shared with the helpers
+                if (COOP && coop && nsep >= COOP_MIN_FRONT) {   // extend-add shared with the helpers
                     if (!coop_call(coop, sh, [&](CoopCtl* c) {
                             c->cmd = COOP_EXTEND; c->pa[0] = M; c->pa[1] = P; c->pa[2] = (void*)rel;
                             c->ia[0] = IsF32<FT>::v; c->ia[1] = nfr; c->ia[2] = nres; c->ia[3] = nsep; c->ia[4] = np;
@@ -1165,7 +1166,7 @@ struct Ctx {
     __device__ void Lsolve_t(const FT* F, double* x) {
         for (int f = 0; f < I.nfront; ++f) {
             int nres = I.fnres[f], nfr = nres + I.fnsep[f];
-            front_lsolve<FT>(F + I.fptr[f], nfr, nres, I.fres0[f], I.fsep + I.fsepp[f], x, sh,
+            front_lsolve<FT, COOP>(F + I.fptr[f], nfr, nres, I.fres0[f], I.fsep + I.fsepp[f], x, sh,
                              nfr >= COOP_MIN_SOLVE ? coop : nullptr);
         }
     }
@@ -1173,7 +1174,7 @@ struct Ctx {
     __device__ void Usolve_t(const FT* F, double* x) {
         for (int f = I.nfront - 1; f >= 0; --f) {
             int nres = I.fnres[f], nfr = nres + I.fnsep[f];
-            front_usolve<FT>(F + I.fptr[f], nfr, nres, I.fres0[f], I.fsep + I.fsepp[f], x, sh,
+            front_usolve<FT, COOP>(F + I.fptr[f], nfr, nres, I.fres0[f], I.fsep + I.fsepp[f], x, sh,
                              nfr >= COOP_MIN_SOLVE ? coop : nullptr);
         }
     }
@@ -1582,13 +1583,14 @@ struct Ctx {
 
 // init (solver/ipm.jl:431-478 and reinit! :375-429), then the solve_impl! loop
 // (solver/solver.jl:119-145) and result, or one of those pieces (mode)
-__device__ void solve_instance(const DevInst& I, const Settings& set, Shared& sh, int mode, CoopCtl* coop = nullptr) {
+template <bool COOP>
+__device__ void solve_instance(const DevInst& I, const Settings& set, Shared& sh, int mode, CoopCtl* coop) {
     const int n = I.n, m = I.m;
     if (mode == MODE_SOLVE || mode == MODE_INIT) {
         if (threadIdx.x == 0) { for (int k = 0; k < NSTAT; ++k) I.status[k] = 0; }
         __syncthreads();
     }
-    Ctx c(I, set, sh, coop);
+    Ctx<COOP> c(I, set, sh, coop);
     if (mode == MODE_SOLVE || mode == MODE_INIT) {
         // working copies of the inputs: a solve never modifies the uploaded problem
         for (int i = threadIdx.x; i < I.B.nnz; i += NT) I.B.val[i] = I.B.val0[i];
@@ -1711,7 +1713,7 @@ __global__ void __launch_bounds__(NT, CTA_PER_SM) ipm_batch_kernel(BatchArgs a) 
         __syncthreads();
         if (k >= a.ninst) break;
         unsigned long long t0 = globaltimer();
-        solve_instance(a.inst[k], a.set, sh, a.mode);
+        solve_instance<false>(a.inst[k], a.set, sh, a.mode, nullptr);
         if (threadIdx.x == 0) {
             a.inst[k].scal[SCAL_T0] = __longlong_as_double((long long)t0);
             a.inst[k].scal[SCAL_T1] = __longlong_as_double((long long)globaltimer());
@@ -1732,7 +1734,7 @@ __global__ void __launch_bounds__(NT, CTA_PER_SM) ipm_coop_kernel(BatchArgs a, C
     if (blockIdx.x != 0) { coop_helper(c, sh); return; }
     const DevInst& I = a.inst[0];
     const unsigned long long t0 = globaltimer();
-    solve_instance(I, a.set, sh, a.mode, c);
+    solve_instance<true>(I, a.set, sh, a.mode, c);
     __syncthreads();
     if (threadIdx.x == 0) {
         I.scal[SCAL_T0] = __longlong_as_double((long long)t0);

@@ -299,9 +299,11 @@ inline std::vector<std::vector<i64>> vertex_graph(const BSM& B, const BSM& Q) {
             for (i64 e = Q.xsrc[v]; e < Q.xsrc[v + 1]; ++e) { i64 u = Q.tgt[e]; ab[u >> 6] |= 1ull << (u & 63); }
             for (i64 q = 0; q < W; ++q) { uint64_t x = ab[q]; while (x) { int b = __builtin_ctzll(x); x &= x - 1; adj[v].push_back(q * 64 + b); } }
         }
-        for (i64 v = 0; v < nv; ++v)   // Q pattern is used symmetrically
-            for (i64 e = Q.xsrc[v]; e < Q.xsrc[v + 1]; ++e) { i64 u = Q.tgt[e]; if (u != v) adj[u].push_back(v); }
-        for (auto& a : adj) { std::sort(a.begin(), a.end()); a.erase(std::unique(a.begin(), a.end()), a.end()); }
+        bool extra = false;            // Q pattern is used symmetrically
+        for (i64 v = 0; v < nv; ++v)
+            for (i64 e = Q.xsrc[v]; e < Q.xsrc[v + 1]; ++e) { i64 u = Q.tgt[e]; if (u != v) { adj[u].push_back(v); extra = true; } }
+        if (extra)   // the bitset lists are sorted and unique already
+            for (auto& a : adj) { std::sort(a.begin(), a.end()); a.erase(std::unique(a.begin(), a.end()), a.end()); }
         return adj;
     }
     std::vector<std::vector<i64>> rows(B.nout), adj(nv);
@@ -449,8 +451,8 @@ inline Fronts analyze(const std::vector<std::vector<i64>>& adj0, const std::vect
         i64 v = post[k];
         w[k] = w0[v];
         par[k] = par0[v] < 0 ? -1 : inv[par0[v]];
-        for (i64 u : adj0[v]) adj[k].push_back(inv[u]);
-        std::sort(adj[k].begin(), adj[k].end());
+        adj[k].reserve(adj0[v].size());
+        for (i64 u : adj0[v]) adj[k].push_back(inv[u]);   // order is irrelevant below (mark arrays)
     }
     std::vector<std::vector<i64>> sv(n), kids(n);
     for (i64 v = 0; v < n; ++v) if (par[v] >= 0) kids[par[v]].push_back(v);

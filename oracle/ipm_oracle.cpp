@@ -412,8 +412,8 @@ static Symbolic analyze(const std::vector<std::vector<i64>>& adj0, const std::ve
         i64 v = post[k];
         w[k] = w0[v];
         par[k] = par0[v] < 0 ? -1 : inv[par0[v]];
-        for (i64 u : adj0[v]) adj[k].push_back(inv[u]);
-        std::sort(adj[k].begin(), adj[k].end());
+        adj[k].reserve(adj0[v].size());
+        for (i64 u : adj0[v]) adj[k].push_back(inv[u]);   // order is irrelevant below (mark arrays)
     }
     // vertex row structure struct(v) (vertices > v), by merging children
     std::vector<std::vector<i64>> sv(n);

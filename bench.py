@@ -371,7 +371,8 @@ def main():
         dt = allreduce_max(pg, dt, local)
         st = main_arm["stats"]
         e2e = {"value": args.count * ws / dt, "unit": "solves/s", "h2d_bytes_per_step": st["input_bytes"],
-               "d2h_bytes_per_step": st["output_bytes"]}
+               "d2h_bytes_per_step": st["output_bytes"],
+               "note": "host symbolic analyses are cached by sparsity structure, warm after the warm-up call"}
     serve = None
     if not args.no_serve:
         serve = serve_arm(args, ctx)

@@ -33,6 +33,15 @@ def test_large_mode_equals_one_cta(name):
         assert np.array_equal(x, y)
 
 
+def test_large_mode_mixed_precision_equals_one_cta():
+    """The FP32 tiles, panel rows and solves of the mixed path, shared with the helpers."""
+    prob = IPMProblem.from_dict(block_problem(CASES["port300"]()), ctx=Context.default())
+    a = solve(prob, IPMSettings(large=-1, precision="mixed"))
+    b = solve(prob, IPMSettings(large=1, precision="mixed"))
+    assert a.status == b.status and a.niter == b.niter and a.nfp32 == b.nfp32
+    assert a.pobj == b.pobj and np.array_equal(a.p, b.p)
+
+
 def test_large_mode_sdp_and_step_api():
     from mumblebee_b200.ipm import init
     prob = IPMProblem.from_dict(block_problem(SDP["sdp1x10"]()), ctx=Context.default())

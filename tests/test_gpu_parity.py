@@ -148,3 +148,23 @@ def test_sdp_batch_equals_alone():
     for a, b in zip(alone, many):
         assert a.niter == b.niter and a.pobj == b.pobj
         assert np.array_equal(a.p, b.p)
+
+
+@pytest.mark.parametrize("name,pb", [
+    ("socp_config1", lambda: G.socp(n=500, m=200, ncone=25, density=0.05, seed=0)),       # n=500, 25 x SOC(20)
+    ("portfolio400", lambda: G.portfolio(400, seed=11)),                                 # largest batch instance
+    ("portfolio400b", lambda: G.portfolio(400, seed=12)),
+])
+def test_full_size_instances_match_oracle(name, pb):
+    """The SOCP and portfolio workloads at their full sizes: same status and iteration count as the
+    oracle, objectives to 1e-9 relative, iterates to 1e-6."""
+    ref = block_problem(pb())
+    prob = _gpu_problem(ref)
+    _, o = oracle_solve(ref, vperm=prob.symbolic()["vperm"], threads=4)
+    r = solve(prob, IPMSettings())
+    assert o["status"] == "OPTIMAL" and r.status == IPMStatus.OPTIMAL
+    assert r.niter == o["niter"]
+    assert _rel(r.pobj, o["pobj"]) < 1e-9 and _rel(r.dobj, o["dobj"]) < 1e-9
+    for k in ("p", "d", "y"):
+        a, b = getattr(r, k), o[k]
+        assert np.linalg.norm(a - b) <= 1e-6 * max(1.0, np.linalg.norm(b)), k

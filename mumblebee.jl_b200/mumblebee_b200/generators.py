@@ -252,3 +252,43 @@ def serving_mix(count, seed=0, nmin=100, nmax=2000):
             pb = maxcut(nodes, extra=nodes // 2, band=2, seed=s)
         out.append((kind, pb))
     return out
+
+
+def socp_infeasible(which="primal", n=200, m=80, ncone=10, density=0.1, seed=0):
+    """SOCP from ``socp`` with a planted infeasibility certificate.
+
+    ``which="primal"``: row r of A is replaced so that Aᵀy_c = −s_c for y_c ~ N(0,1) and s_c in
+    the cone interior, and b = A x0 + δ y_c with δ = (x0ᵀs_c + 1)/‖y_c‖², so bᵀy_c = 1 > 0.
+    y_c is then a Farkas certificate: no x ∈ K has Ax = b.
+
+    ``which="dual"``: column j of A is replaced so that A r = 0 for r in the cone interior, and
+    c = Aᵀy0 + s0 − α r with α = (s0ᵀr + 1)/‖r‖², so cᵀr = −1 < 0. With the feasible b = A x0,
+    x0 + t r stays feasible and cᵀx → −∞ as t grows: the problem is unbounded."""
+    rng = np.random.default_rng(seed)
+    k = n // ncone
+    assert k * ncone == n
+    A = sp.random(m, n, density=density, format="csc", random_state=rng,
+                  data_rvs=lambda s: rng.standard_normal(s)).toarray()
+    x0 = np.concatenate([_soc_interior(rng, k) for _ in range(ncone)])
+    s0 = np.concatenate([_soc_interior(rng, k) for _ in range(ncone)])
+    y0 = rng.standard_normal(m)
+    if which == "primal":
+        yc = rng.standard_normal(m)
+        sc = np.concatenate([_soc_interior(rng, k) for _ in range(ncone)])
+        r = int(np.argmax(np.abs(yc)))
+        rest = np.delete(np.arange(m), r)
+        A[r, :] = (-sc - A[rest, :].T @ yc[rest]) / yc[r]
+        b = A @ x0 + (x0 @ sc + 1.0) / (yc @ yc) * yc
+        c = A.T @ y0 + s0
+    elif which == "dual":
+        rr = np.concatenate([_soc_interior(rng, k) for _ in range(ncone)])
+        j = int(np.argmax(rr))
+        rest = np.delete(np.arange(n), j)
+        A[:, j] = -(A[:, rest] @ rr[rest]) / rr[j]
+        b = A @ x0
+        c = A.T @ y0 + s0 - (s0 @ rr + 1.0) / (rr @ rr) * rr
+    else:
+        raise ValueError(which)
+    return dict(Q=sp.csc_matrix((n, n)), B=sp.csc_matrix(A), f=-c, g=b, mu=0.0,
+                kinds=[CONE_SOC] * ncone, sizes=[k] * ncone, params=[0.0] * ncone,
+                name=f"socp-{which}-infeasible n={n} m={m} {ncone}xSOC({k}) seed={seed}")

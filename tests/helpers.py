@@ -55,3 +55,46 @@ SDP = {
     "sdp1x10": lambda: G.sdp(1, 10, 20, 0.2, 0, 3),
     "maxcut12": lambda: G.maxcut(12, 6, 2, 0),
 }
+
+
+def _lp(B, f, g, kinds, sizes):
+    import scipy.sparse as sp
+    n = np.asarray(B).shape[1]
+    return dict(Q=sp.csc_matrix((n, n)), B=sp.csc_matrix(np.asarray(B, float)), f=np.asarray(f, float),
+                g=np.asarray(g, float), mu=0.0, kinds=list(kinds), sizes=list(sizes), params=[0.0] * len(kinds))
+
+
+def _pinf_pos():
+    rng = np.random.default_rng(0)
+    return _lp(np.vstack([np.ones(20), rng.standard_normal(20)]), -rng.uniform(0.5, 1, 20), [-1.0, 0.3], [1], [20])
+
+
+# infeasible and unbounded problems with the status the oracle reaches on them: x >= 0 with
+# 1ᵀx = -1; ‖u‖ <= t with t = 1, u1 = 2; an unbounded ray along x1 = x2 >= 0; an unbounded t with
+# u1 = 0; and SOCPs with a planted Farkas certificate or unbounded ray (generators.socp_infeasible)
+INFEAS = {
+    "pinf_pos": (_pinf_pos, "PRIMAL_INFEASIBLE"),
+    "pinf_soc": (lambda: _lp([[1, 0, 0], [0, 1, 0]], [-1, 0, 0], [1.0, 2.0], [2], [3]), "NEAR_PRIMAL_INFEASIBLE"),
+    "dinf_pos": (lambda: _lp([[1.0, -1.0]], [1.0, 0.0], [0.0], [1], [2]), "DUAL_INFEASIBLE"),
+    "dinf_soc": (lambda: _lp([[0, 1.0, 0]], [1.0, 0, 0], [0.0], [2], [3]), "DUAL_INFEASIBLE"),
+    "pinf_socp40": (lambda: G.socp_infeasible("primal", 40, 12, 4, 0.1, 0), "PRIMAL_INFEASIBLE"),
+    "pinf_socp200": (lambda: G.socp_infeasible("primal", 200, 80, 10, 0.1, 2), "PRIMAL_INFEASIBLE"),
+    "pinf_socp500": (lambda: G.socp_infeasible("primal", 500, 200, 25, 0.1, 3), "PRIMAL_INFEASIBLE"),
+    "dinf_socp40": (lambda: G.socp_infeasible("dual", 40, 12, 4, 0.1, 0), "DUAL_INFEASIBLE"),
+    "dinf_socp100": (lambda: G.socp_infeasible("dual", 100, 40, 5, 0.1, 1), "NEAR_DUAL_INFEASIBLE"),
+    "dinf_socp200": (lambda: G.socp_infeasible("dual", 200, 80, 10, 0.1, 2), "DUAL_INFEASIBLE"),
+}
+
+
+def cone_violation(x, kinds, sizes):
+    """Largest distance outside the cone product (POS, SOC, free; the self-dual ones) of x,
+    measured as max(-x_i) on POS and ‖u‖ - t on SOC."""
+    v, o = 0.0, 0
+    for k, s in zip(kinds, sizes):
+        z = x[o:o + s]
+        if k == 1:
+            v = max(v, float(-z.min()))
+        elif k == 2:
+            v = max(v, float(np.linalg.norm(z[1:]) - z[0]))
+        o += s
+    return v

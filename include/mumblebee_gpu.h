@@ -188,10 +188,12 @@ int mb_batch_run(mb_batch* b, int32_t grid, float* ms);
 int mb_batch_fetch(mb_batch* b, double* const* p_out, double* const* d_out, double* const* y_out,
                    mb_result* results);
 int mb_batch_stats(mb_batch* b, int64_t* stats8);   /* bytes: input, workspace, factor; kernel launches */
-/* per-instance section timers after mb_batch_fetch, (NSEC + 2) doubles each: SM clocks spent in
- * equilibrate, BᵀB, scale, initkkt, predictor, corrector, maxsteps, triangular solves, matvecs,
- * then the number of triangular-solve sweeps and of matvecs (the TimerOutputs sections of the
- * reference, solver/ipm.jl:137-755) */
+/* per-instance section timers after mb_batch_fetch, MB_NSECTIONS + 2 doubles each: SM clocks spent
+ * in equilibrate, BᵀB, scale, initkkt, predictor, corrector, maxsteps, triangular solves, matvecs,
+ * KKT assembly, residuals, getaug, and inside initkkt the factor's trailing updates, diagonal
+ * blocks, panel rows and extend-add; then the number of triangular-solve sweeps and of matvecs
+ * (the TimerOutputs sections of the reference, solver/ipm.jl:137-755, split further) */
+#define MB_NSECTIONS 16
 int mb_batch_timers(mb_batch* b, double* out, int64_t cap);
 /* per-instance device timestamps after mb_batch_fetch, 2 int64 each: the GPU global timer (ns)
  * when a CTA took the instance from the work queue and when its solve finished.  Latency of an

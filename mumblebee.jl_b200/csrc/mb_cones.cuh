@@ -80,29 +80,43 @@ __device__ bool w_socpoint(double* c, const double* p, const double* d, int n, d
     return flag;
 }
 
-// H ← H + (2 (Jw)(Jw)ᵀ − J) / β² on an (n x n) block  (soc.jl:231-256), all threads of the CTA;
-// each unordered pair is written to both halves from the upper addend, as the reference does.
-__device__ void b_sochess(double* H, const double* c, int n) {
+// H = Q + (2 (Jw)(Jw)ᵀ − J) / β² on an (n x n) block (soc.jl:231-256), all threads of the CTA, in
+// one pass over H: each unordered pair takes the upper entry of Q as its addend and is written to
+// both halves, as the reference does; `qzero` skips the reads of an all-zero Q block.
+__device__ void b_sochess(double* H, const double* Q, bool qzero, const double* c, int n) {
     const double* w = c + 5;
     const double beta = c[0];
     const double eta = 1.0 / (beta * beta), eta2 = 2 * eta;
     const double w1 = w[0];
-    const int64_t np = (int64_t)n * (n + 1) / 2;
-    for (int64_t t = threadIdx.x; t < np; t += NT) {
-        // column-major lower enumeration: t -> (i >= j)
-        int j = (int)((2.0 * n + 1.0 - sqrt((2.0 * n + 1.0) * (2.0 * n + 1.0) - 8.0 * (double)t)) * 0.5);
-        while (j > 0 && (int64_t)j * (2 * n - j + 1) / 2 > t) --j;
-        while ((int64_t)(j + 1) * (2 * n - j) / 2 <= t) ++j;
-        int i = j + (int)(t - (int64_t)j * (2 * n - j + 1) / 2);
-        if (i == j) {
-            if (j == 0) H[0] = fma(eta2, w1 * w1, H[0] - eta);
-            else H[(int64_t)j * n + j] = fma(eta2, w[j] * w[j], H[(int64_t)j * n + j] + eta);
-        } else {
-            double t2 = (j == 0) ? fma(-eta2 * w1, w[i], H[(int64_t)i * n]) : fma(eta2 * w[j], w[i], H[j + (int64_t)i * n]);
-            H[i + (int64_t)j * n] = t2;
-            H[j + (int64_t)i * n] = t2;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int cc = warp; cc < n; cc += NW) {
+        for (int r = lane; r < n; r += 32) {
+            const int a = min(r, cc), b = max(r, cc);
+            const double q = qzero ? 0.0 : Q[a + (int64_t)b * n];
+            double v;
+            if (a == b) v = a == 0 ? fma(eta2, w1 * w1, q - eta) : fma(eta2, w[a] * w[a], q + eta);
+            else v = a == 0 ? fma(-eta2 * w1, w[b], q) : fma(eta2 * w[a], w[b], q);
+            H[r + (int64_t)cc * n] = v;
         }
     }
+}
+
+// (H x)_i for row i of an SOC block with a zero Q block: H = (2 z zᵀ − diag(1, −1, …, −1)) / β² with
+// z = Jw = (w₁, −w₂, …), so H x = η (−x₁, x₂, …) + 2η z (zᵀx); `zx` = zᵀx of the cone
+__device__ __forceinline__ double socz_row(const double* c, const double* x, int i, double zx) {
+    const double* w = c + 5;
+    const double eta = 1.0 / (c[0] * c[0]), eta2 = 2 * eta;
+    const double zi = i == 0 ? w[0] : -w[i];
+    return fma(eta2 * zi, zx, i == 0 ? -eta * x[0] : eta * x[i]);
+}
+
+// zᵀx of one cone (warp): z = (w₁, −w₂, …)
+__device__ __forceinline__ double w_soczdot(const double* c, const double* x, int n) {
+    const double* w = c + 5;
+    const int lane = threadIdx.x & 31;
+    double s = 0;
+    for (int i = lane; i < n; i += 32) s = fma(i == 0 ? w[0] : -w[i], x[i], s);
+    return warp_sum(s);
 }
 
 // Mehrotra corrector  (soc.jl:282-351); work holds 2n doubles owned by this warp

@@ -1097,6 +1097,7 @@ int mb_batch_stats(mb_batch* b, int64_t* s) {
 int mb_batch_timers(mb_batch* b, double* out, int64_t cap) {
     if (!b || !out) return MB_E_ARG;
     // per instance: NSEC section clocks, trsv sweeps, gemv calls (needs a prior mb_batch_fetch)
+    static_assert(mb::NSEC == MB_NSECTIONS, "section count of the C header");
     const int W = mb::NSEC + 2;
     for (size_t k = 0; k < b->pk.plans.size() && (int64_t)((k + 1) * W) <= cap; ++k) {
         const double* sc = b->h_out + b->pk.plans[k].scal;

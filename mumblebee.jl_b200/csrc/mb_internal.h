@@ -100,16 +100,20 @@ struct DevInst {
 constexpr int NVEC_N = 12;  // Df Qp wf Dpa Dda Dp Dd df dx cgw  tmp1 tmp2 (tmp2 also: column maxima)
 constexpr int NVEC_M = 8;   // Dg Dya Dy dg dy cgp tmp1 tmp2
 // two more n-vectors and one m-vector follow the above (saved p, d, y of a mixed-precision redo)
-constexpr int NVEC_V = 6;   // step spsd flag vscl vnrm vswp
+constexpr int NVEC_V = 8;   // step spsd flag vscl vnrm vswp socz socdot
 constexpr int NSCAL = 32;   // mu pres dres pobj dobj | nf ng sf sg nB | section clocks (NSEC) | counters
-// section timers (SM clock cycles), the TimerOutputs sections of the reference plus set-up
+// section timers (SM clock cycles), the TimerOutputs sections of the reference plus set-up; the
+// last four split the numeric factorization (inside initkkt)
 enum Section { SEC_EQUIL = 0, SEC_FINIT, SEC_SCALE, SEC_INITKKT, SEC_PRED, SEC_CORR, SEC_MAXSTEPS, SEC_TRSV, SEC_GEMV,
-               SEC_ASSEMBLE, SEC_RESID, SEC_AUG, NSEC };
+               SEC_ASSEMBLE, SEC_RESID, SEC_AUG, SEC_FUPD, SEC_FDIAG, SEC_FPANEL, SEC_FEXTEND, NSEC };
 constexpr int SCAL_SEC = 10;        // scal[10 .. 10+NSEC)
-constexpr int SCAL_NTRSV = 22;      // triangular solve sweeps
-constexpr int SCAL_NGEMV = 23;      // block-sparse matvecs
-constexpr int SCAL_T0 = 24;         // %globaltimer (ns, bit pattern) when a CTA took the instance
-constexpr int SCAL_T1 = 25;         // %globaltimer (ns, bit pattern) when its solve finished
+constexpr int SCAL_NTRSV = 26;      // triangular solve sweeps
+constexpr int SCAL_NGEMV = 27;      // block-sparse matvecs
+constexpr int SCAL_T0 = 28;         // %globaltimer (ns, bit pattern) when a CTA took the instance
+constexpr int SCAL_T1 = 29;         // %globaltimer (ns, bit pattern) when its solve finished
+constexpr int SCAL_NSOCZ = 30;      // second-order cones whose diagonal block of Q is zero
+constexpr int SCAL_STALL0 = 31;     // history rows before the mixed-precision switch after an FP32 stall
+static_assert(SCAL_SEC + NSEC <= SCAL_NTRSV, "section clocks overlap the counters");
 constexpr int NSTAT = 8;    // status, history rows, factor retries, factorizations, FP32 iterations, FP64 redos,
                             // switched-to-FP64 flag, grid-barrier timeout flag
 

@@ -26,17 +26,14 @@ constexpr int TS = 64;   // trailing-update tile
 constexpr double MIXED_MAX_SOLVES = 4;   // KKT solves (IR passes + CG steps) an FP32 iteration may take
 constexpr int TLD = 36;  // tile row stride (doubles): 8-byte fragment loads of 8 rows x 4 columns hit 32 distinct banks
 
-// Block-shared scratch (dynamic shared memory: it exceeds the 48 KB static limit).  ta/tb and
-// ta2/tb2 are the two stages of the double-buffered tiles of the FP64 front update.
+// Block-shared scratch (dynamic shared memory: it exceeds the 48 KB static limit).  `tile` holds the
+// two stages (A and B operand each) of the double-buffered front update.
 struct Shared {
     double red[NW + 2];
     double diag[32 * 33];
     double xs[32];
     double acc[32];
-    double ta[TS * TLD];
-    double tb[TS * TLD];
-    double ta2[TS * TLD];
-    double tb2[TS * TLD];
+    double tile[4 * TS * TLD];   // stage 0 A, B, stage 1 A, B of the front update; x slices in solves
     int flag;
     int ibuf[8];
 };
@@ -48,53 +45,49 @@ __device__ __forceinline__ void dmma(double& c0, double& c1, double a, double b)
                  : "+d"(c0), "+d"(c1) : "d"(a), "d"(b));
 }
 
-// Factor the kb x kb diagonal block at k0 (warp 0; the factor is kept in sh.diag and written back
-// to M).  Returns the failing pivot (1-based in the front) or 0.
+// Factor the kb x kb diagonal block at k0 (warp 0: lane l holds row l in registers, column c's
+// entries come from lane c by shuffle; the factor is also left in sh.diag for the panel solve and
+// written back to M).  Returns the failing pivot (1-based in the front) or 0.  Not inlined, so the
+// register-resident rows get their own allocation.
 template <class FT>
-__device__ int diag_factor(FT* M, int nf, int k0, int kb, Shared& sh) {
+__device__ __noinline__ int diag_factor(FT* M, int nf, int k0, int kb, Shared& sh) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     FT* S = reinterpret_cast<FT*>(sh.diag);
-    {
-        if (warp == 0) {
-            if (lane < kb)
-                for (int c = 0; c <= lane; ++c) S[lane * 33 + c] = M[(k0 + lane) + (int64_t)(k0 + c) * nf];
-            __syncwarp();
-            int fail = 0;
-            for (int c = 0; c < kb; ++c) {
-                if (lane == c) {
-                    FT v = S[c * 33 + c];
-                    if (!(v > FT(0))) fail = c + 1; else S[c * 33 + c] = sqrt(v);
-                }
-                fail = __shfl_sync(0xffffffffu, fail, c);
-                if (fail) break;
-                __syncwarp();
-                FT dc = S[c * 33 + c];
-                if (lane > c && lane < kb) {
-                    FT l = S[lane * 33 + c] / dc;
-                    S[lane * 33 + c] = l;
-                }
-                __syncwarp();
-                if (lane > c && lane < kb) {
-                    FT l = S[lane * 33 + c];
-                    for (int cc = c + 1; cc <= lane; ++cc) S[lane * 33 + cc] -= l * S[cc * 33 + c];
-                }
-                __syncwarp();
+    if (warp == 0) {
+        FT v[32];
+#pragma unroll
+        for (int c = 0; c < 32; ++c) v[c] = (lane < kb && c <= lane) ? M[(k0 + lane) + (int64_t)(k0 + c) * nf] : FT(0);
+        int fail = 0;
+#pragma unroll
+        for (int c = 0; c < 32; ++c) {
+            if (c >= kb || fail) continue;
+            const FT dd = __shfl_sync(0xffffffffu, v[c], c);   // the updated pivot, from lane c
+            if (!(dd > FT(0))) { fail = c + 1; continue; }
+            const FT dc = sqrt(dd);
+            if (lane == c) v[c] = dc;
+            else if (lane > c) v[c] = v[c] / dc;               // L[lane][c]
+#pragma unroll
+            for (int cc = c + 1; cc < 32; ++cc) {
+                const FT lcc = __shfl_sync(0xffffffffu, v[c], cc);   // L[cc][c]
+                if (lane >= cc) v[cc] -= v[c] * lcc;
             }
-            if (!fail && lane < kb)
-                for (int c = 0; c <= lane; ++c) M[(k0 + lane) + (int64_t)(k0 + c) * nf] = S[lane * 33 + c];
-            if (lane == 0) sh.flag = fail ? k0 + fail : 0;
         }
-        __syncthreads();
-        if (sh.flag) return sh.flag;
+        if (!fail && lane < kb) {
+#pragma unroll
+            for (int c = 0; c < 32; ++c)
+                if (c <= lane) { S[lane * 33 + c] = v[c]; M[(k0 + lane) + (int64_t)(k0 + c) * nf] = v[c]; }
+        }
+        if (lane == 0) sh.flag = fail ? k0 + fail : 0;
     }
-    return 0;
+    __syncthreads();
+    return sh.flag;
 }
 
 // Panel solve L21 = A21 L11^{-T} for the rows [k0 + kb, nf) owned by this rank (row blocks of NT
 // rows dealt round-robin over nranks CTAs).  With `load`, the factored diagonal block is first read
 // back from M into sh.diag (a helper CTA that did not factor it).
 template <class FT>
-__device__ void panel_rows(FT* M, int nf, int k0, int kb, Shared& sh, int rank, int nranks, bool load) {
+__device__ __noinline__ void panel_rows(FT* M, int nf, int k0, int kb, Shared& sh, int rank, int nranks, bool load) {
     const int tid = threadIdx.x;
     FT* S = reinterpret_cast<FT*>(sh.diag);
     if (load) {
@@ -158,76 +151,103 @@ __device__ __forceinline__ void stage_tile_f64(double* buf, const double* M, int
     }
 }
 
-// M[r, c] -= Σ_{k in [K0, K1)} M[r, k] M[c, k] for c in [J0, J0 + nb) (nb <= 64), r in [J0, nf),
-// r >= c: each 64-row tile accumulates over K in registers (FP64 DMMA) from double-buffered
-// asynchronous copies and is written back once.  Requires K1 <= J0 (the K columns are final).
-// one 64-row tile at rb of the column block [J0, J0 + nb): accumulate over K, write back once
-__device__ void tile_f64(double* M, int nf, int rb, int J0, int nb, int K0, int K1, Shared& sh) {
+// One 64 x nb tile of the trailing update: rows [rb, rb + 64) x columns [J, J + nb) (nb <= 64) of
+// the column-major front M (leading dimension nf), M[r, c] -= Σ_{k in [K0, K1)} M[r, k] M[c, k] for
+// r >= c.  The K columns must be final (K1 <= J).
+struct UTile { int rb, J, nb; };
+
+// The tiles one CTA updates, in order, and the K range they share.  Every tile takes
+// nk = ceil((K1 - K0) / 32) chunks; the (tile, chunk) sequence is one software pipeline: the copy
+// of the next chunk (of this tile or the next one) is in flight while the current chunk is on the
+// tensor pipe, so a tile costs no prologue of its own.  The accumulators start from the tile's
+// current values of M (loaded while the first chunk's copy is in flight) and take the update
+// with negated B fragments, so the epilogue is a plain store.
+template <class TileAt>
+__device__ __noinline__ void tiles_f64(double* M, int nf, int ntile, int K0, int K1, Shared& sh, TileAt at) {
     constexpr int WRN = NW / 4, RW = TS / WRN, MR = RW / 8;
+    if (ntile <= 0 || K1 <= K0) return;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int g = lane >> 2, t = lane & 3;
     const int wr = warp >> 2, wc = warp & 3;
     const int nk = (K1 - K0 + 31) / 32;
-    const int cmax = min(nf, J0 + nb);
-    double* A[2] = {sh.ta, sh.ta2};
-    double* B[2] = {sh.tb, sh.tb2};
-    {
-        const bool skip = wc * 16 >= nb || (rb == J0 && wr * RW + RW - 1 < wc * 16);
-        double acc[MR][2][2];
-#pragma unroll
-        for (int a = 0; a < MR; ++a)
-#pragma unroll
-            for (int b = 0; b < 2; ++b) { acc[a][b][0] = 0; acc[a][b][1] = 0; }
-        stage_tile_f64(A[0], M, nf, rb, nf, K0, K1);
-        stage_tile_f64(B[0], M, nf, J0, cmax, K0, K1);
+    const int nstep = ntile * nk;
+    double* A[2] = {sh.tile, sh.tile + 2 * TS * TLD};
+    double* B[2] = {sh.tile + TS * TLD, sh.tile + 3 * TS * TLD};
+    auto stage = [&](int s, int buf) {
+        const UTile u = at(s / nk);
+        const int k0 = K0 + 32 * (s % nk);
+        stage_tile_f64(A[buf], M, nf, u.rb, nf, k0, K1);
+        stage_tile_f64(B[buf], M, nf, u.J, min(nf, u.J + u.nb), k0, K1);
         cp_async_commit();
-        for (int q = 0; q < nk; ++q) {
-            const int cur = q & 1;
-            if (q + 1 < nk) {
-                stage_tile_f64(A[cur ^ 1], M, nf, rb, nf, K0 + 32 * (q + 1), K1);
-                stage_tile_f64(B[cur ^ 1], M, nf, J0, cmax, K0 + 32 * (q + 1), K1);
-                cp_async_commit();
-                cp_async_wait<1>();
-            } else {
-                cp_async_wait<0>();
-            }
-            __syncthreads();
-            if (!skip) {
-                const double* ta = A[cur];
-                const double* tb = B[cur];
-                const int kb4 = (min(32, K1 - K0 - 32 * q) + 3) & ~3;
-                for (int k = 0; k < kb4; k += 4) {
-                    double b0 = tb[(wc * 16 + g) * TLD + k + t], b1 = tb[(wc * 16 + 8 + g) * TLD + k + t];
-#pragma unroll
-                    for (int a = 0; a < MR; ++a) {
-                        double av = ta[(wr * RW + a * 8 + g) * TLD + k + t];
-                        dmma(acc[a][0][0], acc[a][0][1], av, b0);
-                        dmma(acc[a][1][0], acc[a][1][1], av, b1);
-                    }
-                }
-            }
-            __syncthreads();
-        }
-        if (!skip) {
+    };
+    double acc[MR][2][2];
+    UTile u = at(0);
+    bool skip = false;
+    stage(0, 0);
+    for (int s = 0; s < nstep; ++s) {
+        const int q = s % nk, cur = s & 1;
+        if (q == 0) {
+            u = at(s / nk);
+            skip = wc * 16 >= u.nb || (u.rb == u.J && wr * RW + RW - 1 < wc * 16);
+            const int cmax = min(nf, u.J + u.nb);
 #pragma unroll
             for (int a = 0; a < MR; ++a)
 #pragma unroll
                 for (int b = 0; b < 2; ++b)
 #pragma unroll
-                    for (int q = 0; q < 2; ++q) {
-                        const int row = rb + wr * RW + a * 8 + g;
-                        const int col = J0 + wc * 16 + b * 8 + 2 * t + q;
-                        if (row < nf && col < cmax && row >= col) M[row + (int64_t)col * nf] -= acc[a][b][q];
+                    for (int e = 0; e < 2; ++e) {
+                        const int row = u.rb + wr * RW + a * 8 + g;
+                        const int col = u.J + wc * 16 + b * 8 + 2 * t + e;
+                        acc[a][b][e] = (!skip && row < nf && col < cmax && row >= col) ? M[row + (int64_t)col * nf] : 0.0;
+                    }
+        }
+        if (s + 1 < nstep) {
+            stage(s + 1, cur ^ 1);
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
+        }
+        __syncthreads();
+        if (!skip) {
+            const double* ta = A[cur];
+            const double* tb = B[cur];
+            const int kb4 = (min(32, K1 - K0 - 32 * q) + 3) & ~3;
+            for (int k = 0; k < kb4; k += 4) {
+                const double b0 = -tb[(wc * 16 + g) * TLD + k + t], b1 = -tb[(wc * 16 + 8 + g) * TLD + k + t];
+#pragma unroll
+                for (int a = 0; a < MR; ++a) {
+                    const double av = ta[(wr * RW + a * 8 + g) * TLD + k + t];
+                    dmma(acc[a][0][0], acc[a][0][1], av, b0);
+                    dmma(acc[a][1][0], acc[a][1][1], av, b1);
+                }
+            }
+        }
+        __syncthreads();
+        if (q == nk - 1 && !skip) {
+            const int cmax = min(nf, u.J + u.nb);
+#pragma unroll
+            for (int a = 0; a < MR; ++a)
+#pragma unroll
+                for (int b = 0; b < 2; ++b)
+#pragma unroll
+                    for (int e = 0; e < 2; ++e) {
+                        const int row = u.rb + wr * RW + a * 8 + g;
+                        const int col = u.J + wc * 16 + b * 8 + 2 * t + e;
+                        if (row < nf && col < cmax && row >= col) M[row + (int64_t)col * nf] = acc[a][b][e];
                     }
         }
     }
     __syncthreads();
 }
 
+// M[r, c] -= Σ_{k in [K0, K1)} M[r, k] M[c, k] for c in [J0, J0 + nb) (nb <= 64), r in [J0, nf),
+// r >= c: the 64-row tiles from J0 down, dealt round-robin over nranks CTAs.  Requires K1 <= J0.
 __device__ void update_cols_f64(double* M, int nf, int J0, int nb, int K0, int K1, Shared& sh, int rank = 0,
                                 int nranks = 1) {
     if (K1 <= K0 || nb <= 0) return;
-    for (int rb = J0 + TS * rank; rb < nf; rb += TS * nranks) tile_f64(M, nf, rb, J0, nb, K0, K1, sh);
+    const int first = J0 + TS * rank, step = TS * nranks;
+    const int ntile = first < nf ? (nf - first + step - 1) / step : 0;
+    tiles_f64(M, nf, ntile, K0, K1, sh, [=](int i) { return UTile{first + step * i, J0, nb}; });
     __syncthreads();
 }
 
@@ -249,57 +269,71 @@ __device__ __forceinline__ void stage_tile_f32(float* buf, const float* M, int n
     }
 }
 
-// FP32 twin of update_cols_f64: each thread owns a 4 x 4 block of the 64 x 64 tile (FFMA)
-__device__ void tile_f32(float* M, int nf, int rb, int J0, int nb, int K0, int K1, Shared& sh) {
+// FP32 twin of tiles_f64: each thread owns a 4 x 4 block of the 64 x 64 tile (FFMA), same
+// cross-tile pipeline, accumulators started from M
+template <class TileAt>
+__device__ __noinline__ void tiles_f32(float* M, int nf, int ntile, int K0, int K1, Shared& sh, TileAt at) {
+    if (ntile <= 0 || K1 <= K0) return;
     const int tr = threadIdx.x & 15, tc = threadIdx.x >> 4;
     const int nk = (K1 - K0 + 31) / 32;
-    const int cmax = min(nf, J0 + nb);
-    float* A[2] = {reinterpret_cast<float*>(sh.ta), reinterpret_cast<float*>(sh.ta2)};
-    float* B[2] = {reinterpret_cast<float*>(sh.tb), reinterpret_cast<float*>(sh.tb2)};
-    {
-        const bool skip = tc * 4 >= nb || (rb == J0 && tr * 4 + 3 < tc * 4);
-        float acc[4][4];
-#pragma unroll
-        for (int a = 0; a < 4; ++a)
-#pragma unroll
-            for (int b = 0; b < 4; ++b) acc[a][b] = 0.f;
-        stage_tile_f32(A[0], M, nf, rb, nf, K0, K1);
-        stage_tile_f32(B[0], M, nf, J0, cmax, K0, K1);
+    const int nstep = ntile * nk;
+    float* A[2] = {reinterpret_cast<float*>(sh.tile), reinterpret_cast<float*>(sh.tile + 2 * TS * TLD)};
+    float* B[2] = {reinterpret_cast<float*>(sh.tile + TS * TLD), reinterpret_cast<float*>(sh.tile + 3 * TS * TLD)};
+    auto stage = [&](int s, int buf) {
+        const UTile u = at(s / nk);
+        const int k0 = K0 + 32 * (s % nk);
+        stage_tile_f32(A[buf], M, nf, u.rb, nf, k0, K1);
+        stage_tile_f32(B[buf], M, nf, u.J, min(nf, u.J + u.nb), k0, K1);
         cp_async_commit();
-        for (int q = 0; q < nk; ++q) {
-            const int cur = q & 1;
-            if (q + 1 < nk) {
-                stage_tile_f32(A[cur ^ 1], M, nf, rb, nf, K0 + 32 * (q + 1), K1);
-                stage_tile_f32(B[cur ^ 1], M, nf, J0, cmax, K0 + 32 * (q + 1), K1);
-                cp_async_commit();
-                cp_async_wait<1>();
-            } else {
-                cp_async_wait<0>();
-            }
-            __syncthreads();
-            if (!skip) {
-                const float* ta = A[cur];
-                const float* tb = B[cur];
-                const int kb = min(32, K1 - K0 - 32 * q);
-                for (int k = 0; k < kb; ++k) {
-                    const float4 av = *reinterpret_cast<const float4*>(ta + k * T32LD + tr * 4);
-                    const float4 bv = *reinterpret_cast<const float4*>(tb + k * T32LD + tc * 4);
-                    const float ar[4] = {av.x, av.y, av.z, av.w}, br[4] = {bv.x, bv.y, bv.z, bv.w};
+    };
+    float acc[4][4];
+    UTile u = at(0);
+    bool skip = false;
+    stage(0, 0);
+    for (int s = 0; s < nstep; ++s) {
+        const int q = s % nk, cur = s & 1;
+        if (q == 0) {
+            u = at(s / nk);
+            skip = tc * 4 >= u.nb || (u.rb == u.J && tr * 4 + 3 < tc * 4);
+            const int cmax = min(nf, u.J + u.nb);
 #pragma unroll
-                    for (int a = 0; a < 4; ++a)
+            for (int a = 0; a < 4; ++a)
 #pragma unroll
-                        for (int b = 0; b < 4; ++b) acc[a][b] = fmaf(ar[a], br[b], acc[a][b]);
+                for (int b = 0; b < 4; ++b) {
+                    const int row = u.rb + tr * 4 + a, col = u.J + tc * 4 + b;
+                    acc[a][b] = (!skip && row < nf && col < cmax && row >= col) ? M[row + (int64_t)col * nf] : 0.f;
                 }
-            }
-            __syncthreads();
         }
+        if (s + 1 < nstep) {
+            stage(s + 1, cur ^ 1);
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
+        }
+        __syncthreads();
         if (!skip) {
+            const float* ta = A[cur];
+            const float* tb = B[cur];
+            const int kb = min(32, K1 - K0 - 32 * q);
+            for (int k = 0; k < kb; ++k) {
+                const float4 av = *reinterpret_cast<const float4*>(ta + k * T32LD + tr * 4);
+                const float4 bv = *reinterpret_cast<const float4*>(tb + k * T32LD + tc * 4);
+                const float ar[4] = {av.x, av.y, av.z, av.w}, br[4] = {-bv.x, -bv.y, -bv.z, -bv.w};
+#pragma unroll
+                for (int a = 0; a < 4; ++a)
+#pragma unroll
+                    for (int b = 0; b < 4; ++b) acc[a][b] = fmaf(ar[a], br[b], acc[a][b]);
+            }
+        }
+        __syncthreads();
+        if (q == nk - 1 && !skip) {
+            const int cmax = min(nf, u.J + u.nb);
 #pragma unroll
             for (int b = 0; b < 4; ++b)
 #pragma unroll
                 for (int a = 0; a < 4; ++a) {
-                    const int row = rb + tr * 4 + a, col = J0 + tc * 4 + b;
-                    if (row < nf && col < cmax && row >= col) M[row + (int64_t)col * nf] -= acc[a][b];
+                    const int row = u.rb + tr * 4 + a, col = u.J + tc * 4 + b;
+                    if (row < nf && col < cmax && row >= col) M[row + (int64_t)col * nf] = acc[a][b];
                 }
         }
     }
@@ -309,22 +343,29 @@ __device__ void tile_f32(float* M, int nf, int rb, int J0, int nb, int K0, int K
 __device__ void update_cols_f32(float* M, int nf, int J0, int nb, int K0, int K1, Shared& sh, int rank = 0,
                                 int nranks = 1) {
     if (K1 <= K0 || nb <= 0) return;
-    for (int rb = J0 + TS * rank; rb < nf; rb += TS * nranks) tile_f32(M, nf, rb, J0, nb, K0, K1, sh);
+    const int first = J0 + TS * rank, step = TS * nranks;
+    const int ntile = first < nf ? (nf - first + step - 1) / step : 0;
+    tiles_f32(M, nf, ntile, K0, K1, sh, [=](int i) { return UTile{first + step * i, J0, nb}; });
     __syncthreads();
 }
 
 // Schur complement of a front's separator block, M[r, c] -= Σ_{k < K1} M[r, k] M[c, k] for
-// J0 <= c <= r < nf: every (row tile, 64-column block) pair, dealt round-robin over nranks CTAs
+// J0 <= c <= r < nf: every (64-column block, row tile) pair in column-block order, dealt
+// round-robin over nranks CTAs, all of one CTA's tiles in one pipeline
 template <class FT>
 __device__ void schur_tiles(FT* M, int nf, int J0, int K1, Shared& sh, int rank, int nranks) {
-    if (K1 <= 0) return;
-    int gi = 0;
-    for (int J = J0; J < nf; J += 64)
-        for (int rb = J; rb < nf; rb += TS, ++gi)
-            if (gi % nranks == rank) {
-                if constexpr (sizeof(FT) == 8) tile_f64((double*)M, nf, rb, J, min(64, nf - J), 0, K1, sh);
-                else tile_f32((float*)M, nf, rb, J, min(64, nf - J), 0, K1, sh);
-            }
+    if (K1 <= 0 || J0 >= nf) return;
+    const int nblk = (nf - J0 + 63) / 64;               // column blocks; block b has nblk - b row tiles
+    const int total = nblk * (nblk + 1) / 2;
+    const int ntile = rank < total ? (total - rank + nranks - 1) / nranks : 0;
+    auto at = [=](int i) {
+        int gi = rank + nranks * i, b = 0;
+        while (gi >= nblk - b) { gi -= nblk - b; ++b; }
+        const int J = J0 + 64 * b;
+        return UTile{J + TS * gi, J, min(64, nf - J)};
+    };
+    if constexpr (sizeof(FT) == 8) tiles_f64((double*)M, nf, ntile, 0, K1, sh, at);
+    else tiles_f32((float*)M, nf, ntile, 0, K1, sh, at);
     __syncthreads();
 }
 
@@ -583,6 +624,142 @@ __device__ void front_usolve(const FT* M, int nf, int nres, int r0, const int* s
 }
 
 
+// ---- triangular solves of one front with its slice of x in shared memory ----------------------
+// Fronts of order [XSM_MIN, COOP_MIN_SOLVE) keep xf[i] = x[front row i] in Shared::tile (idle during a solve)
+// for the whole front: the panel loads do not depend on x, so they are issued before each diagonal
+// solve and the row updates and dots read x from shared memory.  The forward sweep does the same
+// arithmetic in the same order as front_lsolve; the backward dots reduce in a different order.
+constexpr int XSM_CAP = 4 * TS * TLD;   // doubles in Shared::tile
+constexpr int XSM_MIN = 64;             // smaller fronts stay on the global-memory sweep (no gather)
+static_assert(COOP_MIN_SOLVE + 8 * 32 <= XSM_CAP, "front slice of x and dot partials must fit");
+
+template <class FT>
+__device__ __noinline__ void front_lsolve_sm(const FT* M, int nf, int nres, int r0, const int* sep, double* x, Shared& sh) {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    double* xf = sh.tile;
+    double* T = sh.diag;   // T[c*33 + r] = L[k0+r, k0+c]
+    for (int i = tid; i < nf; i += NT) xf[i] = x[i < nres ? r0 + i : sep[i - nres]];
+    __syncthreads();
+    for (int k0 = 0; k0 < nres; k0 += 32) {
+        const int kb = min(32, nres - k0);
+        const int i0 = k0 + kb + tid;
+        FT v[32];
+        if (kb == 32 && i0 < nf) {   // first panel row of this thread, in flight during the diagonal solve
+            const FT* Mi = M + i0 + (int64_t)k0 * nf;
+#pragma unroll
+            for (int c = 0; c < 32; ++c) v[c] = Mi[(int64_t)c * nf];
+        }
+        for (int idx = tid; idx < 32 * 32; idx += NT) {
+            int r = idx & 31, c = idx >> 5;
+            if (r < kb && c < kb && r >= c) T[c * 33 + r] = (double)M[(k0 + r) + (int64_t)(k0 + c) * nf];
+        }
+        __syncthreads();
+        if (warp == 0) {
+            double xv = lane < kb ? xf[k0 + lane] : 0.0;
+            for (int c = 0; c < kb; ++c) {
+                if (lane == c) xv = xv / T[c * 33 + c];
+                double xc = __shfl_sync(0xffffffffu, xv, c);
+                if (lane > c && lane < kb) xv -= T[c * 33 + lane] * xc;
+            }
+            if (lane < kb) { xf[k0 + lane] = xv; sh.xs[lane] = xv; }
+        }
+        __syncthreads();
+        for (int i = i0; i < nf; i += NT) {
+            const FT* Mi = M + i + (int64_t)k0 * nf;
+            double t = 0;
+            if (kb == 32) {
+                if (i != i0) {
+#pragma unroll
+                    for (int c = 0; c < 32; ++c) v[c] = Mi[(int64_t)c * nf];
+                }
+#pragma unroll
+                for (int c = 0; c < 32; ++c) t = fma((double)v[c], sh.xs[c], t);
+            } else {
+                for (int c = 0; c < kb; ++c) t = fma((double)Mi[(int64_t)c * nf], sh.xs[c], t);
+            }
+            xf[i] -= t;
+        }
+        __syncthreads();
+    }
+    for (int i = tid; i < nf; i += NT) x[i < nres ? r0 + i : sep[i - nres]] = xf[i];
+    __syncthreads();
+}
+
+// backward sweep of one front: for each 32-column block from the last, the dots
+// L[k0+kb:, k0+c] · xf[k0+kb:] (16 columns at a time in registers, a warp reduce-scatter, then
+// across warps), then the transposed diagonal solve
+template <class FT>
+__device__ __noinline__ void front_usolve_sm(const FT* M, int nf, int nres, int r0, const int* sep, double* x, Shared& sh) {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int nblk = (nres + 31) / 32;
+    double* xf = sh.tile;
+    double* part = sh.tile + XSM_CAP - NW * 32;   // part[w*32 + c]: warp w's share of column c's dot
+    double* T = sh.diag;
+    for (int i = tid; i < nf; i += NT) xf[i] = x[i < nres ? r0 + i : sep[i - nres]];
+    __syncthreads();
+    for (int bk = nblk - 1; bk >= 0; --bk) {
+        const int k0 = bk * 32, kb = min(32, nres - k0);
+        for (int h = 0; h < kb; h += 16) {
+            const int hb = min(16, kb - h);
+            double acc[16];
+#pragma unroll
+            for (int j = 0; j < 16; ++j) acc[j] = 0;
+            for (int i = k0 + kb + tid; i < nf; i += NT) {
+                const FT* Mi = M + i + (int64_t)(k0 + h) * nf;
+                const double xi = xf[i];
+                if (hb == 16) {
+                    FT v[16];
+#pragma unroll
+                    for (int j = 0; j < 16; ++j) v[j] = Mi[(int64_t)j * nf];
+#pragma unroll
+                    for (int j = 0; j < 16; ++j) acc[j] = fma((double)v[j], xi, acc[j]);
+                } else {
+#pragma unroll
+                    for (int j = 0; j < 16; ++j)
+                        if (j < hb) acc[j] = fma((double)Mi[(int64_t)j * nf], xi, acc[j]);
+                }
+            }
+            // reduce over the warp: afterwards lane l (and l + 16) holds column h + (l & 15)
+#pragma unroll
+            for (int j = 0; j < 16; ++j) acc[j] += __shfl_xor_sync(0xffffffffu, acc[j], 16);
+#pragma unroll
+            for (int o = 8; o >= 1; o >>= 1) {
+                const bool up = lane & o;
+#pragma unroll
+                for (int j = 0; j < o; ++j) {
+                    const double send = up ? acc[j] : acc[j + o];
+                    const double keep = up ? acc[j + o] : acc[j];
+                    acc[j] = keep + __shfl_xor_sync(0xffffffffu, send, o);
+                }
+            }
+            if (lane < 16) part[warp * 32 + h + lane] = acc[0];
+        }
+        for (int idx = tid; idx < 32 * 32; idx += NT) {
+            int r = idx & 31, c = idx >> 5;
+            if (r < kb && c < kb && r >= c) T[c * 33 + r] = (double)M[(k0 + r) + (int64_t)(k0 + c) * nf];
+        }
+        __syncthreads();
+        if (warp == 0) {
+            double dot = 0;
+            if (lane < kb) {
+#pragma unroll
+                for (int w = 0; w < NW; ++w) dot += part[w * 32 + lane];
+            }
+            double yv = lane < kb ? xf[k0 + lane] - dot : 0.0;
+            for (int c = kb - 1; c >= 0; --c) {
+                if (lane == c) yv = yv / T[c * 33 + c];
+                double xc = __shfl_sync(0xffffffffu, yv, c);
+                if (lane < c) yv -= T[lane * 33 + c] * xc;
+            }
+            if (lane < kb) xf[k0 + lane] = yv;
+        }
+        __syncthreads();
+    }
+    for (int i = tid; i < nres; i += NT) x[r0 + i] = xf[i];
+    __syncthreads();
+}
+
+
 template <class FT>
 __device__ __forceinline__ void update_cols(FT* M, int nf, int J0, int nb, int K0, int K1, Shared& sh);
 template <>
@@ -601,15 +778,22 @@ constexpr int COOP_ABORTED = -1;   // front_chol result when the grid barrier ti
 // (the update matrix handed to the parent by extend-add).  With `coop` and a front of at least
 // COOP_MIN_FRONT, the update tiles and panel rows are shared with the helper CTAs.
 template <class FT, bool COOP>
-__device__ int front_chol_ll(FT* M, int nf, int nres, Shared& sh, CoopCtl* coop) {
+__device__ int front_chol_ll(FT* M, int nf, int nres, Shared& sh, CoopCtl* coop, long long* tf) {
     const bool big = COOP && coop != nullptr && nf >= COOP_MIN_FRONT;
+    // tf[0..2]: SM clocks in the trailing updates, the diagonal blocks and the panel rows
+    auto tic = [&]() -> long long { __syncthreads(); return clock64(); };
+    auto toc = [&](int k, long long t0) { __syncthreads(); tf[k] += clock64() - t0; };
     auto upd = [&](int J0, int nb, int K0, int K1) -> bool {
         if (K1 <= K0 || nb <= 0) return true;
-        if (!big) { update_cols<FT>(M, nf, J0, nb, K0, K1, sh); return true; }
-        return coop_call(coop, sh, [&](CoopCtl* c) {
+        const long long t0 = tic();
+        bool ok = true;
+        if (!big) update_cols<FT>(M, nf, J0, nb, K0, K1, sh);
+        else ok = coop_call(coop, sh, [&](CoopCtl* c) {
             c->cmd = COOP_UPDATE; c->pa[0] = M;
             c->ia[0] = IsF32<FT>::v; c->ia[1] = nf; c->ia[2] = J0; c->ia[3] = nb; c->ia[4] = K0; c->ia[5] = K1;
         });
+        toc(0, t0);
+        return ok;
     };
     for (int J = 0; J < nres; J += 64) {
         const int nb = min(64, nres - J);
@@ -617,18 +801,23 @@ __device__ int front_chol_ll(FT* M, int nf, int nres, Shared& sh, CoopCtl* coop)
         for (int h = 0; h < nb; h += 32) {
             const int k0 = J + h, kb = min(32, nb - h);
             if (h > 0 && !upd(k0, kb, J, J + 32)) return COOP_ABORTED;
+            long long t0 = tic();
             const int info = diag_factor<FT>(M, nf, k0, kb, sh);
+            toc(1, t0);
             if (info) return info;
+            t0 = tic();
             if (!big) panel_rows<FT>(M, nf, k0, kb, sh, 0, 1, false);
             else if (!coop_call(coop, sh, [&](CoopCtl* c) {
                          c->cmd = COOP_PANEL; c->pa[0] = M;
                          c->ia[0] = IsF32<FT>::v; c->ia[1] = nf; c->ia[2] = k0; c->ia[3] = kb;
                      }))
                 return COOP_ABORTED;
+            toc(2, t0);
         }
     }
+    const long long t0 = tic();
     if (!big) {
-        for (int J = nres; J < nf; J += 64) upd(J, min(64, nf - J), 0, nres);
+        schur_tiles<FT>(M, nf, nres, nres, sh, 0, 1);
     } else if (nres > 0 && nf > nres &&
                !coop_call(coop, sh, [&](CoopCtl* c) {   // the whole separator block in one command
                    c->cmd = COOP_SCHUR; c->pa[0] = M;
@@ -636,6 +825,7 @@ __device__ int front_chol_ll(FT* M, int nf, int nres, Shared& sh, CoopCtl* coop)
                })) {
         return COOP_ABORTED;
     }
+    toc(0, t0);
     return 0;
 }
 
@@ -655,11 +845,16 @@ struct Ctx {
     bool fellback;          // mixed precision: the FP64 factor is in use for good
     int switched;           // mixed precision: moved to FP64 after a solve-heavy FP32 iteration
     int nfp32, nfallback;   // iterations accepted with the FP32 factor; FP64 redos
+    int stall0;             // history rows before the last precision switch (the stall window starts there)
+    bool stallhit;          // the last step_ ended on the stall test
     bool kktfail;           // the last iteration's factorization or a KKT solve failed
     int n, m, nv;
     double *Df, *Qp, *wf, *Dpa, *Dda, *Dp, *Dd, *df, *dx, *cgw, *tn;
     double *Dg, *Dya, *Dy, *dg, *dyv, *cgp, *tm1, *tm2;
     double *vstep, *vspsd, *vflag, *vscl, *vnrm, *vswp;
+    double *vsocz;          // 1: an SOC vertex whose diagonal block of Q is zero (H applied in O(n))
+    double *vsocdot;        // zᵀx of such a cone during a product with H
+    int nsocz;              // how many such vertices
     double delta;
     double nf, ng, sf, sg, nB;
     int nrow_hist;
@@ -688,6 +883,9 @@ struct Ctx {
         cgp = w + 5 * (int64_t)m; tm1 = w + 6 * (int64_t)m; tm2 = w + 7 * (int64_t)m;
         double* z = I.vv;
         vstep = z; vspsd = z + nv; vflag = z + 2 * nv; vscl = z + 3 * nv; vnrm = z + 4 * nv; vswp = z + 5 * nv;
+        vsocz = z + 6 * nv; vsocdot = z + 7 * nv;
+        nsocz = (int)I.scal[SCAL_NSOCZ];
+        stall0 = (int)I.scal[SCAL_STALL0]; stallhit = false;
         delta = 1; nrow_hist = 0; nretry = 0;
         nf = I.scal[5]; ng = I.scal[6]; sf = I.scal[7]; sg = I.scal[8]; nB = I.scal[9];
         nrow_hist = I.status[1]; nretry = I.status[2]; nfact = I.status[3];
@@ -701,6 +899,7 @@ struct Ctx {
             I.status[4] = nfp32; I.status[5] = nfallback; I.status[6] = switched;
             for (int k = 0; k < NSEC; ++k) I.scal[SCAL_SEC + k] = (double)tsec[k];
             I.scal[SCAL_NTRSV] = (double)ntrsv; I.scal[SCAL_NGEMV] = (double)ngemv;
+            I.scal[SCAL_STALL0] = (double)stall0;
         }
         __syncthreads();
     }
@@ -822,18 +1021,51 @@ struct Ctx {
     __device__ void amul(const double* Dblk, const double* x, double* y, double alpha, double beta) {
         const DevSp& Q = I.Q;
         const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, gl = lane % G, sub = lane / G;
+        const bool isH = Dblk == I.Hd;
+        if (isH && nsocz > 0) {   // zᵀx of the SOC cones applied in structured form
+            for (int v = warp; v < nv; v += NW) {
+                if (vsocz[v] == 0.0) continue;
+                const int c0 = I.xcol[v];
+                const double s = w_soczdot(I.cache + I.cxblk[v], x + c0, I.xcol[v + 1] - c0);
+                if (lane == 0) vsocdot[v] = s;
+            }
+            __syncthreads();
+        }
         for (int i0 = warp * GPW; i0 < n; i0 += NW * GPW) {
             const int i = i0 + sub;
             double acc = 0;
             if (i < n) {
                 int v = I.colvtx[i], c0 = I.xcol[v], nc = I.xcol[v + 1] - c0;
-                const double* row = Dblk + I.hdoff[v] + (int64_t)(i - c0) * nc;   // symmetric: row = column
-                for (int j = gl; j < nc; j += G) acc = fma(row[j], x[c0 + j], acc);
+                if (nsocz > 0 && vsocz[v] != 0.0) {   // zero Q block: H in structured form, Qd block skipped
+                    if (isH && gl == 0) acc = socz_row(I.cache + I.cxblk[v], x + c0, i - c0, vsocdot[v]);
+                } else {
+                    const double* row = Dblk + I.hdoff[v] + (int64_t)(i - c0) * nc;   // symmetric: row = column
+                    for (int j = gl; j < nc; j += G) acc = fma(row[j], x[c0 + j], acc);
+                }
                 for (int k = Q.rptr[i] + gl; k < Q.rptr[i + 1]; k += G) acc = fma(Q.val[k], x[Q.cidx[k]], acc);
             }
             acc = group_reduce(acc, OpSum());
             if (i < n && gl == 0) y[i] = beta == 0.0 ? alpha * acc : fma(alpha, acc, beta * y[i]);
         }
+        __syncthreads();
+    }
+
+    // vsocz / nsocz: SOC vertices whose diagonal block of Q is zero (after equilibration)
+    __device__ void mark_socz() {
+        int cnt = 0;
+        for (int v = threadIdx.x; v < nv; v += NT) vsocz[v] = 0;
+        __syncthreads();
+        for (int v = 0; v < nv; ++v) {
+            if (I.kind[v] != CONE_SOC) continue;
+            const int nc = I.xcol[v + 1] - I.xcol[v];
+            const double* q = I.Qd + I.hdoff[v];
+            double nz = 0;
+            for (int64_t t = threadIdx.x; t < (int64_t)nc * nc; t += NT) nz = fmax(nz, fabs(q[t]));
+            nz = block_reduce(nz, red, OpMax(), 0.0);
+            if (nz == 0.0) { cnt++; if (threadIdx.x == 0) vsocz[v] = 1; }
+        }
+        nsocz = cnt;
+        if (threadIdx.x == 0) I.scal[SCAL_NSOCZ] = (double)cnt;
         __syncthreads();
     }
 
@@ -867,7 +1099,7 @@ struct Ctx {
         const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
         // H_vv ← Q_vv for every cone block (cone.jl:146-174)
         for (int v = 0; v < nv; ++v) {
-            if (I.kind[v] == CONE_FREE) continue;
+            if (I.kind[v] == CONE_FREE || I.kind[v] == CONE_SOC) continue;   // SOC blocks: written below
             int nc = I.xcol[v + 1] - I.xcol[v];
             const double* q = I.Qd + I.hdoff[v];
             double* h = I.Hd + I.hdoff[v];
@@ -912,11 +1144,14 @@ struct Ctx {
             if (threadIdx.x == 0) { vflag[v] = fl ? 1.0 : 0.0; vspsd[v] = sp; }
         }
         __syncthreads();
-        // SOC Hessian blocks H = (2 (Jw)(Jw)ᵀ − J) / β² added in place (soc.jl:231-256)
+        // SOC Hessian blocks H = Q + (2 (Jw)(Jw)ᵀ − J) / β² (soc.jl:231-256); H = Q where the scaling failed
         for (int v = 0; v < nv; ++v) {
-            if (I.kind[v] != CONE_SOC || vflag[v] == 0.0) continue;
+            if (I.kind[v] != CONE_SOC) continue;
             int nc = I.xcol[v + 1] - I.xcol[v];
-            b_sochess(I.Hd + I.hdoff[v], I.cache + I.cxblk[v], nc);
+            const double* q = I.Qd + I.hdoff[v];
+            double* h = I.Hd + I.hdoff[v];
+            if (vflag[v] == 0.0) { for (int t = tid; t < nc * nc; t += NT) h[t] = q[t]; }
+            else b_sochess(h, q, vsocz[v] != 0.0, I.cache + I.cxblk[v], nc);
         }
         __syncthreads();
         double ok = 1, s = 0;
@@ -1105,11 +1340,12 @@ struct Ctx {
         for (int f = 0; f < I.nfront; ++f) {
             int nres = I.fnres[f], nsep = I.fnsep[f], nfr = nres + nsep;
             FT* M = F + I.fptr[f];
-            int info = front_chol_ll<FT, COOP>(M, nfr, nres, sh, coop);
+            int info = front_chol_ll<FT, COOP>(M, nfr, nres, sh, coop, tsec + SEC_FUPD);
             if (info == COOP_ABORTED) return COOP_ABORTED;
             if (info) return I.fres0[f] + info;
             int p = I.fparent[f];
             if (p >= 0 && nsep > 0) {
+                const long long te = tic();
                 int np = I.fnres[p] + I.fnsep[p];
                 FT* P = F + I.fptr[p];
                 const int* rel = I.frel + I.fsepp[f];
@@ -1119,13 +1355,15 @@ struct Ctx {
                             c->ia[0] = IsF32<FT>::v; c->ia[1] = nfr; c->ia[2] = nres; c->ia[3] = nsep; c->ia[4] = np;
                         }))
                         return COOP_ABORTED;
+                    toc(SEC_FEXTEND, te);
                     continue;
                 }
-                for (int64_t t = threadIdx.x; t < (int64_t)nsep * nsep; t += NT) {
-                    int i = (int)(t % nsep), j = (int)(t / nsep);
-                    if (i >= j) P[rel[i] + (int64_t)rel[j] * np] += M[(nres + i) + (int64_t)(nres + j) * nfr];
+                for (int j = threadIdx.x >> 5; j < nsep; j += NW) {   // column j of the update matrix per warp
+                    const FT* Mj = M + nres + (int64_t)(nres + j) * nfr;
+                    FT* Pj = P + (int64_t)rel[j] * np;
+                    for (int i = j + (threadIdx.x & 31); i < nsep; i += 32) Pj[rel[i]] += Mj[i];
                 }
-                __syncthreads();
+                toc(SEC_FEXTEND, te);
             }
         }
         return 0;
@@ -1166,7 +1404,8 @@ struct Ctx {
     __device__ void Lsolve_t(const FT* F, double* x) {
         for (int f = 0; f < I.nfront; ++f) {
             int nres = I.fnres[f], nfr = nres + I.fnsep[f];
-            front_lsolve<FT, COOP>(F + I.fptr[f], nfr, nres, I.fres0[f], I.fsep + I.fsepp[f], x, sh,
+            if (nfr >= XSM_MIN && nfr < COOP_MIN_SOLVE) front_lsolve_sm<FT>(F + I.fptr[f], nfr, nres, I.fres0[f], I.fsep + I.fsepp[f], x, sh);
+            else front_lsolve<FT, COOP>(F + I.fptr[f], nfr, nres, I.fres0[f], I.fsep + I.fsepp[f], x, sh,
                              nfr >= COOP_MIN_SOLVE ? coop : nullptr);
         }
     }
@@ -1174,7 +1413,8 @@ struct Ctx {
     __device__ void Usolve_t(const FT* F, double* x) {
         for (int f = I.nfront - 1; f >= 0; --f) {
             int nres = I.fnres[f], nfr = nres + I.fnsep[f];
-            front_usolve<FT, COOP>(F + I.fptr[f], nfr, nres, I.fres0[f], I.fsep + I.fsepp[f], x, sh,
+            if (nfr >= XSM_MIN && nfr < COOP_MIN_SOLVE) front_usolve_sm<FT>(F + I.fptr[f], nfr, nres, I.fres0[f], I.fsep + I.fsepp[f], x, sh);
+            else front_usolve<FT, COOP>(F + I.fptr[f], nfr, nres, I.fres0[f], I.fsep + I.fsepp[f], x, sh,
                              nfr >= COOP_MIN_SOLVE ? coop : nullptr);
         }
     }
@@ -1370,7 +1610,7 @@ struct Ctx {
         const int window = 5;
         int nh = nrow_hist;
         double tol = set.stall_tol;
-        if (nh > window) {
+        if (nh - stall0 > window) {
             for (int i = nh - window; i < nh; ++i) {
                 bool muok = hrow(i).mu < (1 - tol) * hrow(i - 1).mu;
                 bool pok = hrow(i).pres < (1 - tol) * hrow(i - 1).pres;
@@ -1410,8 +1650,9 @@ struct Ctx {
         for (int64_t i = threadIdx.x; i < I.cxblk[nv]; i += NT) I.cache2[i] = I.cache[i];
         __syncthreads();
         use32 = true;
+        stallhit = false;
         int st = step_();
-        if (!kktfail) {
+        if (!kktfail && !stallhit) {
             nfp32++;
             // an FP32 factor that needed more KKT solves than MIXED_MAX_SOLVES costs more in solves
             // than it saved in the factorization: keep this iteration and factor in FP64 from now on
@@ -1419,11 +1660,14 @@ struct Ctx {
             if (r.piter + r.ppass + r.citer + r.cpass > MIXED_MAX_SOLVES) { fellback = true; switched = 1; }
             return st;
         }
+        // a KKT solve missed its tolerance, or the FP32 iterates stalled: redo this iteration from the
+        // saved iterate with the FP64 factor, kept from now on (after a stall the stall window restarts)
         for (int i = threadIdx.x; i < n; i += NT) { I.p[i] = sp[i]; I.d[i] = sd[i]; }
         for (int i = threadIdx.x; i < m; i += NT) I.y[i] = sy[i];
         for (int64_t i = threadIdx.x; i < I.cxblk[nv]; i += NT) I.cache[i] = I.cache2[i];
         __syncthreads();
         nrow_hist--;
+        if (stallhit) { switched = 1; stall0 = nrow_hist; }
         fellback = true; use32 = false; nfallback++;
         return step_();
     }
@@ -1460,7 +1704,7 @@ struct Ctx {
             else if (isprimalinfeasible(set.infeas_rel, set.infeas_abs)) status = PRIMAL_INFEASIBLE;
             else if (isdualinfeasible(set.infeas_rel, set.infeas_abs)) status = DUAL_INFEASIBLE;
             else if (nrow_hist >= set.max_iter) status = nearstatus(ITERATION_LIMIT, mu, mus, pobj, dobj, pres, dres);
-            else if (isstalled()) status = nearstatus(STALLED, mu, mus, pobj, dobj, pres, dres);
+            else if (isstalled()) { stallhit = true; status = nearstatus(STALLED, mu, mus, pobj, dobj, pres, dres); }
             else if (I.nu == 0) {
                 double rho;
                 bool iok = initkkt(dl, rho);
@@ -1602,6 +1846,7 @@ __device__ void solve_instance(const DevInst& I, const Settings& set, Shared& sh
         // H = copy(Q) happens after equilibration (IPMSolver constructor order)
         for (int k = threadIdx.x; k < NSCAL; k += NT) I.scal[k] = 0;
         for (int k = 0; k < NSEC; ++k) c.tsec[k] = 0;
+        c.stall0 = 0;
         c.ntrsv = 0; c.ngemv = 0;
         long long t0 = c.tic();
         if (set.scale_max_iter > 0) c.equilibrate(set.scale_max_iter, 1e-3);
@@ -1615,6 +1860,7 @@ __device__ void solve_instance(const DevInst& I, const Settings& set, Shared& sh
         c.build_finit();
         c.toc(SEC_FINIT, t0);
         for (int64_t i = threadIdx.x; i < I.hdoff[I.nvtx]; i += NT) I.Hd[i] = I.Qd[i];   // H = copy(Q)
+        c.mark_socz();
         double s = 0;
         for (int i = threadIdx.x; i < I.B.nnz; i += NT) s += I.B.val[i] * I.B.val[i];
         c.nB = sqrt(block_reduce(s, c.red, OpSum(), 0.0));

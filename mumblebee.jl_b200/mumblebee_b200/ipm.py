@@ -447,10 +447,13 @@ class Batch:
         return out
 
     SECTIONS = ["equilibrate", "BtB", "scale", "initkkt", "predictor", "corrector", "maxsteps", "trsv", "gemv",
-                "assemble", "residual", "getaug", "ntrsv", "ngemv"]
+                "assemble", "residual", "getaug", "factor_update", "factor_diag", "factor_panel", "extend_add",
+                "ntrsv", "ngemv"]
 
     def timers(self):
-        """Per-instance section clocks (after fetch): array (ninst, 11), columns SECTIONS."""
+        """Per-instance section clocks (after fetch): array (ninst, len(SECTIONS)), columns SECTIONS.  The
+        factor_* and extend_add clocks are part of initkkt; trsv and gemv are part of predictor and
+        corrector; the last two columns count triangular-solve sweeps and matvecs."""
         W = len(self.SECTIONS)
         a = np.zeros(len(self.probs) * W)
         check(self.L.mb_batch_timers(self.h, _p(a, C.c_double), a.size), self.ctx.h, "timers")

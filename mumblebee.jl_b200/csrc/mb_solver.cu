@@ -31,6 +31,8 @@ constexpr int TLD = 36;  // tile row stride (doubles): 8-byte fragment loads of 
 struct Shared {
     double red[NW + 2];
     double diag[32 * 33];
+    double dinv[32];        // 1 / L[c][c] of the diagonal block in sh.diag
+    double col[32];         // one column of the diagonal block being factored
     double xs[32];
     double acc[32];
     double tile[4 * TS * TLD];   // stage 0 A, B, stage 1 A, B of the front update; x slices in solves
@@ -45,14 +47,16 @@ __device__ __forceinline__ void dmma(double& c0, double& c1, double a, double b)
                  : "+d"(c0), "+d"(c1) : "d"(a), "d"(b));
 }
 
-// Factor the kb x kb diagonal block at k0 (warp 0: lane l holds row l in registers, column c's
-// entries come from lane c by shuffle; the factor is also left in sh.diag for the panel solve and
-// written back to M).  Returns the failing pivot (1-based in the front) or 0.  Not inlined, so the
-// register-resident rows get their own allocation.
+// Factor the kb x kb diagonal block at k0 (warp 0: lane l holds row l in registers; each finished
+// column is broadcast through sh.col).  The factor is left in sh.diag, with 1 / L[c][c] in
+// sh.dinv for the panel solve, and written back to M.  Returns the failing pivot (1-based in the
+// front) or 0.  Not inlined, so the register-resident rows get their own allocation.
 template <class FT>
 __device__ __noinline__ int diag_factor(FT* M, int nf, int k0, int kb, Shared& sh) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     FT* S = reinterpret_cast<FT*>(sh.diag);
+    FT* col = reinterpret_cast<FT*>(sh.col);
+    FT* dinv = reinterpret_cast<FT*>(sh.dinv);
     if (warp == 0) {
         FT v[32];
 #pragma unroll
@@ -64,13 +68,17 @@ __device__ __noinline__ int diag_factor(FT* M, int nf, int k0, int kb, Shared& s
             const FT dd = __shfl_sync(0xffffffffu, v[c], c);   // the updated pivot, from lane c
             if (!(dd > FT(0))) { fail = c + 1; continue; }
             const FT dc = sqrt(dd);
-            if (lane == c) v[c] = dc;
-            else if (lane > c) v[c] = v[c] / dc;               // L[lane][c]
+            const FT r = FT(1) / dc;
+            if (lane == c) { v[c] = dc; dinv[c] = r; }
+            else if (lane > c) v[c] = v[c] * r;                  // L[lane][c]
+            col[lane] = v[c];
+            __syncwarp();
 #pragma unroll
             for (int cc = c + 1; cc < 32; ++cc) {
-                const FT lcc = __shfl_sync(0xffffffffu, v[c], cc);   // L[cc][c]
+                const FT lcc = col[cc];                            // L[cc][c], one broadcast read
                 if (lane >= cc) v[cc] -= v[c] * lcc;
             }
+            __syncwarp();
         }
         if (!fail && lane < kb) {
 #pragma unroll
@@ -84,22 +92,29 @@ __device__ __noinline__ int diag_factor(FT* M, int nf, int k0, int kb, Shared& s
 }
 
 // Panel solve L21 = A21 L11^{-T} for the rows [k0 + kb, nf) owned by this rank (row blocks of NT
-// rows dealt round-robin over nranks CTAs).  With `load`, the factored diagonal block is first read
-// back from M into sh.diag (a helper CTA that did not factor it).
+// rows dealt round-robin over nranks CTAs), multiplying by the reciprocal pivots.  With `load`, the
+// factored diagonal block is first read back from M into sh.diag (a helper CTA that did not
+// factor it) and its reciprocal pivots recomputed.
 template <class FT>
 __device__ __noinline__ void panel_rows(FT* M, int nf, int k0, int kb, Shared& sh, int rank, int nranks, bool load) {
     const int tid = threadIdx.x;
     FT* S = reinterpret_cast<FT*>(sh.diag);
+    FT* dinv = reinterpret_cast<FT*>(sh.dinv);
     if (load) {
         for (int t = tid; t < 32 * 32; t += NT) {
             const int r = t & 31, c = t >> 5;
             if (r < kb && c <= r) S[r * 33 + c] = M[(k0 + r) + (int64_t)(k0 + c) * nf];
         }
         __syncthreads();
+        if (tid < kb) dinv[tid] = FT(1) / S[tid * 33 + tid];   // as diag_factor computes it
+        __syncthreads();
     }
     {
         const int j0 = k0 + kb;
         for (int i = j0 + rank * NT + tid; i < nf; i += NT * nranks) {
+            // keeps the triangle's shared-memory reads inside the row loop: hoisted out of it, its
+            // 528 entries do not fit in registers and spill
+            asm volatile("" ::: "memory");
             FT x[32];
 #pragma unroll
             for (int c = 0; c < 32; ++c) {
@@ -107,7 +122,7 @@ __device__ __noinline__ void panel_rows(FT* M, int nf, int k0, int kb, Shared& s
                     FT t = M[i + (int64_t)(k0 + c) * nf];
 #pragma unroll
                     for (int cc = 0; cc < c; ++cc) t -= x[cc] * S[c * 33 + cc];
-                    x[c] = t / S[c * 33 + c];
+                    x[c] = t * dinv[c];
                 }
             }
 #pragma unroll
@@ -627,8 +642,8 @@ __device__ void front_usolve(const FT* M, int nf, int nres, int r0, const int* s
 // ---- triangular solves of one front with its slice of x in shared memory ----------------------
 // Fronts of order [XSM_MIN, COOP_MIN_SOLVE) keep xf[i] = x[front row i] in Shared::tile (idle during a solve)
 // for the whole front: the panel loads do not depend on x, so they are issued before each diagonal
-// solve and the row updates and dots read x from shared memory.  The forward sweep does the same
-// arithmetic in the same order as front_lsolve; the backward dots reduce in a different order.
+// solve and the row updates and dots read x from shared memory.  The diagonal steps multiply by
+// reciprocal pivots (one division per pivot, off the serial chain).
 constexpr int XSM_CAP = 4 * TS * TLD;   // doubles in Shared::tile
 constexpr int XSM_MIN = 64;             // smaller fronts stay on the global-memory sweep (no gather)
 static_assert(COOP_MIN_SOLVE + 8 * 32 <= XSM_CAP, "front slice of x and dot partials must fit");
@@ -653,11 +668,12 @@ __device__ __noinline__ void front_lsolve_sm(const FT* M, int nf, int nres, int 
             int r = idx & 31, c = idx >> 5;
             if (r < kb && c < kb && r >= c) T[c * 33 + r] = (double)M[(k0 + r) + (int64_t)(k0 + c) * nf];
         }
+        if (tid < kb) sh.dinv[tid] = 1.0 / (double)M[(k0 + tid) + (int64_t)(k0 + tid) * nf];
         __syncthreads();
         if (warp == 0) {
             double xv = lane < kb ? xf[k0 + lane] : 0.0;
             for (int c = 0; c < kb; ++c) {
-                if (lane == c) xv = xv / T[c * 33 + c];
+                if (lane == c) xv = xv * sh.dinv[c];
                 double xc = __shfl_sync(0xffffffffu, xv, c);
                 if (lane > c && lane < kb) xv -= T[c * 33 + lane] * xc;
             }
@@ -738,6 +754,7 @@ __device__ __noinline__ void front_usolve_sm(const FT* M, int nf, int nres, int 
             int r = idx & 31, c = idx >> 5;
             if (r < kb && c < kb && r >= c) T[c * 33 + r] = (double)M[(k0 + r) + (int64_t)(k0 + c) * nf];
         }
+        if (tid < kb) sh.dinv[tid] = 1.0 / (double)M[(k0 + tid) + (int64_t)(k0 + tid) * nf];
         __syncthreads();
         if (warp == 0) {
             double dot = 0;
@@ -747,7 +764,7 @@ __device__ __noinline__ void front_usolve_sm(const FT* M, int nf, int nres, int 
             }
             double yv = lane < kb ? xf[k0 + lane] - dot : 0.0;
             for (int c = kb - 1; c >= 0; --c) {
-                if (lane == c) yv = yv / T[c * 33 + c];
+                if (lane == c) yv = yv * sh.dinv[c];
                 double xc = __shfl_sync(0xffffffffu, yv, c);
                 if (lane < c) yv -= T[lane * 33 + c] * xc;
             }

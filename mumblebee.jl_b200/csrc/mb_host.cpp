@@ -440,6 +440,22 @@ static void merge(Packed& dst, Packed& src) {
     dst.plans.push_back(std::move(ip));
 }
 
+// Work-queue order of a batch: the persistent grid takes instances in DevInst-array order, so the
+// array is uploaded largest estimated cost first (LPT: the long solves start early and the short
+// ones fill the tail).  Cost = one factorization's flops + 16 x the factor's entries (the
+// triangular solves, assembly and matvecs that scale with its size).  Each DevInst carries its own
+// output pointers, so the order changes nothing a caller reads back.
+static void order_by_cost(std::vector<mb::DevInst>& hi, const std::vector<InstPlan>& plans) {
+    if (hi.size() < 2) return;
+    std::vector<size_t> idx(hi.size());
+    for (size_t k = 0; k < idx.size(); ++k) idx[k] = k;
+    auto cost = [&](size_t k) { return plans[k].fflops + 16.0 * (double)plans[k].fsize; };
+    std::stable_sort(idx.begin(), idx.end(), [&](size_t a, size_t b) { return cost(a) > cost(b); });
+    std::vector<mb::DevInst> out(hi.size());
+    for (size_t j = 0; j < idx.size(); ++j) out[j] = hi[idx[j]];
+    hi.swap(out);
+}
+
 struct mb_batch {
     mb_ctx* ctx = nullptr;
     mb_settings set{};
@@ -525,6 +541,7 @@ static int upload(mb_batch* b) {
         I.hist = ot + p.hist; I.uhist = wk + p.uhist; I.cghist = wk + p.cghist;
         I.status = b->d_ost + p.status; I.scal = ot + p.scal;
     }
+    order_by_cost(hi, pk.plans);
     CUDA_TRY(ctx, cudaMalloc((void**)&b->d_inst, hi.size() * sizeof(mb::DevInst)));
     CUDA_TRY(ctx, cudaMemcpyAsync(b->d_inst, hi.data(), hi.size() * sizeof(mb::DevInst), cudaMemcpyHostToDevice, st));
     CUDA_TRY(ctx, cudaEventCreate(&b->e0));
@@ -1272,6 +1289,7 @@ extern "C" int mb_batch_solve_static(mb_ctx* ctx, mb_problem* const* probs, int3
     hi.reserve(pk.plans.size());
     for (const InstPlan& p : pk.plans)
         hi.push_back(static_devinst(p, s_i32, s_i64, s_din, s_work, s_out, s_ost, base + L.F));
+    order_by_cost(hi, pk.plans);
     cudaStream_t st = ctx->stream;
     if (pk.i32.size()) CUDA_TRY(ctx, cudaMemcpyAsync(s_i32, pk.i32.h.data(), pk.i32.size() * sizeof(int32_t), cudaMemcpyHostToDevice, st));
     if (pk.i64a.size()) CUDA_TRY(ctx, cudaMemcpyAsync(s_i64, pk.i64a.h.data(), pk.i64a.size() * sizeof(i64), cudaMemcpyHostToDevice, st));

@@ -215,8 +215,8 @@ struct Packed {
 };
 
 // cachesize / workspacesize / degree  (soc.jl:116-134, tdc.jl:122-143, pos.jl:21-31, noc.jl:20-28,
-// sdp.jl:41-70: an SDP block of svec length n has order d = triroot(n), cache R | S | s = 2d² + d,
-// workspace max(3d², 2d² + 2d))
+// sdp.jl:41-70: an SDP block of svec length n has order d = triroot(n), cache R | S | s = 2d² + d
+// plus the scaling point W (d², for the structured H x), workspace max(3d², 2d² + 2d))
 static int64_t triroot(i64 n) {
     int64_t t = 1 + 8 * n, r = (int64_t)std::sqrt((double)t);
     while (r * r > t) --r;
@@ -224,7 +224,7 @@ static int64_t triroot(i64 n) {
     return (r - 1) / 2;
 }
 static int64_t cone_cachesize(int k, i64 n) {
-    if (k == MB_CONE_SDP) { int64_t d = triroot(n); return 2 * d * d + d; }
+    if (k == MB_CONE_SDP) { int64_t d = triroot(n); return 3 * d * d + d; }
     return k == MB_CONE_SOC ? 5 + n : ((k == MB_CONE_EXP || k == MB_CONE_POW) ? 19 : 0);
 }
 static int64_t cone_workspacesize(int k, i64 n) {

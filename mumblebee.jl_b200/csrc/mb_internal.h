@@ -97,7 +97,7 @@ struct DevInst {
     double* scal;           // NSCAL: mu pres dres pobj dobj nf ng sf sg nB, timers, counters
 };
 
-constexpr int NVEC_N = 12;  // Df Qp wf Dpa Dda Dp Dd df dx cgw  tmp1 tmp2 (tmp2 also: column maxima)
+constexpr int NVEC_N = 13;  // Df Qp wf Dpa Dda Dp Dd df dx cgw  tmp1 tmp2 (tmp2 also: column maxima)  hx
 constexpr int NVEC_M = 8;   // Dg Dya Dy dg dy cgp tmp1 tmp2
 // two more n-vectors and one m-vector follow the above (saved p, d, y of a mixed-precision redo)
 constexpr int NVEC_V = 8;   // step spsd flag vscl vnrm vswp socz socdot

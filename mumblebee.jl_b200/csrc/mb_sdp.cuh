@@ -19,8 +19,10 @@
 namespace mb {
 
 struct SdpSh {
-    double* red;   // ≥ 1 double of block-shared scratch (the reduction buffer)
-    int* flag;     // one block-shared int
+    double* red;       // ≥ 1 double of block-shared scratch (the reduction buffer)
+    int* flag;         // one block-shared int
+    double* tile = nullptr;   // optional block-shared scratch for b_skron_sm
+    int tilecap = 0;          // its size in doubles
 };
 
 #define SAT(A, i, j) (A)[(size_t)(i) + (size_t)(j) * (size_t)d]
@@ -165,6 +167,44 @@ __device__ void b_skron(double* H, int64_t ldh, const double* A, int d) {
         H[r + (int64_t)c * ldh] += v;
     }
     __syncthreads();
+}
+
+// b_skron with A and the svec index table (r -> (i, j)) staged in shared memory `sm` of at least
+// d² + n doubles: a warp per column of H, its lanes down the rows, each entry from the same formula
+// and operand order as b_skron.  With `assign` H is overwritten instead of added to.
+__device__ void b_skron_sm(double* H, int64_t ldh, const double* A, int d, double* sm, bool assign) {
+    const double a = sqrt(2.0);
+    const int n = d * (d + 1) / 2;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    double* As = sm;
+    int* tab = reinterpret_cast<int*>(sm + (size_t)d * d);
+    for (int t = threadIdx.x; t < d * d; t += NT) As[t] = A[t];
+    for (int r = threadIdx.x; r < n; r += NT) { int i, j; sdp_ij(r, d, i, j); tab[2 * r] = i; tab[2 * r + 1] = j; }
+    __syncthreads();
+    for (int c = warp; c < n; c += NW) {
+        const int k = tab[2 * c], l = tab[2 * c + 1];
+        double* Hc = H + (int64_t)c * ldh;
+        for (int r = lane; r < n; r += 32) {
+            const int i = tab[2 * r], j = tab[2 * r + 1];
+            double v;
+            if (k == l) v = i == j ? SAT(As, j, l) * SAT(As, j, l) : a * SAT(As, i, l) * SAT(As, j, l);
+            else v = i == j ? a * SAT(As, j, k) * SAT(As, j, l) : SAT(As, i, k) * SAT(As, j, l) + SAT(As, i, l) * SAT(As, j, k);
+            if (assign) Hc[r] = v; else Hc[r] += v;
+        }
+    }
+    __syncthreads();
+}
+
+// H x for an SDP block whose Q block is zero, H = W ⊗ₛ W: (W ⊗ₛ W) svec(X) = svec(W X W), two d×d
+// products instead of a pass over the n×n block.  Workspace 2d².
+__device__ void b_sdphx(double* y, const double* W, const double* x, int n, double* work) {
+    const int d = sdp_triroot(n);
+    const size_t m = (size_t)d * d;
+    double *X = work, *T = work + m;
+    b_smat(X, x, d, true);
+    b_mul(T, W, false, X, false, d);   // T = W X
+    b_mul(X, T, false, W, false, d);   // X = W X W
+    b_svec(y, X, d);
 }
 
 // one-sided Jacobi SVD (eig.jl:1-175): U ← left singular vectors, sg ← singular values; the
@@ -317,6 +357,65 @@ __device__ void t_tridiagonalize(double* M, double* a, double* b, int d) {
     for (int i = 0; i < d; ++i) a[i] = SAT(M, i, i);
 }
 
+// tridiagonalize! on the whole block: the same Householder steps as t_tridiagonalize, with each
+// element's arithmetic unchanged; the O(d²) parts of a step (scaling the reflector, w = τ M v and
+// the rank-2 update) run one element or row per thread, the two inner products on thread 0 in
+// their sequential order.  M is d×d (lower triangle used) in shared or global memory.
+__device__ void b_tridiagonalize(double* M, double* a, double* b, int d, SdpSh sh) {
+    double* sc = sh.red;   // sc[0] = r, sc[1] = τ, sc[2] = c, sc[3] = 1 when the reflector is trivial
+    for (int k = 0; k < d - 2; ++k) {
+        if (threadIdx.x == 0) {
+            double nxr = 0;
+            for (int i = k + 2; i < d; ++i) nxr += SAT(M, i, k) * SAT(M, i, k);
+            double x1 = SAT(M, k + 1, k);
+            if (nxr == 0) {
+                b[k] = x1;
+                SAT(M, k + 1, k) = 0;
+                sc[3] = 1;
+            } else {
+                double bk = -copysign(sqrt(x1 * x1 + nxr), x1);
+                b[k] = bk;
+                SAT(M, k + 1, k) = 1;
+                sc[0] = 1.0 / (x1 - bk);
+                sc[1] = (bk - x1) / bk;
+                sc[3] = 0;
+            }
+        }
+        __syncthreads();
+        if (sc[3] != 0) { __syncthreads(); continue; }
+        const double r = sc[0], tau = sc[1];
+        for (int i = k + 2 + threadIdx.x; i < d; i += NT) SAT(M, i, k) *= r;
+        __syncthreads();
+        for (int i = k + 1 + threadIdx.x; i < d; i += NT) {
+            double wi = 0;
+            for (int j = k + 1; j <= i; ++j) wi += SAT(M, i, j) * SAT(M, j, k);
+            for (int j = i + 1; j < d; ++j) wi += SAT(M, j, i) * SAT(M, j, k);
+            a[i] = wi * tau;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double c = 0;
+            for (int i = k + 1; i < d; ++i) c += a[i] * SAT(M, i, k);
+            sc[2] = c * (tau / 2);
+        }
+        __syncthreads();
+        const double c = sc[2];
+        for (int i = k + 1 + threadIdx.x; i < d; i += NT) a[i] -= c * SAT(M, i, k);
+        __syncthreads();
+        const int w = d - k - 1;   // trailing order; element (i, j), i ≥ j ≥ k + 1
+        for (int t = threadIdx.x; t < w * w; t += NT) {
+            const int i = k + 1 + t % w, j = k + 1 + t / w;
+            if (i >= j) SAT(M, i, j) -= SAT(M, i, k) * a[j] + a[i] * SAT(M, j, k);
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        if (d >= 2) b[d - 2] = SAT(M, d - 1, d - 2);
+        for (int i = 0; i < d; ++i) a[i] = SAT(M, i, i);
+    }
+    __syncthreads();
+}
+
 // minorpass (eig.jl:391-462)
 __device__ bool t_minorpass(const double* a, const double* b, double lam, int n, double& s1, double& s2) {
     bool flag = false;
@@ -366,8 +465,13 @@ __device__ double t_laguerremin(const double* a, const double* b, double lo, dou
 }
 
 // eigminsturm! (eig.jl:487-589)
+__device__ double t_eigminsturm_ab(double* a, double* b, int d, double lmax);
 __device__ double t_eigminsturm(double* M, double* a, double* b, int d, double lmax) {
     t_tridiagonalize(M, a, b, d);
+    return t_eigminsturm_ab(a, b, d, lmax);
+}
+// the Sturm / Laguerre part of eigminsturm! on the tridiagonal (a, b)
+__device__ double t_eigminsturm_ab(double* a, double* b, int d, double lmax) {
     double tmax = 0;
     for (int i = 0; i < d; ++i) tmax = sdp_nanmax(tmax, fabs(a[i]));
     for (int i = 0; i < d - 1; ++i) tmax = sdp_nanmax(tmax, fabs(b[i]));
@@ -405,11 +509,11 @@ __device__ __forceinline__ void w_sdpidentity(double* x, int n) {
     __syncwarp();
 }
 
-// sdpscale! (sdp.jl:121-263): H += W ⊗ₛ W, W = R Σ Rᵀ; cache R = LP⁻ᵀU | S = LP U | s = Σ;
-// spsd = Σ 1/sᵢ².  Workspace 2d².  false (uniformly) when p or d is not positive definite or the
-// SVD did not converge.
+// sdpscale! (sdp.jl:121-263): H += W ⊗ₛ W (H = W ⊗ₛ W with `assign`), W = R Σ Rᵀ; cache
+// R = LP⁻ᵀU | S = LP U | s = Σ | W; spsd = Σ 1/sᵢ².  Workspace 2d².  false (uniformly) when p or d
+// is not positive definite or the SVD did not converge.
 __device__ bool b_sdpscale(double* H, int n, double* c, const double* p, const double* dv, double* work,
-                           double& spsd, SdpSh sh) {
+                           double& spsd, SdpSh sh, bool assign = false) {
     const int d = sdp_triroot(n);
     const size_t m = (size_t)d * d;
     double *R = c, *S = c + m, *sg = c + 2 * m;
@@ -430,7 +534,13 @@ __device__ bool b_sdpscale(double* H, int n, double* c, const double* p, const d
     for (int t = threadIdx.x; t < d * d; t += NT) P[t] = R[t] * sqrt(sg[t / d]);
     __syncthreads();
     b_syrk_full(D, P, d);                      // W = (R Σ^½)(R Σ^½)ᵀ
-    b_skron(H, n, D, d);
+    double* Wc = c + 2 * m + d;
+    for (int t = threadIdx.x; t < d * d; t += NT) Wc[t] = D[t];
+    if (sh.tile && (int64_t)d * d + n <= sh.tilecap) b_skron_sm(H, n, D, d, sh.tile, assign);
+    else {
+        if (assign) { for (int64_t t = threadIdx.x; t < (int64_t)n * n; t += NT) H[t] = 0.0; __syncthreads(); }
+        b_skron(H, n, D, d);
+    }
     if (threadIdx.x == 0) {
         double sp = 0;
         for (int i = 0; i < d; ++i) sp += 1.0 / (sg[i] * sg[i]);
@@ -507,8 +617,13 @@ __device__ double b_sdpmaxstep(const double* F, const double* Dx, const double* 
     }
     __syncthreads();
     if (b_chol(C, d, sh)) return 1.0;
+    if (d > 3) {   // the tridiagonalization on the whole block, in shared memory when it fits
+        double* T = (sh.tile && (int64_t)d * d <= sh.tilecap) ? sh.tile : M;
+        if (T != M) { for (int t = threadIdx.x; t < d * d; t += NT) T[t] = M[t]; __syncthreads(); }
+        b_tridiagonalize(T, a, b, d, sh);
+    }
     if (threadIdx.x == 0) {
-        double lam = d <= 3 ? t_eigmin_small(M, d) : t_eigminsturm(M, a, b, d, -1.0);
+        double lam = d <= 3 ? t_eigmin_small(M, d) : t_eigminsturm_ab(a, b, d, -1.0);
         sh.red[0] = 1.0 / sdp_nanmax(1.0, -lam);
     }
     __syncthreads();

@@ -869,9 +869,11 @@ struct Ctx {
     double *Df, *Qp, *wf, *Dpa, *Dda, *Dp, *Dd, *df, *dx, *cgw, *tn;
     double *Dg, *Dya, *Dy, *dg, *dyv, *cgp, *tm1, *tm2;
     double *vstep, *vspsd, *vflag, *vscl, *vnrm, *vswp;
-    double *vsocz;          // 1: an SOC vertex whose diagonal block of Q is zero (H applied in O(n))
-    double *vsocdot;        // zᵀx of such a cone during a product with H
+    double *vsocz;          // vertices whose diagonal block of Q is zero and whose H block is applied
+                            // in structured form: 1 = SOC (rank one plus diagonal), 2 = SDP (W ⊗ₛ W)
+    double *vsocdot;        // zᵀx of such an SOC cone during a product with H
     int nsocz;              // how many such vertices
+    double *hx;             // (H x) of the structured SDP blocks during a product with H
     double delta;
     double nf, ng, sf, sg, nB;
     int nrow_hist;
@@ -894,7 +896,7 @@ struct Ctx {
         double* v = I.vn;
         Df = v; Qp = v + n; wf = v + 2 * (int64_t)n; Dpa = v + 3 * (int64_t)n; Dda = v + 4 * (int64_t)n;
         Dp = v + 5 * (int64_t)n; Dd = v + 6 * (int64_t)n; df = v + 7 * (int64_t)n; dx = v + 8 * (int64_t)n;
-        cgw = v + 9 * (int64_t)n; tn = v + 10 * (int64_t)n;
+        cgw = v + 9 * (int64_t)n; tn = v + 10 * (int64_t)n; hx = v + 12 * (int64_t)n;
         double* w = I.vm;
         Dg = w; Dya = w + m; Dy = w + 2 * (int64_t)m; dg = w + 3 * (int64_t)m; dyv = w + 4 * (int64_t)m;
         cgp = w + 5 * (int64_t)m; tm1 = w + 6 * (int64_t)m; tm2 = w + 7 * (int64_t)m;
@@ -1039,12 +1041,17 @@ struct Ctx {
         const DevSp& Q = I.Q;
         const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, gl = lane % G, sub = lane / G;
         const bool isH = Dblk == I.Hd;
-        if (isH && nsocz > 0) {   // zᵀx of the SOC cones applied in structured form
+        if (isH && nsocz > 0) {   // zᵀx of the structured SOC cones, (W ⊗ₛ W) x of the structured SDP cones
             for (int v = warp; v < nv; v += NW) {
-                if (vsocz[v] == 0.0) continue;
+                if (vsocz[v] != 1.0) continue;
                 const int c0 = I.xcol[v];
                 const double s = w_soczdot(I.cache + I.cxblk[v], x + c0, I.xcol[v + 1] - c0);
                 if (lane == 0) vsocdot[v] = s;
+            }
+            for (int v = 0; v < nv; ++v) {
+                if (vsocz[v] != 2.0) continue;
+                const int c0 = I.xcol[v], nc = I.xcol[v + 1] - c0, d = sdp_triroot(nc);
+                b_sdphx(hx + c0, I.cache + I.cxblk[v] + 2 * (int64_t)d * d + d, x + c0, nc, I.work);
             }
             __syncthreads();
         }
@@ -1054,7 +1061,8 @@ struct Ctx {
             if (i < n) {
                 int v = I.colvtx[i], c0 = I.xcol[v], nc = I.xcol[v + 1] - c0;
                 if (nsocz > 0 && vsocz[v] != 0.0) {   // zero Q block: H in structured form, Qd block skipped
-                    if (isH && gl == 0) acc = socz_row(I.cache + I.cxblk[v], x + c0, i - c0, vsocdot[v]);
+                    if (isH && gl == 0)
+                        acc = vsocz[v] == 1.0 ? socz_row(I.cache + I.cxblk[v], x + c0, i - c0, vsocdot[v]) : hx[i];
                 } else {
                     const double* row = Dblk + I.hdoff[v] + (int64_t)(i - c0) * nc;   // symmetric: row = column
                     for (int j = gl; j < nc; j += G) acc = fma(row[j], x[c0 + j], acc);
@@ -1067,19 +1075,19 @@ struct Ctx {
         __syncthreads();
     }
 
-    // vsocz / nsocz: SOC vertices whose diagonal block of Q is zero (after equilibration)
+    // vsocz / nsocz: SOC and SDP vertices whose diagonal block of Q is zero (after equilibration)
     __device__ void mark_socz() {
         int cnt = 0;
         for (int v = threadIdx.x; v < nv; v += NT) vsocz[v] = 0;
         __syncthreads();
         for (int v = 0; v < nv; ++v) {
-            if (I.kind[v] != CONE_SOC) continue;
+            if (I.kind[v] != CONE_SOC && I.kind[v] != CONE_SDP) continue;
             const int nc = I.xcol[v + 1] - I.xcol[v];
             const double* q = I.Qd + I.hdoff[v];
             double nz = 0;
             for (int64_t t = threadIdx.x; t < (int64_t)nc * nc; t += NT) nz = fmax(nz, fabs(q[t]));
             nz = block_reduce(nz, red, OpMax(), 0.0);
-            if (nz == 0.0) { cnt++; if (threadIdx.x == 0) vsocz[v] = 1; }
+            if (nz == 0.0) { cnt++; if (threadIdx.x == 0) vsocz[v] = I.kind[v] == CONE_SOC ? 1 : 2; }
         }
         nsocz = cnt;
         if (threadIdx.x == 0) I.scal[SCAL_NSOCZ] = (double)cnt;
@@ -1116,7 +1124,8 @@ struct Ctx {
         const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
         // H_vv ← Q_vv for every cone block (cone.jl:146-174)
         for (int v = 0; v < nv; ++v) {
-            if (I.kind[v] == CONE_FREE || I.kind[v] == CONE_SOC) continue;   // SOC blocks: written below
+            // SOC blocks are written below; structured SDP blocks are assigned by b_sdpscale
+            if (I.kind[v] == CONE_FREE || I.kind[v] == CONE_SOC || vsocz[v] == 2.0) continue;
             int nc = I.xcol[v + 1] - I.xcol[v];
             const double* q = I.Qd + I.hdoff[v];
             double* h = I.Hd + I.hdoff[v];
@@ -1157,7 +1166,7 @@ struct Ctx {
             int c0 = I.xcol[v], nc = I.xcol[v + 1] - c0;
             double sp = 0;
             bool fl = b_sdpscale(I.Hd + I.hdoff[v], nc, I.cache + I.cxblk[v], I.p + c0, I.d + c0, I.work, sp,
-                                 SdpSh{red, &sh.flag});
+                                 SdpSh{red, &sh.flag, sh.tile, XSM_CAP}, vsocz[v] == 2.0);
             if (threadIdx.x == 0) { vflag[v] = fl ? 1.0 : 0.0; vspsd[v] = sp; }
         }
         __syncthreads();
@@ -1265,8 +1274,8 @@ struct Ctx {
             int c0 = I.xcol[v], nc = I.xcol[v + 1] - c0;
             const double* c = I.cache + I.cxblk[v];
             const int64_t dd = sdp_triroot(nc);
-            double tp = b_sdpmaxstep(c, Dpv + c0, nullptr, nc, I.work, SdpSh{red, &sh.flag});
-            double td = b_sdpmaxstep(c + dd * dd, Ddv + c0, c + 2 * dd * dd, nc, I.work, SdpSh{red, &sh.flag});
+            double tp = b_sdpmaxstep(c, Dpv + c0, nullptr, nc, I.work, SdpSh{red, &sh.flag, sh.tile, XSM_CAP});
+            double td = b_sdpmaxstep(c + dd * dd, Ddv + c0, c + 2 * dd * dd, nc, I.work, SdpSh{red, &sh.flag, sh.tile, XSM_CAP});
             if (threadIdx.x == 0) vstep[v] = jmin(tp * step_frac, td * step_frac);
         }
         __syncthreads();

@@ -1304,12 +1304,28 @@ struct Ctx {
                 c->cmd = COOP_COPY; c->pa[0] = F; c->pa[1] = I.Finit; c->la[0] = I.fsize; c->ia[0] = IsF32<FT>::v;
             });
         } else {
-            int64_t i = tid;
-            for (; i + 3 * NT < I.fsize; i += 4 * NT) {
-                double a0 = I.Finit[i], a1 = I.Finit[i + NT], a2 = I.Finit[i + 2 * NT], a3 = I.Finit[i + 3 * NT];
-                F[i] = (FT)a0; F[i + NT] = (FT)a1; F[i + 2 * NT] = (FT)a2; F[i + 3 * NT] = (FT)a3;
+            // only the lower triangle of each front is ever read (factor, solves, extend-add, norms):
+            // large fronts copy it a warp per column, small ones whole and flat
+            const int lane = tid & 31, warp = tid >> 5;
+            for (int f = 0; f < I.nfront; ++f) {
+                const int nfr = I.fnres[f] + I.fnsep[f];
+                FT* M = F + I.fptr[f];
+                const double* M0 = I.Finit + I.fptr[f];
+                if (nfr < 64) {
+                    for (int t = tid; t < nfr * nfr; t += NT) M[t] = (FT)M0[t];
+                    continue;
+                }
+                for (int j = warp; j < nfr; j += NW) {
+                    FT* Mj = M + (int64_t)j * nfr;
+                    const double* Aj = M0 + (int64_t)j * nfr;
+                    int i = j + lane;
+                    for (; i + 96 < nfr; i += 128) {
+                        const double a0 = Aj[i], a1 = Aj[i + 32], a2 = Aj[i + 64], a3 = Aj[i + 96];
+                        Mj[i] = (FT)a0; Mj[i + 32] = (FT)a1; Mj[i + 64] = (FT)a2; Mj[i + 96] = (FT)a3;
+                    }
+                    for (; i < nfr; i += 32) Mj[i] = (FT)Aj[i];
+                }
             }
-            for (; i < I.fsize; i += NT) F[i] = (FT)I.Finit[i];
         }
         __syncthreads();
         // + δ H: diagonal blocks (lower part) and the off-diagonal nonzeros of Q (chordal.jl:1-80)

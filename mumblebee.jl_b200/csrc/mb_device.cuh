@@ -120,8 +120,9 @@ __device__ __forceinline__ void baxpy(double a, const double* x, double* y, int 
 }
 
 // Sparse products over the nonzeros of a block-sparse matrix (BlockSparseArrays/src/blas/gemv.jl:
-// 321-343 computes the same sums over the dense blocks; their explicit zeros add nothing).  A group
-// of G lanes owns one row (CSR) or one column (CSC) and reduces in a fixed order.
+// 321-343 computes the same sums over the dense blocks; their explicit zeros add nothing).  A thread
+// owns a row (CSR) or column (CSC) of at most LONG_ROW entries, a warp a longer one; each sum runs
+// in a fixed order.
 constexpr int G = 16;
 
 template <class Op>
@@ -131,48 +132,68 @@ __device__ __forceinline__ double group_reduce(double v, Op op) {
     return v;
 }
 
-// y <- alpha A x + beta y.  The loop bound is uniform per warp (both groups of a warp enter
-// group_reduce together).
+// Groups of G lanes (equilibration's row and column maxima).  The loop bound is uniform per warp
+// (both groups of a warp enter group_reduce together).
 constexpr int GPW = 32 / G;   // groups per warp
 
+// y <- alpha A x + beta y: a thread per row of at most LONG_ROW entries, a warp per longer row
+// (A.longr, listed by the host); each row is summed in a fixed order.
 __device__ void spmv(const DevSp& A, const double* x, double* y, double alpha, double beta) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, gl = lane % G, sub = lane / G;
-    for (int i0 = warp * GPW; i0 < A.nrow; i0 += NW * GPW) {
-        const int i = i0 + sub;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int i = threadIdx.x; i < A.nrow; i += NT) {
+        const int k0 = A.rptr[i], k1 = A.rptr[i + 1];
+        if (k1 - k0 > LONG_ROW) continue;
         double acc = 0;
-        if (i < A.nrow)
-            for (int k = A.rptr[i] + gl; k < A.rptr[i + 1]; k += G) acc = fma(A.val[k], x[A.cidx[k]], acc);
-        acc = group_reduce(acc, OpSum());
-        if (i < A.nrow && gl == 0) y[i] = beta == 0.0 ? alpha * acc : fma(alpha, acc, beta * y[i]);
+        for (int k = k0; k < k1; ++k) acc = fma(A.val[k], x[A.cidx[k]], acc);
+        y[i] = beta == 0.0 ? alpha * acc : fma(alpha, acc, beta * y[i]);
+    }
+    for (int t = warp; t < A.nlongr; t += NW) {
+        const int i = A.longr[t];
+        double acc = 0;
+        for (int k = A.rptr[i] + lane; k < A.rptr[i + 1]; k += 32) acc = fma(A.val[k], x[A.cidx[k]], acc);
+        acc = warp_sum(acc);
+        if (lane == 0) y[i] = beta == 0.0 ? alpha * acc : fma(alpha, acc, beta * y[i]);
     }
     __syncthreads();
 }
 
-// y <- alpha Aᵀ x + beta y
+// y <- alpha Aᵀ x + beta y, by columns of A the same way (A.longc)
 __device__ void spmvT(const DevSp& A, const double* x, double* y, double alpha, double beta) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, gl = lane % G, sub = lane / G;
-    for (int j0 = warp * GPW; j0 < A.ncol; j0 += NW * GPW) {
-        const int j = j0 + sub;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int j = threadIdx.x; j < A.ncol; j += NT) {
+        const int k0 = A.cptr[j], k1 = A.cptr[j + 1];
+        if (k1 - k0 > LONG_ROW) continue;
         double acc = 0;
-        if (j < A.ncol)
-            for (int k = A.cptr[j] + gl; k < A.cptr[j + 1]; k += G) acc = fma(A.val[A.cpos[k]], x[A.ridx[k]], acc);
-        acc = group_reduce(acc, OpSum());
-        if (j < A.ncol && gl == 0) y[j] = beta == 0.0 ? alpha * acc : fma(alpha, acc, beta * y[j]);
+        for (int k = k0; k < k1; ++k) acc = fma(A.val[A.cpos[k]], x[A.ridx[k]], acc);
+        y[j] = beta == 0.0 ? alpha * acc : fma(alpha, acc, beta * y[j]);
+    }
+    for (int t = warp; t < A.nlongc; t += NW) {
+        const int j = A.longc[t];
+        double acc = 0;
+        for (int k = A.cptr[j] + lane; k < A.cptr[j + 1]; k += 32) acc = fma(A.val[A.cpos[k]], x[A.ridx[k]], acc);
+        acc = warp_sum(acc);
+        if (lane == 0) y[j] = beta == 0.0 ? alpha * acc : fma(alpha, acc, beta * y[j]);
     }
     __syncthreads();
 }
 
 // dot(x, A, y)  (block_sparse_matrix.jl:1094-1109)
 __device__ double spdot(const DevSp& A, const double* x, const double* y, double* red) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, gl = lane % G, sub = lane / G;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     double s = 0;
-    for (int i0 = warp * GPW; i0 < A.nrow; i0 += NW * GPW) {
-        const int i = i0 + sub;
+    for (int i = threadIdx.x; i < A.nrow; i += NT) {
+        const int k0 = A.rptr[i], k1 = A.rptr[i + 1];
+        if (k1 - k0 > LONG_ROW) continue;
         double acc = 0;
-        if (i < A.nrow)
-            for (int k = A.rptr[i] + gl; k < A.rptr[i + 1]; k += G) acc = fma(A.val[k], y[A.cidx[k]], acc);
-        acc = group_reduce(acc, OpSum());
-        if (i < A.nrow && gl == 0) s = fma(x[i], acc, s);
+        for (int k = k0; k < k1; ++k) acc = fma(A.val[k], y[A.cidx[k]], acc);
+        s = fma(x[i], acc, s);
+    }
+    for (int t = warp; t < A.nlongr; t += NW) {
+        const int i = A.longr[t];
+        double acc = 0;
+        for (int k = A.rptr[i] + lane; k < A.rptr[i + 1]; k += 32) acc = fma(A.val[k], y[A.cidx[k]], acc);
+        acc = warp_sum(acc);
+        if (lane == 0) s = fma(x[i], acc, s);
     }
     return block_reduce(s, red, OpSum(), 0.0);
 }

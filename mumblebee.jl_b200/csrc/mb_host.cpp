@@ -178,8 +178,10 @@ struct InstPlan {
     i64 fsize;
     double fflops;            // algorithmic flops of one factorization
     i64 Bnnz, Qnnz, nqoff;
+    i64 nBlongr, nBlongc, nhlong;
     // i32
     size_t xcol, colvtx, cfront, Brptr, Bcidx, Bcptr, Bridx, Bcpos, Qrptr, Qcidx, Qcptr, Qridx, Qcpos, hdld, qoffk;
+    size_t Blongr, Blongc, hlong, hflag;
     size_t kind, fres0, fnres, fnsep, fparent, fsepp, fsep, frel;
     // i64
     size_t hdoff, hdpos, qoffpos, cxblk, fptr;
@@ -346,6 +348,25 @@ static int plan_instance(const mb_problem* P, const mb_settings& set, const doub
             qoffpos.push_back(fr.fptr[f] + rp + (j - fr.res0[f]) * nf);
         }
     ip.nqoff = (i64)qoffk.size();
+    // rows and columns with more than LONG_ROW terms in the sparse products: a warp each on the device.
+    // A row of the H (or Q) product has its vertex block's nc terms, or one when the block is applied in
+    // structured form (an SOC or SDP vertex whose Q block is zero), plus its off-diagonal-block Q terms.
+    auto longlist = [](const std::vector<i64>& ptr) {
+        std::vector<i64> L;
+        for (size_t i = 0; i + 1 < ptr.size(); ++i) if (ptr[i + 1] - ptr[i] > mb::LONG_ROW) L.push_back((i64)i);
+        return L;
+    };
+    std::vector<i64> Blongr = longlist(Brptr), Blongc = longlist(Bcptr), hlong, hflag(n, 0);
+    for (i64 v = 0; v < nv; ++v) {
+        const i64 nc = B.ncols(v);
+        const int kv = P->kind[vp[v]];
+        bool qzero = true;
+        for (i64 t = hdoff[v]; t < hdoff[v + 1] && qzero; ++t) qzero = Qd[t] == 0.0;
+        const i64 blk = ((kv == MB_CONE_SOC || kv == MB_CONE_SDP) && qzero) ? 1 : nc;
+        for (i64 i = B.xcol[v]; i < B.xcol[v + 1]; ++i)
+            if (blk + (Qrptr[i + 1] - Qrptr[i]) > mb::LONG_ROW) { hflag[i] = 1; hlong.push_back(i); }
+    }
+    ip.nBlongr = (i64)Blongr.size(); ip.nBlongc = (i64)Blongc.size(); ip.nhlong = (i64)hlong.size();
     // fronts
     std::vector<i64> fnsep(fr.nfront), fsepp(fr.nfront + 1, 0), fsep, frel;
     for (i64 f = 0; f < fr.nfront; ++f) {
@@ -381,6 +402,8 @@ static int plan_instance(const mb_problem* P, const mb_settings& set, const doub
     ip.fres0 = pk.i32.put(to32(fr.res0)); ip.fnres = pk.i32.put(to32(fr.nres)); ip.fnsep = pk.i32.put(to32(fnsep));
     ip.fparent = pk.i32.put(to32(fr.parent)); ip.fsepp = pk.i32.put(to32(fsepp)); ip.fsep = pk.i32.put(to32(fsep));
     ip.frel = pk.i32.put(to32(frel));
+    ip.Blongr = pk.i32.put(to32(Blongr)); ip.Blongc = pk.i32.put(to32(Blongc));
+    ip.hlong = pk.i32.put(to32(hlong)); ip.hflag = pk.i32.put(to32(hflag));
     // i64 arena
     ip.hdoff = pk.i64a.put(hdoff); ip.hdpos = pk.i64a.put(hdpos); ip.qoffpos = pk.i64a.put(qoffpos);
     ip.cxblk = pk.i64a.put(cx); ip.fptr = pk.i64a.put(fr.fptr);
@@ -427,7 +450,8 @@ static void merge(Packed& dst, Packed& src) {
     size_t bw = cat(dst.work, src.work), bo = cat(dst.out, src.out), bs = cat(dst.ost, src.ost);
     for (size_t* f : {&ip.xcol, &ip.colvtx, &ip.cfront, &ip.Brptr, &ip.Bcidx, &ip.Bcptr, &ip.Bridx, &ip.Bcpos,
                       &ip.Qrptr, &ip.Qcidx, &ip.Qcptr, &ip.Qridx, &ip.Qcpos, &ip.hdld, &ip.qoffk, &ip.kind,
-                      &ip.fres0, &ip.fnres, &ip.fnsep, &ip.fparent, &ip.fsepp, &ip.fsep, &ip.frel}) *f += b32;
+                      &ip.fres0, &ip.fnres, &ip.fnsep, &ip.fparent, &ip.fsepp, &ip.fsep, &ip.frel,
+                      &ip.Blongr, &ip.Blongc, &ip.hlong, &ip.hflag}) *f += b32;
     for (size_t* f : {&ip.hdoff, &ip.hdpos, &ip.qoffpos, &ip.cxblk, &ip.fptr}) *f += b64;
     for (size_t* f : {&ip.Bval, &ip.Qval, &ip.Qd, &ip.f, &ip.g, &ip.kpar, &ip.p, &ip.d, &ip.y}) *f += bin;
     for (size_t* f : {&ip.wBval, &ip.wQval, &ip.wQd, &ip.Hd, &ip.Finit, &ip.pscl, &ip.yscl, &ip.vn, &ip.vm, &ip.vv,
@@ -439,6 +463,11 @@ static void merge(Packed& dst, Packed& src) {
     dst.fbytes = fb + src.fbytes;
     dst.plans.push_back(std::move(ip));
 }
+
+namespace {
+mb::DevInst static_devinst(const InstPlan& p, int32_t* i32, i64* q64, double* dn, double* wk, double* ot,
+                           int32_t* ost, char* F);
+}  // namespace
 
 // Work-queue order of a batch: the persistent grid takes instances in DevInst-array order, so the
 // array is uploaded largest estimated cost first (LPT: the long solves start early and the short
@@ -508,39 +537,8 @@ static int upload(mb_batch* b) {
     CUDA_TRY(ctx, cudaMemsetAsync(b->d_ost, 0, std::max<size_t>(pk.ost.size(), 1) * sizeof(int32_t), st));
     CUDA_TRY(ctx, cudaMallocHost((void**)&b->h_i32, std::max<size_t>(pk.ost.size(), 1) * sizeof(int32_t)));
     std::vector<mb::DevInst> hi(pk.plans.size());
-    for (size_t k = 0; k < pk.plans.size(); ++k) {
-        const InstPlan& p = pk.plans[k];
-        mb::DevInst& I = hi[k];
-        int32_t* i32 = b->d_i32; i64* q64 = b->d_i64; double* dn = b->d_din; double* wk = b->d_work; double* ot = b->d_out;
-        I.n = (int)p.n; I.m = (int)p.m; I.nvtx = (int)p.nvtx; I.nfront = (int)p.nfront; I.nu = (int)p.nu;
-        I.has_p0 = p.has_p0; I.has_d0 = p.has_d0; I.has_y0 = p.has_y0; I.mut = p.mut;
-        I.xcol = i32 + p.xcol; I.colvtx = i32 + p.colvtx; I.cfront = i32 + p.cfront;
-        auto fillsp = [&](mb::DevSp& A, i64 nrow, i64 ncol, i64 nnz, size_t rptr, size_t cidx, size_t wval, size_t val0,
-                          size_t cptr, size_t ridx, size_t cpos) {
-            A.nrow = (int)nrow; A.ncol = (int)ncol; A.nnz = (int)nnz;
-            A.rptr = i32 + rptr; A.cidx = i32 + cidx; A.val = wk + wval; A.val0 = dn + val0;
-            A.cptr = i32 + cptr; A.ridx = i32 + ridx; A.cpos = i32 + cpos;
-        };
-        fillsp(I.B, p.m, p.n, p.Bnnz, p.Brptr, p.Bcidx, p.wBval, p.Bval, p.Bcptr, p.Bridx, p.Bcpos);
-        fillsp(I.Q, p.n, p.n, p.Qnnz, p.Qrptr, p.Qcidx, p.wQval, p.Qval, p.Qcptr, p.Qridx, p.Qcpos);
-        I.hdoff = (const int64_t*)(q64 + p.hdoff); I.Qd = wk + p.wQd; I.Qd0 = dn + p.Qd; I.Hd = wk + p.Hd;
-        I.hdpos = (const int64_t*)(q64 + p.hdpos); I.hdld = i32 + p.hdld;
-        I.nqoff = (int)p.nqoff; I.qoffk = i32 + p.qoffk; I.qoffpos = (const int64_t*)(q64 + p.qoffpos);
-        I.kind = i32 + p.kind; I.kpar = dn + p.kpar; I.cxblk = (const int64_t*)(q64 + p.cxblk); I.cache = wk + p.cache;
-        I.cache2 = wk + p.cache2;
-        I.wsize = p.wsize;
-        I.fres0 = i32 + p.fres0; I.fnres = i32 + p.fnres; I.fnsep = i32 + p.fnsep; I.fparent = i32 + p.fparent;
-        I.fptr = (const int64_t*)(q64 + p.fptr); I.fsepp = i32 + p.fsepp; I.fsep = i32 + p.fsep; I.frel = i32 + p.frel;
-        I.fsize = p.fsize;
-        I.Finit = wk + p.Finit; I.F = (char*)b->d_F + p.F;
-        I.f0 = dn + p.f; I.g0 = dn + p.g; I.p0 = dn + p.p; I.d0 = dn + p.d; I.y0 = dn + p.y;
-        I.f = wk + p.wf; I.g = wk + p.wg; I.pscl = wk + p.pscl; I.yscl = wk + p.yscl;
-        I.p = wk + p.wp; I.d = wk + p.wd; I.y = wk + p.wy;
-        I.vn = wk + p.vn; I.vm = wk + p.vm; I.vv = wk + p.vv; I.work = wk + p.work;
-        I.po = ot + p.po; I.dout = ot + p.dout; I.yo = ot + p.yo;
-        I.hist = ot + p.hist; I.uhist = wk + p.uhist; I.cghist = wk + p.cghist;
-        I.status = b->d_ost + p.status; I.scal = ot + p.scal;
-    }
+    for (size_t k = 0; k < pk.plans.size(); ++k)
+        hi[k] = static_devinst(pk.plans[k], b->d_i32, b->d_i64, b->d_din, b->d_work, b->d_out, b->d_ost, (char*)b->d_F);
     order_by_cost(hi, pk.plans);
     CUDA_TRY(ctx, cudaMalloc((void**)&b->d_inst, hi.size() * sizeof(mb::DevInst)));
     CUDA_TRY(ctx, cudaMemcpyAsync(b->d_inst, hi.data(), hi.size() * sizeof(mb::DevInst), cudaMemcpyHostToDevice, st));
@@ -591,7 +589,8 @@ static void merge_all(Packed& dst, std::vector<Packed>& src, int nth) {
             InstPlan ip = std::move(s.plans[0]);
             for (size_t* f : {&ip.xcol, &ip.colvtx, &ip.cfront, &ip.Brptr, &ip.Bcidx, &ip.Bcptr, &ip.Bridx, &ip.Bcpos,
                               &ip.Qrptr, &ip.Qcidx, &ip.Qcptr, &ip.Qridx, &ip.Qcpos, &ip.hdld, &ip.qoffk, &ip.kind,
-                              &ip.fres0, &ip.fnres, &ip.fnsep, &ip.fparent, &ip.fsepp, &ip.fsep, &ip.frel}) *f += b32[k];
+                              &ip.fres0, &ip.fnres, &ip.fnsep, &ip.fparent, &ip.fsepp, &ip.fsep, &ip.frel,
+                      &ip.Blongr, &ip.Blongc, &ip.hlong, &ip.hflag}) *f += b32[k];
             for (size_t* f : {&ip.hdoff, &ip.hdpos, &ip.qoffpos, &ip.cxblk, &ip.fptr}) *f += b64[k];
             for (size_t* f : {&ip.Bval, &ip.Qval, &ip.Qd, &ip.f, &ip.g, &ip.kpar, &ip.p, &ip.d, &ip.y}) *f += bin[k];
             for (size_t* f : {&ip.wBval, &ip.wQval, &ip.wQd, &ip.Hd, &ip.Finit, &ip.pscl, &ip.yscl, &ip.vn, &ip.vm, &ip.vv,
@@ -1201,6 +1200,9 @@ mb::DevInst static_devinst(const InstPlan& p, int32_t* i32, i64* q64, double* dn
     };
     fillsp(I.B, p.m, p.n, p.Bnnz, p.Brptr, p.Bcidx, p.wBval, p.Bval, p.Bcptr, p.Bridx, p.Bcpos);
     fillsp(I.Q, p.n, p.n, p.Qnnz, p.Qrptr, p.Qcidx, p.wQval, p.Qval, p.Qcptr, p.Qridx, p.Qcpos);
+    I.B.nlongr = (int)p.nBlongr; I.B.longr = i32 + p.Blongr; I.B.nlongc = (int)p.nBlongc; I.B.longc = i32 + p.Blongc;
+    I.Q.nlongr = 0; I.Q.longr = nullptr; I.Q.nlongc = 0; I.Q.longc = nullptr;   // Q's rows go through hlong
+    I.nhlong = (int)p.nhlong; I.hlong = i32 + p.hlong; I.hflag = i32 + p.hflag;
     I.hdoff = (const int64_t*)(q64 + p.hdoff); I.Qd = wk + p.wQd; I.Qd0 = dn + p.Qd; I.Hd = wk + p.Hd;
     I.hdpos = (const int64_t*)(q64 + p.hdpos); I.hdld = i32 + p.hdld;
     I.nqoff = (int)p.nqoff; I.qoffk = i32 + p.qoffk; I.qoffpos = (const int64_t*)(q64 + p.qoffpos);

@@ -46,7 +46,12 @@ struct DevSp {
     const int* cptr;        // ncol+1
     const int* ridx;        // nnz: row of each CSC entry (ascending within a column)
     const int* cpos;        // nnz: CSR position of each CSC entry
+    int nlongr, nlongc;     // rows / columns with more than LONG_ROW entries (a warp each; the rest a thread each)
+    const int* longr;       // nlongr rows
+    const int* longc;       // nlongc columns
 };
+
+constexpr int LONG_ROW = 32;   // sparse products: longer rows or columns go to a warp, shorter ones to a thread
 
 struct DevInst {
     int n, m, nvtx, nfront;
@@ -57,6 +62,11 @@ struct DevInst {
     const int* colvtx;      // n: vertex of each column
     const int* cfront;      // n: front owning each column
     DevSp B, Q;
+    // rows of the product (blockdiag(Hd or Qd) + Q off-diagonal blocks) x that have more than LONG_ROW
+    // terms (a warp each); hflag[i] = 1 marks them for the thread-per-row pass to skip
+    int nhlong;
+    const int* hlong;
+    const int* hflag;
     // dense diagonal blocks (nc x nc per vertex, column-major): Q's (working + pristine) and H's
     const int64_t* hdoff;   // nvtx+1
     double* Qd; const double* Qd0; double* Hd;

@@ -1039,7 +1039,7 @@ struct Ctx {
     // y <- alpha (blockdiag(D) + Qo) x + beta y with D = Qd (the data Q) or Hd (the scaled H)
     __device__ void amul(const double* Dblk, const double* x, double* y, double alpha, double beta) {
         const DevSp& Q = I.Q;
-        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, gl = lane % G, sub = lane / G;
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
         const bool isH = Dblk == I.Hd;
         if (isH && nsocz > 0) {   // zᵀx of the structured SOC cones, (W ⊗ₛ W) x of the structured SDP cones
             for (int v = warp; v < nv; v += NW) {
@@ -1055,22 +1055,37 @@ struct Ctx {
             }
             __syncthreads();
         }
-        for (int i0 = warp * GPW; i0 < n; i0 += NW * GPW) {
-            const int i = i0 + sub;
+        auto head = [&](int i, double acc) {   // y[i] from the row's sum
+            y[i] = beta == 0.0 ? alpha * acc : fma(alpha, acc, beta * y[i]);
+        };
+        // rows with at most LONG_ROW terms: a thread each (I.hflag marks the others)
+        for (int i = threadIdx.x; i < n; i += NT) {
+            if (I.hflag[i]) continue;
+            const int v = I.colvtx[i], c0 = I.xcol[v], nc = I.xcol[v + 1] - c0;
             double acc = 0;
-            if (i < n) {
-                int v = I.colvtx[i], c0 = I.xcol[v], nc = I.xcol[v + 1] - c0;
-                if (nsocz > 0 && vsocz[v] != 0.0) {   // zero Q block: H in structured form, Qd block skipped
-                    if (isH && gl == 0)
-                        acc = vsocz[v] == 1.0 ? socz_row(I.cache + I.cxblk[v], x + c0, i - c0, vsocdot[v]) : hx[i];
-                } else {
-                    const double* row = Dblk + I.hdoff[v] + (int64_t)(i - c0) * nc;   // symmetric: row = column
-                    for (int j = gl; j < nc; j += G) acc = fma(row[j], x[c0 + j], acc);
-                }
-                for (int k = Q.rptr[i] + gl; k < Q.rptr[i + 1]; k += G) acc = fma(Q.val[k], x[Q.cidx[k]], acc);
+            if (nsocz > 0 && vsocz[v] != 0.0) {   // zero Q block: H in structured form, Qd block skipped
+                if (isH) acc = vsocz[v] == 1.0 ? socz_row(I.cache + I.cxblk[v], x + c0, i - c0, vsocdot[v]) : hx[i];
+            } else {
+                const double* row = Dblk + I.hdoff[v] + (int64_t)(i - c0) * nc;   // symmetric: row = column
+                for (int j = 0; j < nc; ++j) acc = fma(row[j], x[c0 + j], acc);
             }
-            acc = group_reduce(acc, OpSum());
-            if (i < n && gl == 0) y[i] = beta == 0.0 ? alpha * acc : fma(alpha, acc, beta * y[i]);
+            for (int k = Q.rptr[i]; k < Q.rptr[i + 1]; ++k) acc = fma(Q.val[k], x[Q.cidx[k]], acc);
+            head(i, acc);
+        }
+        // longer rows (I.hlong): a warp each
+        for (int t = warp; t < I.nhlong; t += NW) {
+            const int i = I.hlong[t];
+            const int v = I.colvtx[i], c0 = I.xcol[v], nc = I.xcol[v + 1] - c0;
+            double acc = 0;
+            if (nsocz > 0 && vsocz[v] != 0.0) {
+                if (isH && lane == 0) acc = vsocz[v] == 1.0 ? socz_row(I.cache + I.cxblk[v], x + c0, i - c0, vsocdot[v]) : hx[i];
+            } else {
+                const double* row = Dblk + I.hdoff[v] + (int64_t)(i - c0) * nc;
+                for (int j = lane; j < nc; j += 32) acc = fma(row[j], x[c0 + j], acc);
+            }
+            for (int k = Q.rptr[i] + lane; k < Q.rptr[i + 1]; k += 32) acc = fma(Q.val[k], x[Q.cidx[k]], acc);
+            acc = warp_sum(acc);
+            if (lane == 0) head(i, acc);
         }
         __syncthreads();
     }

@@ -362,9 +362,12 @@ static int plan_instance(const mb_problem* P, const mb_settings& set, const doub
         const int kv = P->kind[vp[v]];
         bool qzero = true;
         for (i64 t = hdoff[v]; t < hdoff[v + 1] && qzero; ++t) qzero = Qd[t] == 0.0;
-        const i64 blk = ((kv == MB_CONE_SOC || kv == MB_CONE_SDP) && qzero) ? 1 : nc;
-        for (i64 i = B.xcol[v]; i < B.xcol[v + 1]; ++i)
-            if (blk + (Qrptr[i + 1] - Qrptr[i]) > mb::LONG_ROW) { hflag[i] = 1; hlong.push_back(i); }
+        const bool structured = (kv == MB_CONE_SOC || kv == MB_CONE_SDP) && qzero;
+        const i64 blk = structured ? 1 : nc;
+        for (i64 i = B.xcol[v]; i < B.xcol[v + 1]; ++i) {
+            if (blk + (Qrptr[i + 1] - Qrptr[i]) > mb::LONG_ROW) { hflag[i] |= 1; hlong.push_back(i); }
+            if (qzero) hflag[i] |= 2;   // the vertex's Q block is zero: equilibration skips it
+        }
     }
     ip.nBlongr = (i64)Blongr.size(); ip.nBlongc = (i64)Blongc.size(); ip.nhlong = (i64)hlong.size();
     // fronts

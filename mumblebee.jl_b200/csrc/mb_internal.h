@@ -63,7 +63,8 @@ struct DevInst {
     const int* cfront;      // n: front owning each column
     DevSp B, Q;
     // rows of the product (blockdiag(Hd or Qd) + Q off-diagonal blocks) x that have more than LONG_ROW
-    // terms (a warp each); hflag[i] = 1 marks them for the thread-per-row pass to skip
+    // terms (a warp each); hflag[i] bit 0 marks them for the thread-per-row pass to skip, bit 1 marks
+    // the rows of a vertex whose diagonal Q block is zero
     int nhlong;
     const int* hlong;
     const int* hflag;

@@ -49,8 +49,9 @@ __device__ __forceinline__ void dmma(double& c0, double& c1, double a, double b)
 
 // Factor the kb x kb diagonal block at k0 (warp 0: lane l holds row l in registers; each finished
 // column is broadcast through sh.col).  The factor is left in sh.diag, with 1 / L[c][c] in
-// sh.dinv for the panel solve, and written back to M.  Returns the failing pivot (1-based in the
-// front) or 0.  Not inlined, so the register-resident rows get their own allocation.
+// sh.dinv for the panel solve, and written back to M; its inverse goes to the block's upper
+// triangle for the triangular solves.  Returns the failing pivot (1-based in the front) or 0.  Not
+// inlined, so the register-resident rows get their own allocation.
 template <class FT>
 __device__ __noinline__ int diag_factor(FT* M, int nf, int k0, int kb, Shared& sh) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -84,6 +85,25 @@ __device__ __noinline__ int diag_factor(FT* M, int nf, int k0, int kb, Shared& s
 #pragma unroll
             for (int c = 0; c < 32; ++c)
                 if (c <= lane) { S[lane * 33 + c] = v[c]; M[(k0 + lane) + (int64_t)(k0 + c) * nf] = v[c]; }
+        }
+        if (!fail) {
+            // X = L⁻¹ for the triangular solves: lane c forms column c of X by forward substitution in axpy
+            // order (X[k][c] = −(Σ_{j<k} L[k][j] X[j][c]) / L[k][k], times the reciprocal pivot) and stores
+            // X[k][c], k > c, transposed into the block's upper triangle, M[k0 + c, k0 + k], which nothing
+            // else reads; X[c][c] = 1 / L[c][c] is not stored
+            __syncwarp();
+            const int c = lane;
+            FT acc[32];
+#pragma unroll
+            for (int i = 0; i < 32; ++i) acc[i] = FT(0);
+#pragma unroll
+            for (int k = 0; k < 32; ++k) {
+                if (k >= kb) continue;
+                const FT xk = k < c ? FT(0) : (k == c ? dinv[c] : -acc[k] * dinv[k]);
+                if (k > c && c < kb) M[(k0 + c) + (int64_t)(k0 + k) * nf] = xk;
+#pragma unroll
+                for (int i = k + 1; i < 32; ++i) acc[i] = fma(S[i * 33 + k], xk, acc[i]);
+            }
         }
         if (lane == 0) sh.flag = fail ? k0 + fail : 0;
     }
@@ -642,8 +662,8 @@ __device__ void front_usolve(const FT* M, int nf, int nres, int r0, const int* s
 // ---- triangular solves of one front with its slice of x in shared memory ----------------------
 // Fronts of order [XSM_MIN, COOP_MIN_SOLVE) keep xf[i] = x[front row i] in Shared::tile (idle during a solve)
 // for the whole front: the panel loads do not depend on x, so they are issued before each diagonal
-// solve and the row updates and dots read x from shared memory.  The diagonal steps multiply by
-// reciprocal pivots (one division per pivot, off the serial chain).
+// solve and the row updates and dots read x from shared memory.  The diagonal steps apply the
+// block inverse diag_factor stored (a lane per row, no serial chain over the block's columns).
 constexpr int XSM_CAP = 4 * TS * TLD;   // doubles in Shared::tile
 constexpr int XSM_MIN = 64;             // smaller fronts stay on the global-memory sweep (no gather)
 static_assert(COOP_MIN_SOLVE + 8 * 32 <= XSM_CAP, "front slice of x and dot partials must fit");
@@ -664,22 +684,22 @@ __device__ __noinline__ void front_lsolve_sm(const FT* M, int nf, int nres, int 
 #pragma unroll
             for (int c = 0; c < 32; ++c) v[c] = Mi[(int64_t)c * nf];
         }
-        for (int idx = tid; idx < 32 * 32; idx += NT) {
-            int r = idx & 31, c = idx >> 5;
-            if (r < kb && c < kb && r >= c) T[c * 33 + r] = (double)M[(k0 + r) + (int64_t)(k0 + c) * nf];
+        for (int idx = tid; idx < 32 * 32; idx += NT) {   // T[r*33 + c] = X[r][c], c < r (L⁻¹ of the block)
+            int c = idx & 31, r = idx >> 5;
+            if (r < kb && c < r) T[r * 33 + c] = (double)M[(k0 + c) + (int64_t)(k0 + r) * nf];
         }
         if (tid < kb) sh.dinv[tid] = 1.0 / (double)M[(k0 + tid) + (int64_t)(k0 + tid) * nf];
         __syncthreads();
-        if (warp == 0) {
-            double xv = lane < kb ? xf[k0 + lane] : 0.0;
-            for (int c = 0; c < kb; ++c) {
-                if (lane == c) xv = xv * sh.dinv[c];
-                double xc = __shfl_sync(0xffffffffu, xv, c);
-                if (lane > c && lane < kb) xv -= T[c * 33 + lane] * xc;
-            }
-            if (lane < kb) { xf[k0 + lane] = xv; sh.xs[lane] = xv; }
+        if (warp == 0 && lane < kb) {   // x = L⁻¹ b for the block, a lane per row
+            const int r = lane;
+            double s0 = 0, s1 = 0;
+            for (int c = 0; c + 1 < r; c += 2) { s0 = fma(T[r * 33 + c], xf[k0 + c], s0); s1 = fma(T[r * 33 + c + 1], xf[k0 + c + 1], s1); }
+            if (r & 1) s0 = fma(T[r * 33 + r - 1], xf[k0 + r - 1], s0);
+            const double xv = fma(sh.dinv[r], xf[k0 + r], s0 + s1);
+            sh.xs[r] = xv;
         }
         __syncthreads();
+        if (tid < kb) xf[k0 + tid] = sh.xs[tid];
         for (int i = i0; i < nf; i += NT) {
             const FT* Mi = M + i + (int64_t)k0 * nf;
             double t = 0;
@@ -750,25 +770,29 @@ __device__ __noinline__ void front_usolve_sm(const FT* M, int nf, int nres, int 
             }
             if (lane < 16) part[warp * 32 + h + lane] = acc[0];
         }
-        for (int idx = tid; idx < 32 * 32; idx += NT) {
-            int r = idx & 31, c = idx >> 5;
-            if (r < kb && c < kb && r >= c) T[c * 33 + r] = (double)M[(k0 + r) + (int64_t)(k0 + c) * nf];
+        for (int idx = tid; idx < 32 * 32; idx += NT) {   // T[r*33 + c] = X[r][c], c < r (L⁻¹ of the block)
+            int c = idx & 31, r = idx >> 5;
+            if (r < kb && c < r) T[r * 33 + c] = (double)M[(k0 + c) + (int64_t)(k0 + r) * nf];
         }
         if (tid < kb) sh.dinv[tid] = 1.0 / (double)M[(k0 + tid) + (int64_t)(k0 + tid) * nf];
         __syncthreads();
-        if (warp == 0) {
+        if (warp == 0) {   // x = L⁻ᵀ y for the block, a lane per row: x_c = Σ_{r ≥ c} X[r][c] y_r
             double dot = 0;
             if (lane < kb) {
 #pragma unroll
                 for (int w = 0; w < NW; ++w) dot += part[w * 32 + lane];
             }
-            double yv = lane < kb ? xf[k0 + lane] - dot : 0.0;
-            for (int c = kb - 1; c >= 0; --c) {
-                if (lane == c) yv = yv * sh.dinv[c];
-                double xc = __shfl_sync(0xffffffffu, yv, c);
-                if (lane < c) yv -= T[lane * 33 + c] * xc;
+            const double yv = lane < kb ? xf[k0 + lane] - dot : 0.0;
+            sh.xs[lane] = yv;
+            __syncwarp();
+            if (lane < kb) {
+                const int c = lane;
+                double s0 = 0, s1 = 0;
+                int r = c + 1;
+                for (; r + 1 < kb; r += 2) { s0 = fma(T[r * 33 + c], sh.xs[r], s0); s1 = fma(T[(r + 1) * 33 + c], sh.xs[r + 1], s1); }
+                if (r < kb) s0 = fma(T[r * 33 + c], sh.xs[r], s0);
+                xf[k0 + c] = fma(sh.dinv[c], yv, s0 + s1);
             }
-            if (lane < kb) xf[k0 + lane] = yv;
         }
         __syncthreads();
     }
@@ -927,32 +951,48 @@ struct Ctx {
     // Ruiz equilibration  (src/IPM/src/scaling/scaling.jl:52-184).  Q = blockdiag(Qd) + Qo.
     __device__ void equilibrate(int itmax, double tol) {
         const DevSp& B = I.B; const DevSp& Q = I.Q;
-        const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, gl = lane % G, sub = lane / G;
+        const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
         double* rnrm = tm1; double* rswp = tm2; double* cmax = tn;
         for (int v = tid; v < nv; v += NT) { vscl[v] = 1; vswp[v] = 1; }
         for (int i = tid; i < m; i += NT) { rswp[i] = 1; I.yscl[i] = 1; }
         __syncthreads();
-        for (int it = 0; it < itmax; ++it) {
-            // infnorms!: row maxima of B; column maxima of B, Qo and the Qd blocks
-            for (int i0 = warp * GPW; i0 < m; i0 += NW * GPW) {
-                const int i = i0 + sub;
-                double mx = 0;
-                if (i < m) for (int k = B.rptr[i] + gl; k < B.rptr[i + 1]; k += G) mx = fmax(mx, fabs(B.val[k]));
-                mx = group_reduce(mx, OpMax());
-                if (i < m && gl == 0) rnrm[i] = mx;
+        // column j's largest |entry| over B, Q's off-diagonal blocks and its Qd block column (skipped when the
+        // block is zero), over the entries l0, l0 + step, ...
+        auto colmax = [&](int j, int l0, int step) {
+            double mx = 0;
+            for (int k = B.cptr[j] + l0; k < B.cptr[j + 1]; k += step) mx = fmax(mx, fabs(B.val[B.cpos[k]]));
+            for (int k = Q.cptr[j] + l0; k < Q.cptr[j + 1]; k += step) mx = fmax(mx, fabs(Q.val[Q.cpos[k]]));
+            if (!(I.hflag[j] & 2)) {
+                const int v = I.colvtx[j], c0 = I.xcol[v], nc = I.xcol[v + 1] - c0;
+                const double* qd = I.Qd + I.hdoff[v] + (int64_t)(j - c0) * nc;
+                for (int r = l0; r < nc; r += step) mx = fmax(mx, fabs(qd[r]));
             }
-            for (int j0 = warp * GPW; j0 < n; j0 += NW * GPW) {
-                const int j = j0 + sub;
+            return mx;
+        };
+        auto longcol = [&](int j) { return B.cptr[j + 1] - B.cptr[j] > LONG_ROW || (I.hflag[j] & 1); };
+        for (int it = 0; it < itmax; ++it) {
+            // infnorms!: row maxima of B; column maxima of B, Qo and the Qd blocks.  A thread per short row or
+            // column, a warp per long one (maxima do not depend on the order)
+            for (int i = tid; i < m; i += NT) {
+                const int k0 = B.rptr[i], k1 = B.rptr[i + 1];
+                if (k1 - k0 > LONG_ROW) continue;
                 double mx = 0;
-                if (j < n) {
-                    for (int k = B.cptr[j] + gl; k < B.cptr[j + 1]; k += G) mx = fmax(mx, fabs(B.val[B.cpos[k]]));
-                    for (int k = Q.cptr[j] + gl; k < Q.cptr[j + 1]; k += G) mx = fmax(mx, fabs(Q.val[Q.cpos[k]]));
-                    int v = I.colvtx[j], c0 = I.xcol[v], nc = I.xcol[v + 1] - c0;
-                    const double* qd = I.Qd + I.hdoff[v] + (int64_t)(j - c0) * nc;
-                    for (int r = gl; r < nc; r += G) mx = fmax(mx, fabs(qd[r]));
-                }
-                mx = group_reduce(mx, OpMax());
-                if (j < n && gl == 0) cmax[j] = mx;
+                for (int k = k0; k < k1; ++k) mx = fmax(mx, fabs(B.val[k]));
+                rnrm[i] = mx;
+            }
+            for (int t = warp; t < B.nlongr; t += NW) {
+                const int i = B.longr[t];
+                double mx = 0;
+                for (int k = B.rptr[i] + lane; k < B.rptr[i + 1]; k += 32) mx = fmax(mx, fabs(B.val[k]));
+                mx = warp_max(mx);
+                if (lane == 0) rnrm[i] = mx;
+            }
+            for (int j = tid; j < n; j += NT) if (!longcol(j)) cmax[j] = colmax(j, 0, 1);
+            for (int t = warp; t < B.nlongc + I.nhlong; t += NW) {
+                const int j = t < B.nlongc ? B.longc[t] : I.hlong[t - B.nlongc];
+                if (t >= B.nlongc && B.cptr[j + 1] - B.cptr[j] > LONG_ROW) continue;   // listed twice: done above
+                const double mx = warp_max(colmax(j, lane, 32));
+                if (lane == 0) cmax[j] = mx;
             }
             __syncthreads();
             double dd = 0;
@@ -969,20 +1009,23 @@ struct Ctx {
                 if (nn != 0) { rswp[i] = 1.0 / nn; I.yscl[i] *= rswp[i]; }
             }
             dd = block_reduce(dd, red, OpMax(), 0.0);
-            // applyscaling!: B ← E B D, Q ← D Q D
-            for (int i0 = warp * GPW; i0 < m; i0 += NW * GPW) {
-                const int i = i0 + sub;
-                if (i < m) for (int k = B.rptr[i] + gl; k < B.rptr[i + 1]; k += G) B.val[k] *= rswp[i] * vswp[I.colvtx[B.cidx[k]]];
+            // applyscaling!: B ← E B D, Q ← D Q D (each entry once, in any order)
+            for (int i = tid; i < m; i += NT) {
+                const int k0 = B.rptr[i], k1 = B.rptr[i + 1];
+                if (k1 - k0 > LONG_ROW) continue;
+                for (int k = k0; k < k1; ++k) B.val[k] *= rswp[i] * vswp[I.colvtx[B.cidx[k]]];
             }
-            for (int i0 = warp * GPW; i0 < n; i0 += NW * GPW) {
-                const int i = i0 + sub;
-                if (i < n) {
-                    double su = vswp[I.colvtx[i]];
-                    for (int k = Q.rptr[i] + gl; k < Q.rptr[i + 1]; k += G) Q.val[k] *= su * vswp[I.colvtx[Q.cidx[k]]];
-                }
+            for (int t = warp; t < B.nlongr; t += NW) {
+                const int i = B.longr[t];
+                for (int k = B.rptr[i] + lane; k < B.rptr[i + 1]; k += 32) B.val[k] *= rswp[i] * vswp[I.colvtx[B.cidx[k]]];
+            }
+            for (int i = tid; i < n; i += NT) {
+                const double su = vswp[I.colvtx[i]];
+                for (int k = Q.rptr[i]; k < Q.rptr[i + 1]; ++k) Q.val[k] *= su * vswp[I.colvtx[Q.cidx[k]]];
             }
             for (int v = 0; v < nv; ++v) {
-                int nc = I.xcol[v + 1] - I.xcol[v];
+                const int c0 = I.xcol[v], nc = I.xcol[v + 1] - c0;
+                if (I.hflag[c0] & 2) continue;   // zero block
                 double sc = vswp[v] * vswp[v];
                 double* qd = I.Qd + I.hdoff[v];
                 for (int t = tid; t < nc * nc; t += NT) qd[t] *= sc;
@@ -1060,7 +1103,7 @@ struct Ctx {
         };
         // rows with at most LONG_ROW terms: a thread each (I.hflag marks the others)
         for (int i = threadIdx.x; i < n; i += NT) {
-            if (I.hflag[i]) continue;
+            if (I.hflag[i] & 1) continue;
             const int v = I.colvtx[i], c0 = I.xcol[v], nc = I.xcol[v + 1] - c0;
             double acc = 0;
             if (nsocz > 0 && vsocz[v] != 0.0) {   // zero Q block: H in structured form, Qd block skipped

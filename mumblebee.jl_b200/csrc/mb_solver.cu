@@ -86,29 +86,30 @@ __device__ __noinline__ int diag_factor(FT* M, int nf, int k0, int kb, Shared& s
             for (int c = 0; c < 32; ++c)
                 if (c <= lane) { S[lane * 33 + c] = v[c]; M[(k0 + lane) + (int64_t)(k0 + c) * nf] = v[c]; }
         }
-        if (!fail) {
-            // X = L⁻¹ for the triangular solves: lane c forms column c of X by forward substitution in axpy
-            // order (X[k][c] = −(Σ_{j<k} L[k][j] X[j][c]) / L[k][k], times the reciprocal pivot) and stores
-            // X[k][c], k > c, transposed into the block's upper triangle, M[k0 + c, k0 + k], which nothing
-            // else reads; X[c][c] = 1 / L[c][c] is not stored
-            __syncwarp();
-            const int c = lane;
-            FT acc[32];
-#pragma unroll
-            for (int i = 0; i < 32; ++i) acc[i] = FT(0);
-#pragma unroll
-            for (int k = 0; k < 32; ++k) {
-                if (k >= kb) continue;
-                const FT xk = k < c ? FT(0) : (k == c ? dinv[c] : -acc[k] * dinv[k]);
-                if (k > c && c < kb) M[(k0 + c) + (int64_t)(k0 + k) * nf] = xk;
-#pragma unroll
-                for (int i = k + 1; i < 32; ++i) acc[i] = fma(S[i * 33 + k], xk, acc[i]);
-            }
-        }
         if (lane == 0) sh.flag = fail ? k0 + fail : 0;
     }
     __syncthreads();
-    return sh.flag;
+    const int flag = sh.flag;
+    if (warp == 1 && !flag) {
+        // X = L⁻¹ for the triangular solves, on warp 1 while the others go on to the panel rows: lane c
+        // forms column c of X by forward substitution in axpy order (X[k][c] = −(Σ_{j<k} L[k][j] X[j][c])
+        // / L[k][k], times the reciprocal pivot) and stores X[k][c], k > c, transposed into the block's
+        // upper triangle, M[k0 + c, k0 + k], which nothing else reads; X[c][c] = 1 / L[c][c] is not stored.
+        // The next barrier (the end of the panel rows) orders it before sh.diag is overwritten.
+        const int c = lane;
+        FT acc[32];
+#pragma unroll
+        for (int i = 0; i < 32; ++i) acc[i] = FT(0);
+#pragma unroll
+        for (int k = 0; k < 32; ++k) {
+            if (k >= kb) continue;
+            const FT xk = k < c ? FT(0) : (k == c ? dinv[c] : -acc[k] * dinv[k]);
+            if (k > c && c < kb) M[(k0 + c) + (int64_t)(k0 + k) * nf] = xk;
+#pragma unroll
+            for (int i = k + 1; i < 32; ++i) acc[i] = fma(S[i * 33 + k], xk, acc[i]);
+        }
+    }
+    return flag;
 }
 
 // Panel solve L21 = A21 L11^{-T} for the rows [k0 + kb, nf) owned by this rank (row blocks of NT
@@ -842,18 +843,20 @@ __device__ int front_chol_ll(FT* M, int nf, int nres, Shared& sh, CoopCtl* coop,
         for (int h = 0; h < nb; h += 32) {
             const int k0 = J + h, kb = min(32, nb - h);
             if (h > 0 && !upd(k0, kb, J, J + 32)) return COOP_ABORTED;
-            long long t0 = tic();
+            // thread 0's clock without barriers around these two, so warp 1 can work on the diagonal
+            // block's inverse while the others start the panel rows
+            long long t0 = clock64();
             const int info = diag_factor<FT>(M, nf, k0, kb, sh);
-            toc(1, t0);
+            tf[1] += clock64() - t0;
             if (info) return info;
-            t0 = tic();
+            t0 = clock64();
             if (!big) panel_rows<FT>(M, nf, k0, kb, sh, 0, 1, false);
             else if (!coop_call(coop, sh, [&](CoopCtl* c) {
                          c->cmd = COOP_PANEL; c->pa[0] = M;
                          c->ia[0] = IsF32<FT>::v; c->ia[1] = nf; c->ia[2] = k0; c->ia[3] = kb;
                      }))
                 return COOP_ABORTED;
-            toc(2, t0);
+            tf[2] += clock64() - t0;
         }
     }
     const long long t0 = tic();

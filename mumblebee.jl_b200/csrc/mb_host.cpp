@@ -184,7 +184,7 @@ struct InstPlan {
     size_t Blongr, Blongc, hlong, hflag;
     size_t kind, fres0, fnres, fnsep, fparent, fsepp, fsep, frel;
     // i64
-    size_t hdoff, hdpos, qoffpos, cxblk, fptr;
+    size_t hdoff, hdpos, qoffpos, cxblk, fptr, qd0off;
     // double in
     size_t Bval, Qval, Qd, f, g, kpar, p, d, y;
     // work
@@ -323,13 +323,23 @@ static int plan_instance(const mb_problem* P, const mb_settings& set, const doub
         return nres + (i64)(it - fr.sep[f].begin());
     };
     // dense diagonal blocks of Q and their place in F; every non-free cone needs one (cone.jl:146-174)
-    std::vector<i64> hdoff(nv + 1, 0), hdpos(nv, 0), hdld(nv, 0);
+    // Only the nonzero blocks are stored (Qd, one after another; qd0off[v] = -1 for a zero or absent
+    // block): the device zero-fills the rest of its working copy, so an instance whose large cone
+    // blocks carry no Q uploads none of them.
+    std::vector<i64> hdoff(nv + 1, 0), hdpos(nv, 0), hdld(nv, 0), qd0off(nv, -1);
     for (i64 v = 0; v < nv; ++v) hdoff[v + 1] = hdoff[v] + B.ncols(v) * B.ncols(v);
-    std::vector<double> Qd(hdoff[nv], 0.0);
+    std::vector<double> Qd;
     for (i64 v = 0; v < nv; ++v) {
         bool found = false;
         for (i64 e = Q.xsrc[v]; e < Q.xsrc[v + 1]; ++e)
-            if (Q.tgt[e] == v) { std::copy(Q.val.begin() + Q.xblk[e], Q.val.begin() + Q.xblk[e + 1], Qd.begin() + hdoff[v]); found = true; }
+            if (Q.tgt[e] == v) {
+                found = true;
+                const auto b0 = Q.val.begin() + Q.xblk[e], b1 = Q.val.begin() + Q.xblk[e + 1];
+                if (std::any_of(b0, b1, [](double x) { return x != 0.0; })) {
+                    qd0off[v] = (i64)Qd.size();
+                    Qd.insert(Qd.end(), b0, b1);
+                }
+            }
         if (!found && P->kind[vp[v]] != MB_CONE_FREE) { err = "Q lacks the diagonal block of a cone vertex"; return MB_E_ARG; }
         i64 f = fr.vfront[v], nf = fr.nres[f] + (i64)fr.sep[f].size();
         hdpos[v] = fr.fptr[f] + (B.xcol[v] - fr.res0[f]) * (nf + 1);
@@ -360,8 +370,7 @@ static int plan_instance(const mb_problem* P, const mb_settings& set, const doub
     for (i64 v = 0; v < nv; ++v) {
         const i64 nc = B.ncols(v);
         const int kv = P->kind[vp[v]];
-        bool qzero = true;
-        for (i64 t = hdoff[v]; t < hdoff[v + 1] && qzero; ++t) qzero = Qd[t] == 0.0;
+        const bool qzero = qd0off[v] < 0;
         const bool structured = (kv == MB_CONE_SOC || kv == MB_CONE_SDP) && qzero;
         const i64 blk = structured ? 1 : nc;
         for (i64 i = B.xcol[v]; i < B.xcol[v + 1]; ++i) {
@@ -409,6 +418,7 @@ static int plan_instance(const mb_problem* P, const mb_settings& set, const doub
     ip.hlong = pk.i32.put(to32(hlong)); ip.hflag = pk.i32.put(to32(hflag));
     // i64 arena
     ip.hdoff = pk.i64a.put(hdoff); ip.hdpos = pk.i64a.put(hdpos); ip.qoffpos = pk.i64a.put(qoffpos);
+    ip.qd0off = pk.i64a.put(qd0off);
     ip.cxblk = pk.i64a.put(cx); ip.fptr = pk.i64a.put(fr.fptr);
     // values
     std::vector<double> f(n), g(P->g);
@@ -422,8 +432,8 @@ static int plan_instance(const mb_problem* P, const mb_settings& set, const doub
     ip.p = pk.din.put(pv); ip.d = pk.din.put(dv); ip.y = pk.din.put(yv);
     // workspace
     ip.fsize = fr.fsize;
-    ip.wBval = pk.work.take(Bval.size()); ip.wQval = pk.work.take(Qval.size()); ip.wQd = pk.work.take(Qd.size());
-    ip.Hd = pk.work.take(Qd.size()); ip.Finit = pk.work.take(fr.fsize);
+    ip.wBval = pk.work.take(Bval.size()); ip.wQval = pk.work.take(Qval.size()); ip.wQd = pk.work.take(hdoff[nv]);
+    ip.Hd = pk.work.take(hdoff[nv]); ip.Finit = pk.work.take(fr.fsize);
     ip.pscl = pk.work.take(n); ip.yscl = pk.work.take(m);
     ip.vn = pk.work.take((size_t)(mb::NVEC_N + 2) * n); ip.vm = pk.work.take((size_t)(mb::NVEC_M + 1) * m);
     ip.vv = pk.work.take((size_t)mb::NVEC_V * nv); ip.work = pk.work.take((size_t)(mb::CTA_THREADS / 32) * wmax);
@@ -455,7 +465,7 @@ static void merge(Packed& dst, Packed& src) {
                       &ip.Qrptr, &ip.Qcidx, &ip.Qcptr, &ip.Qridx, &ip.Qcpos, &ip.hdld, &ip.qoffk, &ip.kind,
                       &ip.fres0, &ip.fnres, &ip.fnsep, &ip.fparent, &ip.fsepp, &ip.fsep, &ip.frel,
                       &ip.Blongr, &ip.Blongc, &ip.hlong, &ip.hflag}) *f += b32;
-    for (size_t* f : {&ip.hdoff, &ip.hdpos, &ip.qoffpos, &ip.cxblk, &ip.fptr}) *f += b64;
+    for (size_t* f : {&ip.hdoff, &ip.hdpos, &ip.qoffpos, &ip.cxblk, &ip.fptr, &ip.qd0off}) *f += b64;
     for (size_t* f : {&ip.Bval, &ip.Qval, &ip.Qd, &ip.f, &ip.g, &ip.kpar, &ip.p, &ip.d, &ip.y}) *f += bin;
     for (size_t* f : {&ip.wBval, &ip.wQval, &ip.wQd, &ip.Hd, &ip.Finit, &ip.pscl, &ip.yscl, &ip.vn, &ip.vm, &ip.vv,
                       &ip.work, &ip.uhist, &ip.cghist, &ip.cache, &ip.cache2, &ip.wf, &ip.wg, &ip.wp, &ip.wd, &ip.wy}) *f += bw;
@@ -594,7 +604,7 @@ static void merge_all(Packed& dst, std::vector<Packed>& src, int nth) {
                               &ip.Qrptr, &ip.Qcidx, &ip.Qcptr, &ip.Qridx, &ip.Qcpos, &ip.hdld, &ip.qoffk, &ip.kind,
                               &ip.fres0, &ip.fnres, &ip.fnsep, &ip.fparent, &ip.fsepp, &ip.fsep, &ip.frel,
                       &ip.Blongr, &ip.Blongc, &ip.hlong, &ip.hflag}) *f += b32[k];
-            for (size_t* f : {&ip.hdoff, &ip.hdpos, &ip.qoffpos, &ip.cxblk, &ip.fptr}) *f += b64[k];
+            for (size_t* f : {&ip.hdoff, &ip.hdpos, &ip.qoffpos, &ip.cxblk, &ip.fptr, &ip.qd0off}) *f += b64[k];
             for (size_t* f : {&ip.Bval, &ip.Qval, &ip.Qd, &ip.f, &ip.g, &ip.kpar, &ip.p, &ip.d, &ip.y}) *f += bin[k];
             for (size_t* f : {&ip.wBval, &ip.wQval, &ip.wQd, &ip.Hd, &ip.Finit, &ip.pscl, &ip.yscl, &ip.vn, &ip.vm, &ip.vv,
                               &ip.work, &ip.uhist, &ip.cghist, &ip.cache, &ip.cache2, &ip.wf, &ip.wg, &ip.wp, &ip.wd, &ip.wy}) *f += bw[k];
@@ -1207,6 +1217,7 @@ mb::DevInst static_devinst(const InstPlan& p, int32_t* i32, i64* q64, double* dn
     I.Q.nlongr = 0; I.Q.longr = nullptr; I.Q.nlongc = 0; I.Q.longc = nullptr;   // Q's rows go through hlong
     I.nhlong = (int)p.nhlong; I.hlong = i32 + p.hlong; I.hflag = i32 + p.hflag;
     I.hdoff = (const int64_t*)(q64 + p.hdoff); I.Qd = wk + p.wQd; I.Qd0 = dn + p.Qd; I.Hd = wk + p.Hd;
+    I.qd0off = (const int64_t*)(q64 + p.qd0off);
     I.hdpos = (const int64_t*)(q64 + p.hdpos); I.hdld = i32 + p.hdld;
     I.nqoff = (int)p.nqoff; I.qoffk = i32 + p.qoffk; I.qoffpos = (const int64_t*)(q64 + p.qoffpos);
     I.kind = i32 + p.kind; I.kpar = dn + p.kpar; I.cxblk = (const int64_t*)(q64 + p.cxblk); I.cache = wk + p.cache;

@@ -71,6 +71,7 @@ struct DevInst {
     // dense diagonal blocks (nc x nc per vertex, column-major): Q's (working + pristine) and H's
     const int64_t* hdoff;   // nvtx+1
     double* Qd; const double* Qd0; double* Hd;
+    const int64_t* qd0off;  // nvtx: offset of a vertex's pristine block in Qd0, -1 when it is zero (not stored)
     const int64_t* hdpos;   // per vertex: offset in F of its diagonal block's (0,0) entry
     const int* hdld;        // per vertex: leading dimension of its front
     // Q nonzeros outside the diagonal blocks, lower triangle: CSR position and F offset

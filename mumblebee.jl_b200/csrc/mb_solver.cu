@@ -1136,20 +1136,16 @@ struct Ctx {
         __syncthreads();
     }
 
-    // vsocz / nsocz: SOC and SDP vertices whose diagonal block of Q is zero (after equilibration)
+    // vsocz / nsocz: SOC and SDP vertices whose diagonal block of Q is zero (not stored: qd0off < 0)
     __device__ void mark_socz() {
         int cnt = 0;
-        for (int v = threadIdx.x; v < nv; v += NT) vsocz[v] = 0;
-        __syncthreads();
-        for (int v = 0; v < nv; ++v) {
-            if (I.kind[v] != CONE_SOC && I.kind[v] != CONE_SDP) continue;
-            const int nc = I.xcol[v + 1] - I.xcol[v];
-            const double* q = I.Qd + I.hdoff[v];
-            double nz = 0;
-            for (int64_t t = threadIdx.x; t < (int64_t)nc * nc; t += NT) nz = fmax(nz, fabs(q[t]));
-            nz = block_reduce(nz, red, OpMax(), 0.0);
-            if (nz == 0.0) { cnt++; if (threadIdx.x == 0) vsocz[v] = I.kind[v] == CONE_SOC ? 1 : 2; }
+        for (int v = threadIdx.x; v < nv; v += NT) {
+            const int k = I.kind[v];
+            const bool st = (k == CONE_SOC || k == CONE_SDP) && I.qd0off[v] < 0;
+            vsocz[v] = st ? (k == CONE_SOC ? 1 : 2) : 0;
+            cnt += st;
         }
+        cnt = (int)block_reduce((double)cnt, red, OpSum(), 0.0);
         nsocz = cnt;
         if (threadIdx.x == 0) I.scal[SCAL_NSOCZ] = (double)cnt;
         __syncthreads();
@@ -1942,7 +1938,10 @@ __device__ void solve_instance(const DevInst& I, const Settings& set, Shared& sh
         // working copies of the inputs: a solve never modifies the uploaded problem
         for (int i = threadIdx.x; i < I.B.nnz; i += NT) I.B.val[i] = I.B.val0[i];
         for (int i = threadIdx.x; i < I.Q.nnz; i += NT) I.Q.val[i] = I.Q.val0[i];
-        for (int64_t i = threadIdx.x; i < I.hdoff[I.nvtx]; i += NT) I.Qd[i] = I.Qd0[i];
+        for (int v = threadIdx.x >> 5; v < I.nvtx; v += NW) {   // Qd ← the stored blocks, zero for the others
+            const int64_t o = I.qd0off[v], h0 = I.hdoff[v], nb = I.hdoff[v + 1] - h0;
+            for (int64_t t = threadIdx.x & 31; t < nb; t += 32) I.Qd[h0 + t] = o < 0 ? 0.0 : I.Qd0[o + t];
+        }
         for (int i = threadIdx.x; i < n; i += NT) { I.f[i] = I.f0[i]; I.p[i] = I.p0[i]; I.d[i] = I.d0[i]; }
         for (int i = threadIdx.x; i < m; i += NT) { I.g[i] = I.g0[i]; I.y[i] = I.y0[i]; }
         __syncthreads();

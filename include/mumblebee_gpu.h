@@ -171,9 +171,12 @@ int mb_solver_result(mb_solver* s, double* p, double* d, double* y, mb_result* r
 int mb_solver_history(mb_solver* s, mb_history_row* rows, int32_t cap, int32_t* nrows);
 int mb_solver_destroy(mb_solver* s);
 
-/* batched solve: every problem solved in one persistent launch (one CTA per instance at a time).
- * Outputs per problem i: p_out[i] (n_i), d_out[i] (n_i), y_out[i] (m_i), results[i]; any output
- * pointer may be NULL to skip it.  `grid` = CTAs of the persistent launch (0 = one per SM). */
+/* batched solve: every problem solved by a persistent launch (one CTA per instance at a time).
+ * With grid = 0 and 1024 or more problems the call is split into two or four chunks (problems
+ * dealt round-robin), each planned, uploaded and launched on its own stream, so host planning
+ * overlaps device work; each instance is solved exactly as alone.  Outputs per problem i:
+ * p_out[i] (n_i), d_out[i] (n_i), y_out[i] (m_i), results[i]; any output pointer may be NULL to
+ * skip it.  `grid` = CTAs of the persistent launch (0 = two per SM). */
 int mb_batch_solve(mb_ctx* ctx, mb_problem* const* probs, int32_t nprob, const mb_settings* settings,
                    int32_t grid, double* const* p_out, double* const* d_out, double* const* y_out,
                    mb_result* results);

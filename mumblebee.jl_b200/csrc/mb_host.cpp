@@ -15,6 +15,7 @@
 #include <cstdlib>
 #include <mutex>
 #include <unordered_map>
+#include <map>
 #include <memory>
 #include <string>
 #include <thread>
@@ -32,12 +33,62 @@ extern "C" int mb_coop_grid(int device, int nsm);
 
 using mbh::i64;
 
+// Device and pinned-host blocks freed by a batch are kept on the context and handed to the next
+// batch that fits (a block at most twice the request), so repeated batch solves pay neither
+// cudaMalloc nor the device-wide synchronisation of cudaFree.  A block returns to the cache only
+// after its batch's results were read back; a failed cudaMalloc empties the cache and retries.
+struct BlockCache {
+    std::mutex mu;
+    std::multimap<size_t, void*> freeb;          // size -> block
+    std::unordered_map<void*, size_t> size;      // every block this cache handed out or holds
+    size_t held = 0;
+    static constexpr size_t LIMIT = (size_t)64 << 30;
+};
+
 struct mb_ctx {
     int device = 0;
     int nsm = 148;
     cudaStream_t stream = nullptr;
     std::string err;
+    BlockCache dev, host;
 };
+
+static cudaError_t cache_alloc(mb_ctx* ctx, BlockCache& c, bool dev, void** p, size_t bytes) {
+    bytes = std::max<size_t>(bytes, 256);
+    {
+        std::lock_guard<std::mutex> g(c.mu);
+        auto it = c.freeb.lower_bound(bytes);
+        if (it != c.freeb.end() && it->first <= 2 * bytes) {
+            *p = it->second; c.held -= it->first; c.freeb.erase(it);
+            return cudaSuccess;
+        }
+    }
+    cudaError_t e = dev ? cudaMalloc(p, bytes) : cudaMallocHost(p, bytes);
+    if (e != cudaSuccess) {   // give the cached blocks back to the driver and retry once
+        cudaGetLastError();
+        std::lock_guard<std::mutex> g(c.mu);
+        for (auto& kv : c.freeb) { if (dev) cudaFree(kv.second); else cudaFreeHost(kv.second); c.size.erase(kv.second); }
+        c.freeb.clear(); c.held = 0;
+        e = dev ? cudaMalloc(p, bytes) : cudaMallocHost(p, bytes);
+    }
+    if (e == cudaSuccess) { std::lock_guard<std::mutex> g(c.mu); c.size[*p] = bytes; }
+    (void)ctx;
+    return e;
+}
+static void cache_free(BlockCache& c, bool dev, void* p) {
+    if (!p) return;
+    std::lock_guard<std::mutex> g(c.mu);
+    auto it = c.size.find(p);
+    if (it == c.size.end()) { if (dev) cudaFree(p); else cudaFreeHost(p); return; }
+    if (c.held + it->second <= BlockCache::LIMIT) { c.freeb.insert({it->second, p}); c.held += it->second; return; }
+    c.size.erase(it);
+    if (dev) cudaFree(p); else cudaFreeHost(p);
+}
+static void cache_clear(BlockCache& c, bool dev) {
+    std::lock_guard<std::mutex> g(c.mu);
+    for (auto& kv : c.freeb) { if (dev) cudaFree(kv.second); else cudaFreeHost(kv.second); }
+    c.freeb.clear(); c.size.clear(); c.held = 0;
+}
 
 struct mb_problem {
     mb_ctx* ctx = nullptr;
@@ -517,23 +568,34 @@ struct mb_batch {
     double* h_out = nullptr;    // pinned output staging
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     int64_t launches = 0;
+    cudaStream_t own = nullptr;   // the batch's own stream (chunks of a split mb_batch_solve), else ctx's
+    cudaStream_t stream() const { return own ? own : ctx->stream; }
     ~mb_batch() {
-        cudaFree(d_i32); cudaFree(d_i64); cudaFree(d_din); cudaFree(d_work); cudaFree(d_out); cudaFree(d_F);
-        cudaFree(d_inst); cudaFree(d_counter); cudaFree(d_ost); cudaFree(d_coop);
-        cudaFreeHost(h_i32); cudaFreeHost(h_out);
+        if (ctx) {
+            cudaStreamSynchronize(stream());   // nothing of this batch may still use a block it returns
+            for (void* p : {(void*)d_i32, (void*)d_i64, (void*)d_din, (void*)d_work, (void*)d_out, d_F, (void*)d_inst,
+                            (void*)d_counter, (void*)d_ost})
+                cache_free(ctx->dev, true, p);
+            cache_free(ctx->host, false, h_i32);
+            cache_free(ctx->host, false, h_out);
+        }
+        cudaFree(d_coop);
         if (e0) cudaEventDestroy(e0);
         if (e1) cudaEventDestroy(e1);
+        if (own) cudaStreamDestroy(own);
     }
 };
 
 static int upload(mb_batch* b) {
     mb_ctx* ctx = b->ctx;
     Packed& pk = b->pk;
-    cudaStream_t st = ctx->stream;
+    cudaStream_t st = b->stream();
+    auto dalloc = [&](void** p, size_t bytes) { return cache_alloc(ctx, ctx->dev, true, p, bytes); };
+    auto halloc = [&](void** p, size_t bytes) { return cache_alloc(ctx, ctx->host, false, p, bytes); };
     auto alloc_copy = [&](auto*& dptr, auto& arena) -> int {
         using T = typename std::remove_reference<decltype(arena.h)>::type::value_type;
         size_t bytes = std::max<size_t>(arena.size(), 1) * sizeof(T);
-        CUDA_TRY(ctx, cudaMalloc((void**)&dptr, bytes));
+        CUDA_TRY(ctx, dalloc((void**)&dptr, bytes));
         if (arena.host && arena.size()) CUDA_TRY(ctx, cudaMemcpyAsync(dptr, arena.h.data(), arena.size() * sizeof(T), cudaMemcpyHostToDevice, st));
         return MB_OK;
     };
@@ -541,19 +603,19 @@ static int upload(mb_batch* b) {
     if ((rc = alloc_copy(b->d_i32, pk.i32))) return rc;
     if ((rc = alloc_copy(b->d_i64, pk.i64a))) return rc;
     if ((rc = alloc_copy(b->d_din, pk.din))) return rc;
-    CUDA_TRY(ctx, cudaMalloc((void**)&b->d_work, std::max<size_t>(pk.work.size(), 1) * sizeof(double)));
-    CUDA_TRY(ctx, cudaMalloc((void**)&b->d_out, std::max<size_t>(pk.out.size(), 1) * sizeof(double)));
-    CUDA_TRY(ctx, cudaMalloc(&b->d_F, std::max<size_t>(pk.fbytes, 256)));
-    CUDA_TRY(ctx, cudaMalloc((void**)&b->d_counter, sizeof(int)));
-    CUDA_TRY(ctx, cudaMallocHost((void**)&b->h_out, std::max<size_t>(pk.out.size(), 1) * sizeof(double)));
-    CUDA_TRY(ctx, cudaMalloc((void**)&b->d_ost, std::max<size_t>(pk.ost.size(), 1) * sizeof(int32_t)));
+    CUDA_TRY(ctx, dalloc((void**)&b->d_work, std::max<size_t>(pk.work.size(), 1) * sizeof(double)));
+    CUDA_TRY(ctx, dalloc((void**)&b->d_out, std::max<size_t>(pk.out.size(), 1) * sizeof(double)));
+    CUDA_TRY(ctx, dalloc(&b->d_F, std::max<size_t>(pk.fbytes, 256)));
+    CUDA_TRY(ctx, dalloc((void**)&b->d_counter, sizeof(int)));
+    CUDA_TRY(ctx, halloc((void**)&b->h_out, std::max<size_t>(pk.out.size(), 1) * sizeof(double)));
+    CUDA_TRY(ctx, dalloc((void**)&b->d_ost, std::max<size_t>(pk.ost.size(), 1) * sizeof(int32_t)));
     CUDA_TRY(ctx, cudaMemsetAsync(b->d_ost, 0, std::max<size_t>(pk.ost.size(), 1) * sizeof(int32_t), st));
-    CUDA_TRY(ctx, cudaMallocHost((void**)&b->h_i32, std::max<size_t>(pk.ost.size(), 1) * sizeof(int32_t)));
+    CUDA_TRY(ctx, halloc((void**)&b->h_i32, std::max<size_t>(pk.ost.size(), 1) * sizeof(int32_t)));
     std::vector<mb::DevInst> hi(pk.plans.size());
     for (size_t k = 0; k < pk.plans.size(); ++k)
         hi[k] = static_devinst(pk.plans[k], b->d_i32, b->d_i64, b->d_din, b->d_work, b->d_out, b->d_ost, (char*)b->d_F);
     order_by_cost(hi, pk.plans);
-    CUDA_TRY(ctx, cudaMalloc((void**)&b->d_inst, hi.size() * sizeof(mb::DevInst)));
+    CUDA_TRY(ctx, dalloc((void**)&b->d_inst, hi.size() * sizeof(mb::DevInst)));
     CUDA_TRY(ctx, cudaMemcpyAsync(b->d_inst, hi.data(), hi.size() * sizeof(mb::DevInst), cudaMemcpyHostToDevice, st));
     CUDA_TRY(ctx, cudaEventCreate(&b->e0));
     CUDA_TRY(ctx, cudaEventCreate(&b->e1));
@@ -622,7 +684,7 @@ static void merge_all(Packed& dst, std::vector<Packed>& src, int nth) {
 }
 
 static int make_batch(mb_ctx* ctx, mb_problem* const* probs, int32_t nprob, const mb_settings* set,
-                      const double* p0, const double* d0, const double* y0, mb_batch** out) {
+                      const double* p0, const double* d0, const double* y0, mb_batch** out, bool own_stream = false) {
     if (!ctx || !out || nprob < 0 || (nprob > 0 && !probs)) return fail(ctx, MB_E_ARG, "bad arguments");
     mb_settings s;
     if (set) s = *set; else mb_settings_default(&s);
@@ -633,6 +695,7 @@ static int make_batch(mb_ctx* ctx, mb_problem* const* probs, int32_t nprob, cons
     b->ctx = ctx; b->set = s;
     const double t_start = host_time();
     CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+    if (own_stream) CUDA_TRY(ctx, cudaStreamCreateWithFlags(&b->own, cudaStreamNonBlocking));
     for (int32_t k = 0; k < nprob; ++k) if (!probs[k]) return fail(ctx, MB_E_ARG, "null problem");
     std::vector<Packed> local(nprob);
     std::vector<int> rcs(nprob, 0);
@@ -677,12 +740,14 @@ static int run_batch(mb_batch* b, int mode, int32_t grid, float* ms) {
     // a lone large instance runs on the whole GPU (grid-cooperative mode)
     const bool coop = ninst == 1 && (b->set.large == 1 || (b->set.large == 0 && b->pk.plans[0].fflops >= MB_LARGE_FLOPS));
     if (coop && !b->d_coop) CUDA_TRY(ctx, cudaMalloc((void**)&b->d_coop, sizeof(mb::CoopCtl)));
-    CUDA_TRY(ctx, cudaEventRecord(b->e0, ctx->stream));
-    int rc = coop ? mb_launch_coop(b->d_inst, mode, &s, b->d_coop, mb_coop_grid(ctx->device, ctx->nsm), ctx->stream)
-                  : mb_launch_batch(b->d_inst, ninst, mode, &s, b->d_counter, g, b->set.precision == MB_PREC_FP32, ctx->stream);
+    cudaStream_t st = b->stream();
+    CUDA_TRY(ctx, cudaEventRecord(b->e0, st));
+    int rc = coop ? mb_launch_coop(b->d_inst, mode, &s, b->d_coop, mb_coop_grid(ctx->device, ctx->nsm), st)
+                  : mb_launch_batch(b->d_inst, ninst, mode, &s, b->d_counter, g, b->set.precision == MB_PREC_FP32, st);
     if (rc) return fail(ctx, MB_E_CUDA, std::string("launch failed: ") + cudaGetErrorString(cudaGetLastError()));
     b->launches++;
-    CUDA_TRY(ctx, cudaEventRecord(b->e1, ctx->stream));
+    CUDA_TRY(ctx, cudaEventRecord(b->e1, st));
+    if (!ms && b->own) return MB_OK;   // a chunk of a split solve: the caller waits on the stream
     CUDA_TRY(ctx, cudaEventSynchronize(b->e1));
     if (ms) CUDA_TRY(ctx, cudaEventElapsedTime(ms, b->e0, b->e1));
     return MB_OK;
@@ -690,9 +755,10 @@ static int run_batch(mb_batch* b, int mode, int32_t grid, float* ms) {
 
 static int fetch_batch(mb_batch* b) {
     mb_ctx* ctx = b->ctx;
-    CUDA_TRY(ctx, cudaMemcpyAsync(b->h_out, b->d_out, std::max<size_t>(b->pk.out.size(), 1) * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
-    CUDA_TRY(ctx, cudaMemcpyAsync(b->h_i32, b->d_ost, std::max<size_t>(b->pk.ost.size(), 1) * sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream));
-    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    cudaStream_t st = b->stream();
+    CUDA_TRY(ctx, cudaMemcpyAsync(b->h_out, b->d_out, std::max<size_t>(b->pk.out.size(), 1) * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(ctx, cudaMemcpyAsync(b->h_i32, b->d_ost, std::max<size_t>(b->pk.ost.size(), 1) * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(ctx, cudaStreamSynchronize(st));
     return MB_OK;
 }
 
@@ -765,6 +831,9 @@ int mb_ctx_create(int32_t device, mb_ctx** out) {
 int mb_ctx_destroy(mb_ctx* ctx) {
     if (!ctx) return MB_E_ARG;
     cudaSetDevice(ctx->device);
+    cudaDeviceSynchronize();
+    cache_clear(ctx->dev, true);
+    cache_clear(ctx->host, false);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
     return MB_OK;
@@ -1153,15 +1222,50 @@ int mb_batch_destroy(mb_batch* b) {
     return MB_OK;
 }
 
+// A large call is split into up to four chunks (instances dealt round-robin, so each holds a like
+// mix), each planned, uploaded and launched on its own stream: the host plans chunk c + 1 while the
+// device runs chunk c, and the chunks' persistent grids fill each other's tails.  Every instance
+// is solved exactly as in a single launch.
 int mb_batch_solve(mb_ctx* ctx, mb_problem* const* probs, int32_t nprob, const mb_settings* settings, int32_t grid,
                    double* const* p_out, double* const* d_out, double* const* y_out, mb_result* results) {
-    mb_batch* b = nullptr;
-    int rc = make_batch(ctx, probs, nprob, settings, nullptr, nullptr, nullptr, &b);
-    if (rc) return rc;
-    std::unique_ptr<mb_batch> hold(b);
-    rc = run_batch(b, mb::MODE_SOLVE, grid, nullptr);
-    if (rc) return rc;
-    return mb_batch_fetch(b, p_out, d_out, y_out, results);
+    const int nch = nprob >= 2048 ? 4 : (nprob >= 1024 ? 2 : 1);
+    if (nch == 1 || grid > 0) {
+        mb_batch* b = nullptr;
+        int rc = make_batch(ctx, probs, nprob, settings, nullptr, nullptr, nullptr, &b);
+        if (rc) return rc;
+        std::unique_ptr<mb_batch> hold(b);
+        rc = run_batch(b, mb::MODE_SOLVE, grid, nullptr);
+        if (rc) return rc;
+        return mb_batch_fetch(b, p_out, d_out, y_out, results);
+    }
+    if (!probs) return fail(ctx, MB_E_ARG, "bad arguments");
+    std::vector<std::unique_ptr<mb_batch>> chunks(nch);
+    std::vector<std::vector<int32_t>> idx(nch);
+    for (int32_t k = 0; k < nprob; ++k) idx[k % nch].push_back(k);
+    for (int c = 0; c < nch; ++c) {
+        std::vector<mb_problem*> sub(idx[c].size());
+        for (size_t j = 0; j < sub.size(); ++j) sub[j] = probs[idx[c][j]];
+        mb_batch* b = nullptr;
+        int rc = make_batch(ctx, sub.data(), (int32_t)sub.size(), settings, nullptr, nullptr, nullptr, &b, true);
+        if (rc) return rc;
+        chunks[c].reset(b);
+        if ((rc = run_batch(b, mb::MODE_SOLVE, 0, nullptr))) return rc;   // returns after the launch
+    }
+    for (int c = 0; c < nch; ++c) {
+        const size_t nk = idx[c].size();
+        std::vector<double*> pp(nk, nullptr), dd(nk, nullptr), yy(nk, nullptr);
+        std::vector<mb_result> rr(results ? nk : 0);
+        for (size_t j = 0; j < nk; ++j) {
+            if (p_out) pp[j] = p_out[idx[c][j]];
+            if (d_out) dd[j] = d_out[idx[c][j]];
+            if (y_out) yy[j] = y_out[idx[c][j]];
+        }
+        int rc = mb_batch_fetch(chunks[c].get(), p_out ? pp.data() : nullptr, d_out ? dd.data() : nullptr,
+                                y_out ? yy.data() : nullptr, results ? rr.data() : nullptr);
+        if (rc) return rc;
+        if (results) for (size_t j = 0; j < nk; ++j) results[idx[c][j]] = rr[j];
+    }
+    return MB_OK;
 }
 
 }  // extern "C"
@@ -1346,6 +1450,7 @@ extern "C" int mb_batch_solve_static(mb_ctx* ctx, mb_problem* const* probs, int3
 #include <map>
 #include <mutex>
 #include <unordered_map>
+#include <map>
 
 extern "C" int mb_launch_wave(const mb::DevInst* d_inst, int ninst, const mb::Settings* set, int* d_counter, int grid,
                               unsigned long long* done, long long seq0, int cap, cudaStream_t stream);

@@ -484,10 +484,28 @@ class Batch:
             self.h = None
 
 
-def batch_solve(probs, settings: IPMSettings | None = None, grid: int = 0):
-    b = Batch(probs, settings)
-    b.run(grid)
-    return b.fetch()
+def batch_solve(probs, settings: IPMSettings | None = None, grid: int = 0, ctx: Context | None = None):
+    """solve over many problems (solver/ipm.jl:798-804) through mb_batch_solve: planning, upload,
+    one persistent launch per chunk, results.  With grid = 0 and 1024 or more problems the library
+    splits the call into chunks on their own streams, so host planning overlaps device work."""
+    probs = list(probs)
+    if not probs:
+        return []
+    ctx = ctx or probs[0].ctx
+    settings = settings or IPMSettings()
+    cs = settings.to_c()
+    k = len(probs)
+    sizes = [p.info() for p in probs]
+    ps = [np.zeros(s["n"]) for s in sizes]
+    ds = [np.zeros(s["n"]) for s in sizes]
+    ys = [np.zeros(s["m"]) for s in sizes]
+    mk = lambda lst: (C.POINTER(C.c_double) * k)(*[_p(a, C.c_double) for a in lst])
+    res = (mb_result * k)()
+    arr = (C.c_void_p * k)(*[p.h.value for p in probs])
+    check(ctx.L.mb_batch_solve(ctx.h, arr, k, C.byref(cs), grid, mk(ps), mk(ds), mk(ys), res), ctx.h, "batch solve")
+    return [IPMResult(ps[i], ds[i], ys[i], IPMStatus(res[i].status), res[i].niter, res[i].nsolve, IPMHistory(),
+                      res[i].mu, res[i].pres, res[i].dres, res[i].pobj, res[i].dobj, res[i].nfactor_retry,
+                      res[i].nfactor, res[i].factor_flops, res[i].nfp32, res[i].nfallback) for i in range(k)]
 
 
 def batch_solve_static(probs, settings: IPMSettings | None = None, grid: int = 0, ctx: Context | None = None):

@@ -172,3 +172,19 @@ def test_full_size_instances_match_oracle(name, pb):
     for k in ("p", "d", "y"):
         a, b = getattr(r, k), o[k]
         assert np.linalg.norm(a - b) <= 1e-5 * max(1.0, np.linalg.norm(b)), k
+
+
+def test_split_batch_solve_equals_alone():
+    """mb_batch_solve splits 1024 or more problems into chunks planned and launched on their own
+    streams; every result equals the problem solved alone, bitwise, in its own output slot."""
+    from helpers import product_problem
+    ctx = Context.default()
+    pbs = [G.portfolio(12 + (i % 7) * 3, seed=900 + i) for i in range(1100)]
+    probs = [product_problem(pb, ctx=ctx) for pb in pbs]
+    many = batch_solve(probs, IPMSettings())
+    assert all(r.status == IPMStatus.OPTIMAL for r in many)
+    for k in (0, 1, 2, 3, 549, 550, 1097, 1099):
+        a = solve(probs[k], IPMSettings())
+        assert a.status == many[k].status and a.niter == many[k].niter
+        np.testing.assert_array_equal(a.p, many[k].p)
+        np.testing.assert_array_equal(a.y, many[k].y)

@@ -372,7 +372,9 @@ def main():
         st = main_arm["stats"]
         e2e = {"value": args.count * ws / dt, "unit": "solves/s", "h2d_bytes_per_step": st["input_bytes"],
                "d2h_bytes_per_step": st["output_bytes"],
-               "note": "host symbolic analyses are cached by sparsity structure, warm after the warm-up call"}
+               "note": "mb_batch_solve splits 1024+ problems into chunks planned and launched on their own "
+                       "streams (planning overlaps device work); host symbolic analyses are cached by sparsity "
+                       "structure and device blocks by the context, warm after the warm-up call"}
     serve = None
     if not args.no_serve:
         serve = serve_arm(args, ctx)

@@ -16,6 +16,8 @@
  *   mb_solver_solve         solve!(solver)                                 src/IPM/src/ipm/solver/solver.jl:119-150
  *   mb_solver_result        result(solver, status) → IPMResult            src/IPM/src/ipm/solver/ipm.jl:30-74
  *   mb_solver_history       IPMHistory rows                                src/IPM/src/ipm/history/ipm.jl:1-71
+ *   mb_solver_reinit        reinit!(s; p0, d0, y0, f, g)                   src/IPM/src/ipm/solver/ipm.jl:371-429
+ *   mb_solver_timers        print_timers(s) (TimerOutput sections)         src/IPM/src/ipm/solver/ipm.jl:137-755
  *   mb_batch_solve          solve(prob, settings) over many problems      src/IPM/src/ipm/solver/ipm.jl:798-804
  *   mb_settings             IPMSettings                                    src/IPM/src/ipm/settings/ipm.jl:1-18
  */
@@ -169,6 +171,14 @@ int mb_solver_step(mb_solver* s, int32_t* status);
 int mb_solver_solve(mb_solver* s, int32_t* status);
 int mb_solver_result(mb_solver* s, double* p, double* d, double* y, mb_result* res);
 int mb_solver_history(mb_solver* s, mb_history_row* rows, int32_t cap, int32_t* nrows);
+/* reinit!(s; p0, d0, y0, f, g)  src/IPM/src/ipm/solver/ipm.jl:371-429: restart from the cone identity
+ * (or the given p0/d0/y0, completed by shadows) with an empty history, on a new f (n) and/or g (m)
+ * when given (user order); NULL keeps the current one.  The equilibration, Q, B and BᵀB stay. */
+int mb_solver_reinit(mb_solver* s, const double* p0, const double* d0, const double* y0, const double* f,
+                     const double* g);
+/* the solver's section timers (print_timers, the TimerOutput of IPMSolver): MB_NSECTIONS + 2 doubles,
+ * laid out as for mb_batch_timers */
+int mb_solver_timers(mb_solver* s, double* out, int64_t cap);
 int mb_solver_destroy(mb_solver* s);
 
 /* batched solve: every problem solved by a persistent launch (one CTA per instance at a time).

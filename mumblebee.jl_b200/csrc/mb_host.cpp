@@ -1143,6 +1143,47 @@ int mb_solver_result(mb_solver* s, double* p, double* d, double* y, mb_result* r
     return MB_OK;
 }
 
+// reinit!(s; p0, d0, y0, f, g) (solver/ipm.jl:371-429): the solver restarts from the cone identity
+// (or the given p0/d0/y0, completed by shadows) with an empty history, optionally on a new f and/or
+// g (user order, the problem's lengths); the equilibration, Q, B and BᵀB of init stay.
+int mb_solver_reinit(mb_solver* s, const double* p0, const double* d0, const double* y0, const double* f,
+                     const double* g) {
+    if (!s) return MB_E_ARG;
+    mb_batch* b = s->b.get();
+    mb_ctx* ctx = b->ctx;
+    InstPlan& ip = b->pk.plans[0];
+    const i64 n = ip.n, m = ip.m;
+    std::vector<double> v(std::max<i64>(std::max<i64>(n, m), 1));
+    auto put = [&](size_t off, const double* src, i64 len, const std::vector<i64>& map) -> int {
+        for (i64 i = 0; i < len; ++i) v[i] = src ? src[map[i]] : 0.0;
+        if (len) CUDA_TRY(ctx, cudaMemcpy(b->d_din + off, v.data(), len * sizeof(double), cudaMemcpyHostToDevice));
+        return MB_OK;
+    };
+    int rc;
+    if (f && (rc = put(ip.f, f, n, ip.colmap))) return rc;
+    if (g && (rc = put(ip.g, g, m, ip.rowmap))) return rc;
+    if ((rc = put(ip.p, p0, n, ip.colmap)) || (rc = put(ip.d, d0, n, ip.colmap)) || (rc = put(ip.y, y0, m, ip.rowmap)))
+        return rc;
+    ip.has_p0 = p0 != nullptr; ip.has_d0 = d0 != nullptr; ip.has_y0 = y0 != nullptr;
+    mb::DevInst I = static_devinst(ip, b->d_i32, b->d_i64, b->d_din, b->d_work, b->d_out, b->d_ost, (char*)b->d_F);
+    I.reinit_fg = (f ? 1 : 0) | (g ? 2 : 0);
+    CUDA_TRY(ctx, cudaMemcpy(b->d_inst, &I, sizeof(I), cudaMemcpyHostToDevice));
+    rc = run_batch(b, mb::MODE_REINIT, 1, nullptr);
+    if (rc) return rc;
+    s->done = false;
+    s->status = MB_CONTINUE;
+    return MB_OK;
+}
+
+// print_timers / the solver's TimerOutput: MB_NSECTIONS section clocks (SM cycles), then the numbers
+// of triangular-solve sweeps and matvecs, as mb_batch_timers reports them for one instance
+int mb_solver_timers(mb_solver* s, double* out, int64_t cap) {
+    if (!s || !out) return MB_E_ARG;
+    int rc = fetch_batch(s->b.get());
+    if (rc) return rc;
+    return mb_batch_timers(s->b.get(), out, cap);
+}
+
 int mb_solver_history(mb_solver* s, mb_history_row* rows, int32_t cap, int32_t* nrows) {
     if (!s) return MB_E_ARG;
     int rc = fetch_batch(s->b.get());

@@ -1929,7 +1929,7 @@ struct Ctx {
 template <bool COOP>
 __device__ void solve_instance(const DevInst& I, const Settings& set, Shared& sh, int mode, CoopCtl* coop) {
     const int n = I.n, m = I.m;
-    if (mode == MODE_SOLVE || mode == MODE_INIT) {
+    if (mode == MODE_SOLVE || mode == MODE_INIT || mode == MODE_REINIT) {
         if (threadIdx.x == 0) { for (int k = 0; k < NSTAT; ++k) I.status[k] = 0; }
         __syncthreads();
     }
@@ -1970,6 +1970,27 @@ __device__ void solve_instance(const DevInst& I, const Settings& set, Shared& sh
         c.ng = bnorm(I.g, m, c.red);
         c.sg = bscalenorm(I.g, I.yscl, m, c.red);
         c.sf = bscalenorm(I.f, I.pscl, n, c.red);
+    } else if (mode == MODE_REINIT) {
+        // reinit! (solver/ipm.jl:375-429): new f or g in the solver's scaling, a fresh start, an empty
+        // history; the equilibration, Q, B and BᵀB of the first init stay
+        if (I.reinit_fg & 1) {
+            for (int i = threadIdx.x; i < n; i += NT) I.f[i] = I.f0[i] * I.pscl[i];
+            __syncthreads();
+            c.nf = bnorm(I.f, n, c.red);
+            c.sf = bscalenorm(I.f, I.pscl, n, c.red);
+        }
+        if (I.reinit_fg & 2) {
+            for (int i = threadIdx.x; i < m; i += NT) I.g[i] = I.g0[i] * I.yscl[i];
+            __syncthreads();
+            c.ng = bnorm(I.g, m, c.red);
+            c.sg = bscalenorm(I.g, I.yscl, m, c.red);
+        }
+        for (int i = threadIdx.x; i < n; i += NT) { I.p[i] = I.p0[i]; I.d[i] = I.d0[i]; }
+        for (int i = threadIdx.x; i < m; i += NT) I.y[i] = I.y0[i];
+        c.stall0 = 0;
+        __syncthreads();
+    }
+    if (mode == MODE_SOLVE || mode == MODE_INIT || mode == MODE_REINIT) {
         if (!I.has_p0 && !I.has_d0) {
             c.startingpoint();
             if (I.has_y0) { for (int i = threadIdx.x; i < m; i += NT) I.y[i] /= I.yscl[i]; }

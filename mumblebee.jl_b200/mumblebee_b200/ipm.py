@@ -365,6 +365,36 @@ class IPMSolver:
         self.status = IPMStatus(st.value)
         return self.result()
 
+    def reinit(self, p0=None, d0=None, y0=None, f=None, g=None) -> "IPMSolver":
+        """reinit!(s; p0, d0, y0, f, g) (solver/ipm.jl:371-429): restart from the cone identity, or from
+        the given p0/d0/y0 completed by shadows, with an empty history, on a new f and/or g when
+        given (user order).  The equilibration, Q, B and BᵀB of init stay."""
+        a = [None if x is None else _f64(x) for x in (p0, d0, y0, f, g)]
+        check(self.L.mb_solver_reinit(self.h, *[_p(x, C.c_double) for x in a]), self.prob.ctx.h, "reinit!")
+        self.status = IPMStatus.CONTINUE
+        return self
+
+    SECTIONS = ["equilibrate", "BtB", "scale", "initkkt", "predictor", "corrector", "maxsteps", "trsv", "gemv",
+                "assemble", "residual", "getaug", "factor_update", "factor_diag", "factor_panel", "extend_add",
+                "ntrsv", "ngemv"]
+
+    def timers(self) -> dict:
+        """The solver's section clocks (SM cycles; TimerOutput sections of the reference plus set-up and
+        the factor's parts), and the counts of triangular-solve sweeps and matvecs."""
+        a = np.zeros(len(self.SECTIONS))
+        check(self.L.mb_solver_timers(self.h, _p(a, C.c_double), a.size), self.prob.ctx.h, "timers")
+        return dict(zip(self.SECTIONS, a.tolist()))
+
+    def print_timers(self, file=None):
+        """print_timers(s): one line per section, SM cycles and share of the iteration sections."""
+        t = self.timers()
+        top = ["equilibrate", "BtB", "scale", "initkkt", "predictor", "corrector", "maxsteps", "residual", "getaug"]
+        tot = sum(t[k] for k in top) or 1.0
+        for k in self.SECTIONS:
+            v = t[k]
+            share = f"{100 * v / tot:5.1f} %" if k not in ("ntrsv", "ngemv") else ""
+            print(f"{k:14s} {v:16.0f} {share}", file=file)
+
     def history(self) -> IPMHistory:
         cap = self.settings.max_iter + 1
         rows = (mb_history_row * cap)()
@@ -385,6 +415,16 @@ class IPMSolver:
         if getattr(self, "h", None):
             self.L.mb_solver_destroy(self.h)
             self.h = None
+
+
+def reinit(solver: IPMSolver, p0=None, d0=None, y0=None, f=None, g=None) -> IPMSolver:
+    """reinit!(solver; p0, d0, y0, f, g)"""
+    return solver.reinit(p0, d0, y0, f, g)
+
+
+def print_timers(solver: IPMSolver, file=None):
+    """print_timers(solver)"""
+    solver.print_timers(file)
 
 
 def init(prob: IPMProblem, settings: IPMSettings | None = None, p0=None, d0=None, y0=None) -> IPMSolver:

@@ -1309,6 +1309,33 @@ int oracle_set_threads(int nthreads) {
     return -1;
 }
 
+// the starting-point part of reinit! (solver/ipm.jl:390-427): from the cone identity scaled by
+// startingpoint!, or the given p0/d0 (user order) completed by shadows; y from y0 or zero; the cone
+// caches reset and the history emptied
+static void reinit_start(Solver& s, const double* p0, const double* d0, const double* y0) {
+    i64 n = s.n, m = s.m, nv = s.B.nvtx;
+    std::fill(s.y.begin(), s.y.end(), 0.0);
+    if (!p0 && !d0) {
+        startingpoint(s);
+        if (y0) for (i64 i = 0; i < m; ++i) s.y[i] = y0[s.P1[i]] / s.yscl[i];
+    } else {
+        if (p0) for (i64 i = 0; i < n; ++i) s.p[i] = p0[s.P2[i]];
+        if (d0) for (i64 i = 0; i < n; ++i) s.d[i] = d0[s.P2[i]];
+        for (i64 v = 0; v < nv; ++v) {
+            i64 c0 = s.B.xcol[v], nc = s.B.ncols(v);
+            double* cv = s.cache.data() + s.cxblk[v];
+            if (!d0) cone_shadow(s.K[v], s.Kp[v], nc, s.d.data() + c0, s.p.data() + c0, cv, s.cwork.data());
+            else if (!p0) cone_pshadow(s.K[v], s.Kp[v], nc, s.p.data() + c0, s.d.data() + c0, cv, s.cwork.data());
+        }
+        if (y0) for (i64 i = 0; i < m; ++i) s.y[i] = y0[s.P1[i]];
+        for (i64 i = 0; i < n; ++i) { s.p[i] /= s.pscl[i]; s.d[i] *= s.pscl[i]; }
+        for (i64 i = 0; i < m; ++i) s.y[i] /= s.yscl[i];
+    }
+    for (i64 v = 0; v < nv; ++v)
+        cone_initcache(s.K[v], s.Kp[v], s.B.ncols(v), s.cache.data() + s.cxblk[v]);
+    s.hist.clear();
+}
+
 // Build a solver: IPMSolver(prob, settings; p0, d0, y0) with the vertex elimination order
 // `vperm` (0-based, length nvtx; NULL = identity) standing in for CliqueTrees.symbolic.
 void* oracle_create(const ob_bsm* Qc, const ob_bsm* Bc, const double* f, const double* g, double mu,
@@ -1382,27 +1409,28 @@ void* oracle_create(const ob_bsm* Qc, const ob_bsm* Bc, const double* f, const d
     s->nf = vnorm(s->f.data(), n); s->ng = vnorm(s->g.data(), m);
     s->sg = scalenorm(s->g.data(), s->yscl.data(), m);
     s->sf = scalenorm(s->f.data(), s->pscl.data(), n);
-    // reinit! (solver/ipm.jl:375-429)
-    if (!p0 && !d0) {
-        startingpoint(*s);
-        if (y0) for (i64 i = 0; i < m; ++i) s->y[i] = y0[s->P1[i]] / s->yscl[i];
-    } else {
-        if (p0) for (i64 i = 0; i < n; ++i) s->p[i] = p0[s->P2[i]];
-        if (d0) for (i64 i = 0; i < n; ++i) s->d[i] = d0[s->P2[i]];
-        for (i64 v = 0; v < nv; ++v) {
-            i64 c0 = s->B.xcol[v], nc = s->B.ncols(v);
-            double* cv = s->cache.data() + s->cxblk[v];
-            if (!d0) cone_shadow(s->K[v], s->Kp[v], nc, s->d.data() + c0, s->p.data() + c0, cv, s->cwork.data());
-            else if (!p0) cone_pshadow(s->K[v], s->Kp[v], nc, s->p.data() + c0, s->d.data() + c0, cv, s->cwork.data());
-        }
-        if (y0) for (i64 i = 0; i < m; ++i) s->y[i] = y0[s->P1[i]];
-        for (i64 i = 0; i < n; ++i) { s->p[i] /= s->pscl[i]; s->d[i] *= s->pscl[i]; }
-        for (i64 i = 0; i < m; ++i) s->y[i] /= s->yscl[i];
-    }
-    for (i64 v = 0; v < nv; ++v)
-        cone_initcache(s->K[v], s->Kp[v], s->B.ncols(v), s->cache.data() + s->cxblk[v]);
-    s->hist.clear();
+    reinit_start(*s, p0, d0, y0);
     return s;
+}
+
+// reinit!(s; p0, d0, y0, f, g) (solver/ipm.jl:371-429): f and g (user order) replace the solver's
+// in its scaling; H, the equilibration and BᵀB stay as they are
+int oracle_reinit(void* h, const double* p0, const double* d0, const double* y0, const double* f, const double* g) {
+    Solver& s = *(Solver*)h;
+    const i64 n = s.n, m = s.m;
+    if (f) {
+        for (i64 i = 0; i < n; ++i) s.f[i] = f[s.P2[i]] * s.pscl[i];
+        s.nf = vnorm(s.f.data(), n);
+        s.sf = scalenorm(s.f.data(), s.pscl.data(), n);
+    }
+    if (g) {
+        for (i64 i = 0; i < m; ++i) s.g[i] = g[s.P1[i]] * s.yscl[i];
+        s.ng = vnorm(s.g.data(), m);
+        s.sg = scalenorm(s.g.data(), s.yscl.data(), m);
+    }
+    reinit_start(s, p0, d0, y0);
+    s.nfactor_retry = 0; s.nfallback = 0; s.switched = false; s.stall0 = 0; s.stallhit = false; s.nfp32 = 0;
+    return 0;
 }
 
 int oracle_step(void* h) { return step(*(Solver*)h); }

@@ -99,6 +99,7 @@ def lib(threads: int = 1):
                                     C.POINTER(C.c_int64), C.POINTER(C.c_int64), C.POINTER(Settings),
                                     C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double)]
         L.oracle_step.argtypes = [C.c_void_p]
+        L.oracle_reinit.argtypes = [C.c_void_p] + [C.POINTER(C.c_double)] * 5
         L.oracle_solve.argtypes = [C.c_void_p]
         L.oracle_result.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double),
                                     C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_int32),
@@ -160,6 +161,14 @@ class OracleSolver:
     def step(self) -> int:
         self.status = self.L.oracle_step(self.h)
         return self.status
+
+    def reinit(self, p0=None, d0=None, y0=None, f=None, g=None):
+        """reinit!(s; p0, d0, y0, f, g), every vector in user order."""
+        arr = [None if a is None else np.ascontiguousarray(a, dtype=np.float64) for a in (p0, d0, y0, f, g)]
+        self._keep_reinit = arr
+        self.L.oracle_reinit(self.h, *[_pd(a) for a in arr])
+        self.status = 0
+        return self
 
     def solve(self):
         self.status = self.L.oracle_solve(self.h)

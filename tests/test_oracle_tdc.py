@@ -127,3 +127,16 @@ def test_tuncel_scaling_and_certified_steps(L, trial):
     tp, td = out[15], out[16]
     assert abs(tp - _brute(kind, a, p, Dp, False)) <= 1e-9
     assert abs(td - _brute(kind, a, d, Dd, True)) <= 1e-9
+
+
+def test_oracle_reinit_reproduces_the_first_solve_before_a_step():
+    """reinit! on a solver that has not stepped (H is still Q) starts over exactly as init did."""
+    from helpers import SMALL, block_problem, oracle_solve
+    import oracle
+    ref = block_problem(SMALL["port_small"]())
+    _, r1 = oracle_solve(ref)
+    s = oracle.OracleSolver(ref, oracle.default_settings())
+    s.reinit()
+    r2 = s.solve()
+    assert r2["status"] == r1["status"] and r2["niter"] == r1["niter"]
+    assert np.array_equal(r2["p"], r1["p"])

@@ -18,6 +18,8 @@
  *   mb_solver_history       IPMHistory rows                                src/IPM/src/ipm/history/ipm.jl:1-71
  *   mb_solver_reinit        reinit!(s; p0, d0, y0, f, g)                   src/IPM/src/ipm/solver/ipm.jl:371-429
  *   mb_solver_timers        print_timers(s) (TimerOutput sections)         src/IPM/src/ipm/solver/ipm.jl:137-755
+ *   mb_solver_frule         frule!(Δp, Δy, Δd, s, Δf, Δg, Δμ)              src/IPM/src/ipm/differential.jl:5-79
+ *   mb_solver_rrule         rrule!(Δf, Δg, s, Δp, Δy, Δd)                  src/IPM/src/ipm/differential.jl:263-334
  *   mb_batch_solve          solve(prob, settings) over many problems      src/IPM/src/ipm/solver/ipm.jl:798-804
  *   mb_settings             IPMSettings                                    src/IPM/src/ipm/settings/ipm.jl:1-18
  */
@@ -176,6 +178,14 @@ int mb_solver_history(mb_solver* s, mb_history_row* rows, int32_t cap, int32_t* 
  * when given (user order); NULL keeps the current one.  The equilibration, Q, B and BᵀB stay. */
 int mb_solver_reinit(mb_solver* s, const double* p0, const double* d0, const double* y0, const double* f,
                      const double* g);
+/* frule!(Δp, Δy, Δd, s, Δf, Δg, Δμ)  src/IPM/src/ipm/differential.jl:5-79: tangents of the current
+ * iterate for seeds on f (n), g (m) and μ; user order, NULL seed = 0, NULL output = skipped.  The
+ * factorization at the current iterate is redone (FP64); MB_E_STATE when it fails. */
+int mb_solver_frule(mb_solver* s, const double* df, const double* dg, double dmu, double* dp, double* dy, double* dd);
+/* rrule!(Δf, Δg, s, Δp, Δy, Δd)  src/IPM/src/ipm/differential.jl:263-334: cotangents of f, g and μ
+ * for seeds on p (n), y (m), d (n); as mb_solver_frule */
+int mb_solver_rrule(mb_solver* s, const double* dp, const double* dy, const double* dd, double* df, double* dg,
+                    double* dmu);
 /* the solver's section timers (print_timers, the TimerOutput of IPMSolver): MB_NSECTIONS + 2 doubles,
  * laid out as for mb_batch_timers */
 int mb_solver_timers(mb_solver* s, double* out, int64_t cap);

@@ -794,6 +794,8 @@ struct mb_solver {
     std::unique_ptr<mb_batch> b;
     bool done = false;
     int32_t status = MB_CONTINUE;
+    double* d_sx = nullptr;   // sensitivity exchange (DevInst::sx), from the first frule / rrule
+    ~mb_solver() { if (d_sx && b && b->ctx) cache_free(b->ctx->dev, true, d_sx); }
 };
 
 extern "C" {
@@ -1167,12 +1169,61 @@ int mb_solver_reinit(mb_solver* s, const double* p0, const double* d0, const dou
     ip.has_p0 = p0 != nullptr; ip.has_d0 = d0 != nullptr; ip.has_y0 = y0 != nullptr;
     mb::DevInst I = static_devinst(ip, b->d_i32, b->d_i64, b->d_din, b->d_work, b->d_out, b->d_ost, (char*)b->d_F);
     I.reinit_fg = (f ? 1 : 0) | (g ? 2 : 0);
+    I.sx = s->d_sx;
     CUDA_TRY(ctx, cudaMemcpy(b->d_inst, &I, sizeof(I), cudaMemcpyHostToDevice));
     rc = run_batch(b, mb::MODE_REINIT, 1, nullptr);
     if (rc) return rc;
     s->done = false;
     s->status = MB_CONTINUE;
     return MB_OK;
+}
+
+// frule! / rrule! (ipm/differential.jl): seeds (user order, NULL = 0) into the exchange buffer in
+// solver order, one MODE_FRULE / MODE_RRULE launch, results back in user order
+static int sens_run(mb_solver* s, int mode, const double* a, const double* bv, const double* c, double dmu,
+                    double* oa, double* ob, double* oc, double* dmu_out) {
+    mb_batch* b = s->b.get();
+    mb_ctx* ctx = b->ctx;
+    InstPlan& ip = b->pk.plans[0];
+    const i64 n = ip.n, m = ip.m;
+    const size_t len = (size_t)(4 * n + 2 * m + 3);
+    if (!s->d_sx) {
+        CUDA_TRY(ctx, cache_alloc(ctx, ctx->dev, true, (void**)&s->d_sx, len * sizeof(double)));
+        mb::DevInst I = static_devinst(ip, b->d_i32, b->d_i64, b->d_din, b->d_work, b->d_out, b->d_ost, (char*)b->d_F);
+        I.sx = s->d_sx;
+        CUDA_TRY(ctx, cudaMemcpy(b->d_inst, &I, sizeof(I), cudaMemcpyHostToDevice));
+    }
+    std::vector<double> h(len, 0.0);
+    for (i64 i = 0; i < n; ++i) {
+        if (a) h[i] = a[ip.colmap[i]];
+        if (c) h[n + m + i] = c[ip.colmap[i]];
+    }
+    if (bv) for (i64 i = 0; i < m; ++i) h[n + i] = bv[ip.rowmap[i]];
+    h[4 * n + 2 * m] = dmu;
+    CUDA_TRY(ctx, cudaMemcpy(s->d_sx, h.data(), len * sizeof(double), cudaMemcpyHostToDevice));
+    int rc = run_batch(b, mode, 1, nullptr);
+    if (rc) return rc;
+    CUDA_TRY(ctx, cudaMemcpy(h.data(), s->d_sx, len * sizeof(double), cudaMemcpyDeviceToHost));
+    if (h[4 * n + 2 * m + 2] != 1.0) return fail(ctx, MB_E_STATE, "the KKT factorization at the current iterate failed");
+    const double* r = h.data() + 2 * n + m;
+    for (i64 i = 0; i < n; ++i) {
+        if (oa) oa[ip.colmap[i]] = r[i];
+        if (oc) oc[ip.colmap[i]] = r[n + m + i];
+    }
+    if (ob) for (i64 i = 0; i < m; ++i) ob[ip.rowmap[i]] = r[n + i];
+    if (dmu_out) *dmu_out = h[4 * n + 2 * m + 1];
+    return MB_OK;
+}
+
+int mb_solver_frule(mb_solver* s, const double* df, const double* dg, double dmu, double* dp, double* dy, double* dd) {
+    if (!s) return MB_E_ARG;
+    return sens_run(s, mb::MODE_FRULE, df, dg, nullptr, dmu, dp, dy, dd, nullptr);
+}
+
+int mb_solver_rrule(mb_solver* s, const double* dp, const double* dy, const double* dd, double* df, double* dg,
+                    double* dmu) {
+    if (!s) return MB_E_ARG;
+    return sens_run(s, mb::MODE_RRULE, dp, dy, dd, 0.0, df, dg, nullptr, dmu);
 }
 
 // print_timers / the solver's TimerOutput: MB_NSECTIONS section clocks (SM cycles), then the numbers

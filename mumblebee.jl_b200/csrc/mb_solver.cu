@@ -1136,6 +1136,71 @@ struct Ctx {
         __syncthreads();
     }
 
+    // d*(p) for every cone, dst ≠ src (dualshadow!, cone.jl:562-608)
+    __device__ void dualshadow_all(double* dst, const double* src) {
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+        for (int v = warp; v < nv; v += NW) {
+            const int k = I.kind[v], c0 = I.xcol[v], nc = I.xcol[v + 1] - c0;
+            if (k == CONE_POS) { for (int i = lane; i < nc; i += 32) dst[c0 + i] = 1.0 / src[c0 + i]; }
+            else if (k == CONE_SOC) w_socshadow(dst + c0, src + c0, nc);
+            else if (k == CONE_EXP || k == CONE_POW) {
+                if (lane == 0) tddualshadow(TD{k, I.kpar[v]}, dst + c0, src + c0, I.cache + I.cxblk[v]);
+                __syncwarp();
+            } else if (k != CONE_SDP) { for (int i = lane; i < nc; i += 32) dst[c0 + i] = 0; }
+        }
+        __syncthreads();
+        for (int v = 0; v < nv; ++v) {
+            if (I.kind[v] != CONE_SDP) continue;
+            const int c0 = I.xcol[v], nc = I.xcol[v + 1] - c0;
+            b_sdpshadow(dst + c0, src + c0, nc, I.work, SdpSh{red, &sh.flag});
+        }
+        __syncthreads();
+    }
+
+    // frule! / rrule! (ipm/differential.jl:5-79, 263-334) at the current iterate: δ = getaug, an FP64
+    // factorization, one KKT solve (cold, at least one refinement pass), the rest H/Q products and the
+    // dual shadow.  Seeds and results in I.sx (solver order, unscaled); sx[4n+2m+2] = 1 on success.
+    __device__ void sensitivity(bool reverse) {
+        double* sa = I.sx; double* sb = sa + n; double* sc = sb + m;
+        double* oa = sc + n; double* ob = oa + n; double* oc = ob + m; double* ss = oc + n;
+        use32 = false;
+        const double dl = getaug();
+        double rho;
+        if (!initkkt(dl, rho)) { if (threadIdx.x == 0) ss[2] = 0; __syncthreads(); return; }
+        const double mu0 = nrow_hist > 0 ? hrow(0).mu : 0.0;
+        const double tol = mu0 == 0 ? 0.1 * set.gap_tol : 0.1 * hrow(nrow_hist - 1).mu / mu0;
+        const double ftol = tol * (1 + nf), gtol = tol * (1 + ng);
+        if (!reverse) {
+            const double dmu = ss[0];
+            for (int i = threadIdx.x; i < n; i += NT) wf[i] = sa[i] * I.pscl[i];
+            for (int i = threadIdx.x; i < m; i += NT) Dg[i] = sb[i] * I.yscl[i];
+            __syncthreads();
+            dualshadow_all(Dd, I.p);
+            for (int i = threadIdx.x; i < n; i += NT) { Dd[i] *= dmu; wf[i] += Dd[i]; }
+            __syncthreads();
+            solvekkt(0, Dp, Dy, I.Hd, wf, Dg, false, ftol, gtol, 1);
+            amul(I.Hd, Dp, Dd, -1, 1);                 // Δd = Δμ d* − (H − Q) Δp
+            amul(I.Qd, Dp, Dd, 1, 1);
+            for (int i = threadIdx.x; i < n; i += NT) { oa[i] = Dp[i] * I.pscl[i]; oc[i] = Dd[i] / I.pscl[i]; }
+            for (int i = threadIdx.x; i < m; i += NT) ob[i] = Dy[i] * I.yscl[i];
+        } else {
+            for (int i = threadIdx.x; i < n; i += NT) { wf[i] = sa[i] * I.pscl[i]; Dd[i] = sc[i] / I.pscl[i]; }
+            for (int i = threadIdx.x; i < m; i += NT) Dg[i] = sb[i] * -I.yscl[i];
+            __syncthreads();
+            amul(I.Hd, Dd, wf, -1, 1);                 // Δp −= (H − Q) Δd
+            amul(I.Qd, Dd, wf, 1, 1);
+            solvekkt(0, Dp, Dy, I.Hd, wf, Dg, false, ftol, gtol, 1);
+            for (int i = threadIdx.x; i < n; i += NT) { Dd[i] += Dp[i]; oa[i] = Dp[i] * I.pscl[i]; }
+            for (int i = threadIdx.x; i < m; i += NT) ob[i] = -Dy[i] * I.yscl[i];
+            __syncthreads();
+            dualshadow_all(wf, I.p);
+            const double dm = bdot(Dd, wf, n, red);
+            if (threadIdx.x == 0) ss[1] = dm;
+        }
+        if (threadIdx.x == 0) ss[2] = 1;
+        __syncthreads();
+    }
+
     // vsocz / nsocz: SOC and SDP vertices whose diagonal block of Q is zero (not stored: qd0off < 0)
     __device__ void mark_socz() {
         int cnt = 0;
@@ -2049,6 +2114,8 @@ __device__ void solve_instance(const DevInst& I, const Settings& set, Shared& sh
         __syncthreads();
     } else if (mode == MODE_RESULT) {
         c.result(I.status[0]);
+    } else if (mode == MODE_FRULE || mode == MODE_RRULE) {
+        c.sensitivity(mode == MODE_RRULE);
     }
 }
 

@@ -374,6 +374,26 @@ class IPMSolver:
         self.status = IPMStatus.CONTINUE
         return self
 
+    def frule(self, df=None, dg=None, dmu=0.0):
+        """frule!(Δp, Δy, Δd, s, Δf, Δg, Δμ) (ipm/differential.jl:5-79): the tangents (Δp, Δy, Δd) of the
+        current iterate for seeds Δf (n), Δg (m), Δμ; user order, None = 0."""
+        i = self.prob.info()
+        dp, dd, dy = np.zeros(i["n"]), np.zeros(i["n"]), np.zeros(i["m"])
+        a = [None if x is None else _f64(x) for x in (df, dg)]
+        check(self.L.mb_solver_frule(self.h, _p(a[0], C.c_double), _p(a[1], C.c_double), float(dmu),
+                                     _p(dp, C.c_double), _p(dy, C.c_double), _p(dd, C.c_double)), self.prob.ctx.h, "frule!")
+        return dp, dy, dd
+
+    def rrule(self, dp=None, dy=None, dd=None):
+        """rrule!(Δf, Δg, s, Δp, Δy, Δd) (ipm/differential.jl:263-334): the cotangents (Δf, Δg, Δμ) for
+        seeds Δp (n), Δy (m), Δd (n); user order, None = 0."""
+        i = self.prob.info()
+        df, dg, dmu = np.zeros(i["n"]), np.zeros(i["m"]), C.c_double()
+        a = [None if x is None else _f64(x) for x in (dp, dy, dd)]
+        check(self.L.mb_solver_rrule(self.h, *[_p(x, C.c_double) for x in a], _p(df, C.c_double),
+                                     _p(dg, C.c_double), C.byref(dmu)), self.prob.ctx.h, "rrule!")
+        return df, dg, dmu.value
+
     SECTIONS = ["equilibrate", "BtB", "scale", "initkkt", "predictor", "corrector", "maxsteps", "trsv", "gemv",
                 "assemble", "residual", "getaug", "factor_update", "factor_diag", "factor_panel", "extend_add",
                 "ntrsv", "ngemv"]
@@ -415,6 +435,16 @@ class IPMSolver:
         if getattr(self, "h", None):
             self.L.mb_solver_destroy(self.h)
             self.h = None
+
+
+def frule(solver: IPMSolver, df=None, dg=None, dmu=0.0):
+    """frule!(Δp, Δy, Δd, solver, Δf, Δg, Δμ) → (Δp, Δy, Δd)"""
+    return solver.frule(df, dg, dmu)
+
+
+def rrule(solver: IPMSolver, dp=None, dy=None, dd=None):
+    """rrule!(Δf, Δg, solver, Δp, Δy, Δd) → (Δf, Δg, Δμ)"""
+    return solver.rrule(dp, dy, dd)
 
 
 def reinit(solver: IPMSolver, p0=None, d0=None, y0=None, f=None, g=None) -> IPMSolver:

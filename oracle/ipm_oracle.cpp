@@ -1433,6 +1433,71 @@ int oracle_reinit(void* h, const double* p0, const double* d0, const double* y0,
     return 0;
 }
 
+// ---- sensitivities (ipm/differential.jl) ---------------------------------------------------
+// d*(p): the dual shadow of every cone at p (dualshadow!, cone.jl:562-608)
+static void dualshadow_all(Solver& s, double* ds) {
+    for (i64 v = 0; v < s.B.nvtx; ++v) {
+        i64 c0 = s.B.xcol[v], nc = s.B.ncols(v);
+        cone_shadow(s.K[v], s.Kp[v], nc, ds + c0, s.p.data() + c0, s.cache.data() + s.cxblk[v], s.cwork.data());
+    }
+}
+
+// the factorization and tolerances every rule starts from (differential.jl:5-14): δ = getaug(s),
+// initkkt!(s, δ), tol from the history's first and last μ
+static bool sens_setup(Solver& s, double& ftol, double& gtol) {
+    double rho;
+    if (!initkkt(s, getaug(s), rho)) return false;
+    const double mu0 = s.hist.empty() ? 0.0 : s.hist.front().mu;
+    const double tol = mu0 == 0 ? FORCING_FRAC * s.set.gap_tol : FORCING_FRAC * s.hist.back().mu / mu0;
+    ftol = tol * (1 + s.nf); gtol = tol * (1 + s.ng);
+    return true;
+}
+
+// frule!(Δp, Δy, Δd, s, Δf, Δg, Δμ) (differential.jl:5-79); every vector in user order, NULL = 0.
+// Returns 0, or -1 when the factorization fails (the reference errors).
+int oracle_frule(void* h, const double* Df, const double* Dg, double Dmu, double* Dp, double* Dy, double* Dd) {
+    Solver& s = *(Solver*)h;
+    const i64 n = s.n, m = s.m;
+    double ftol, gtol;
+    if (!sens_setup(s, ftol, gtol)) return -1;
+    std::vector<double> fx(n), gx(m), px(n, 0.0), yx(m, 0.0), dx(n);
+    for (i64 i = 0; i < n; ++i) fx[i] = (Df ? Df[s.P2[i]] : 0.0) * s.pscl[i];
+    for (i64 i = 0; i < m; ++i) gx[i] = (Dg ? Dg[s.P1[i]] : 0.0) * s.yscl[i];
+    dualshadow_all(s, dx.data());
+    for (i64 i = 0; i < n; ++i) { dx[i] *= Dmu; fx[i] += dx[i]; }
+    solvekkt(s, never, never, px.data(), yx.data(), s.H, fx.data(), gx.data(), false, ftol, gtol,
+             s.set.refine_stall_tol, s.set.refine_max_iter, s.set.newton_max_iter, 1);
+    gemvN(s.H, px.data(), dx.data(), -1, 1);           // Δd = Δμ d* − (H − Q) Δp
+    gemvN(s.Q, px.data(), dx.data(), 1, 1);
+    for (i64 i = 0; i < n; ++i) { Dp[s.P2[i]] = px[i] * s.pscl[i]; Dd[s.P2[i]] = dx[i] / s.pscl[i]; }
+    for (i64 i = 0; i < m; ++i) Dy[s.P1[i]] = yx[i] * s.yscl[i];
+    return 0;
+}
+
+// rrule!(Δf, Δg, s, Δp, Δy, Δd) (differential.jl:263-334); *Dmu = the μ cotangent
+int oracle_rrule(void* h, const double* Dp, const double* Dy, const double* Dd, double* Df, double* Dg, double* Dmu) {
+    Solver& s = *(Solver*)h;
+    const i64 n = s.n, m = s.m;
+    double ftol, gtol;
+    if (!sens_setup(s, ftol, gtol)) return -1;
+    std::vector<double> px(n), dx(n), yx(m), fx(n, 0.0), gx(m, 0.0);
+    for (i64 i = 0; i < n; ++i) {
+        px[i] = (Dp ? Dp[s.P2[i]] : 0.0) * s.pscl[i];
+        dx[i] = (Dd ? Dd[s.P2[i]] : 0.0) / s.pscl[i];
+    }
+    for (i64 i = 0; i < m; ++i) yx[i] = (Dy ? Dy[s.P1[i]] : 0.0) * -s.yscl[i];
+    gemvN(s.H, dx.data(), px.data(), -1, 1);           // Δp −= (H − Q) Δd
+    gemvN(s.Q, dx.data(), px.data(), 1, 1);
+    solvekkt(s, never, never, fx.data(), gx.data(), s.H, px.data(), yx.data(), false, ftol, gtol,
+             s.set.refine_stall_tol, s.set.refine_max_iter, s.set.newton_max_iter, 1);
+    for (i64 i = 0; i < n; ++i) dx[i] += fx[i];         // λd = Δd + λp
+    for (i64 i = 0; i < n; ++i) Df[s.P2[i]] = fx[i] * s.pscl[i];
+    for (i64 i = 0; i < m; ++i) Dg[s.P1[i]] = -gx[i] * s.yscl[i];
+    dualshadow_all(s, px.data());
+    *Dmu = vdot(dx.data(), px.data(), n);
+    return 0;
+}
+
 int oracle_step(void* h) { return step(*(Solver*)h); }
 
 int oracle_solve(void* h) {

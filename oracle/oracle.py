@@ -100,6 +100,9 @@ def lib(threads: int = 1):
                                     C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double)]
         L.oracle_step.argtypes = [C.c_void_p]
         L.oracle_reinit.argtypes = [C.c_void_p] + [C.POINTER(C.c_double)] * 5
+        L.oracle_frule.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_double] + \
+            [C.POINTER(C.c_double)] * 3
+        L.oracle_rrule.argtypes = [C.c_void_p] + [C.POINTER(C.c_double)] * 6
         L.oracle_solve.argtypes = [C.c_void_p]
         L.oracle_result.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double),
                                     C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_int32),
@@ -161,6 +164,24 @@ class OracleSolver:
     def step(self) -> int:
         self.status = self.L.oracle_step(self.h)
         return self.status
+
+    def frule(self, df=None, dg=None, dmu=0.0):
+        """frule!(Δp, Δy, Δd, s, Δf, Δg, Δμ): tangents of (p, y, d) for seeds on (f, g, μ); user order."""
+        a = [None if x is None else np.ascontiguousarray(x, dtype=np.float64) for x in (df, dg)]
+        dp, dd, dy = np.zeros(self.n), np.zeros(self.n), np.zeros(self.m)
+        rc = self.L.oracle_frule(self.h, _pd(a[0]), _pd(a[1]), float(dmu), _pd(dp), _pd(dy), _pd(dd))
+        if rc:
+            raise RuntimeError("frule!: the factorization failed")
+        return dp, dy, dd
+
+    def rrule(self, dp=None, dy=None, dd=None):
+        """rrule!(Δf, Δg, s, Δp, Δy, Δd): cotangents of (f, g) and μ for seeds on (p, y, d)."""
+        a = [None if x is None else np.ascontiguousarray(x, dtype=np.float64) for x in (dp, dy, dd)]
+        df, dg, dmu = np.zeros(self.n), np.zeros(self.m), C.c_double()
+        rc = self.L.oracle_rrule(self.h, _pd(a[0]), _pd(a[1]), _pd(a[2]), _pd(df), _pd(dg), C.byref(dmu))
+        if rc:
+            raise RuntimeError("rrule!: the factorization failed")
+        return df, dg, dmu.value
 
     def reinit(self, p0=None, d0=None, y0=None, f=None, g=None):
         """reinit!(s; p0, d0, y0, f, g), every vector in user order."""

@@ -20,6 +20,7 @@
  *   mb_solver_timers        print_timers(s) (TimerOutput sections)         src/IPM/src/ipm/solver/ipm.jl:137-755
  *   mb_solver_frule         frule!(Δp, Δy, Δd, s, Δf, Δg, Δμ)              src/IPM/src/ipm/differential.jl:5-79
  *   mb_solver_rrule         rrule!(Δf, Δg, s, Δp, Δy, Δd)                  src/IPM/src/ipm/differential.jl:263-334
+ *   mb_solver_frule2        frule2!(…, s, Δf1, Δg1, Δμ1, Δf2, Δg2, Δμ2)    src/IPM/src/ipm/differential.jl:82-260
  *   mb_batch_solve          solve(prob, settings) over many problems      src/IPM/src/ipm/solver/ipm.jl:798-804
  *   mb_settings             IPMSettings                                    src/IPM/src/ipm/settings/ipm.jl:1-18
  */
@@ -182,6 +183,11 @@ int mb_solver_reinit(mb_solver* s, const double* p0, const double* d0, const dou
  * iterate for seeds on f (n), g (m) and μ; user order, NULL seed = 0, NULL output = skipped.  The
  * factorization at the current iterate is redone (FP64); MB_E_STATE when it fails. */
 int mb_solver_frule(mb_solver* s, const double* df, const double* dg, double dmu, double* dp, double* dy, double* dd);
+/* frule2!  src/IPM/src/ipm/differential.jl:82-260: tangents for two seed sets (Δf1 Δg1 Δμ1,
+ * Δf2 Δg2 Δμ2) and the second-order tangent; out = nine output pointers Δp1 Δy1 Δd1 Δp2 Δy2 Δd2
+ * Δp12 Δy12 Δd12 (each NULL to skip); as mb_solver_frule */
+int mb_solver_frule2(mb_solver* s, const double* df1, const double* dg1, double dmu1, const double* df2,
+                     const double* dg2, double dmu2, double* const* out);
 /* rrule!(Δf, Δg, s, Δp, Δy, Δd)  src/IPM/src/ipm/differential.jl:263-334: cotangents of f, g and μ
  * for seeds on p (n), y (m), d (n); as mb_solver_frule */
 int mb_solver_rrule(mb_solver* s, const double* dp, const double* dy, const double* dd, double* df, double* dg,

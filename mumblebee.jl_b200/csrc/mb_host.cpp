@@ -1187,12 +1187,13 @@ static int sens_run(mb_solver* s, int mode, const double* a, const double* bv, c
     InstPlan& ip = b->pk.plans[0];
     const i64 n = ip.n, m = ip.m;
     const size_t len = (size_t)(4 * n + 2 * m + 3);
-    if (!s->d_sx) {
-        CUDA_TRY(ctx, cache_alloc(ctx, ctx->dev, true, (void**)&s->d_sx, len * sizeof(double)));
+    if (!s->d_sx) {   // room for frule2!'s exchange too (8n + 5m + 3)
+        CUDA_TRY(ctx, cache_alloc(ctx, ctx->dev, true, (void**)&s->d_sx, (size_t)(8 * n + 5 * m + 3) * sizeof(double)));
         mb::DevInst I = static_devinst(ip, b->d_i32, b->d_i64, b->d_din, b->d_work, b->d_out, b->d_ost, (char*)b->d_F);
         I.sx = s->d_sx;
         CUDA_TRY(ctx, cudaMemcpy(b->d_inst, &I, sizeof(I), cudaMemcpyHostToDevice));
     }
+    if (mode < 0) return MB_OK;   // bind the buffer only
     std::vector<double> h(len, 0.0);
     for (i64 i = 0; i < n; ++i) {
         if (a) h[i] = a[ip.colmap[i]];
@@ -1212,6 +1213,49 @@ static int sens_run(mb_solver* s, int mode, const double* a, const double* bv, c
     }
     if (ob) for (i64 i = 0; i < m; ++i) ob[ip.rowmap[i]] = r[n + i];
     if (dmu_out) *dmu_out = h[4 * n + 2 * m + 1];
+    return MB_OK;
+}
+
+// frule2! (ipm/differential.jl:82-260): seeds f1 g1 f2 g2 at sx[0 .. 2n+2m), nine results after them,
+// then [Δμ1, Δμ2, ok]
+int mb_solver_frule2(mb_solver* s, const double* df1, const double* dg1, double dmu1, const double* df2,
+                     const double* dg2, double dmu2, double* const* out) {
+    if (!s) return MB_E_ARG;
+    if (!s->d_sx) {   // allocate and bind the exchange buffer through a first-order call's path
+        int rc = sens_run(s, -1, nullptr, nullptr, nullptr, 0.0, nullptr, nullptr, nullptr, nullptr);
+        if (rc) return rc;
+    }
+    mb_batch* b = s->b.get();
+    mb_ctx* ctx = b->ctx;
+    InstPlan& ip = b->pk.plans[0];
+    const i64 n = ip.n, m = ip.m;
+    const size_t len = (size_t)(8 * n + 5 * m + 3);
+    std::vector<double> h(len, 0.0);
+    const double* fs[2] = {df1, df2};
+    const double* gs[2] = {dg1, dg2};
+    for (int k = 0; k < 2; ++k) {
+        double* f = h.data() + (size_t)k * (n + m);
+        double* g = f + n;
+        if (fs[k]) for (i64 i = 0; i < n; ++i) f[i] = fs[k][ip.colmap[i]];
+        if (gs[k]) for (i64 i = 0; i < m; ++i) g[i] = gs[k][ip.rowmap[i]];
+    }
+    double* ss = h.data() + len - 3;
+    ss[0] = dmu1; ss[1] = dmu2;
+    CUDA_TRY(ctx, cudaMemcpy(s->d_sx, h.data(), len * sizeof(double), cudaMemcpyHostToDevice));
+    int rc = run_batch(b, mb::MODE_FRULE2, 1, nullptr);
+    if (rc) return rc;
+    CUDA_TRY(ctx, cudaMemcpy(h.data(), s->d_sx, len * sizeof(double), cudaMemcpyDeviceToHost));
+    if (ss[2] != 1.0) return fail(ctx, MB_E_STATE, "the KKT factorization at the current iterate failed");
+    const double* r = h.data() + 2 * (n + m);
+    for (int k = 0; k < 9; ++k) {
+        const bool row = k % 3 == 1;
+        const i64 len_k = row ? m : n;
+        if (out && out[k]) {
+            if (row) for (i64 i = 0; i < m; ++i) out[k][ip.rowmap[i]] = r[i];
+            else for (i64 i = 0; i < n; ++i) out[k][ip.colmap[i]] = r[i];
+        }
+        r += len_k;
+    }
     return MB_OK;
 }
 

@@ -59,7 +59,9 @@ struct DevInst {
     int has_p0, has_d0, has_y0;
     int reinit_fg;          // MODE_REINIT: bit 0 = f0 holds a new f, bit 1 = g0 holds a new g
     double* sx;             // MODE_FRULE / MODE_RRULE exchange, solver order, unscaled: seeds a (n), b (m),
-                            // c (n), then results a (n), b (m), c (n), then [Δμ in, dμ out, ok]
+                            // c (n), then results a (n), b (m), c (n), then [Δμ in, dμ out, ok];
+                            // MODE_FRULE2: Δf1, Δg1, Δf2, Δg2, then nine results (Δp, Δy, Δd for
+                            // sets 1, 2 and the second order), then [Δμ1, Δμ2, ok]
     double mut;             // barrier target μ′ (0 = exact solve)
     const int* xcol;        // nvtx+1: columns of each vertex
     const int* colvtx;      // n: vertex of each column
@@ -134,7 +136,7 @@ constexpr int NSTAT = 8;    // status, history rows, factor retries, factorizati
 
 // kernel modes: a full solve, or the pieces used by the step-wise API
 enum Mode { MODE_SOLVE = 0, MODE_INIT = 1, MODE_STEP = 2, MODE_RESULT = 3, MODE_REINIT = 4, MODE_FRULE = 5,
-            MODE_RRULE = 6 };
+            MODE_RRULE = 6, MODE_FRULE2 = 7 };
 
 // Grid-cooperative mode for one large instance: CTA 0 (the leader) runs the iteration; the other
 // CTAs of a cooperative launch help with the dense work of large fronts (assembly copy, factor

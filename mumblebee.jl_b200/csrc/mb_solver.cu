@@ -1157,6 +1157,165 @@ struct Ctx {
         __syncthreads();
     }
 
+    // r = F2(p) dp, the second derivative of the barrier per cone (primalhess!, cone.jl:579-591):
+    // pos.jl:193-203, soc.jl:510-530 (det(p) from the cache), tdc.jl:509-511 (the cached factor L),
+    // sdp.jl:696-742 (the cached R); free: 0
+    __device__ void primalhess_all(double* r, const double* pv, const double* dp) {
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+        for (int v = warp; v < nv; v += NW) {
+            const int k = I.kind[v], c0 = I.xcol[v], nc = I.xcol[v + 1] - c0;
+            const double* C = I.cache + I.cxblk[v];
+            if (k == CONE_POS) {
+                for (int i = lane; i < nc; i += 32) { const double q = pv[c0 + i]; r[c0 + i] = dp[c0 + i] / (q * q); }
+            } else if (k == CONE_SOC) {
+                double hi, lo;
+                w_socdot(pv + c0, dp + c0, nc, hi, lo);
+                const double pdet = C[1], t = hi / pdet, gm = 2 / pdet, t2 = 2 * t;
+                for (int i = lane; i < nc; i += 32)
+                    r[c0 + i] = i == 0 ? gm * fma(t2, pv[c0], -dp[c0]) : gm * fma(-t2, pv[c0 + i], dp[c0 + i]);
+            } else if (k == CONE_EXP || k == CONE_POW) {
+                if (lane == 0) tdhessmul(r + c0, C + TD_L, dp + c0);
+            } else if (k != CONE_SDP) {
+                for (int i = lane; i < nc; i += 32) r[c0 + i] = 0;
+            }
+            __syncwarp();
+        }
+        __syncthreads();
+        for (int v = 0; v < nv; ++v) {
+            if (I.kind[v] != CONE_SDP) continue;
+            const int c0 = I.xcol[v], nc = I.xcol[v + 1] - c0, d = sdp_triroot(nc);
+            const double* R = I.cache + I.cxblk[v];
+            double *U = I.work, *A = I.work + (int64_t)d * d;
+            b_smat(U, dp + c0, d, true);
+            b_mul(A, R, true, U, false, d);  b_mul(U, A, false, R, false, d);    // Ũ = Rᵀ U R
+            b_mul(A, R, false, U, false, d); b_mul(U, A, false, R, true, d);     // R Ũ Rᵀ
+            b_svec(r + c0, U, d);
+        }
+        __syncthreads();
+    }
+
+    // r = F3(p)[u, w], the third derivative of the barrier per cone (primalthird!, cone.jl:595-607):
+    // pos.jl:209-219, soc.jl:535-560, tdc.jl:517-521, sdp.jl:747-790; free: 0
+    __device__ void primalthird_all(double* r, const double* pv, const double* u, const double* w) {
+        const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+        for (int v = warp; v < nv; v += NW) {
+            const int k = I.kind[v], c0 = I.xcol[v], nc = I.xcol[v + 1] - c0;
+            const double* C = I.cache + I.cxblk[v];
+            if (k == CONE_POS) {
+                for (int i = lane; i < nc; i += 32) {
+                    const double q = pv[c0 + i];
+                    r[c0 + i] = -2 * u[c0 + i] * w[c0 + i] / (q * q * q);
+                }
+            } else if (k == CONE_SOC) {
+                double a1, a2, a3, lo;
+                w_socdot(pv + c0, u + c0, nc, a1, lo);
+                w_socdot(pv + c0, w + c0, nc, a2, lo);
+                w_socdot(u + c0, w + c0, nc, a3, lo);
+                const double pdet = C[1], u1 = a1 / pdet, u2 = a2 / pdet, vv = a3 / pdet, gm = 4 / pdet;
+                const double cc = fma(-4 * u1, u2, vv);
+                for (int i = lane; i < nc; i += 32) {
+                    const double t = fma(u1, w[c0 + i], fma(u2, u[c0 + i], cc * pv[c0 + i]));
+                    r[c0 + i] = i == 0 ? gm * t : -gm * t;
+                }
+            } else if (k == CONE_EXP || k == CONE_POW) {
+                if (lane == 0) {
+                    double D[9];
+                    tdbarrthird(TD{k, I.kpar[v]}, D, pv + c0, u + c0, C);
+                    for (int i = 0; i < 3; ++i)
+                        r[c0 + i] = D[i] * w[c0] + D[i + 3] * w[c0 + 1] + D[i + 6] * w[c0 + 2];
+                }
+            } else if (k != CONE_SDP) {
+                for (int i = lane; i < nc; i += 32) r[c0 + i] = 0;
+            }
+            __syncwarp();
+        }
+        __syncthreads();
+        for (int v = 0; v < nv; ++v) {
+            if (I.kind[v] != CONE_SDP) continue;
+            const int c0 = I.xcol[v], nc = I.xcol[v + 1] - c0, d = sdp_triroot(nc);
+            const int64_t q = (int64_t)d * d;
+            const double* R = I.cache + I.cxblk[v];
+            double *U = I.work, *V = I.work + q, *A = I.work + 2 * q;
+            b_smat(U, u + c0, d, true);
+            b_smat(V, w + c0, d, true);
+            b_mul(A, R, true, U, false, d); b_mul(U, A, false, R, false, d);     // Ũ
+            b_mul(A, R, true, V, false, d); b_mul(V, A, false, R, false, d);     // Ṽ
+            b_mul(A, U, false, V, false, d);                                     // Ũ Ṽ
+            for (int t = threadIdx.x; t < d * d; t += NT) {                      // Ũ Ṽ + Ṽ Ũ, into V
+                const int i = t % d, j = t / d;
+                V[t] = i == j ? 2 * A[t] : A[t] + A[j + (int64_t)i * d];
+            }
+            __syncthreads();
+            b_mul(U, R, false, V, false, d); b_mul(A, U, false, R, true, d);     // R (Ũ Ṽ + Ṽ Ũ) Rᵀ
+            b_svec(r + c0, A, d);
+            for (int i = threadIdx.x; i < nc; i += NT) r[c0 + i] = -r[c0 + i];
+            __syncthreads();
+        }
+        __syncthreads();
+    }
+
+    // frule2! (ipm/differential.jl:82-260): two first-order solves, then the second-order solve on
+    // -(μ′ F3(p)[Δp1, Δp2] + Δμ1 F2(p) Δp2 + Δμ2 F2(p) Δp1); the exchange layout is DevInst::sx's
+    __device__ void sensitivity2() {
+        double* f1 = I.sx; double* g1 = f1 + n; double* f2 = g1 + m; double* g2 = f2 + n;
+        double* o = g2 + m;                                  // p1 y1 d1 p2 y2 d2 p12 y12 d12
+        double *op1 = o, *oy1 = op1 + n, *od1 = oy1 + m, *op2 = od1 + n, *oy2 = op2 + n, *od2 = oy2 + m;
+        double *op12 = od2 + n, *oy12 = op12 + n, *od12 = oy12 + m, *ss = od12 + n;
+        use32 = false;
+        const double dl = getaug();
+        double rho;
+        if (!initkkt(dl, rho)) { if (threadIdx.x == 0) ss[2] = 0; __syncthreads(); return; }
+        const double mu0 = nrow_hist > 0 ? hrow(0).mu : 0.0;
+        const double tol = mu0 == 0 ? 0.1 * set.gap_tol : 0.1 * hrow(nrow_hist - 1).mu / mu0;
+        const double ftol = tol * (1 + nf), gtol = tol * (1 + ng);
+        const double dmu1 = ss[0], dmu2 = ss[1];
+        double* ds = Dd;           // d*(p), then F2 scratch
+        double* fx = wf; double* gx = Dg;
+        double* p1 = Dpa; double* y1 = Dya; double* d1 = Dda;
+        double* p2 = Dp; double* y2 = Dy; double* d2 = df;
+        dualshadow_all(ds, I.p);
+        for (int set2 = 0; set2 < 2; ++set2) {
+            const double* fs = set2 ? f2 : f1; const double* gs = set2 ? g2 : g1;
+            const double dm = set2 ? dmu2 : dmu1;
+            double* px = set2 ? p2 : p1; double* yx = set2 ? y2 : y1; double* dx = set2 ? d2 : d1;
+            for (int i = threadIdx.x; i < n; i += NT) fx[i] = fma(dm, ds[i], fs[i] * I.pscl[i]);
+            for (int i = threadIdx.x; i < m; i += NT) gx[i] = gs[i] * I.yscl[i];
+            __syncthreads();
+            solvekkt(0, px, yx, I.Hd, fx, gx, false, ftol, gtol, 1);
+            amul(I.Hd, px, dx, 1, 0);                      // Δd = Δμ d* - (H - Q) Δp
+            amul(I.Qd, px, dx, -1, 1);
+            for (int i = threadIdx.x; i < n; i += NT) dx[i] = fma(dm, ds[i], -dx[i]);
+            __syncthreads();
+        }
+        primalthird_all(fx, I.p, p1, p2);
+        for (int i = threadIdx.x; i < n; i += NT) fx[i] *= I.mut;
+        __syncthreads();
+        if (dmu1 != 0) {
+            primalhess_all(ds, I.p, p2);
+            for (int i = threadIdx.x; i < n; i += NT) fx[i] = fma(dmu1, ds[i], fx[i]);
+            __syncthreads();
+        }
+        if (dmu2 != 0) {
+            primalhess_all(ds, I.p, p1);
+            for (int i = threadIdx.x; i < n; i += NT) fx[i] = fma(dmu2, ds[i], fx[i]);
+            __syncthreads();
+        }
+        for (int i = threadIdx.x; i < n; i += NT) {
+            fx[i] = -fx[i];
+            op1[i] = p1[i] * I.pscl[i]; od1[i] = d1[i] / I.pscl[i];
+            op2[i] = p2[i] * I.pscl[i]; od2[i] = d2[i] / I.pscl[i];
+        }
+        for (int i = threadIdx.x; i < m; i += NT) { oy1[i] = y1[i] * I.yscl[i]; oy2[i] = y2[i] * I.yscl[i]; gx[i] = 0; }
+        __syncthreads();
+        solvekkt(0, p2, y2, I.Hd, fx, gx, false, ftol, gtol, 1);
+        amul(I.Hd, p2, fx, -1, 1);                         // Δd12 = rhs - (H - Q) Δp12
+        amul(I.Qd, p2, fx, 1, 1);
+        for (int i = threadIdx.x; i < n; i += NT) { op12[i] = p2[i] * I.pscl[i]; od12[i] = fx[i] / I.pscl[i]; }
+        for (int i = threadIdx.x; i < m; i += NT) oy12[i] = y2[i] * I.yscl[i];
+        if (threadIdx.x == 0) ss[2] = 1;
+        __syncthreads();
+    }
+
     // frule! / rrule! (ipm/differential.jl:5-79, 263-334) at the current iterate: δ = getaug, an FP64
     // factorization, one KKT solve (cold, at least one refinement pass), the rest H/Q products and the
     // dual shadow.  Seeds and results in I.sx (solver order, unscaled); sx[4n+2m+2] = 1 on success.
@@ -2116,6 +2275,8 @@ __device__ void solve_instance(const DevInst& I, const Settings& set, Shared& sh
         c.result(I.status[0]);
     } else if (mode == MODE_FRULE || mode == MODE_RRULE) {
         c.sensitivity(mode == MODE_RRULE);
+    } else if (mode == MODE_FRULE2) {
+        c.sensitivity2();
     }
 }
 

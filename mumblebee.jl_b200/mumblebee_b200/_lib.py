@@ -73,6 +73,7 @@ SIGNATURES = {
     "mb_solver_timers": (I32, [C.c_void_p, PF64, I64]),
     "mb_solver_frule": (I32, [C.c_void_p, PF64, PF64, F64, PF64, PF64, PF64]),
     "mb_solver_rrule": (I32, [C.c_void_p, PF64, PF64, PF64, PF64, PF64, PF64]),
+    "mb_solver_frule2": (I32, [C.c_void_p, PF64, PF64, F64, PF64, PF64, F64, C.POINTER(PF64)]),
     "mb_solver_destroy": (I32, [C.c_void_p]),
     "mb_batch_solve": (I32, [C.c_void_p, C.POINTER(C.c_void_p), I32, C.POINTER(mb_settings), I32,
                              C.POINTER(PF64), C.POINTER(PF64), C.POINTER(PF64), C.POINTER(mb_result)]),

@@ -384,6 +384,18 @@ class IPMSolver:
                                      _p(dp, C.c_double), _p(dy, C.c_double), _p(dd, C.c_double)), self.prob.ctx.h, "frule!")
         return dp, dy, dd
 
+    def frule2(self, df1=None, dg1=None, dmu1=0.0, df2=None, dg2=None, dmu2=0.0):
+        """frule2! (ipm/differential.jl:82-260): the first-order tangents for two seed sets and the
+        second-order tangent, as (Δp1, Δy1, Δd1, Δp2, Δy2, Δd2, Δp12, Δy12, Δd12); user order."""
+        i = self.prob.info()
+        outs = [np.zeros(i["m"] if k % 3 == 1 else i["n"]) for k in range(9)]
+        arr = (C.POINTER(C.c_double) * 9)(*[_p(x, C.c_double) for x in outs])
+        a = [None if x is None else _f64(x) for x in (df1, dg1, df2, dg2)]
+        check(self.L.mb_solver_frule2(self.h, _p(a[0], C.c_double), _p(a[1], C.c_double), float(dmu1),
+                                      _p(a[2], C.c_double), _p(a[3], C.c_double), float(dmu2), arr),
+              self.prob.ctx.h, "frule2!")
+        return tuple(outs)
+
     def rrule(self, dp=None, dy=None, dd=None):
         """rrule!(Δf, Δg, s, Δp, Δy, Δd) (ipm/differential.jl:263-334): the cotangents (Δf, Δg, Δμ) for
         seeds Δp (n), Δy (m), Δd (n); user order, None = 0."""
@@ -440,6 +452,11 @@ class IPMSolver:
 def frule(solver: IPMSolver, df=None, dg=None, dmu=0.0):
     """frule!(Δp, Δy, Δd, solver, Δf, Δg, Δμ) → (Δp, Δy, Δd)"""
     return solver.frule(df, dg, dmu)
+
+
+def frule2(solver: IPMSolver, df1=None, dg1=None, dmu1=0.0, df2=None, dg2=None, dmu2=0.0):
+    """frule2!(…, solver, Δf1, Δg1, Δμ1, Δf2, Δg2, Δμ2) → nine tangents"""
+    return solver.frule2(df1, dg1, dmu1, df2, dg2, dmu2)
 
 
 def rrule(solver: IPMSolver, dp=None, dy=None, dd=None):

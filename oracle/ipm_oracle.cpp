@@ -1453,6 +1453,112 @@ static bool sens_setup(Solver& s, double& ftol, double& gtol) {
     return true;
 }
 
+// r = F2(p) Δp and r = F3(p)[u, w] per cone (primalhess!, primalthird!; cone.jl:579-607): pos.jl:193-219,
+// soc.jl:510-560 (det(p) from the cache), tdc.jl:509-521, sdp.jl:696-790 (the cached R)
+static void primalhess_all(Solver& s, double* r, const double* dp) {
+    for (i64 v = 0; v < s.B.nvtx; ++v) {
+        const i64 c0 = s.B.xcol[v], nc = s.B.ncols(v);
+        const double* p = s.p.data() + c0; const double* x = dp + c0; double* o = r + c0;
+        const double* C = s.cache.data() + s.cxblk[v];
+        const int k = s.K[v];
+        if (k == CONE_POS) { for (i64 i = 0; i < nc; ++i) o[i] = x[i] / (p[i] * p[i]); }
+        else if (k == CONE_SOC) {
+            double hi, lo;
+            socdot(p, x, nc, hi, lo);
+            const double pdet = C[1], t = hi / pdet, gm = 2 / pdet, t2 = 2 * t;
+            o[0] = gm * std::fma(t2, p[0], -x[0]);
+            for (i64 i = 1; i < nc; ++i) o[i] = gm * std::fma(-t2, p[i], x[i]);
+        } else if (k == CONE_EXP || k == CONE_POW) tdhessmul(o, C + TD_L, x);
+        else if (k == CONE_SDP) {
+            const int d = (int)triroot(nc);
+            std::vector<double> U((size_t)d * d), A((size_t)d * d);
+            sdp_smat(U.data(), x, d); sdp_symm(U.data(), d);
+            sdp_mul(A.data(), C, true, U.data(), false, d); sdp_mul(U.data(), A.data(), false, C, false, d);
+            sdp_mul(A.data(), C, false, U.data(), false, d); sdp_mul(U.data(), A.data(), false, C, true, d);
+            sdp_svec(o, U.data(), d);
+        } else { for (i64 i = 0; i < nc; ++i) o[i] = 0; }
+    }
+}
+
+static void primalthird_all(Solver& s, double* r, const double* u, const double* w) {
+    for (i64 v = 0; v < s.B.nvtx; ++v) {
+        const i64 c0 = s.B.xcol[v], nc = s.B.ncols(v);
+        const double* p = s.p.data() + c0; const double* a = u + c0; const double* b = w + c0; double* o = r + c0;
+        const double* C = s.cache.data() + s.cxblk[v];
+        const int k = s.K[v];
+        if (k == CONE_POS) { for (i64 i = 0; i < nc; ++i) o[i] = -2 * a[i] * b[i] / (p[i] * p[i] * p[i]); }
+        else if (k == CONE_SOC) {
+            double a1, a2, a3, lo;
+            socdot(p, a, nc, a1, lo); socdot(p, b, nc, a2, lo); socdot(a, b, nc, a3, lo);
+            const double pdet = C[1], u1 = a1 / pdet, u2 = a2 / pdet, vv = a3 / pdet, gm = 4 / pdet;
+            const double cc = std::fma(-4 * u1, u2, vv);
+            for (i64 i = 0; i < nc; ++i) {
+                const double t = std::fma(u1, b[i], std::fma(u2, a[i], cc * p[i]));
+                o[i] = i == 0 ? gm * t : -gm * t;
+            }
+        } else if (k == CONE_EXP || k == CONE_POW) {
+            double D[9];
+            tdbarrthird(TD{k, s.Kp[v]}, D, p, a, C);
+            for (int i = 0; i < 3; ++i) o[i] = D[i] * b[0] + D[i + 3] * b[1] + D[i + 6] * b[2];
+        } else if (k == CONE_SDP) {
+            const int d = (int)triroot(nc);
+            std::vector<double> U((size_t)d * d), V((size_t)d * d), A((size_t)d * d);
+            sdp_smat(U.data(), a, d); sdp_symm(U.data(), d); sdp_smat(V.data(), b, d); sdp_symm(V.data(), d);
+            sdp_mul(A.data(), C, true, U.data(), false, d); sdp_mul(U.data(), A.data(), false, C, false, d);
+            sdp_mul(A.data(), C, true, V.data(), false, d); sdp_mul(V.data(), A.data(), false, C, false, d);
+            sdp_mul(A.data(), U.data(), false, V.data(), false, d);
+            for (int j = 0; j < d; ++j)
+                for (int i = 0; i < d; ++i) V[i + (size_t)j * d] = i == j ? 2 * A[i + (size_t)j * d] : A[i + (size_t)j * d] + A[j + (size_t)i * d];
+            sdp_mul(U.data(), C, false, V.data(), false, d); sdp_mul(A.data(), U.data(), false, C, true, d);
+            sdp_svec(o, A.data(), d);
+            for (i64 i = 0; i < nc; ++i) o[i] = -o[i];
+        } else { for (i64 i = 0; i < nc; ++i) o[i] = 0; }
+    }
+}
+
+// frule2! (ipm/differential.jl:82-260); every vector in user order, NULL seed = 0; outputs
+// p1 y1 d1 p2 y2 d2 p12 y12 d12 (each may be NULL).  Returns 0, or -1 when the factorization fails.
+int oracle_frule2(void* h, const double* Df1, const double* Dg1, double Dmu1, const double* Df2,
+                  const double* Dg2, double Dmu2, double* const* out) {
+    Solver& s = *(Solver*)h;
+    const i64 n = s.n, m = s.m;
+    double ftol, gtol;
+    if (!sens_setup(s, ftol, gtol)) return -1;
+    std::vector<double> ds(n), fx(n), gx(m), p1(n, 0.0), y1(m, 0.0), d1(n), p2(n, 0.0), y2(m, 0.0), d2(n);
+    dualshadow_all(s, ds.data());
+    for (int k = 0; k < 2; ++k) {
+        const double* Df = k ? Df2 : Df1; const double* Dg = k ? Dg2 : Dg1; const double dm = k ? Dmu2 : Dmu1;
+        std::vector<double>& px = k ? p2 : p1; std::vector<double>& yx = k ? y2 : y1; std::vector<double>& dx = k ? d2 : d1;
+        for (i64 i = 0; i < n; ++i) fx[i] = std::fma(dm, ds[i], (Df ? Df[s.P2[i]] : 0.0) * s.pscl[i]);
+        for (i64 i = 0; i < m; ++i) gx[i] = (Dg ? Dg[s.P1[i]] : 0.0) * s.yscl[i];
+        solvekkt(s, never, never, px.data(), yx.data(), s.H, fx.data(), gx.data(), false, ftol, gtol,
+                 s.set.refine_stall_tol, s.set.refine_max_iter, s.set.newton_max_iter, 1);
+        gemvN(s.H, px.data(), dx.data(), 1, 0);            // Δd = Δμ d* − (H − Q) Δp
+        gemvN(s.Q, px.data(), dx.data(), -1, 1);
+        for (i64 i = 0; i < n; ++i) dx[i] = std::fma(dm, ds[i], -dx[i]);
+    }
+    primalthird_all(s, fx.data(), p1.data(), p2.data());
+    for (i64 i = 0; i < n; ++i) fx[i] *= s.mut;
+    if (Dmu1 != 0) { primalhess_all(s, ds.data(), p2.data()); for (i64 i = 0; i < n; ++i) fx[i] = std::fma(Dmu1, ds[i], fx[i]); }
+    if (Dmu2 != 0) { primalhess_all(s, ds.data(), p1.data()); for (i64 i = 0; i < n; ++i) fx[i] = std::fma(Dmu2, ds[i], fx[i]); }
+    for (i64 i = 0; i < n; ++i) fx[i] = -fx[i];
+    auto pull = [&](double* o, const std::vector<double>& v, bool col, int how) {   // how: 0 ×scl, 1 ÷scl
+        if (!o) return;
+        if (col) for (i64 i = 0; i < n; ++i) o[s.P2[i]] = how ? v[i] / s.pscl[i] : v[i] * s.pscl[i];
+        else for (i64 i = 0; i < m; ++i) o[s.P1[i]] = v[i] * s.yscl[i];
+    };
+    pull(out[0], p1, true, 0); pull(out[1], y1, false, 0); pull(out[2], d1, true, 1);
+    pull(out[3], p2, true, 0); pull(out[4], y2, false, 0); pull(out[5], d2, true, 1);
+    std::fill(gx.begin(), gx.end(), 0.0);
+    std::fill(p2.begin(), p2.end(), 0.0); std::fill(y2.begin(), y2.end(), 0.0);
+    solvekkt(s, never, never, p2.data(), y2.data(), s.H, fx.data(), gx.data(), false, ftol, gtol,
+             s.set.refine_stall_tol, s.set.refine_max_iter, s.set.newton_max_iter, 1);
+    gemvN(s.H, p2.data(), fx.data(), -1, 1);               // Δd12 = rhs − (H − Q) Δp12
+    gemvN(s.Q, p2.data(), fx.data(), 1, 1);
+    pull(out[6], p2, true, 0); pull(out[7], y2, false, 0); pull(out[8], fx, true, 1);
+    return 0;
+}
+
 // frule!(Δp, Δy, Δd, s, Δf, Δg, Δμ) (differential.jl:5-79); every vector in user order, NULL = 0.
 // Returns 0, or -1 when the factorization fails (the reference errors).
 int oracle_frule(void* h, const double* Df, const double* Dg, double Dmu, double* Dp, double* Dy, double* Dd) {

@@ -103,6 +103,9 @@ def lib(threads: int = 1):
         L.oracle_frule.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_double] + \
             [C.POINTER(C.c_double)] * 3
         L.oracle_rrule.argtypes = [C.c_void_p] + [C.POINTER(C.c_double)] * 6
+        L.oracle_frule2.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_double,
+                                    C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_double,
+                                    C.POINTER(C.POINTER(C.c_double))]
         L.oracle_solve.argtypes = [C.c_void_p]
         L.oracle_result.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double),
                                     C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_int32),
@@ -173,6 +176,17 @@ class OracleSolver:
         if rc:
             raise RuntimeError("frule!: the factorization failed")
         return dp, dy, dd
+
+    def frule2(self, df1=None, dg1=None, dmu1=0.0, df2=None, dg2=None, dmu2=0.0):
+        """frule2!: first-order tangents for two seed sets and the second-order tangent, as nine
+        vectors (Δp1, Δy1, Δd1, Δp2, Δy2, Δd2, Δp12, Δy12, Δd12); user order."""
+        a = [None if x is None else np.ascontiguousarray(x, dtype=np.float64) for x in (df1, dg1, df2, dg2)]
+        outs = [np.zeros(self.m if k % 3 == 1 else self.n) for k in range(9)]
+        arr = (C.POINTER(C.c_double) * 9)(*[_pd(x) for x in outs])
+        rc = self.L.oracle_frule2(self.h, _pd(a[0]), _pd(a[1]), float(dmu1), _pd(a[2]), _pd(a[3]), float(dmu2), arr)
+        if rc:
+            raise RuntimeError("frule2!: the factorization failed")
+        return tuple(outs)
 
     def rrule(self, dp=None, dy=None, dd=None):
         """rrule!(Δf, Δg, s, Δp, Δy, Δd): cotangents of (f, g) and μ for seeds on (p, y, d)."""

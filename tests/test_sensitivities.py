@@ -72,3 +72,59 @@ def test_device_rules_match_oracle(name, tol):
     for a, b in zip(da[:2], db[:2]):
         assert np.linalg.norm(a - b) <= tol * max(1.0, np.linalg.norm(b))
     assert abs(da[2] - db[2]) <= tol * max(1.0, abs(db[2]))
+
+
+# frule2! (differential.jl:82-260) needs a barrier target μ′ > 0 for its third-order term; the
+# problems below solve to the central-path point at μ′ = 0.05, which is smooth in the data
+BARRIER = {
+    "port": lambda: dict(SMALL["port_small"](), mu=0.05),
+    "socp": lambda: dict(SMALL["socp_tiny"](), mu=0.05),
+    "sdp": lambda: dict(__import__("helpers").SDP["sdp1x10"](), mu=0.05),
+    "exp": lambda: dict(__import__("helpers").TDC["exp_small"](), mu=0.05),
+    "pow": lambda: dict(__import__("helpers").TDC["pow_small"](), mu=0.05),
+}
+TIGHT = dict(gap_tol=1e-12, feas_tol=1e-12, max_iter=200)
+TOLS = {"port": TIGHT, "socp": TIGHT, "sdp": {}, "exp": dict(gap_tol=1e-7, feas_tol=1e-7),
+        "pow": dict(gap_tol=1e-7, feas_tol=1e-7)}
+
+
+def _seeds2(n, m, seed=0):
+    rng = np.random.default_rng(seed)
+    return (rng.standard_normal(n), 0.1 * rng.standard_normal(m), 0.01,
+            rng.standard_normal(n), 0.1 * rng.standard_normal(m), -0.02)
+
+
+def test_oracle_frule2_matches_finite_differences():
+    pb = BARRIER["port"]()
+    s, r = oracle_solve(block_problem(pb), **TIGHT)
+    assert r["status"] == "OPTIMAL"
+    n, m = len(r["p"]), len(r["y"])
+    df1, dg1, dm1, df2, dg2, dm2 = _seeds2(n, m)
+    out = s.frule2(df1, dg1, dm1, df2, dg2, dm2)
+    for k, x in enumerate(s.frule(df1, dg1, dm1)):   # the same solve; only the RHS's rounding differs
+        np.testing.assert_allclose(out[k], x, rtol=1e-12, atol=1e-12)
+    eps = 1e-3
+
+    def p_at(e1, e2):
+        q = dict(pb, f=pb["f"] + e1 * df1 + e2 * df2, g=pb["g"] + e1 * dg1 + e2 * dg2, mu=pb["mu"] + e1 * dm1 + e2 * dm2)
+        _, rr = oracle_solve(block_problem(q), **TIGHT)
+        assert rr["status"] == "OPTIMAL"
+        return rr["p"]
+    fd = (p_at(eps, eps) - p_at(eps, -eps) - p_at(-eps, eps) + p_at(-eps, -eps)) / (4 * eps * eps)
+    assert np.linalg.norm(out[6] - fd) <= 1e-3 * np.linalg.norm(fd)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", list(BARRIER))
+def test_device_frule2_matches_oracle(name):
+    pb = BARRIER[name]()
+    ref = block_problem(pb)
+    prob = IPMProblem.from_dict(ref, ctx=Context.default())
+    o, ro = oracle_solve(ref, vperm=prob.symbolic()["vperm"], **TOLS[name])
+    s = init(prob, IPMSettings(**TOLS[name]))
+    r = s.solve()
+    assert r.status.name == ro["status"] == "OPTIMAL"
+    n, m = len(r.p), len(r.y)
+    seeds = _seeds2(n, m, 1)
+    for a, b in zip(s.frule2(*seeds), o.frule2(*seeds)):
+        assert np.linalg.norm(a - b) <= 1e-5 * max(1.0, np.linalg.norm(b))

@@ -98,3 +98,28 @@ def cone_violation(x, kinds, sizes):
             v = max(v, float(np.linalg.norm(z[1:]) - z[0]))
         o += s
     return v
+
+
+def _edge(Q, B, f, g, kinds, sizes, mu=0.0):
+    import scipy.sparse as sp
+    return dict(Q=sp.csc_matrix(np.asarray(Q, float)), B=sp.csc_matrix(np.asarray(B, float)), f=np.asarray(f, float),
+                g=np.asarray(g, float), mu=mu, kinds=list(kinds), sizes=list(sizes), params=[0.0] * len(kinds))
+
+
+def _edge_cases():
+    rng = np.random.default_rng(0)
+    return {
+        # no equality rows: min ½‖p‖² − fᵀp over the orthant
+        "m0_qp_pos": _edge(np.eye(5), np.zeros((0, 5)), rng.standard_normal(5), [], [1], [5]),
+        # no cones (ν = 0: the exact solve of step!): min ½pᵀQp − fᵀp s.t. Bp = g
+        "free_eqqp": _edge(np.diag([2.0, 1.0, 3.0, 1.0]), rng.standard_normal((2, 4)), rng.standard_normal(4),
+                           rng.standard_normal(2), [0], [4]),
+        # a standard-form LP
+        "lp": _edge(np.zeros((6, 6)), np.hstack([np.eye(3), rng.uniform(0.1, 1, (3, 3))]), -rng.uniform(0.5, 1.5, 6),
+                    rng.uniform(0.5, 1, 3), [1], [6]),
+        # one variable: min p s.t. p = 2, p ≥ 0
+        "one_var": _edge(np.zeros((1, 1)), np.ones((1, 1)), [-1.0], [2.0], [1], [1]),
+    }
+
+
+EDGE = _edge_cases()

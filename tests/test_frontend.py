@@ -145,3 +145,13 @@ def test_footprint_covers_workspace(name):
     fp32 = prob.footprint(IPMSettings(precision="fp32"))
     assert fp64 >= 8 * (2 * fr + 12 * n + 8 * m)
     assert fp64 - fp32 >= 4 * fr - 256
+
+
+@pytest.mark.parametrize("name", ["m0_qp_pos", "free_eqqp", "lp", "one_var"])
+def test_oracle_solves_edge_cases(name):
+    """Degenerate shapes the reference accepts: no equality rows, no cones, one variable."""
+    from helpers import EDGE, block_problem, oracle_solve
+    _, o = oracle_solve(block_problem(EDGE[name]))
+    assert o["status"] == "OPTIMAL"
+    if name == "one_var":
+        assert abs(o["pobj"] - 2.0) < 1e-7

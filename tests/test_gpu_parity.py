@@ -188,3 +188,17 @@ def test_split_batch_solve_equals_alone():
         assert a.status == many[k].status and a.niter == many[k].niter
         np.testing.assert_array_equal(a.p, many[k].p)
         np.testing.assert_array_equal(a.y, many[k].y)
+
+
+@pytest.mark.parametrize("name", ["m0_qp_pos", "free_eqqp", "lp", "one_var"])
+def test_edge_cases_match_oracle(name):
+    """No equality rows, no cones (ν = 0), a plain LP and a single variable: same status, iteration
+    count and objectives as the oracle."""
+    from helpers import EDGE
+    ref = block_problem(EDGE[name])
+    prob = _gpu_problem(ref)
+    _, o = oracle_solve(ref, vperm=prob.symbolic()["vperm"])
+    r = solve(prob, IPMSettings())
+    assert o["status"] == "OPTIMAL" and r.status == IPMStatus.OPTIMAL
+    assert r.niter == o["niter"]
+    assert _rel(r.pobj, o["pobj"]) < 1e-9 and _rel(r.dobj, o["dobj"]) < 1e-9

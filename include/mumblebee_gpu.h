@@ -72,7 +72,12 @@ typedef struct mb_settings {
     int32_t scale_max_iter;    /* 10  equilibration sweeps */
     int32_t refine_max_iter;   /* 10  KKT iterative-refinement passes */
     int32_t newton_max_iter;   /* 100 CG iterations per KKT solve */
-    int32_t stable;            /* 0   (StableUzawaSolver not available: must be 0) */
+    int32_t stable;            /* 0   1: the StableUzawaSolver factor (kkt/uzawa.jl:117-163): per-vertex
+                                      Cholesky of H updated by the rows of B, no BᵀB, no ρ retry; a
+                                      nonzero diagonal block of H that is not positive definite, or a
+                                      zero pivot, ends the solve with NUMERICAL_FAILURE.  Needs
+                                      precision MB_PREC_FP64 and Q without off-diagonal blocks
+                                      (MB_E_UNSUPPORTED otherwise); never grid-cooperative */
     int32_t precision;         /* MB_PREC_FP64 */
     int32_t large;             /* 0: a single instance whose factorization exceeds MB_LARGE_FLOPS runs
                                   grid-cooperatively (all SMs help with its large fronts); 1: always

@@ -233,13 +233,14 @@ struct InstPlan {
     // i32
     size_t xcol, colvtx, cfront, Brptr, Bcidx, Bcptr, Bridx, Bcpos, Qrptr, Qcidx, Qcptr, Qridx, Qcpos, hdld, qoffk;
     size_t Blongr, Blongc, hlong, hflag;
+    size_t sbrp, sbrow, sbloc, fchp, fch;   // stable factor: B rows per front, their front positions, children
     size_t kind, fres0, fnres, fnsep, fparent, fsepp, fsep, frel;
     // i64
     size_t hdoff, hdpos, qoffpos, cxblk, fptr, qd0off;
     // double in
     size_t Bval, Qval, Qd, f, g, kpar, p, d, y;
     // work
-    size_t wBval, wQval, wQd, Hd, Finit, pscl, yscl, vn, vm, vv, work, uhist, cghist, cache, cache2, wf, wg, wp, wd, wy;
+    size_t wBval, wQval, wQd, Hd, Finit, pscl, yscl, vn, vm, vv, work, uhist, cghist, cache, cache2, wf, wg, wp, wd, wy, swork;
     // factor (bytes)
     size_t F;
     // out
@@ -439,6 +440,41 @@ static int plan_instance(const mb_problem* P, const mb_settings& set, const doub
         if (fr.parent[f] >= 0) frel.insert(frel.end(), fr.rel[f].begin(), fr.rel[f].end());
         else frel.insert(frel.end(), fr.sep[f].size(), 0);
     }
+    // StableUzawaSolver (kkt/uzawa.jl:32-67,117-163): each nonempty row of B goes to the front of its
+    // first column (its columns are a clique of BᵀB, so they all lie in that front's rows), with the
+    // front position of each entry; the children of each front; the QR scratch, the largest
+    // (rows x columns) front of the stacked system [√δ Uᵀ; B rows; children's triangles]
+    std::vector<i64> sbrp(fr.nfront + 1, 0), sbrow, sbloc, fchp(fr.nfront + 1, 0), fch;
+    i64 sworksz = 0;
+    if (set.stable) {
+        if (ip.nqoff > 0) { err = "stable=true needs Q without off-diagonal blocks (uzawa.jl:136 copies H into its block diagonal)"; return MB_E_UNSUPPORTED; }
+        std::vector<i64> rf(m, -1);
+        sbloc.assign(ip.Bnnz, 0);
+        for (i64 i = 0; i < m; ++i) {
+            if (Brptr[i + 1] == Brptr[i]) continue;
+            const i64 f = cfront[Bcidx[Brptr[i]]];
+            rf[i] = f;
+            sbrp[f + 1]++;
+            for (i64 k = Brptr[i]; k < Brptr[i + 1]; ++k) {
+                sbloc[k] = rowpos(f, Bcidx[k]);
+                if (sbloc[k] < 0) { err = "internal: a row of B outside its front"; return MB_E_ARG; }
+            }
+        }
+        for (i64 f = 0; f < fr.nfront; ++f) sbrp[f + 1] += sbrp[f];
+        sbrow.assign(sbrp[fr.nfront], 0);
+        std::vector<i64> pos(sbrp.begin(), sbrp.end() - 1);
+        for (i64 i = 0; i < m; ++i) if (rf[i] >= 0) sbrow[pos[rf[i]]++] = i;
+        for (i64 f = 0; f < fr.nfront; ++f) if (fr.parent[f] >= 0) fchp[fr.parent[f] + 1]++;
+        for (i64 f = 0; f < fr.nfront; ++f) fchp[f + 1] += fchp[f];
+        fch.assign(fchp[fr.nfront], 0);
+        std::vector<i64> cp(fchp.begin(), fchp.end() - 1);
+        for (i64 f = 0; f < fr.nfront; ++f) if (fr.parent[f] >= 0) fch[cp[fr.parent[f]]++] = f;
+        for (i64 f = 0; f < fr.nfront; ++f) {
+            i64 rows = fr.nres[f] + (sbrp[f + 1] - sbrp[f]);
+            for (i64 k = fchp[f]; k < fchp[f + 1]; ++k) rows += fnsep[fch[k]];
+            sworksz = std::max(sworksz, rows * (fr.nres[f] + fnsep[f]));
+        }
+    }
     std::vector<i64> kind(nv), cx(nv + 1, 0);
     std::vector<double> kpar(nv);
     i64 wmax = 1;
@@ -467,6 +503,8 @@ static int plan_instance(const mb_problem* P, const mb_settings& set, const doub
     ip.frel = pk.i32.put(to32(frel));
     ip.Blongr = pk.i32.put(to32(Blongr)); ip.Blongc = pk.i32.put(to32(Blongc));
     ip.hlong = pk.i32.put(to32(hlong)); ip.hflag = pk.i32.put(to32(hflag));
+    ip.sbrp = pk.i32.put(to32(sbrp)); ip.sbrow = pk.i32.put(to32(sbrow)); ip.sbloc = pk.i32.put(to32(sbloc));
+    ip.fchp = pk.i32.put(to32(fchp)); ip.fch = pk.i32.put(to32(fch));
     // i64 arena
     ip.hdoff = pk.i64a.put(hdoff); ip.hdpos = pk.i64a.put(hdpos); ip.qoffpos = pk.i64a.put(qoffpos);
     ip.qd0off = pk.i64a.put(qd0off);
@@ -491,6 +529,7 @@ static int plan_instance(const mb_problem* P, const mb_settings& set, const doub
     ip.uhist = pk.work.take(set.refine_max_iter + 2); ip.cghist = pk.work.take(set.newton_max_iter + 1);
     ip.cache = pk.work.take(std::max<i64>(cx[nv], 1)); ip.cache2 = pk.work.take(std::max<i64>(cx[nv], 1));
     ip.wf = pk.work.take(n); ip.wg = pk.work.take(m); ip.wp = pk.work.take(n); ip.wd = pk.work.take(n); ip.wy = pk.work.take(m);
+    ip.swork = pk.work.take(sworksz);
     size_t esz = set.precision == MB_PREC_FP32 ? 4 : 8;   // mixed needs room for the FP64 factor
     ip.F = (pk.fbytes + 255) / 256 * 256;
     pk.fbytes = ip.F + fr.fsize * esz;
@@ -515,11 +554,11 @@ static void merge(Packed& dst, Packed& src) {
     for (size_t* f : {&ip.xcol, &ip.colvtx, &ip.cfront, &ip.Brptr, &ip.Bcidx, &ip.Bcptr, &ip.Bridx, &ip.Bcpos,
                       &ip.Qrptr, &ip.Qcidx, &ip.Qcptr, &ip.Qridx, &ip.Qcpos, &ip.hdld, &ip.qoffk, &ip.kind,
                       &ip.fres0, &ip.fnres, &ip.fnsep, &ip.fparent, &ip.fsepp, &ip.fsep, &ip.frel,
-                      &ip.Blongr, &ip.Blongc, &ip.hlong, &ip.hflag}) *f += b32;
+                      &ip.Blongr, &ip.Blongc, &ip.hlong, &ip.hflag, &ip.sbrp, &ip.sbrow, &ip.sbloc, &ip.fchp, &ip.fch}) *f += b32;
     for (size_t* f : {&ip.hdoff, &ip.hdpos, &ip.qoffpos, &ip.cxblk, &ip.fptr, &ip.qd0off}) *f += b64;
     for (size_t* f : {&ip.Bval, &ip.Qval, &ip.Qd, &ip.f, &ip.g, &ip.kpar, &ip.p, &ip.d, &ip.y}) *f += bin;
     for (size_t* f : {&ip.wBval, &ip.wQval, &ip.wQd, &ip.Hd, &ip.Finit, &ip.pscl, &ip.yscl, &ip.vn, &ip.vm, &ip.vv,
-                      &ip.work, &ip.uhist, &ip.cghist, &ip.cache, &ip.cache2, &ip.wf, &ip.wg, &ip.wp, &ip.wd, &ip.wy}) *f += bw;
+                      &ip.work, &ip.uhist, &ip.cghist, &ip.cache, &ip.cache2, &ip.wf, &ip.wg, &ip.wp, &ip.wd, &ip.wy, &ip.swork}) *f += bw;
     for (size_t* f : {&ip.po, &ip.dout, &ip.yo, &ip.scal, &ip.hist}) *f += bo;
     ip.status += bs;
     size_t fb = (dst.fbytes + 255) / 256 * 256;
@@ -665,11 +704,11 @@ static void merge_all(Packed& dst, std::vector<Packed>& src, int nth) {
             for (size_t* f : {&ip.xcol, &ip.colvtx, &ip.cfront, &ip.Brptr, &ip.Bcidx, &ip.Bcptr, &ip.Bridx, &ip.Bcpos,
                               &ip.Qrptr, &ip.Qcidx, &ip.Qcptr, &ip.Qridx, &ip.Qcpos, &ip.hdld, &ip.qoffk, &ip.kind,
                               &ip.fres0, &ip.fnres, &ip.fnsep, &ip.fparent, &ip.fsepp, &ip.fsep, &ip.frel,
-                      &ip.Blongr, &ip.Blongc, &ip.hlong, &ip.hflag}) *f += b32[k];
+                      &ip.Blongr, &ip.Blongc, &ip.hlong, &ip.hflag, &ip.sbrp, &ip.sbrow, &ip.sbloc, &ip.fchp, &ip.fch}) *f += b32[k];
             for (size_t* f : {&ip.hdoff, &ip.hdpos, &ip.qoffpos, &ip.cxblk, &ip.fptr, &ip.qd0off}) *f += b64[k];
             for (size_t* f : {&ip.Bval, &ip.Qval, &ip.Qd, &ip.f, &ip.g, &ip.kpar, &ip.p, &ip.d, &ip.y}) *f += bin[k];
             for (size_t* f : {&ip.wBval, &ip.wQval, &ip.wQd, &ip.Hd, &ip.Finit, &ip.pscl, &ip.yscl, &ip.vn, &ip.vm, &ip.vv,
-                              &ip.work, &ip.uhist, &ip.cghist, &ip.cache, &ip.cache2, &ip.wf, &ip.wg, &ip.wp, &ip.wd, &ip.wy}) *f += bw[k];
+                              &ip.work, &ip.uhist, &ip.cghist, &ip.cache, &ip.cache2, &ip.wf, &ip.wg, &ip.wp, &ip.wd, &ip.wy, &ip.swork}) *f += bw[k];
             for (size_t* f : {&ip.po, &ip.dout, &ip.yo, &ip.scal, &ip.hist}) *f += bo[k];
             ip.status += bs[k];
             ip.F += bf[k];
@@ -688,7 +727,8 @@ static int make_batch(mb_ctx* ctx, mb_problem* const* probs, int32_t nprob, cons
     if (!ctx || !out || nprob < 0 || (nprob > 0 && !probs)) return fail(ctx, MB_E_ARG, "bad arguments");
     mb_settings s;
     if (set) s = *set; else mb_settings_default(&s);
-    if (s.stable) return fail(ctx, MB_E_UNSUPPORTED, "stable=true (StableUzawaSolver) is not available");
+    if (s.stable && s.precision != MB_PREC_FP64)
+        return fail(ctx, MB_E_UNSUPPORTED, "stable=true (StableUzawaSolver) factors in FP64: precision must be 0");
     if (s.max_iter < 0 || s.refine_max_iter < 0 || s.newton_max_iter < 0) return fail(ctx, MB_E_ARG, "negative iteration limit");
     if (s.precision < 0 || s.precision > 2) return fail(ctx, MB_E_ARG, "precision must be 0 (FP64), 1 (FP32) or 2 (mixed)");
     auto b = std::make_unique<mb_batch>();
@@ -738,7 +778,7 @@ static int run_batch(mb_batch* b, int mode, int32_t grid, float* ms) {
     std::memcpy(&s, &b->set, sizeof(s));
     CUDA_TRY(ctx, cudaSetDevice(ctx->device));
     // a lone large instance runs on the whole GPU (grid-cooperative mode)
-    const bool coop = ninst == 1 && (b->set.large == 1 || (b->set.large == 0 && b->pk.plans[0].fflops >= MB_LARGE_FLOPS));
+    const bool coop = ninst == 1 && !b->set.stable && (b->set.large == 1 || (b->set.large == 0 && b->pk.plans[0].fflops >= MB_LARGE_FLOPS));
     if (coop && !b->d_coop) CUDA_TRY(ctx, cudaMalloc((void**)&b->d_coop, sizeof(mb::CoopCtl)));
     cudaStream_t st = b->stream();
     CUDA_TRY(ctx, cudaEventRecord(b->e0, st));
@@ -1467,6 +1507,8 @@ mb::DevInst static_devinst(const InstPlan& p, int32_t* i32, i64* q64, double* dn
     I.fptr = (const int64_t*)(q64 + p.fptr); I.fsepp = i32 + p.fsepp; I.fsep = i32 + p.fsep; I.frel = i32 + p.frel;
     I.fsize = p.fsize;
     I.Finit = wk + p.Finit; I.F = F + p.F;
+    I.sbrp = i32 + p.sbrp; I.sbrow = i32 + p.sbrow; I.sbloc = i32 + p.sbloc; I.fchp = i32 + p.fchp; I.fch = i32 + p.fch;
+    I.swork = wk + p.swork;
     I.f0 = dn + p.f; I.g0 = dn + p.g; I.p0 = dn + p.p; I.d0 = dn + p.d; I.y0 = dn + p.y;
     I.f = wk + p.wf; I.g = wk + p.wg; I.pscl = wk + p.pscl; I.yscl = wk + p.yscl;
     I.p = wk + p.wp; I.d = wk + p.wd; I.y = wk + p.wy;
@@ -1506,7 +1548,8 @@ extern "C" int mb_batch_solve_static(mb_ctx* ctx, mb_problem* const* probs, int3
     if (!ctx || nprob < 0 || (nprob > 0 && !probs)) return fail(ctx, MB_E_ARG, "bad arguments");
     mb_settings s;
     if (settings) s = *settings; else mb_settings_default(&s);
-    if (s.stable) return fail(ctx, MB_E_UNSUPPORTED, "stable=true (StableUzawaSolver) is not available");
+    if (s.stable && s.precision != MB_PREC_FP64)
+        return fail(ctx, MB_E_UNSUPPORTED, "stable=true (StableUzawaSolver) factors in FP64: precision must be 0");
     if (s.max_iter < 0 || s.refine_max_iter < 0 || s.newton_max_iter < 0) return fail(ctx, MB_E_ARG, "negative iteration limit");
     if (s.precision < 0 || s.precision > 2) return fail(ctx, MB_E_ARG, "precision must be 0 (FP64), 1 (FP32) or 2 (mixed)");
     for (int32_t k = 0; k < nprob; ++k) if (!probs[k]) return fail(ctx, MB_E_ARG, "null problem");
@@ -1865,7 +1908,8 @@ int mb_server_create(mb_ctx* ctx, const mb_settings* settings, int64_t arena_byt
     if (!ctx || !out || arena_bytes <= 0 || capacity <= 0) return fail(ctx, MB_E_ARG, "bad arguments");
     mb_settings s;
     if (settings) s = *settings; else mb_settings_default(&s);
-    if (s.stable) return fail(ctx, MB_E_UNSUPPORTED, "stable=true (StableUzawaSolver) is not available");
+    if (s.stable && s.precision != MB_PREC_FP64)
+        return fail(ctx, MB_E_UNSUPPORTED, "stable=true (StableUzawaSolver) factors in FP64: precision must be 0");
     if (s.precision < 0 || s.precision > 2) return fail(ctx, MB_E_ARG, "precision must be 0, 1 or 2");
     auto sv = std::make_unique<mb_server>();
     sv->ctx = ctx; sv->set = s; sv->cap = capacity;

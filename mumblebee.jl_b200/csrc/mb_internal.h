@@ -96,6 +96,11 @@ struct DevInst {
     int64_t fsize;
     double* Finit;          // fsize doubles: lower part of BᵀB in front layout, built on the device
     void* F;                // fsize FT (double or float)
+    // stable factor (settings.stable): rows of B per front (sbrp[f] .. sbrp[f+1] of sbrow), the front
+    // position of each CSR entry of B in its row's front, the children of each front (fchp / fch),
+    // and the scratch of one front's stacked QR system
+    const int* sbrp; const int* sbrow; const int* sbloc; const int* fchp; const int* fch;
+    double* swork;
     // pristine vectors and working copies
     const double* f0; const double* g0; const double* p0; const double* d0; const double* y0;
     double* f; double* g;

@@ -112,6 +112,30 @@ __device__ __noinline__ int diag_factor(FT* M, int nf, int k0, int kb, Shared& s
     return flag;
 }
 
+// The inverses of the 32 x 32 diagonal blocks of a front whose residual columns already hold L
+// (the stable factor writes L directly): the layout diag_factor leaves, a warp per block, lane c
+// forming column c of X = L⁻¹ in the same axpy order and storing X[k][c], k > c, at M[k0 + c, k0 + k].
+__device__ __noinline__ void front_block_inverses(double* M, int nf, int nres) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int b = warp; b * 32 < nres; b += NW) {
+        const int k0 = b * 32, kb = min(32, nres - k0), c = lane;
+        double acc[32];
+#pragma unroll
+        for (int i = 0; i < 32; ++i) acc[i] = 0.0;
+#pragma unroll
+        for (int k = 0; k < 32; ++k) {
+            if (k >= kb) continue;
+            const double dk = 1.0 / M[(k0 + k) + (int64_t)(k0 + k) * nf];
+            const double xk = k < c ? 0.0 : (k == c ? dk : -acc[k] * dk);
+            if (k > c && c < kb) M[(k0 + c) + (int64_t)(k0 + k) * nf] = xk;
+#pragma unroll
+            for (int i = k + 1; i < 32; ++i)
+                if (i < kb) acc[i] = fma(M[(k0 + i) + (int64_t)(k0 + k) * nf], xk, acc[i]);
+        }
+    }
+    __syncthreads();
+}
+
 // Panel solve L21 = A21 L11^{-T} for the rows [k0 + kb, nf) owned by this rank (row blocks of NT
 // rows dealt round-robin over nranks CTAs), multiplying by the reciprocal pivots.  With `load`, the
 // factored diagonal block is first read back from M into sh.diag (a helper CTA that did not
@@ -1692,8 +1716,138 @@ struct Ctx {
         return 0;
     }
 
+    // ---- stable factor  (kkt/uzawa.jl:117-163; utils.jl:186-200) ----------------------------
+    // F Fᵀ = δ H + Bᵀ B without forming BᵀB.  Front by front, the stacked system
+    //   W = [ √δ U_v  for the front's vertices (U_vᵀ U_v = H_vv, a Cholesky per nonzero diagonal
+    //                 block, as cholblockdiag!; a zero block gives no rows) ;
+    //         the rows of B whose first column lies in the front ;
+    //         each child's R triangle over its separator ]
+    // has WᵀW = the front's part of δH + BᵀB plus what its descendants pass up, and its Householder
+    // QR gives R with RᵀR = WᵀW: the front's rows of R, signed to a positive diagonal, are the
+    // factor's columns (the rank-m update of √δ·chol(H) by the rows of B that the reference's
+    // lowrankupdate! makes, in exact arithmetic), and the trailing triangle goes to the parent,
+    // kept in the upper triangle of the front's separator block.  Returns 0, the 1-based column
+    // of a zero pivot, or -1 when a nonzero diagonal block of H is not positive definite.  FP64.
+    __device__ int stable_factor(double dl) {
+        double* F = F64;
+        const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+        const double sd = sqrt(dl);
+        double* W = I.swork;
+        for (int f = 0; f < I.nfront; ++f) {
+            const int nres = I.fnres[f], nsep = I.fnsep[f], nfr = nres + nsep, r0 = I.fres0[f];
+            const int b0 = I.sbrp[f], nb = I.sbrp[f + 1] - b0;
+            int rows = nres + nb;
+            for (int k = I.fchp[f]; k < I.fchp[f + 1]; ++k) rows += I.fnsep[I.fch[k]];
+            const int64_t ld = rows;
+            for (int64_t t = tid; t < ld * nfr; t += NT) W[t] = 0.0;
+            __syncthreads();
+            // √δ U_v in rows and columns [c0, c0 + nc) of W
+            const int v1 = nres > 0 ? I.colvtx[r0 + nres - 1] + 1 : 0;
+            for (int v = nres > 0 ? I.colvtx[r0] : 0; v < v1; ++v) {
+                const int c0 = I.xcol[v] - r0, nc = I.xcol[v + 1] - I.xcol[v];
+                const double* h = I.Hd + I.hdoff[v];   // lower triangle read
+                int nz = 0;
+                for (int t = tid; t < nc * nc; t += NT) nz |= (t % nc >= t / nc && h[t] != 0.0);
+                if (!__syncthreads_or(nz)) continue;
+                for (int t = tid; t < nc * nc; t += NT) {
+                    const int i = t % nc, j = t / nc;
+                    if (i <= j) W[(c0 + i) + (int64_t)(c0 + j) * ld] = h[j + i * nc];
+                }
+                for (int j = 0; j < nc; ++j) {
+                    __syncthreads();
+                    double* Wjj = W + (c0 + j) + (int64_t)(c0 + j) * ld;
+                    const double dd = *Wjj;
+                    if (!(dd > 0.0)) return -1;
+                    const double u = sqrt(dd), ru = 1.0 / u;
+                    __syncthreads();
+                    for (int k = j + 1 + tid; k < nc; k += NT) Wjj[(int64_t)(k - j) * ld] *= ru;
+                    if (tid == 0) *Wjj = u;
+                    __syncthreads();
+                    const int mt = nc - j - 1;
+                    for (int t = tid; t < mt * mt; t += NT) {
+                        const int i = j + 1 + t % mt, k = j + 1 + t / mt;
+                        if (i <= k)
+                            W[(c0 + i) + (int64_t)(c0 + k) * ld] -= W[(c0 + j) + (int64_t)(c0 + i) * ld] * W[(c0 + j) + (int64_t)(c0 + k) * ld];
+                    }
+                }
+                __syncthreads();
+                for (int t = tid; t < nc * nc; t += NT) {
+                    const int i = t % nc, j = t / nc;
+                    if (i <= j) W[(c0 + i) + (int64_t)(c0 + j) * ld] *= sd;
+                }
+            }
+            // the front's rows of B, then the children's triangles
+            for (int t = tid; t < nb; t += NT) {
+                const int i = I.sbrow[b0 + t];
+                for (int k = I.B.rptr[i]; k < I.B.rptr[i + 1]; ++k) W[(nres + t) + (int64_t)I.sbloc[k] * ld] = I.B.val[k];
+            }
+            int rc = nres + nb;
+            for (int q = I.fchp[f]; q < I.fchp[f + 1]; ++q) {
+                const int c = I.fch[q], cres = I.fnres[c], cs = I.fnsep[c], cn = cres + cs;
+                const double* Mc = F + I.fptr[c];
+                const int* rel = I.frel + I.fsepp[c];
+                for (int t = tid; t < cs * cs; t += NT) {
+                    const int r = t % cs, j = t / cs;
+                    if (r <= j) W[(rc + r) + (int64_t)rel[j] * ld] = Mc[(cres + r) + (int64_t)(cres + j) * cn];
+                }
+                rc += cs;
+            }
+            __syncthreads();
+            if (rows < nres) return r0 + rows + 1;
+            // Householder QR: column j's reflector v = (a − β, w[j+1..]), β = −sign(a)‖w[j..]‖,
+            // applied as w_k −= (vᵀw_k) / (β(β − a)) v, a warp per column
+            const int jmax = min(rows, nfr);
+            for (int j = 0; j < jmax; ++j) {
+                double* wj = W + (int64_t)j * ld;
+                const double a = wj[j];
+                double s = 0.0;
+                for (int i = j + 1 + tid; i < rows; i += NT) s += wj[i] * wj[i];
+                s = block_reduce(s, red, OpSum(), 0.0);
+                double beta = a;
+                if (s > 0.0) {
+                    const double nrm = sqrt(a * a + s);
+                    beta = a > 0.0 ? -nrm : nrm;
+                    const double cf = 1.0 / (beta * (beta - a));
+                    if (tid == 0) wj[j] = a - beta;
+                    __syncthreads();
+                    for (int k = j + 1 + warp; k < nfr; k += NW) {
+                        double* wk = W + (int64_t)k * ld;
+                        double dt = 0.0;
+                        for (int i = j + lane; i < rows; i += 32) dt += wj[i] * wk[i];
+                        dt = warp_sum(dt) * cf;
+                        for (int i = j + lane; i < rows; i += 32) wk[i] -= dt * wj[i];
+                    }
+                    __syncthreads();
+                    if (tid == 0) wj[j] = beta;
+                }
+                if (j < nres && !(fabs(beta) > 0.0)) return r0 + j + 1;
+            }
+            __syncthreads();
+            double* M = F + I.fptr[f];
+            for (int64_t t = tid; t < (int64_t)nfr * nres; t += NT) {
+                const int i = (int)(t % nfr), j = (int)(t / nfr);
+                if (i >= j) M[t] = (W[j + (int64_t)j * ld] < 0.0 ? -1.0 : 1.0) * W[j + (int64_t)i * ld];
+            }
+            for (int t = tid; t < nsep * nsep; t += NT) {
+                const int r = t % nsep, c = t / nsep;
+                if (r <= c) M[(nres + r) + (int64_t)(nres + c) * nfr] = nres + r < jmax ? W[(nres + r) + (int64_t)(nres + c) * ld] : 0.0;
+            }
+            __syncthreads();
+            front_block_inverses(M, nfr, nres);
+        }
+        return 0;
+    }
+
     __device__ bool initkkt(double dl, double& rho) {
         delta = dl;
+        if (set.stable) {   // StableUzawaSolver: no ρ retry (uzawa.jl:162 returns zero(T))
+            long long ta = tic();
+            const int info = stable_factor(dl);
+            toc(SEC_FUPD, ta);
+            nfact++;
+            rho = 0;
+            return info == 0;
+        }
         long long ta = tic();
         assemble(dl, 0.0);
         toc(SEC_ASSEMBLE, ta);

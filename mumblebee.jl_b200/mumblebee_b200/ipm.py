@@ -102,7 +102,7 @@ class IPMSettings:
     refine_max_iter: int = 10
     newton_max_iter: int = 100
     aug_tol: float = 1e-7
-    stable: bool = False
+    stable: bool = False             # StableUzawaSolver factor (FP64 only; Q block-diagonal)
     infeas_abs: float = 1e-8
     infeas_rel: float = 1e-8
     precision: str = "fp64"          # "fp64", "fp32" or "mixed" (factor precision; refinement stays FP64)

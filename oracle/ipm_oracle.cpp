@@ -790,8 +790,121 @@ static void mulkkt(const Solver& s, double* u, double* v, const BSM& A, const do
     gemvN(s.B, x, v, 1, 0);
 }
 
+// StableUzawaSolver's initkkt! (uzawa.jl:117-163; cholblockdiag! utils.jl:186-200): F Fᵀ = δH + BᵀB
+// without forming BᵀB.  The reference factors each nonzero diagonal block of H (failing when one is
+// not positive definite), scales by √δ and updates by the rows of B (CliqueTrees lowrankupdate!,
+// absent here).  Restated as multifrontal Householder QR: front f stacks √δ U_v (U_vᵀU_v = H_vv) for
+// its vertices, the rows of B whose first nonzero column lies in f, and each child's R triangle over
+// its separator; R of that stack satisfies RᵀR = WᵀW, its first nres rows (signed to a positive
+// diagonal) are the factor's columns and the trailing triangle passes to the parent.  In exact
+// arithmetic this is the unique Cholesky factor the rank-m update produces.  Returns 0, the 1-based
+// column of a zero pivot, or -1 for a diagonal block of H that is not positive definite.
+static int stable_factor(Solver& s, double delta) {
+    const Symbolic& S = s.S;
+    const BSM& B = s.B;
+    const BSM& H = s.H;
+    const double sd = std::sqrt(delta);
+    // rows of B: nonzeros in ascending column order, assigned to the front of the first column
+    std::vector<std::vector<std::pair<i64, double>>> brow(B.nrow);
+    for (i64 v = 0; v < B.nvtx; ++v)
+        for (i64 jl = 0; jl < B.ncols(v); ++jl)
+            for (i64 e = B.xsrc[v]; e < B.xsrc[v + 1]; ++e) {
+                i64 u = B.tgt[e], nr = B.nrows(u);
+                const double* blk = B.val.data() + B.xblk[e] + jl * nr;
+                for (i64 il = 0; il < nr; ++il)
+                    if (blk[il] != 0) brow[B.xrow[u] + il].push_back({B.xcol[v] + jl, blk[il]});
+            }
+    std::vector<std::vector<i64>> frows(S.nfront), fch(S.nfront);
+    for (i64 i = 0; i < B.nrow; ++i) {
+        if (brow[i].empty()) continue;
+        std::sort(brow[i].begin(), brow[i].end());
+        frows[S.colfront[brow[i][0].first]].push_back(i);
+    }
+    for (i64 f = 0; f < S.nfront; ++f) if (S.parent[f] >= 0) fch[S.parent[f]].push_back(f);
+    std::vector<double> W;
+    for (i64 f = 0; f < S.nfront; ++f) {
+        const i64 nres = S.nres[f], nsep = (i64)S.sep[f].size(), nf = nres + nsep, r0 = S.res0[f];
+        i64 rows = nres + (i64)frows[f].size();
+        for (i64 c : fch[f]) rows += (i64)S.sep[c].size();
+        const i64 ld = rows;
+        W.assign((size_t)(ld * nf), 0.0);
+        auto w = [&](i64 i, i64 j) -> double& { return W[(size_t)(i + j * ld)]; };
+        auto pos = [&](i64 col) -> i64 {
+            if (col >= r0 && col < r0 + nres) return col - r0;
+            auto it = std::lower_bound(S.sep[f].begin(), S.sep[f].end(), col);
+            return nres + (i64)(it - S.sep[f].begin());
+        };
+        for (i64 v = S.fvtx[f]; v < S.fvtx[f + 1]; ++v) {
+            const i64 c0 = B.xcol[v] - r0, nc = B.ncols(v);
+            const double* h = nullptr;
+            for (i64 e = H.xsrc[v]; e < H.xsrc[v + 1]; ++e) if (H.tgt[e] == v) h = H.val.data() + H.xblk[e];
+            if (!h) continue;
+            bool nz = false;
+            for (i64 j = 0; j < nc; ++j) for (i64 i = j; i < nc; ++i) nz |= h[i + j * nc] != 0.0;
+            if (!nz) continue;
+            for (i64 j = 0; j < nc; ++j) for (i64 i = 0; i <= j; ++i) w(c0 + i, c0 + j) = h[j + i * nc];
+            for (i64 j = 0; j < nc; ++j) {   // upper Cholesky in place: UᵀU = H_vv
+                const double dd = w(c0 + j, c0 + j);
+                if (!(dd > 0.0)) return -1;
+                const double u = std::sqrt(dd), ru = 1.0 / u;
+                for (i64 k = j + 1; k < nc; ++k) w(c0 + j, c0 + k) *= ru;
+                w(c0 + j, c0 + j) = u;
+                for (i64 k = j + 1; k < nc; ++k)
+                    for (i64 i = j + 1; i <= k; ++i) w(c0 + i, c0 + k) -= w(c0 + j, c0 + i) * w(c0 + j, c0 + k);
+            }
+            for (i64 j = 0; j < nc; ++j) for (i64 i = 0; i <= j; ++i) w(c0 + i, c0 + j) *= sd;
+        }
+        i64 rc = nres;
+        for (i64 i : frows[f]) {
+            for (const auto& e : brow[i]) w(rc, pos(e.first)) = e.second;
+            ++rc;
+        }
+        for (i64 c : fch[f]) {
+            const i64 cres = S.nres[c], cs = (i64)S.sep[c].size(), cn = cres + cs;
+            const double* Mc = s.F.val.data() + S.fptr[c];
+            for (i64 j = 0; j < cs; ++j)
+                for (i64 r = 0; r <= j; ++r) w(rc + r, S.rel[c][j]) = Mc[(cres + r) + (cres + j) * cn];
+            rc += cs;
+        }
+        if (rows < nres) return (int)(r0 + rows + 1);
+        const i64 jmax = std::min(rows, nf);
+        for (i64 j = 0; j < jmax; ++j) {   // Householder: v = (a − β, w[j+1..]), β = −sign(a)‖w[j..]‖
+            const double a = w(j, j);
+            double ss = 0.0;
+            for (i64 i = j + 1; i < rows; ++i) ss += w(i, j) * w(i, j);
+            double beta = a;
+            if (ss > 0.0) {
+                const double nrm = std::sqrt(a * a + ss);
+                beta = a > 0.0 ? -nrm : nrm;
+                const double cf = 1.0 / (beta * (beta - a));
+                w(j, j) = a - beta;
+                for (i64 k = j + 1; k < nf; ++k) {
+                    double dt = 0.0;
+                    for (i64 i = j; i < rows; ++i) dt += w(i, j) * w(i, k);
+                    dt *= cf;
+                    for (i64 i = j; i < rows; ++i) w(i, k) -= dt * w(i, j);
+                }
+                w(j, j) = beta;
+            }
+            if (j < nres && !(std::fabs(beta) > 0.0)) return (int)(r0 + j + 1);
+        }
+        double* M = s.F.val.data() + S.fptr[f];
+        for (i64 j = 0; j < nres; ++j) {
+            const double sg = w(j, j) < 0.0 ? -1.0 : 1.0;
+            for (i64 i = j; i < nf; ++i) M[i + j * nf] = sg * w(j, i);
+        }
+        for (i64 c = 0; c < nsep; ++c)
+            for (i64 r = 0; r <= c; ++r) M[(nres + r) + (nres + c) * nf] = nres + r < jmax ? w(nres + r, nres + c) : 0.0;
+    }
+    return 0;
+}
+
 static bool initkkt(Solver& s, double delta, double& rho) {
     s.delta = delta;
+    if (s.set.stable) {   // no ρ retry (uzawa.jl:162)
+        rho = 0;
+        return stable_factor(s, delta) == 0;
+    }
     auto assemble = [&]() {
         std::fill(s.F.val.begin(), s.F.val.end(), 0.0);
         scatter_add(s.F, s.L, 1.0);

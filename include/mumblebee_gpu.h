@@ -23,6 +23,8 @@
  *   mb_solver_frule2        frule2!(…, s, Δf1, Δg1, Δμ1, Δf2, Δg2, Δμ2)    src/IPM/src/ipm/differential.jl:82-260
  *   mb_batch_solve          solve(prob, settings) over many problems      src/IPM/src/ipm/solver/ipm.jl:798-804
  *   mb_settings             IPMSettings                                    src/IPM/src/ipm/settings/ipm.jl:1-18
+ *   mb_extmul / mb_twomul   extmul!(c, A, b, α, β), twomul!(c, cc, A, b, α, β)
+ *                                                                          src/BlockSparseArrays/src/comp/comp.jl:280-311
  */
 #ifndef MUMBLEBEE_GPU_H
 #define MUMBLEBEE_GPU_H
@@ -278,6 +280,25 @@ int mb_server_result(mb_server* s, int64_t ticket, double* p, double* d, double*
 /* queued, planned, running, completed, failed, kernel launches, arena bytes in use, arena bytes */
 int mb_server_stats(mb_server* s, int64_t* stats8);
 int mb_server_destroy(mb_server* s);
+
+/* ---- compensated block-sparse products --------------------------------------------------------
+ * extmul!(c, A, b, α, β[, s, cs]) and twomul!(c, cc, A, b, α, β[, s, cs]) of BlockSparseArrays
+ * (src/comp/comp.jl:280-311, src/comp/twogemv.jl:87-121): c ← α op(A) b + β c with op(A) = A
+ * (trans = 0) or Aᵀ (trans = 1), phase 1 accumulated with error-free transformations.  extmul
+ * leaves c as accurate as if computed in doubled precision and rounded once; twomul leaves the
+ * normalized pair (c, cc) whose hi part equals extmul's c bitwise.  Each output entry takes its
+ * terms in the reference's order, so results are bitwise those of the reference.  b has ncol
+ * (trans = 0) or nrow (trans = 1) entries, c / cc the other count; c is read only when β ≠ 0; s
+ * and cs (both or neither) receive the unscaled pair of op(A) b.  Host buffers; the call returns
+ * when the outputs are written. */
+typedef struct mb_matrix mb_matrix;
+/* uploads A (mb_bsm, 1-based) once, as scalar CSR and CSC views of all its stored block entries */
+int mb_matrix_create(mb_ctx* ctx, const mb_bsm* A, mb_matrix** out);
+int mb_matrix_destroy(mb_matrix* A);
+int mb_extmul(mb_matrix* A, int32_t trans, const double* b, double alpha, double beta, double* c,
+              double* s, double* cs);
+int mb_twomul(mb_matrix* A, int32_t trans, const double* b, double alpha, double beta, double* c,
+              double* cc, double* s, double* cs);
 
 #ifdef __cplusplus
 }

@@ -20,11 +20,12 @@ NVCC = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-lineinfo"]
 
-SOURCES_CU = ["mb_solver.cu"]
+SOURCES_CU = ["mb_solver.cu", "mb_comp.cu"]
 SOURCES_CPP = ["mb_host.cpp"]
 # headers each source includes (a change rebuilds only the sources that use it)
 DEPS = {
     "mb_solver.cu": ["mb_internal.h", "mb_device.cuh", "mb_cones.cuh", "mb_tdc.cuh", "mb_sdp.cuh"],
+    "mb_comp.cu": ["mb_internal.h"],
     "mb_host.cpp": ["mb_internal.h", "mb_symbolic.hpp"],
 }
 HEADERS = sorted({h for v in DEPS.values() for h in v})

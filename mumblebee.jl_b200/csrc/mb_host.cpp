@@ -30,6 +30,7 @@ extern "C" int mb_launch_batch(const mb::DevInst* d_inst, int ninst, int mode, c
 extern "C" int mb_launch_coop(const mb::DevInst* d_inst, int mode, const mb::Settings* set, mb::CoopCtl* d_ctl,
                               int grid, cudaStream_t stream);
 extern "C" int mb_coop_grid(int device, int nsm);
+extern "C" int mb_launch_twomv(const mb::TwoMv* a, cudaStream_t st);
 
 using mbh::i64;
 
@@ -915,6 +916,131 @@ static int read_bsm(mb_ctx* ctx, const mb_bsm* A, mbh::BSM& R, const char* name)
     }
     for (i64 u = 0; u < R.nout; ++u) if (R.xrow[u] > R.xrow[u + 1]) return fail(ctx, MB_E_ARG, std::string(name) + ": xrow not monotone");
     return MB_OK;
+}
+
+// ---- compensated products: extmul! / twomul! (BlockSparseArrays/src/comp/comp.jl:280-311) ------
+// A BlockSparseMatrix resident on the device as two scalar views of ALL its stored block entries
+// (explicit zeros too, as the reference's block loops visit them): the CSR with each row's
+// columns ascending (the order twogemv_impl! adds into an entry of A b) and the CSC with each
+// column's rows ascending plus block marks (the order, and the register pairs, of Aᵀ b).
+struct mb_matrix {
+    mb_ctx* ctx = nullptr;
+    i64 nrow = 0, ncol = 0, nnz = 0;
+    int64_t* rptr = nullptr; int32_t* cidx = nullptr; double* rval = nullptr;
+    int64_t* cptr = nullptr; int32_t* ridx = nullptr; double* cval = nullptr; unsigned char* brk = nullptr;
+    double* vec = nullptr;   // b | c | cc | s | cs, max(nrow, ncol) each
+    ~mb_matrix() {
+        for (void* p : {(void*)rptr, (void*)cidx, (void*)rval, (void*)cptr, (void*)ridx, (void*)cval, (void*)brk, (void*)vec})
+            if (p) cudaFree(p);
+    }
+};
+
+int mb_matrix_create(mb_ctx* ctx, const mb_bsm* A, mb_matrix** out) {
+    if (!ctx || !A || !out) return fail(ctx, MB_E_ARG, "bad arguments");
+    mbh::BSM R;
+    if (int rc = read_bsm(ctx, A, R, "A")) return rc;
+    if (R.nbnz > INT64_C(0x7fffffff) || R.nrow > INT64_C(0x7fffffff) || R.ncol > INT64_C(0x7fffffff))
+        return fail(ctx, MB_E_ARG, "A: more than 2^31 - 1 rows, columns or stored entries");
+    const i64 nr = R.nrow, nc = R.ncol, nz = R.nbnz;
+    std::vector<int64_t> rptr(nr + 1, 0), cptr(nc + 1, 0);
+    for (i64 v = 0; v < R.nvtx; ++v)
+        for (i64 e = R.xsrc[v]; e < R.xsrc[v + 1]; ++e) {
+            const i64 u = R.tgt[e];
+            for (i64 i = R.xrow[u]; i < R.xrow[u + 1]; ++i) rptr[i + 1] += R.ncols(v);
+            for (i64 j = R.xcol[v]; j < R.xcol[v + 1]; ++j) cptr[j + 1] += R.nrows(u);
+        }
+    for (i64 i = 0; i < nr; ++i) rptr[i + 1] += rptr[i];
+    for (i64 j = 0; j < nc; ++j) cptr[j + 1] += cptr[j];
+    std::vector<int32_t> cidx(nz), ridx(nz);
+    std::vector<double> rval(nz), cval(nz);
+    std::vector<unsigned char> brk(nz, 0);
+    std::vector<int64_t> rpos(rptr.begin(), rptr.end() - 1), cpos(cptr.begin(), cptr.end() - 1);
+    // vertices, arcs and columns ascending: each row receives its entries in ascending column order,
+    // each column its blocks in ascending target order
+    for (i64 v = 0; v < R.nvtx; ++v)
+        for (i64 e = R.xsrc[v]; e < R.xsrc[v + 1]; ++e) {
+            const i64 u = R.tgt[e], r0 = R.xrow[u], nru = R.nrows(u), ncv = R.ncols(v);
+            const double* blk = R.val.data() + R.xblk[e];
+            for (i64 jl = 0; jl < ncv; ++jl) {
+                const i64 j = R.xcol[v] + jl;
+                for (i64 il = 0; il < nru; ++il) {
+                    const double a = blk[il + jl * nru];
+                    const i64 q = rpos[r0 + il]++;
+                    cidx[q] = (int32_t)j; rval[q] = a;
+                    const i64 t = cpos[j]++;
+                    ridx[t] = (int32_t)(r0 + il); cval[t] = a;
+                    if (il == 0) brk[t] = (nru == 1 && ncv == 1) ? 2 : 1;
+                }
+            }
+        }
+    auto m = std::make_unique<mb_matrix>();
+    m->ctx = ctx; m->nrow = nr; m->ncol = nc; m->nnz = nz;
+    CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+    auto up = [&](auto*& d, const auto& h) -> cudaError_t {
+        const size_t bytes = std::max<size_t>(h.size(), 1) * sizeof(h[0]);
+        cudaError_t e = cudaMalloc((void**)&d, bytes);
+        if (e == cudaSuccess && !h.empty()) e = cudaMemcpyAsync(d, h.data(), h.size() * sizeof(h[0]), cudaMemcpyHostToDevice, ctx->stream);
+        return e;
+    };
+    CUDA_TRY(ctx, up(m->rptr, rptr)); CUDA_TRY(ctx, up(m->cidx, cidx)); CUDA_TRY(ctx, up(m->rval, rval));
+    CUDA_TRY(ctx, up(m->cptr, cptr)); CUDA_TRY(ctx, up(m->ridx, ridx)); CUDA_TRY(ctx, up(m->cval, cval));
+    CUDA_TRY(ctx, up(m->brk, brk));
+    CUDA_TRY(ctx, cudaMalloc((void**)&m->vec, 5 * (size_t)std::max<i64>(std::max(nr, nc), 1) * sizeof(double)));
+    CUDA_TRY(ctx, cudaStreamSynchronize(ctx->stream));
+    *out = m.release();
+    return MB_OK;
+}
+
+int mb_matrix_destroy(mb_matrix* A) {
+    if (!A) return MB_E_ARG;
+    cudaSetDevice(A->ctx->device);
+    delete A;
+    return MB_OK;
+}
+
+// c ← α op(A) b + β c through host buffers: b and (β ≠ 0) c in, c (and cc, s, cs) out
+static int twomv(mb_matrix* A, int32_t trans, const double* b, double alpha, double beta, double* c, double* cc,
+                 double* s, double* cs) {
+    if (!A) return MB_E_ARG;
+    mb_ctx* ctx = A->ctx;
+    const i64 nin = trans ? A->nrow : A->ncol, nout = trans ? A->ncol : A->nrow;
+    if ((nin > 0 && !b) || (nout > 0 && !c) || (s == nullptr) != (cs == nullptr))
+        return fail(ctx, MB_E_ARG, "null vector (b and c are required; s and cs go together)");
+    CUDA_TRY(ctx, cudaSetDevice(ctx->device));
+    const size_t w = (size_t)std::max<i64>(std::max(A->nrow, A->ncol), 1);
+    double* db = A->vec; double* dc = db + w; double* dcc = dc + w; double* ds = dcc + w; double* dcs = ds + w;
+    cudaStream_t st = ctx->stream;
+    if (nin > 0) CUDA_TRY(ctx, cudaMemcpyAsync(db, b, nin * sizeof(double), cudaMemcpyHostToDevice, st));
+    if (beta != 0.0 && nout > 0) CUDA_TRY(ctx, cudaMemcpyAsync(dc, c, nout * sizeof(double), cudaMemcpyHostToDevice, st));
+    mb::TwoMv a{};
+    a.nout = nout; a.trans = trans ? 1 : 0;
+    a.acls = alpha == 1.0 ? 1 : (alpha == -1.0 ? 2 : 0);
+    a.bcls = beta == 0.0 ? 0 : (beta == 1.0 ? 1 : (beta == -1.0 ? 2 : 3));
+    a.ptr = trans ? A->cptr : A->rptr; a.idx = trans ? A->ridx : A->cidx; a.val = trans ? A->cval : A->rval;
+    a.brk = A->brk; a.b = db; a.alpha = alpha; a.beta = beta;
+    a.c = dc; a.cc = cc ? dcc : nullptr; a.s = s ? ds : nullptr; a.cs = s ? dcs : nullptr;
+    CUDA_TRY(ctx, (cudaError_t)mb_launch_twomv(&a, st));
+    if (nout > 0) {
+        CUDA_TRY(ctx, cudaMemcpyAsync(c, dc, nout * sizeof(double), cudaMemcpyDeviceToHost, st));
+        if (cc) CUDA_TRY(ctx, cudaMemcpyAsync(cc, dcc, nout * sizeof(double), cudaMemcpyDeviceToHost, st));
+        if (s) {
+            CUDA_TRY(ctx, cudaMemcpyAsync(s, ds, nout * sizeof(double), cudaMemcpyDeviceToHost, st));
+            CUDA_TRY(ctx, cudaMemcpyAsync(cs, dcs, nout * sizeof(double), cudaMemcpyDeviceToHost, st));
+        }
+    }
+    CUDA_TRY(ctx, cudaStreamSynchronize(st));
+    return MB_OK;
+}
+
+int mb_extmul(mb_matrix* A, int32_t trans, const double* b, double alpha, double beta, double* c, double* s,
+              double* cs) {
+    return twomv(A, trans, b, alpha, beta, c, nullptr, s, cs);
+}
+
+int mb_twomul(mb_matrix* A, int32_t trans, const double* b, double alpha, double beta, double* c, double* cc,
+              double* s, double* cs) {
+    if (!cc && A) return fail(A->ctx, MB_E_ARG, "cc is required");
+    return twomv(A, trans, b, alpha, beta, c, cc, s, cs);
 }
 
 int mb_problem_create(mb_ctx* ctx, const mb_bsm* Q, const mb_bsm* B, const double* f, const double* g, double mu,

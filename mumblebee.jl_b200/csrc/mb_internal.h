@@ -161,5 +161,19 @@ struct CoopCtl {
 enum CoopCmd { COOP_NONE = 0, COOP_EXIT = 1, COOP_FILL = 2, COOP_COPY = 3, COOP_UPDATE = 4, COOP_PANEL = 5,
                COOP_EXTEND = 6, COOP_LROWS = 7, COOP_UDOTS = 8, COOP_SCHUR = 9 };
 
+// One compensated product c ← α op(A) b + β c (extmul! / twomul!), a thread per output: N walks
+// the CSR of A's stored entries, T the CSC with block marks (brk: 1 opens a block of the column,
+// 2 opens a 1 x 1 block).  cc == nullptr: folded result (extmul!); else the pair (twomul!).
+// s, cs (nullable) receive phase 1's pair.  acls / bcls classify α and β as the reference's
+// epilogue branches do (acls 1: α = 1, 2: α = -1, 0 else; bcls 0: β = 0, 1: β = 1, 2: β = -1, 3 else).
+struct TwoMv {
+    int64_t nout;
+    int trans, acls, bcls;
+    const int64_t* ptr; const int32_t* idx; const double* val; const unsigned char* brk;
+    const double* b;
+    double alpha, beta;
+    double* c; double* cc; double* s; double* cs;
+};
+
 
 }  // namespace mb

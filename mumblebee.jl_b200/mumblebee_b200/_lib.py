@@ -92,6 +92,10 @@ SIGNATURES = {
     "mb_server_result": (I32, [C.c_void_p, I64, PF64, PF64, PF64, C.POINTER(mb_result), PF64]),
     "mb_server_stats": (I32, [C.c_void_p, PI64]),
     "mb_server_destroy": (I32, [C.c_void_p]),
+    "mb_matrix_create": (I32, [C.c_void_p, C.POINTER(mb_bsm), C.POINTER(C.c_void_p)]),
+    "mb_matrix_destroy": (I32, [C.c_void_p]),
+    "mb_extmul": (I32, [C.c_void_p, I32, PF64, F64, F64, PF64, PF64, PF64]),
+    "mb_twomul": (I32, [C.c_void_p, I32, PF64, F64, F64, PF64, PF64, PF64, PF64]),
     "mb_batch_solve_static": (I32, [C.c_void_p, C.POINTER(C.c_void_p), I32, C.POINTER(mb_settings), I32,
                                     C.POINTER(PF64), C.POINTER(PF64), C.POINTER(PF64), C.POINTER(mb_result)]),
 }

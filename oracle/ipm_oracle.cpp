@@ -1397,11 +1397,26 @@ static void startingpoint(Solver& s) {
     for (i64 i = 0; i < n; ++i) { s.p[i] *= sp; s.d[i] *= sd; }
 }
 
+#include "oracle_comp.hpp"
+
 }  // namespace orc
 
 using namespace orc;
 
 extern "C" {
+
+// extmul! (pair = 0) / twomul! (pair = 1) of BlockSparseArrays on the host (comp.jl:280-311):
+// c ← α op(A) b + β c with op = transpose when trans; s, cs (nullable) get phase 1's pair
+int oracle_twomul(const ob_bsm* Ac, int trans, const double* b, double alpha, double beta, double* c, double* cc,
+                  double* s, double* cs) {
+    const BSM A = from_c(Ac);
+    const i64 nout = trans ? A.ncol : A.nrow;
+    std::vector<double> sv(nout), csv(nout);
+    c_twogemv(A, trans != 0, b, sv.data(), csv.data());
+    if (s) { std::copy(sv.begin(), sv.end(), s); std::copy(csv.begin(), csv.end(), cs); }
+    c_epilogue(nout, c, cc, alpha, sv.data(), csv.data(), beta, cc != nullptr);
+    return 0;
+}
 
 int oracle_set_blas(const char* path, int nthreads) {
     void* h = dlopen(path, RTLD_NOW | RTLD_LOCAL);

@@ -124,6 +124,7 @@ def lib(threads: int = 1):
         L.oracle_sdp_probe.restype = C.c_int
         L.oracle_sdp_eig.argtypes = [C.c_int, PD, C.c_double, PD, PD, PD, PD]
         L.oracle_sdp_eig.restype = C.c_int
+        L.oracle_twomul.argtypes = [C.POINTER(BSM), C.c_int, PD, C.c_double, C.c_double, PD, PD, PD, PD]
         L.oracle_set_blas.argtypes = [C.c_char_p, C.c_int]
         L.oracle_set_threads.argtypes = [C.c_int]
         path = find_openblas()
@@ -251,6 +252,20 @@ class OracleSolver:
 def solve(prob, settings=None, vperm=None, **kw):
     s = OracleSolver(prob, settings, vperm, **kw)
     return s.solve()
+
+
+def twomul(A, trans, b, alpha, beta, c, pair):
+    """extmul! (pair False) or twomul! (pair True) on the host: returns (c, cc or None, s, cs); c is
+    a copy of the input c, updated."""
+    keep = []
+    Ab = bsm_struct(A, keep)
+    nout = A["ncol"] if trans else A["nrow"]
+    b = np.ascontiguousarray(b, dtype=np.float64)
+    c = np.array(c, dtype=np.float64, copy=True)
+    cc = np.zeros(nout) if pair else None
+    s, cs = np.zeros(nout), np.zeros(nout)
+    lib(0).oracle_twomul(C.byref(Ab), int(trans), _pd(b), float(alpha), float(beta), _pd(c), _pd(cc), _pd(s), _pd(cs))
+    return c, cc, s, cs
 
 
 def sdp_probe(p, d, Dp, Dd, sm):

@@ -63,6 +63,11 @@ def parse():
     ap.add_argument("--serve-nmin", type=int, default=100)
     ap.add_argument("--serve-nmax", type=int, default=2000)
     ap.add_argument("--serve-arena-gb", type=int, default=32)
+    ap.add_argument("--extras", default="", choices=["", "stable", "comp", "all"],
+                    help="instead of the main line: one JSON line each for the stable factor against the default "
+                         "one, and for the compensated products (1 GPU)")
+    ap.add_argument("--extras-count", type=int, default=1184, help="instances of the stable-factor arm")
+    ap.add_argument("--comp-rows", type=int, default=1 << 20, help="rows = columns of the compensated-product matrix")
     return ap.parse_args()
 
 
@@ -328,9 +333,89 @@ def serve_arm(args, ctx):
             "arena_gb": args.serve_arena_gb, "precision": args.precision}
 
 
+def stable_arm(args, ctx):
+    """The StableUzawaSolver factor against the default one on the same portfolio instances: one
+    persistent launch per step, CUDA-event time, FP64."""
+    from mumblebee_b200.ipm import Batch, IPMSettings
+    probs, sizes = make_problems(args.extras_count, args.seed, 0, ctx)
+    out = {"extra": "stable_factor", "workload": WORKLOAD, "instances": len(probs), "steps": args.steps,
+           "warmup": args.warmup, "unit": "solves/s"}
+    for name, st in (("default", IPMSettings()), ("stable", IPMSettings(stable=True))):
+        batch = Batch(probs, st, ctx=ctx)
+        for _ in range(args.warmup):
+            batch.run()
+        ms = [batch.run() for _ in range(args.steps)]
+        res = batch.fetch(want_vectors=False)
+        out[name] = {"solves_per_s": len(probs) / (statistics.mean(ms) / 1e3), "ms_per_step": statistics.mean(ms),
+                     "optimal": sum(r.status.name == "OPTIMAL" for r in res),
+                     "near_optimal": sum(r.status.name == "NEAR_OPTIMAL" for r in res),
+                     "iters_mean": float(np.mean([r.niter for r in res])),
+                     "factorizations_mean": float(np.mean([r.nfactor for r in res]))}
+        del batch
+    out["stable_over_default"] = out["stable"]["solves_per_s"] / out["default"]["solves_per_s"]
+    print(json.dumps(out), flush=True)
+
+
+def comp_arm(args, ctx):
+    """extmul! with A and Aᵀ on a square block-sparse matrix of 4 x 4 blocks, up to 8 random
+    target blocks per column block (N(0,1) entries), α = 1, β = 0: host-synchronous calls through
+    the C ABI (b uploaded, c read back each call).  The kernel's own duration comes from an ncu
+    launch list of the same command; the algorithmic bytes of one launch are printed for it."""
+    from mumblebee_b200.comp import BlockSparseMatrix, extmul
+    rng = np.random.default_rng(args.seed)
+    nb, per = 4, 8
+    n = args.comp_rows // nb * nb
+    nblk = n // nb
+    t = np.sort(rng.integers(0, nblk, size=(nblk, per)), axis=1)
+    keep = np.ones_like(t, dtype=bool)
+    keep[:, 1:] = np.diff(t, axis=1) > 0
+    cnt = keep.sum(axis=1)
+    tgt = t[keep]
+    narc = int(tgt.size)
+    xb = np.concatenate([[0], np.cumsum(cnt)])
+    d = dict(nout=nblk, nvtx=nblk, narc=narc, ncol=n, nrow=n, nbnz=narc * nb * nb,
+             xsrc=xb + 1, xcol=np.arange(nblk + 1, dtype=np.int64) * nb + 1,
+             xrow=np.arange(nblk + 1, dtype=np.int64) * nb + 1,
+             xblk=np.arange(narc + 1, dtype=np.int64) * nb * nb + 1, tgt=tgt + 1,
+             val=rng.standard_normal(narc * nb * nb))
+    t0 = time.time()
+    A = BlockSparseMatrix(d, ctx=ctx)
+    t_up = time.time() - t0
+    b = rng.standard_normal(n)
+    c = np.zeros(n)
+    nnz = narc * nb * nb
+    out = {"extra": "compensated_products", "kernel": "twomv_kernel", "rows": n, "cols": n, "stored_entries": nnz,
+           "block": f"{nb}x{nb}, up to {per} target blocks per column block", "alpha": 1.0, "beta": 0.0,
+           "upload_s": t_up, "calls": args.steps}
+    for name, op, extra in (("A_b", A, 0), ("At_b", A.T, nnz)):
+        for _ in range(args.warmup):
+            extmul(c, op, b, 1.0, 0.0)
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            extmul(c, op, b, 1.0, 0.0)
+        sec = (time.perf_counter() - t0) / args.steps
+        alg = 12 * nnz + extra + 8 * (n + 1) + 8 * n + 8 * n   # ptr, idx + val (+ block marks), b, c
+        out[name] = {"call_ms": sec * 1e3, "algorithmic_bytes_per_launch": alg, "h2d_d2h_bytes_per_call": 16 * n}
+    peaks = os.path.join(os.path.dirname(os.path.abspath(__file__)), "MEASURED_PEAKS.json")
+    if os.path.exists(peaks):
+        with open(peaks) as f:
+            out["hbm_peak_gbs"] = {"value": json.load(f).get("hbm_gbs"), "source": "measured"}
+    else:
+        out["hbm_peak_gbs"] = {"value": 6650.0, "source": "fallback"}
+    print(json.dumps(out), flush=True)
+
+
 def main():
     args = parse()
     ws, rank, local, pg = dist_setup(args)
+    if args.extras:
+        from mumblebee_b200.ipm import Context
+        ctx = Context.default(local)
+        if args.extras in ("stable", "all"):
+            stable_arm(args, ctx)
+        if args.extras in ("comp", "all"):
+            comp_arm(args, ctx)
+        return
     if args.impl == "reference":
         run_reference(args, ws, rank)
         if pg is not None:

@@ -1760,9 +1760,14 @@ struct Ctx {
                     if (!(dd > 0.0)) return -1;
                     const double u = sqrt(dd), ru = 1.0 / u;
                     __syncthreads();
-                    for (int k = j + 1 + tid; k < nc; k += NT) Wjj[(int64_t)(k - j) * ld] *= ru;
+                    int nzr = 0;
+                    for (int k = j + 1 + tid; k < nc; k += NT) {
+                        const double x = Wjj[(int64_t)(k - j) * ld] * ru;
+                        Wjj[(int64_t)(k - j) * ld] = x;
+                        nzr |= x != 0.0;
+                    }
                     if (tid == 0) *Wjj = u;
-                    __syncthreads();
+                    if (!__syncthreads_or(nzr)) continue;   // an empty row updates nothing (a diagonal block)
                     const int mt = nc - j - 1;
                     for (int t = tid; t < mt * mt; t += NT) {
                         const int i = j + 1 + t % mt, k = j + 1 + t / mt;
@@ -1795,13 +1800,16 @@ struct Ctx {
             __syncthreads();
             if (rows < nres) return r0 + rows + 1;
             // Householder QR: column j's reflector v = (a − β, w[j+1..]), β = −sign(a)‖w[j..]‖,
-            // applied as w_k −= (vᵀw_k) / (β(β − a)) v, a warp per column
+            // applied as w_k −= (vᵀw_k) / (β(β − a)) v, a warp per column.  The vertex rows form an
+            // upper triangle that no reflector fills (each touches row j and the rows from nres
+            // on), so v lives on row j and rows [lo, rows), lo = max(j + 1, nres).
             const int jmax = min(rows, nfr);
             for (int j = 0; j < jmax; ++j) {
                 double* wj = W + (int64_t)j * ld;
                 const double a = wj[j];
+                const int lo = max(j + 1, nres), cnt = 1 + rows - lo;
                 double s = 0.0;
-                for (int i = j + 1 + tid; i < rows; i += NT) s += wj[i] * wj[i];
+                for (int i = lo + tid; i < rows; i += NT) s += wj[i] * wj[i];
                 s = block_reduce(s, red, OpSum(), 0.0);
                 double beta = a;
                 if (s > 0.0) {
@@ -1813,9 +1821,15 @@ struct Ctx {
                     for (int k = j + 1 + warp; k < nfr; k += NW) {
                         double* wk = W + (int64_t)k * ld;
                         double dt = 0.0;
-                        for (int i = j + lane; i < rows; i += 32) dt += wj[i] * wk[i];
+                        for (int t = lane; t < cnt; t += 32) {
+                            const int i = t == 0 ? j : lo + t - 1;
+                            dt += wj[i] * wk[i];
+                        }
                         dt = warp_sum(dt) * cf;
-                        for (int i = j + lane; i < rows; i += 32) wk[i] -= dt * wj[i];
+                        for (int t = lane; t < cnt; t += 32) {
+                            const int i = t == 0 ? j : lo + t - 1;
+                            wk[i] -= dt * wj[i];
+                        }
                     }
                     __syncthreads();
                     if (tid == 0) wj[j] = beta;

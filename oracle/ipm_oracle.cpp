@@ -847,8 +847,10 @@ static int stable_factor(Solver& s, double delta) {
                 const double dd = w(c0 + j, c0 + j);
                 if (!(dd > 0.0)) return -1;
                 const double u = std::sqrt(dd), ru = 1.0 / u;
-                for (i64 k = j + 1; k < nc; ++k) w(c0 + j, c0 + k) *= ru;
+                bool nzr = false;
+                for (i64 k = j + 1; k < nc; ++k) { w(c0 + j, c0 + k) *= ru; nzr |= w(c0 + j, c0 + k) != 0.0; }
                 w(c0 + j, c0 + j) = u;
+                if (!nzr) continue;   // an empty row updates nothing (a diagonal block)
                 for (i64 k = j + 1; k < nc; ++k)
                     for (i64 i = j + 1; i <= k; ++i) w(c0 + i, c0 + k) -= w(c0 + j, c0 + i) * w(c0 + j, c0 + k);
             }
@@ -868,10 +870,13 @@ static int stable_factor(Solver& s, double delta) {
         }
         if (rows < nres) return (int)(r0 + rows + 1);
         const i64 jmax = std::min(rows, nf);
-        for (i64 j = 0; j < jmax; ++j) {   // Householder: v = (a − β, w[j+1..]), β = −sign(a)‖w[j..]‖
+        // Householder: v = (a − β, w[j+1..]), β = −sign(a)‖w[j..]‖.  The vertex rows form an upper
+        // triangle that no reflector fills, so v lives on row j and rows [lo, rows), lo = max(j + 1, nres).
+        for (i64 j = 0; j < jmax; ++j) {
             const double a = w(j, j);
+            const i64 lo = std::max(j + 1, nres);
             double ss = 0.0;
-            for (i64 i = j + 1; i < rows; ++i) ss += w(i, j) * w(i, j);
+            for (i64 i = lo; i < rows; ++i) ss += w(i, j) * w(i, j);
             double beta = a;
             if (ss > 0.0) {
                 const double nrm = std::sqrt(a * a + ss);
@@ -879,10 +884,11 @@ static int stable_factor(Solver& s, double delta) {
                 const double cf = 1.0 / (beta * (beta - a));
                 w(j, j) = a - beta;
                 for (i64 k = j + 1; k < nf; ++k) {
-                    double dt = 0.0;
-                    for (i64 i = j; i < rows; ++i) dt += w(i, j) * w(i, k);
+                    double dt = w(j, j) * w(j, k);
+                    for (i64 i = lo; i < rows; ++i) dt += w(i, j) * w(i, k);
                     dt *= cf;
-                    for (i64 i = j; i < rows; ++i) w(i, k) -= dt * w(i, j);
+                    w(j, k) -= dt * w(j, j);
+                    for (i64 i = lo; i < rows; ++i) w(i, k) -= dt * w(i, j);
                 }
                 w(j, j) = beta;
             }

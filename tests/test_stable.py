@@ -8,12 +8,13 @@ exact arithmetic both give the unique Cholesky factor).  Tolerances:
   solves stop at their forcing tolerance, so the history rows move apart at about that level.
   The first four rows are held to 1e-5 relative, the final objective to 1e-7.
 - device vs oracle (both stable): the same algorithm with different reduction orders and FMA
-  contraction.  The portfolio and SDP cases meet the bar of the default path: the first four
+  contraction.  The portfolio cases and sdp4x3 meet the bar of the default path: the first four
   history rows to 1e-6 relative, same status and iteration count, objectives within 1e-9 relative,
-  iterates within 1e-6 relative.  socp_small tracks its first four rows to 1e-6, then ends optimal
-  or near-optimal with objectives within 1e-6.  Its endgame is decided by rounding: the per-vertex
-  Cholesky of an SOC Hessian at μ ≈ 1e-7 (condition ≈ 1e14), as cholblockdiag! runs it in the
-  reference, passes on one side and fails on the other.  The exponential and power cases get the
+  iterates within 1e-6 relative.  socp_small and sdp1x10 track their first four rows to 1e-6, then
+  end optimal or near-optimal with objectives within 1e-6.  Their endgames are decided by rounding:
+  the per-vertex Cholesky of an SOC Hessian or of an SDP block's W ⊗ₛ W at μ ≈ 1e-7 (condition
+  ≈ 1/μ² ≈ 1e14), as cholblockdiag! runs it in the reference, passes on one side and fails on the
+  other, and which side depends on the reduction order.  The exponential and power cases get the
   default path's bar for those cones: the certified step (nflog3 bands) moves with the rounding of
   the direction from the first iteration on, so iteration counts within 2, and objectives within
   1e-6 at an optimal or near-optimal end.
@@ -76,7 +77,7 @@ def test_oracle_stable_zero_pivot_fails():
     assert o1["status"] == "NUMERICAL_FAILURE" and o1["niter"] == 1
 
 
-ENDGAME = ("socp_small",)
+ENDGAME = ("socp_small", "sdp1x10")
 
 
 @pytest.mark.gpu

@@ -148,3 +148,57 @@ def test_stable_rejections():
     coupled = IPMProblem.from_dict(block_problem(pb), ctx=ctx)
     with pytest.raises(_lib.MBError, match="off-diagonal"):
         solve(coupled, IPMSettings(stable=True))
+
+
+# Sensitivities under the stable factor: frule! / rrule! / frule2! call initkkt! (differential.jl:7,
+# 94, 260), which the stable setting routes to its own factor.  At the barrier points of μ′ = 0.05
+# (a well-conditioned KKT matrix) the stable and default factors give the same tangents up to the
+# rules' solve tolerance, and the device's stable rules follow the oracle's as the default ones do.
+SENS = ("port", "sdp")
+
+
+def _barrier(name):
+    from test_sensitivities import BARRIER, TOLS
+    return BARRIER[name](), TOLS[name]
+
+
+@pytest.mark.parametrize("name", SENS)
+def test_oracle_stable_rules_match_default(name):
+    from test_sensitivities import _adjoint_gap, _seeds, _seeds2
+    pb, tol = _barrier(name)
+    ref = block_problem(pb)
+    o0, r0 = oracle_solve(ref, **tol)
+    o1, r1 = oracle_solve(ref, stable=1, **tol)
+    assert r0["status"] == r1["status"] == "OPTIMAL"
+    n, m = len(r1["p"]), len(r1["y"])
+    assert _adjoint_gap(o1.frule, o1.rrule, n, m) < 1e-4
+    (df, dg, dmu), _ = _seeds(n, m, 2)
+    for a, b in zip(o1.frule(df, dg, dmu), o0.frule(df, dg, dmu)):
+        assert np.linalg.norm(a - b) <= 1e-5 * max(1.0, np.linalg.norm(b))
+    seeds = _seeds2(n, m, 1)
+    for a, b in zip(o1.frule2(*seeds), o0.frule2(*seeds)):
+        assert np.linalg.norm(a - b) <= 1e-5 * max(1.0, np.linalg.norm(b))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("name", SENS)
+def test_device_stable_rules_match_oracle(name):
+    from test_sensitivities import _adjoint_gap, _seeds, _seeds2
+    pb, tol = _barrier(name)
+    ref = block_problem(pb)
+    prob = IPMProblem.from_dict(ref, ctx=Context.default())
+    o, ro = oracle_solve(ref, vperm=prob.symbolic()["vperm"], stable=1, **tol)
+    s = init(prob, IPMSettings(stable=True, **tol))
+    r = s.solve()
+    assert r.status.name == ro["status"] == "OPTIMAL"
+    n, m = len(r.p), len(r.y)
+    assert _adjoint_gap(s.frule, s.rrule, n, m) < 1e-4
+    (df, dg, dmu), (wp, wy, wd) = _seeds(n, m, 2)
+    for a, b in zip(s.frule(df, dg, dmu), o.frule(df, dg, dmu)):
+        assert np.linalg.norm(a - b) <= 1e-5 * max(1.0, np.linalg.norm(b))
+    da, db = s.rrule(wp, wy, wd), o.rrule(wp, wy, wd)
+    for a, b in zip(da[:2], db[:2]):
+        assert np.linalg.norm(a - b) <= 1e-5 * max(1.0, np.linalg.norm(b))
+    seeds = _seeds2(n, m, 1)
+    for a, b in zip(s.frule2(*seeds), o.frule2(*seeds)):
+        assert np.linalg.norm(a - b) <= 1e-5 * max(1.0, np.linalg.norm(b))

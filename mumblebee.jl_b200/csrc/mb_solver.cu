@@ -1818,17 +1818,26 @@ struct Ctx {
                     const double cf = 1.0 / (beta * (beta - a));
                     if (tid == 0) wj[j] = a - beta;
                     __syncthreads();
+                    // the reflector's support staged in shared memory when it fits, so that only w_k
+                    // comes from global memory; the same values in the same order either way
+                    double* vs = sh.tile;
+                    const bool vsm = cnt <= XSM_CAP;
+                    if (vsm)
+                        for (int t = tid; t < cnt; t += NT) vs[t] = wj[t == 0 ? j : lo + t - 1];
+                    __syncthreads();
                     for (int k = j + 1 + warp; k < nfr; k += NW) {
                         double* wk = W + (int64_t)k * ld;
                         double dt = 0.0;
+#pragma unroll 4
                         for (int t = lane; t < cnt; t += 32) {
                             const int i = t == 0 ? j : lo + t - 1;
-                            dt += wj[i] * wk[i];
+                            dt += (vsm ? vs[t] : wj[i]) * wk[i];
                         }
                         dt = warp_sum(dt) * cf;
+#pragma unroll 4
                         for (int t = lane; t < cnt; t += 32) {
                             const int i = t == 0 ? j : lo + t - 1;
-                            wk[i] -= dt * wj[i];
+                            wk[i] -= dt * (vsm ? vs[t] : wj[i]);
                         }
                     }
                     __syncthreads();

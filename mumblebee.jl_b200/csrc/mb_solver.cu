@@ -136,6 +136,60 @@ __device__ __noinline__ void front_block_inverses(double* M, int nf, int nres) {
     __syncthreads();
 }
 
+// The stable factor's blocked Householder step: apply the reflectors of panel columns
+// [j0, j0 + np) to the trailing columns [j0 + np, nfr) of the column-major W (leading dimension
+// ld).  Reflector p lives on row j0 + p and rows [lo, lo + cnt - 1); its values are staged at
+// vs[p * cnt + t] (t = 0: the row j0 + p entry) and cf[p] is its scale (0: no reflection).  A warp
+// holds one trailing column in registers (rows [lo, ..) across the lanes as the unblocked loop
+// indexes them, the panel rows one per lane), applies the np reflectors in order with the same
+// per-lane accumulation, butterfly reduction and fused forms as applying them one at a time, and
+// stores the column once: the same values, with the trailing block read and written once per
+// panel instead of once per column.
+constexpr int QR_PANEL = 16;   // reflectors per panel
+constexpr int QR_SEG = 16;     // register slots per lane: supports of up to 32 * QR_SEG values
+__device__ __noinline__ void qr_apply_panel(double* W, int64_t ld, int nfr, int j0, int np, int lo, int cnt,
+                                            const double* vs, const double* cf) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int k = j0 + np + warp; k < nfr; k += NW) {
+        double* wk = W + (int64_t)k * ld;
+        double x[QR_SEG];
+#pragma unroll
+        for (int r = 0; r < QR_SEG; ++r) {
+            const int t = lane + 32 * r;
+            x[r] = (t >= 1 && t < cnt) ? wk[lo + t - 1] : 0.0;
+        }
+        double h = lane < np ? wk[j0 + lane] : 0.0;   // lane p: row j0 + p
+        for (int p = 0; p < np; ++p) {
+            const double c = cf[p];
+            if (c == 0.0) continue;
+            const double* v = vs + (int64_t)p * cnt;
+            const double h0 = __shfl_sync(0xffffffffu, h, p);
+            if (lane == 0) x[0] = h0;                   // slot t = 0 is row j0 + p
+            double dt = 0.0;
+#pragma unroll
+            for (int r = 0; r < QR_SEG; ++r) {
+                const int t = lane + 32 * r;
+                if (t < cnt) dt += v[t] * x[r];
+            }
+            dt = warp_sum(dt) * c;
+#pragma unroll
+            for (int r = 0; r < QR_SEG; ++r) {
+                const int t = lane + 32 * r;
+                if (t < cnt) x[r] -= dt * v[t];
+            }
+            const double hn = __shfl_sync(0xffffffffu, x[0], 0);
+            if (lane == p) h = hn;
+        }
+#pragma unroll
+        for (int r = 0; r < QR_SEG; ++r) {
+            const int t = lane + 32 * r;
+            if (t >= 1 && t < cnt) wk[lo + t - 1] = x[r];
+        }
+        if (lane < np) wk[j0 + lane] = h;
+    }
+    __syncthreads();
+}
+
 // Panel solve L21 = A21 L11^{-T} for the rows [k0 + kb, nf) owned by this rank (row blocks of NT
 // rows dealt round-robin over nranks CTAs), multiplying by the reciprocal pivots.  With `load`, the
 // factored diagonal block is first read back from M into sh.diag (a helper CTA that did not
@@ -1804,7 +1858,15 @@ struct Ctx {
             // upper triangle that no reflector fills (each touches row j and the rows from nres
             // on), so v lives on row j and rows [lo, rows), lo = max(j + 1, nres).
             const int jmax = min(rows, nfr);
-            for (int j = 0; j < jmax; ++j) {
+            // columns j < nres share the support size cntp; they go in panels of np reflectors when
+            // the panel's supports fit in shared memory and a column's in registers
+            const int cntp = 1 + rows - nres;
+            const int pmax = cntp <= 32 * QR_SEG ? min(QR_PANEL, XSM_CAP / cntp) : 1;
+            for (int j0 = 0; j0 < jmax;) {
+              const int np = (pmax > 1 && j0 < nres) ? min(pmax, min(nres, jmax) - j0) : 1;
+              const bool panel = np > 1;
+              const int kend = panel ? j0 + np : nfr;   // a panel's reflectors reach later columns in qr_apply_panel
+              for (int j = j0; j < j0 + np; ++j) {
                 double* wj = W + (int64_t)j * ld;
                 const double a = wj[j];
                 const int lo = max(j + 1, nres), cnt = 1 + rows - lo;
@@ -1820,12 +1882,13 @@ struct Ctx {
                     __syncthreads();
                     // the reflector's support staged in shared memory when it fits, so that only w_k
                     // comes from global memory; the same values in the same order either way
-                    double* vs = sh.tile;
+                    double* vs = sh.tile + (panel ? (j - j0) * cnt : 0);
                     const bool vsm = cnt <= XSM_CAP;
                     if (vsm)
                         for (int t = tid; t < cnt; t += NT) vs[t] = wj[t == 0 ? j : lo + t - 1];
+                    if (panel && tid == 0) sh.acc[j - j0] = cf;
                     __syncthreads();
-                    for (int k = j + 1 + warp; k < nfr; k += NW) {
+                    for (int k = j + 1 + warp; k < kend; k += NW) {
                         double* wk = W + (int64_t)k * ld;
                         double dt = 0.0;
 #pragma unroll 4
@@ -1842,8 +1905,16 @@ struct Ctx {
                     }
                     __syncthreads();
                     if (tid == 0) wj[j] = beta;
+                } else if (panel && tid == 0) {
+                    sh.acc[j - j0] = 0.0;
                 }
                 if (j < nres && !(fabs(beta) > 0.0)) return r0 + j + 1;
+              }
+              if (panel) {
+                  __syncthreads();
+                  qr_apply_panel(W, ld, nfr, j0, np, nres, cntp, sh.tile, sh.acc);
+              }
+              j0 += np;
             }
             __syncthreads();
             double* M = F + I.fptr[f];

@@ -150,42 +150,57 @@ constexpr int QR_SEG = 16;     // register slots per lane: supports of up to 32 
 __device__ __noinline__ void qr_apply_panel(double* W, int64_t ld, int nfr, int j0, int np, int lo, int cnt,
                                             const double* vs, const double* cf) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    for (int k = j0 + np + warp; k < nfr; k += NW) {
+    // two columns per warp (k and k + NW): their reflector chains are independent and interleave
+    for (int k = j0 + np + warp; k < nfr; k += 2 * NW) {
+        const bool two = k + NW < nfr;
         double* wk = W + (int64_t)k * ld;
-        double x[QR_SEG];
+        double* wl = W + (int64_t)(two ? k + NW : k) * ld;
+        double x[QR_SEG], y[QR_SEG];
 #pragma unroll
         for (int r = 0; r < QR_SEG; ++r) {
             const int t = lane + 32 * r;
-            x[r] = (t >= 1 && t < cnt) ? wk[lo + t - 1] : 0.0;
+            const bool in = t >= 1 && t < cnt;
+            x[r] = in ? wk[lo + t - 1] : 0.0;
+            y[r] = in ? wl[lo + t - 1] : 0.0;
         }
         double h = lane < np ? wk[j0 + lane] : 0.0;   // lane p: row j0 + p
+        double g = lane < np ? wl[j0 + lane] : 0.0;
         for (int p = 0; p < np; ++p) {
             const double c = cf[p];
             if (c == 0.0) continue;
             const double* v = vs + (int64_t)p * cnt;
             const double h0 = __shfl_sync(0xffffffffu, h, p);
-            if (lane == 0) x[0] = h0;                   // slot t = 0 is row j0 + p
-            double dt = 0.0;
+            const double g0 = __shfl_sync(0xffffffffu, g, p);
+            if (lane == 0) { x[0] = h0; y[0] = g0; }   // slot t = 0 is row j0 + p
+            double dt = 0.0, du = 0.0;
 #pragma unroll
             for (int r = 0; r < QR_SEG; ++r) {
                 const int t = lane + 32 * r;
-                if (t < cnt) dt += v[t] * x[r];
+                if (t < cnt) { dt += v[t] * x[r]; du += v[t] * y[r]; }
             }
             dt = warp_sum(dt) * c;
+            du = warp_sum(du) * c;
 #pragma unroll
             for (int r = 0; r < QR_SEG; ++r) {
                 const int t = lane + 32 * r;
-                if (t < cnt) x[r] -= dt * v[t];
+                if (t < cnt) { x[r] -= dt * v[t]; y[r] -= du * v[t]; }
             }
             const double hn = __shfl_sync(0xffffffffu, x[0], 0);
-            if (lane == p) h = hn;
+            const double gn = __shfl_sync(0xffffffffu, y[0], 0);
+            if (lane == p) { h = hn; g = gn; }
         }
 #pragma unroll
         for (int r = 0; r < QR_SEG; ++r) {
             const int t = lane + 32 * r;
-            if (t >= 1 && t < cnt) wk[lo + t - 1] = x[r];
+            if (t >= 1 && t < cnt) {
+                wk[lo + t - 1] = x[r];
+                if (two) wl[lo + t - 1] = y[r];
+            }
         }
-        if (lane < np) wk[j0 + lane] = h;
+        if (lane < np) {
+            wk[j0 + lane] = h;
+            if (two) wl[j0 + lane] = g;
+        }
     }
     __syncthreads();
 }

@@ -42,6 +42,8 @@ extern "C" {
 #define MB_E_NOMEM (-3)    /* device or host allocation failed */
 #define MB_E_STATE (-4)    /* call not valid in the handle's current state */
 #define MB_E_UNSUPPORTED (-5)
+#define MB_E_TIMEOUT (-6)  /* a bounded device-side wait ran out (a grid barrier of the grid-cooperative
+                              mode, settings.coop_wait): the solve was abandoned, the context stays usable */
 
 /* cone kinds (the AbstractCone subtypes of src/IPM/src/cone/) */
 #define MB_CONE_FREE 0     /* CofreeCone        cone/noc.jl */
@@ -93,6 +95,9 @@ typedef struct mb_settings {
     double aug_tol;            /* 1e-7 */
     double infeas_abs;         /* 1e-8 */
     double infeas_rel;         /* 1e-8 */
+    double coop_wait;          /* 60  seconds a CTA of the grid-cooperative mode waits at a grid barrier;
+                                      when a wait runs out every CTA returns and the call fails with
+                                      MB_E_TIMEOUT (<= 0: 60) */
 } mb_settings;
 
 /* BlockSparseMatrix{Float64,Int64} (BlockSparseArrays/src/block_sparse_matrix.jl:10-158), 1-based */
@@ -250,8 +255,12 @@ int mb_batch_destroy(mb_batch* b);
  * return MB_E_NOMEM before any device work, with the needed size in mb_last_error.
  * The scratch is one per device and per process: calls that overlap in time on one device (two
  * host threads, or two contexts on the same device) race on it and corrupt each other's results.
- * The first call on a device does the set-up (looks up the scratch address, which may load the
- * module); make it before any stream capture begins.  Arguments and outputs as mb_batch_solve. */
+ * Every call looks up the scratch's device address with that device current (the first call on a
+ * device may load the module, so make it before any stream capture begins); the lookup is repeated
+ * on each call, so a cudaDeviceReset by the host application between calls is harmless (the
+ * scratch then starts over with undefined contents, which every call overwrites before use).
+ * Arguments, outputs and the grid-cooperative rule for a lone large instance (settings.large) as
+ * mb_batch_solve; the control block of that mode lives in the scratch too. */
 #define MB_STATIC_SCRATCH_BYTES (32u << 20)
 int mb_batch_solve_static(mb_ctx* ctx, mb_problem* const* probs, int32_t nprob, const mb_settings* settings,
                           int32_t grid, double* const* p_out, double* const* d_out, double* const* y_out,

@@ -794,12 +794,17 @@ static int run_batch(mb_batch* b, int mode, int32_t grid, float* ms) {
     return MB_OK;
 }
 
+static const char* COOP_TIMEOUT_MSG =
+    "a grid-barrier wait of the grid-cooperative mode ran past settings.coop_wait; the solve was abandoned";
+
 static int fetch_batch(mb_batch* b) {
     mb_ctx* ctx = b->ctx;
     cudaStream_t st = b->stream();
     CUDA_TRY(ctx, cudaMemcpyAsync(b->h_out, b->d_out, std::max<size_t>(b->pk.out.size(), 1) * sizeof(double), cudaMemcpyDeviceToHost, st));
     CUDA_TRY(ctx, cudaMemcpyAsync(b->h_i32, b->d_ost, std::max<size_t>(b->pk.ost.size(), 1) * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
     CUDA_TRY(ctx, cudaStreamSynchronize(st));
+    for (const InstPlan& ip : b->pk.plans)
+        if (b->h_i32[ip.status + 7]) return fail(ctx, MB_E_TIMEOUT, COOP_TIMEOUT_MSG);
     return MB_OK;
 }
 
@@ -851,7 +856,7 @@ void mb_settings_default(mb_settings* s) {
     if (!s) return;
     std::memset(s, 0, sizeof(*s));
     s->verbose = 0; s->max_iter = 100; s->scale_max_iter = 10; s->refine_max_iter = 10; s->newton_max_iter = 100;
-    s->stable = 0; s->precision = MB_PREC_FP64; s->large = 0;
+    s->stable = 0; s->precision = MB_PREC_FP64; s->large = 0; s->coop_wait = 60.0;
     s->step_frac = 0.99; s->feas_tol = 1e-8; s->gap_tol = 1e-8; s->near_factor = 1000.0; s->stall_tol = 1e-3;
     s->refine_stall_tol = 0.5; s->aug_tol = 1e-7; s->infeas_abs = 1e-8; s->infeas_rel = 1e-8;
 }
@@ -1587,12 +1592,13 @@ namespace {
 
 // byte offsets of the batch's arrays inside the scratch, each rounded up to 256 bytes
 struct StaticLayout {
-    size_t inst, counter, ost, i32, i64a, din, work, out, F, total;
+    size_t inst, counter, coop, ost, i32, i64a, din, work, out, F, total;
     StaticLayout(const Packed& pk) {
         size_t off = 0;
         auto region = [&](size_t bytes) { size_t o = off; off += (std::max<size_t>(bytes, 1) + 255) / 256 * 256; return o; };
         inst = region(pk.plans.size() * sizeof(mb::DevInst));
         counter = region(sizeof(int));
+        coop = region(sizeof(mb::CoopCtl));
         ost = region(pk.ost.size() * sizeof(int32_t));
         i32 = region(pk.i32.size() * sizeof(int32_t));
         i64a = region(pk.i64a.size() * sizeof(i64));
@@ -1710,6 +1716,7 @@ extern "C" int mb_batch_solve_static(mb_ctx* ctx, mb_problem* const* probs, int3
     int32_t* s_ost = (int32_t*)(base + L.ost);
     mb::DevInst* s_inst = (mb::DevInst*)(base + L.inst);
     int* s_counter = (int*)(base + L.counter);
+    mb::CoopCtl* s_coop = (mb::CoopCtl*)(base + L.coop);
     std::vector<mb::DevInst> hi;
     hi.reserve(pk.plans.size());
     for (const InstPlan& p : pk.plans)
@@ -1727,13 +1734,19 @@ extern "C" int mb_batch_solve_static(mb_ctx* ctx, mb_problem* const* probs, int3
     int g = std::min(grid > 0 ? grid : ctx->nsm * mb::CTA_PER_SM, ninst);
     mb::Settings ds;
     std::memcpy(&ds, &s, sizeof(ds));
-    if (mb_launch_batch(s_inst, ninst, mb::MODE_SOLVE, &ds, s_counter, g, s.precision == MB_PREC_FP32, st))
-        return fail(ctx, MB_E_CUDA, std::string("launch failed: ") + cudaGetErrorString(cudaGetLastError()));
+    // the same choice as mb_batch_solve: a lone large instance runs grid-cooperatively, its control
+    // block in the scratch
+    const bool coop = ninst == 1 && !s.stable && (s.large == 1 || (s.large == 0 && pk.plans[0].fflops >= MB_LARGE_FLOPS));
+    const int lrc = coop ? mb_launch_coop(s_inst, mb::MODE_SOLVE, &ds, s_coop, mb_coop_grid(ctx->device, ctx->nsm), st)
+                         : mb_launch_batch(s_inst, ninst, mb::MODE_SOLVE, &ds, s_counter, g, s.precision == MB_PREC_FP32, st);
+    if (lrc) return fail(ctx, MB_E_CUDA, std::string("launch failed: ") + cudaGetErrorString(cudaGetLastError()));
     std::vector<double> h_out(std::max<size_t>(pk.out.size(), 1));
     std::vector<int32_t> h_ost(std::max<size_t>(pk.ost.size(), 1));
     CUDA_TRY(ctx, cudaMemcpyAsync(h_out.data(), s_out, h_out.size() * sizeof(double), cudaMemcpyDeviceToHost, st));
     CUDA_TRY(ctx, cudaMemcpyAsync(h_ost.data(), s_ost, h_ost.size() * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
     CUDA_TRY(ctx, cudaStreamSynchronize(st));
+    for (const InstPlan& ip : pk.plans)
+        if (h_ost[ip.status + 7]) return fail(ctx, MB_E_TIMEOUT, COOP_TIMEOUT_MSG);
     for (size_t k = 0; k < pk.plans.size(); ++k)
         static_unpack(pk.plans[k], h_out.data(), h_ost.data(), s.max_iter, p_out ? p_out[k] : nullptr,
                       d_out ? d_out[k] : nullptr, y_out ? y_out[k] : nullptr, results ? &results[k] : nullptr);

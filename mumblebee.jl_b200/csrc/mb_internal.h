@@ -24,6 +24,7 @@ enum CGStatus { CG_CONTINUE = 0, CG_SOLVED, CG_NUMERICAL_FAILURE, CG_ITMAX };
 struct Settings {
     int32_t verbose, max_iter, scale_max_iter, refine_max_iter, newton_max_iter, stable, precision, large;
     double step_frac, feas_tol, gap_tol, near_factor, stall_tol, refine_stall_tol, aug_tol, infeas_abs, infeas_rel;
+    double coop_wait;   // seconds at a grid barrier of the grid-cooperative mode (<= 0: 60)
 };
 
 // One history row: the 17 fields of IPMHistoryRow (history/ipm.jl:1-4), stored as doubles.

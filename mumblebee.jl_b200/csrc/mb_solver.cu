@@ -38,6 +38,7 @@ struct Shared {
     double tile[4 * TS * TLD];   // stage 0 A, B, stage 1 A, B of the front update; x slices in solves
     int flag;
     int ibuf[8];
+    long long wait_ns;      // grid-cooperative mode: longest wait at a grid barrier
 };
 
 // D += A·B on the FP64 tensor path (mma.m8n8k4, fragments: A[g][t], B[t][g], C[g][2t+i] with
@@ -557,7 +558,7 @@ __device__ void usolve_dots(const FT* M, int nf, int nres, int r0, const int* se
 }
 
 // ---- grid-cooperative help for large fronts (CoopCtl) ----------------------------------------
-constexpr long long COOP_WAIT_NS = 60000000000LL;   // longest wait at a grid barrier (60 s)
+constexpr long long COOP_WAIT_NS = 60000000000LL;   // default longest wait at a grid barrier (60 s)
 constexpr int COOP_MIN_FRONT = 192;                 // fronts from this order up use the helpers
 constexpr int COOP_MIN_SOLVE = 2048;                // ... and in the triangular solves from this order up
 
@@ -574,8 +575,8 @@ __device__ __forceinline__ unsigned long long gtimer() {
 }
 
 // Grid barrier over all CTAs of the cooperative launch.  Returns false (on every thread) once any
-// wait has timed out; the barrier then no longer waits.
-__device__ bool coop_barrier(CoopCtl* c) {
+// wait has run past sh.wait_ns; the barrier then no longer waits.
+__device__ bool coop_barrier(CoopCtl* c, const Shared& sh) {
     __syncthreads();
     if (threadIdx.x == 0 && ld_volatile_i32(&c->abort) == 0) {
         const unsigned int g = ld_acquire_u32(&c->gen);
@@ -590,7 +591,7 @@ __device__ bool coop_barrier(CoopCtl* c) {
             unsigned int nap = 100;   // ns; backs off to 8 us so idle helpers poll the hot word rarely
             while (ld_acquire_u32(&c->gen) == g) {
                 if (ld_volatile_i32(&c->abort) != 0) break;
-                if ((long long)(gtimer() - t0) > COOP_WAIT_NS) { atomicExch(&c->abort, 1); break; }
+                if ((long long)(gtimer() - t0) > sh.wait_ns) { atomicExch(&c->abort, 1); break; }
                 __nanosleep(nap);
                 if (nap < 8000) nap *= 2;
             }
@@ -659,22 +660,22 @@ __device__ void coop_exec(CoopCtl* c, Shared& sh, int rank, int nranks) {
 template <class Post>
 __device__ bool coop_call(CoopCtl* c, Shared& sh, Post post) {
     if (threadIdx.x == 0) post(c);
-    if (!coop_barrier(c)) return false;
+    if (!coop_barrier(c, sh)) return false;
     coop_exec(c, sh, 0, gridDim.x);
-    return coop_barrier(c);
+    return coop_barrier(c, sh);
 }
 
 // helpers: serve commands until COOP_EXIT or an abort
 __device__ void coop_helper(CoopCtl* c, Shared& sh) {
     for (;;) {
-        if (!coop_barrier(c)) return;
+        if (!coop_barrier(c, sh)) return;
         if (threadIdx.x == 0) sh.ibuf[0] = ((const volatile CoopCtl*)c)->cmd;
         __syncthreads();
         const int cmd = sh.ibuf[0];
         __syncthreads();
         if (cmd == COOP_EXIT) return;
         coop_exec(c, sh, blockIdx.x, gridDim.x);
-        if (!coop_barrier(c)) return;
+        if (!coop_barrier(c, sh)) return;
     }
 }
 
@@ -2591,6 +2592,8 @@ __global__ void __launch_bounds__(NT, CTA_PER_SM) ipm_batch_kernel(BatchArgs a) 
 __global__ void __launch_bounds__(NT, CTA_PER_SM) ipm_coop_kernel(BatchArgs a, CoopCtl* c) {
     extern __shared__ __align__(16) unsigned char mb_dsmem[];
     Shared& sh = *reinterpret_cast<Shared*>(mb_dsmem);
+    if (threadIdx.x == 0) sh.wait_ns = a.set.coop_wait > 0 ? (long long)(a.set.coop_wait * 1e9) : COOP_WAIT_NS;
+    __syncthreads();
     if (blockIdx.x != 0) { coop_helper(c, sh); return; }
     const DevInst& I = a.inst[0];
     const unsigned long long t0 = globaltimer();
@@ -2601,7 +2604,7 @@ __global__ void __launch_bounds__(NT, CTA_PER_SM) ipm_coop_kernel(BatchArgs a, C
         I.scal[SCAL_T1] = __longlong_as_double((long long)globaltimer());
         c->cmd = COOP_EXIT;
     }
-    coop_barrier(c);
+    coop_barrier(c, sh);
     if (threadIdx.x == 0 && ld_volatile_i32(&c->abort) != 0) I.status[7] = 1;
 }
 
@@ -2651,35 +2654,29 @@ extern "C" int mb_launch_batch(const mb::DevInst* d_inst, int ninst, int mode, c
 // file-scope array, which the driver places when it loads this module.  It is one per device and
 // per process: calls that overlap in time on one device race on it.
 // ---------------------------------------------------------------------------------------------
-#include <mutex>
 #include "../../include/mumblebee_gpu.h"
 
 static __device__ __align__(256) unsigned char mb_static_scratch_buf[MB_STATIC_SCRATCH_BYTES];
 
-// Device address and size of the scratch on `device`.  The address is looked up once per device
-// with that device current (cudaGetSymbolAddress, which may load the module) and cached; the
-// previously current device is restored.  Returns a cudaError_t value (0 on success).
+// Device address and size of the scratch on `device`.  The address is looked up on every call,
+// with that device current (cudaGetSymbolAddress, which loads the module on the first call and is
+// a table lookup after that), so it stays right if the host application resets the device or
+// tears down and recreates its primary context between calls; the previously current device is
+// restored.  Returns a cudaError_t value (0 on success).
 extern "C" int mb_static_scratch(int device, void** ptr, size_t* bytes) {
-    constexpr int MAXDEV = 64;
-    static std::mutex mu;
-    static void* addr[MAXDEV] = {};
-    if (!ptr || !bytes || device < 0 || device >= MAXDEV) return (int)cudaErrorInvalidValue;
-    std::lock_guard<std::mutex> lock(mu);
-    if (!addr[device]) {
-        int cur = -1;
-        cudaError_t e = cudaGetDevice(&cur);
-        if (e != cudaSuccess) return (int)e;
-        if (cur != device && (e = cudaSetDevice(device)) != cudaSuccess) return (int)e;
-        void* p = nullptr;
-        e = cudaGetSymbolAddress(&p, mb_static_scratch_buf);
-        if (cur != device) {
-            cudaError_t r = cudaSetDevice(cur);
-            if (e == cudaSuccess) e = r;
-        }
-        if (e != cudaSuccess) return (int)e;
-        addr[device] = p;
+    if (!ptr || !bytes || device < 0) return (int)cudaErrorInvalidValue;
+    int cur = -1;
+    cudaError_t e = cudaGetDevice(&cur);
+    if (e != cudaSuccess) return (int)e;
+    if (cur != device && (e = cudaSetDevice(device)) != cudaSuccess) return (int)e;
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, mb_static_scratch_buf);
+    if (cur != device) {
+        cudaError_t r = cudaSetDevice(cur);
+        if (e == cudaSuccess) e = r;
     }
-    *ptr = addr[device];
+    if (e != cudaSuccess) return (int)e;
+    *ptr = p;
     *bytes = sizeof(mb_static_scratch_buf);
     return (int)cudaSuccess;
 }

@@ -124,7 +124,8 @@ def exppow(nexp=3000, npow=1000, nfree=4000, npos=4000, m=5000, density=0.001, s
     ``npow`` 3-d power cones with α ~ U(0.2, 0.8), plus free and nonnegative columns (the
     log-sum-exp / relative-entropy epigraph variables), A sparse N(0,1) at the given density.
     Feasible by construction: x0 in the cone interior, s0 in the dual-cone interior (0 on free
-    columns), y0 ~ U(-1, 1), b = A x0, c = Aᵀ y0 + s0."""
+    columns), y0 ~ U(-1, 1), b = A x0, c = Aᵀ y0 + s0.  Free columns each carry an entry in a row of
+    their own, so the free variables are determined by the equalities."""
     rng = np.random.default_rng(seed)
     alphas = rng.uniform(0.2, 0.8, npow)
     kinds, sizes, params, x0, s0 = [], [], [], [], []
@@ -147,6 +148,16 @@ def exppow(nexp=3000, npow=1000, nfree=4000, npos=4000, m=5000, density=0.001, s
     empty = np.where(np.diff(sp.csc_matrix(A).indptr) == 0)[0]
     for j in empty:
         A[int(rng.integers(m)), j] = rng.standard_normal()
+    # each free column also gets an entry in a row of its own (a random injection of the free
+    # columns into the rows), so the free block has full structural column rank.  A free column has
+    # a zero Hessian block, so only BᵀB can make δH + BᵀB definite on it; with the random pattern
+    # alone, seed 0 at n = 20000 has free columns with a single entry in the same row (structural
+    # rank 3995 of 4000), δH + BᵀB is singular and every factorization needs the ρ retry.
+    if nfree and nfree <= m:
+        f0 = 3 * (nexp + npow)
+        rows = rng.permutation(m)[:nfree]
+        for j in range(nfree):
+            A[int(rows[j]), f0 + j] = rng.standard_normal()
     A = sp.csc_matrix(A)
     x0 = np.array(x0); s0 = np.array(s0)
     y0 = rng.uniform(-1, 1, m)

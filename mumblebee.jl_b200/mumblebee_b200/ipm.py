@@ -107,6 +107,7 @@ class IPMSettings:
     infeas_rel: float = 1e-8
     precision: str = "fp64"          # "fp64", "fp32" or "mixed" (factor precision; refinement stays FP64)
     large: int = 0                   # a lone large instance runs grid-cooperatively: 0 auto, 1 always, -1 never
+    coop_wait: float = 60.0          # seconds a CTA of that mode waits at a grid barrier (then MB_E_TIMEOUT)
 
     def to_c(self) -> mb_settings:
         s = mb_settings()
@@ -601,6 +602,8 @@ def batch_solve_static(probs, settings: IPMSettings | None = None, grid: int = 0
     synchronisation.  All problems together must fit in MB_STATIC_SCRATCH_BYTES (32 MiB), else
     MBError (MB_E_NOMEM).  Calls that overlap in time on one device race on the scratch."""
     probs = list(probs)
+    if not probs:
+        return []
     ctx = ctx or probs[0].ctx
     settings = settings or IPMSettings()
     cs = settings.to_c()

@@ -15,11 +15,11 @@ def pytest_configure(config):
 
 @pytest.fixture(scope="session", autouse=True)
 def _built():
-    """Build the oracle (checker) and the product library once per session if missing."""
+    """Bring the oracle (checker) and the product library up to date once per session: both builds
+    compare source and object times, so an up-to-date tree costs only the checks, and a library
+    older than its sources is rebuilt rather than tested as it is."""
     import oracle
-    if not os.path.exists(oracle.LIB):
-        oracle.build()
-    from build import LIB, build
-    if not os.path.exists(LIB):
-        build()
+    oracle.build()
+    from build import build
+    build()
     yield

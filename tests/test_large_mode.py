@@ -42,6 +42,20 @@ def test_large_mode_mixed_precision_equals_one_cta():
     assert a.pobj == b.pobj and np.array_equal(a.p, b.p)
 
 
+def test_grid_barrier_wait_runs_out():
+    """settings.coop_wait bounds every wait at a grid barrier.  With a limit far shorter than the
+    leader's serial work before its first command, a helper's wait runs out: every CTA returns, the
+    call fails with MB_E_TIMEOUT, and the same context then solves normally."""
+    from mumblebee_b200._lib import MBError
+    prob = IPMProblem.from_dict(block_problem(CASES["port300"]()), ctx=Context.default())
+    with pytest.raises(MBError, match="code -6.*coop_wait"):
+        solve(prob, IPMSettings(large=1, coop_wait=1e-6))
+    a = solve(prob, IPMSettings(large=-1))
+    b = solve(prob, IPMSettings(large=1))
+    assert a.status == b.status == IPMStatus.OPTIMAL
+    assert a.niter == b.niter and a.pobj == b.pobj and np.array_equal(a.p, b.p)
+
+
 def test_large_mode_sdp_and_step_api():
     from mumblebee_b200.ipm import init
     prob = IPMProblem.from_dict(block_problem(SDP["sdp1x10"]()), ctx=Context.default())

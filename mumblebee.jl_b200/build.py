@@ -39,10 +39,15 @@ def _newer(target, deps):
 
 
 def build(verbose: bool = False, force: bool = False) -> str:
+    api = os.path.join(HERE, "..", "include", "mumblebee_gpu.h")
+    sources = [os.path.join(CSRC, f) for f in SOURCES_CU + SOURCES_CPP + HEADERS] + [api, os.path.abspath(__file__)]
+    # a library newer than every source is up to date even where the object files are absent (a
+    # copy of the tree that carries the built library but not the intermediate objects)
+    if not force and not _newer(LIB, sources):
+        return LIB
     os.makedirs(LIBDIR, exist_ok=True)
     objdir = os.path.join(HERE, "_build")
     os.makedirs(objdir, exist_ok=True)
-    api = os.path.join(HERE, "..", "include", "mumblebee_gpu.h")
     objs = []
     for src in SOURCES_CU + SOURCES_CPP:
         s = os.path.join(CSRC, src)

@@ -53,7 +53,7 @@ def parse():
     ap.add_argument("--count", type=int, default=4096, help="instances per step per GPU")
     ap.add_argument("--precision", default="fp64", choices=["fp64", "fp32", "mixed"])
     ap.add_argument("--seed", type=int, default=0)
-    ap.add_argument("--cpu-seconds", type=float, default=15.0, help="bounded CPU-baseline sample length")
+    ap.add_argument("--ref-per-core", type=int, default=8, help="reference arm: instances per host core per step")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-compare", action="store_true", help="skip the other precision's arm")
@@ -63,9 +63,12 @@ def parse():
     ap.add_argument("--serve-nmin", type=int, default=100)
     ap.add_argument("--serve-nmax", type=int, default=2000)
     ap.add_argument("--serve-arena-gb", type=int, default=32)
-    ap.add_argument("--extras", default="", choices=["", "stable", "comp", "all"],
+    ap.add_argument("--extras", default="", choices=["", "stable", "comp", "coop", "config4", "all"],
                     help="instead of the main line: one JSON line each for the stable factor against the default "
-                         "one, and for the compensated products (1 GPU)")
+                         "one, the compensated products, one grid-cooperative SOCP solve (n = 2000), and the "
+                         "n = 20000 exponential/power-cone problem (1 GPU; 'all' runs the first three)")
+    ap.add_argument("--config4-scale", type=float, default=1.0,
+                    help="size of the exponential/power-cone problem relative to n = 20000")
     ap.add_argument("--extras-count", type=int, default=1184, help="instances of the stable-factor arm")
     ap.add_argument("--comp-rows", type=int, default=1 << 20, help="rows = columns of the compensated-product matrix")
     return ap.parse_args()
@@ -176,43 +179,6 @@ def measure_peaks():
 
 
 # ------------------------------------------------------------------------------------------ oracle
-def _oracle_worker(args):
-    seed, deadline, count_max = args
-    sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import frontend
-    import oracle
-    from mumblebee_b200 import generators as G
-    oracle.lib(threads=1)
-    rng = np.random.default_rng(seed)
-    done, secs = 0, 0.0
-    while time.time() < deadline and done < count_max:
-        pb = G.portfolio(int(rng.integers(50, 401)), rng=np.random.default_rng([seed, done]))
-        prob = frontend.ipmproblem_from_csc(pb["Q"], pb["B"], pb["f"], pb["g"], pb["mu"], pb["kinds"], pb["sizes"],
-                                            pb["params"])
-        adj, w = frontend.vertex_graph(prob)
-        vp = frontend.minimum_degree(adj, w)
-        t = time.perf_counter()
-        s = oracle.OracleSolver(prob, oracle.default_settings(), vperm=vp, threads=1)
-        r = s.solve()
-        secs += time.perf_counter() - t
-        done += 1
-        assert r["status"] in ("OPTIMAL", "NEAR_OPTIMAL")
-    return done, secs
-
-
-def cpu_oracle_rate(seconds, cores, seed=1234):
-    """Solves/s of the FP64 oracle on `cores` host processes (one OpenBLAS thread each), timing
-    the init+solve of each instance (problem construction excluded, as for the GPU)."""
-    ctx = mp.get_context("spawn")
-    deadline = time.time() + seconds
-    with ctx.Pool(cores) as pool:
-        res = pool.map(_oracle_worker, [(seed + k, deadline, 10 ** 6) for k in range(cores)])
-    done = sum(r[0] for r in res)
-    busy = max(r[1] for r in res) if res else 0
-    per_core = [r[0] / r[1] for r in res if r[1] > 0]
-    return sum(per_core), done, busy
-
-
 # ------------------------------------------------------------------------------------------ main
 def make_problems(count, seed, rank, ctx):
     from mumblebee_b200 import generators as G
@@ -228,29 +194,86 @@ def make_problems(count, seed, rank, ctx):
     return probs, sizes
 
 
+_REF_PROBS = None
+
+
+def _ref_init(seed, idx):
+    """Pool initializer of the reference arm: build the oracle's block form of instances `idx` of
+    the GPU arm's own seeded list (make_problems' sizes and per-instance seeds, rank 0) with the
+    oracle's ordering, once per worker, outside the timed region."""
+    global _REF_PROBS
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import frontend
+    import oracle
+    from mumblebee_b200 import generators as G
+    oracle.lib(threads=1)
+    sizes = np.random.default_rng([seed, 0]).integers(50, 401, size=max(idx) + 1)
+    _REF_PROBS = {}
+    for i in idx:
+        pb = G.portfolio(int(sizes[i]), rng=np.random.default_rng([seed, 0, i]))
+        prob = frontend.ipmproblem_from_csc(pb["Q"], pb["B"], pb["f"], pb["g"], pb["mu"], pb["kinds"], pb["sizes"],
+                                            pb["params"])
+        adj, w = frontend.vertex_graph(prob)
+        _REF_PROBS[i] = (prob, frontend.minimum_degree(adj, w))
+
+
+def _ref_solve(i):
+    import oracle
+    prob, vp = _REF_PROBS[i]
+    r = oracle.OracleSolver(prob, oracle.default_settings(), vperm=vp, threads=1).solve()
+    return i, r["status"], r["niter"]
+
+
+def oracle_steps(args, steps, warmup):
+    """The reference algorithm's FP64 CPU restatement (the oracle; the reference itself is a Julia
+    package and Julia is absent) on every host core.  One step solves the first K instances of the
+    GPU arm's own list (same sizes and seeds), largest first, one instance per process at a time;
+    K = ref_per_core per core, so that a step is a bounded sample of the workload.  Timed by the
+    host clock around each step (problem construction excluded, as for the GPU)."""
+    cores = os.cpu_count() or 1
+    k = min(args.count, args.ref_per_core * cores)
+    sizes = np.random.default_rng([args.seed, 0]).integers(50, 401, size=k)
+    order = [int(i) for i in np.argsort(-sizes, kind="stable")]
+    ctx = mp.get_context("spawn")
+    ms, status = [], []
+    with ctx.Pool(cores, initializer=_ref_init, initargs=(args.seed, list(range(k)))) as pool:
+        for _ in range(warmup):
+            pool.map(_ref_solve, order, chunksize=1)
+        for _ in range(steps):
+            t = time.perf_counter()
+            status = pool.map(_ref_solve, order, chunksize=1)
+            ms.append(1e3 * (time.perf_counter() - t))
+    opt = sum(1 for _, st, _ in status if st == "OPTIMAL")
+    sample = (f"instances 0..{k - 1} of the {args.count}-instance list (same sizes and seeds) per step, FP64 oracle "
+              f"(CPU restatement of the reference; Julia is not installed), {cores} processes x 1 OpenBLAS thread, "
+              f"largest first; {opt}/{k} OPTIMAL")
+    return k, ms, cores, sample
+
+
 def run_reference(args, ws, rank):
+    """`--impl reference`: rank 0 alone times the oracle steps; other ranks exit without work."""
     if rank != 0:
         return
-    cores = os.cpu_count() or 1
-    per_step = max(2.0, args.cpu_seconds / max(1, args.steps))
-    rates = []
-    cpu_oracle_rate(1.0, cores)     # warm-up (process spawn, library load)
-    for _ in range(args.steps):
-        r, _, _ = cpu_oracle_rate(per_step, cores)
-        rates.append(r)
-    v = statistics.median(rates)
+    k, ms, cores, sample = oracle_steps(args, args.steps, args.warmup)
+    step_ms = statistics.mean(ms)
+    v = k / (step_ms / 1e3)
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "solves/s", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * args.count / v,
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "instances": args.count},
-            "cpu_baseline": {"value": v, "unit": "solves/s", "cores": cores, "kind": "port",
-                             "sample": f"FP64 oracle (CPU restatement of the reference; Julia is not installed), "
-                                       f"{cores} processes x 1 OpenBLAS thread, {per_step:.0f} s of instances per step"},
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": step_ms, "step_ms": ms,
+            "instances_per_step": k, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic", "config": main_config(args, ws),
+            "cpu_baseline": {"value": v, "unit": "solves/s", "cores": cores, "kind": "port", "sample": sample},
             "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
-def timed_arm(probs, precision, args, pg, local, ws, ctx):
+def main_config(args, ws):
+    """The workload's name and sizes, identical in both arms."""
+    return {"workload": WORKLOAD, "instances_per_gpu": args.count, "precision": args.precision,
+            "parallelism": f"instances sharded over {ws} GPU(s), one persistent launch per step",
+            "l2": "inputs and workspace larger than the 126 MB L2 (sizes under footprint)"}
+
+
+def timed_arm(probs, precision, args, pg, local, ws, ctx, lower):
     """Prepare a batch at `precision`, warm up, time `steps` persistent launches (CUDA events on the
     launching stream, max over ranks) and read back statuses, iterations and latencies."""
     from mumblebee_b200.ipm import Batch, IPMSettings
@@ -269,6 +292,7 @@ def timed_arm(probs, precision, args, pg, local, ws, ctx):
     ms_max = allreduce_max(pg, ms, local)
     res = batch.fetch(want_vectors=False)          # results of the last timed launch
     lat, svc = batch.latencies_ms()
+    ntrsv = batch.timers()[:, batch.SECTIONS.index("ntrsv")]
     out = {"precision": precision, "ms": ms, "ms_max": ms_max, "ms_steps": ms_steps, "clocks": clocks,
            "value": args.count * ws / (ms_max / 1e3), "res": res, "stats": st, "prepare_s": t_prep,
            "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
@@ -278,8 +302,41 @@ def timed_arm(probs, precision, args, pg, local, ws, ctx):
            "near_optimal": sum(1 for r in res if r.status.name == "NEAR_OPTIMAL"),
            "iters_mean": float(np.mean([r.niter for r in res])),
            "flops": float(sum(r.nfactor * r.factor_flops for r in res))}
+    out.update(factor_accounting(res, ntrsv, lower, precision))
     del batch
     return out
+
+
+def lower_entries(probs):
+    """Stored lower-triangle entries of each instance's factor: Σ over fronts of r (r + 1) / 2, r the
+    front's order (residual + separator columns), from the host symbolic analysis."""
+    out = []
+    for p in probs:
+        s = p.symbolic()
+        r = (np.asarray(s["nres"]) + np.asarray(s["nsep"])).astype(np.float64)
+        out.append(float((r * (r + 1) / 2).sum()))
+    return np.array(out)
+
+
+def factor_accounting(res, ntrsv, lower, precision):
+    """Factorizations by precision and the launch's algorithmic DRAM bytes.  In the mixed path every
+    iteration factors in FP32 first; an iteration redone in FP64 (nfallback) adds an FP64
+    factorization, and after the switch every factorization is FP64, so the FP32 count is
+    nfp32 + nfallback (capped by nfactor) and the rest are FP64.  Algorithmic bytes: a
+    factorization reads the assembled BᵀB (8 B per lower entry) and writes L once (8 B FP64, 4 B FP32);
+    a triangular-solve sweep reads L once."""
+    n32 = np.array([min(r.nfactor, r.nfp32 + r.nfallback) if precision != "fp64" else 0 for r in res], float)
+    if precision == "fp32":
+        n32 = np.array([r.nfactor for r in res], float)
+    nfac = np.array([r.nfactor for r in res], float)
+    n64 = nfac - n32
+    ff = np.array([r.factor_flops for r in res])
+    # a sweep reads the factor of its iteration: FP32 on the FP32 share of the factorizations
+    esz = 8.0 - 4.0 * n32 / np.maximum(nfac, 1.0)
+    alg = float((n64 * 16 * lower + n32 * 12 * lower + ntrsv * esz * lower).sum())
+    return {"flops_fp32": float((n32 * ff).sum()), "flops_fp64": float((n64 * ff).sum()),
+            "factorizations": {"fp32": float(n32.sum()), "fp64": float(n64.sum())}, "alg_bytes": alg,
+            "trsv_sweeps": float(np.sum(ntrsv))}
 
 
 def serve_arm(args, ctx):
@@ -405,6 +462,61 @@ def comp_arm(args, ctx):
     print(json.dumps(out), flush=True)
 
 
+def coop_arm(args, ctx):
+    """One SOCP instance (n = 2000, m = 800, 100 x SOC(20), density 0.0125, seed 0: one front of
+    2000) solved once in the grid-cooperative mode (settings large = 1: CTA 0 runs the iteration,
+    the other CTAs take the factor's tiles): the command behind the ipm_coop_kernel profile."""
+    from mumblebee_b200 import generators as G
+    from mumblebee_b200.ipm import Batch, IPMProblem, IPMSettings, _CONES
+    pb = G.socp(2000, 800, 100, 0.0125, 0)
+    prob = IPMProblem(pb["Q"], pb["B"], pb["f"], pb["g"], pb["mu"], [_CONES[k]() for k in pb["kinds"]], pb["sizes"],
+                      ctx=ctx)
+    batch = Batch([prob], IPMSettings(large=1), ctx=ctx)
+    ms = batch.run()
+    r = batch.fetch(want_vectors=False)[0]
+    print(json.dumps({"extra": "coop_socp2000", "kernel": "ipm_coop_kernel", "ms": ms, "status": r.status.name,
+                      "niter": r.niter, "nfactor": r.nfactor, "factor_flops": r.factor_flops}), flush=True)
+
+
+def config4_arm(args, ctx):
+    """The exponential/power-cone configuration: n = 20000 (3000 EXP, 1000 POW, 4000 free, 4000
+    nonnegative columns), m = 5000, A at 0.1% density, seed 0, at the default 1e-8 tolerances,
+    solved alone (grid-cooperative: its factorization exceeds the large-instance threshold).
+    Wall time of init + solve; section clocks of the leader CTA; the last history rows."""
+    from mumblebee_b200 import generators as G
+    from mumblebee_b200.ipm import IPMProblem, IPMSettings, init, _CONES, PowerCone
+    f = args.config4_scale
+    pb = G.exppow(nexp=int(3000 * f), npow=int(1000 * f), nfree=int(4000 * f), npos=int(4000 * f), m=int(5000 * f),
+                  density=0.001 / f)
+    K = [PowerCone(a) if k == 5 else _CONES[k]() for k, a in zip(pb["kinds"], pb["params"])]
+    t0 = time.time()
+    prob = IPMProblem(pb["Q"], pb["B"], pb["f"], pb["g"], pb["mu"], K, pb["sizes"], ctx=ctx)
+    sym = prob.symbolic()
+    r_ = np.asarray(sym["nres"]) + np.asarray(sym["nsep"])
+    t_sym = time.time() - t0
+    clk = Clocks(0)
+    t0 = time.time()
+    s = init(prob, IPMSettings())
+    r = s.solve()
+    wall = time.time() - t0
+    clocks = clk.stop()
+    tm = s.timers()
+    h = s.history()
+    mhz = clocks.get("sm_mhz") or 1965.0
+    fac_s = (tm["factor_update"] + tm["factor_diag"] + tm["factor_panel"]) / (mhz * 1e6)
+    gap = (r.pobj - r.dobj) / max(1.0, min(abs(r.pobj), abs(r.dobj)))
+    print(json.dumps({"extra": "config4_exppow", "n": int(sum(pb["sizes"])), "m": int(pb["B"].shape[0]),
+                      "fronts": int(sym["nfront"]), "largest_front": int(r_.max()), "symbolic_s": t_sym,
+                      "status": r.status.name, "niter": r.niter, "pobj": r.pobj, "dobj": r.dobj, "rel_gap": gap,
+                      "pres": r.pres, "dres": r.dres, "mu": r.mu, "nfactor": r.nfactor,
+                      "nfactor_retry": r.nfactor_retry, "factor_flops": r.factor_flops, "wall_s": wall,
+                      "factor_s": fac_s, "factor_tflops": r.nfactor * r.factor_flops / max(fac_s, 1e-9) / 1e12,
+                      "sections_s": {k: v / (mhz * 1e6) for k, v in tm.items() if not k.startswith("n")},
+                      "last_rows": [{k: h[i][k] for k in ("mu", "pres", "dres", "pobj", "dobj", "step", "rho")}
+                                    for i in range(max(0, len(h) - 4), len(h))],
+                      "clocks": clocks}), flush=True)
+
+
 def main():
     args = parse()
     ws, rank, local, pg = dist_setup(args)
@@ -415,6 +527,10 @@ def main():
             stable_arm(args, ctx)
         if args.extras in ("comp", "all"):
             comp_arm(args, ctx)
+        if args.extras in ("coop", "all"):
+            coop_arm(args, ctx)
+        if args.extras == "config4":
+            config4_arm(args, ctx)
         return
     if args.impl == "reference":
         run_reference(args, ws, rank)
@@ -426,23 +542,35 @@ def main():
     t0 = time.time()
     probs, sizes = make_problems(args.count, args.seed, rank, ctx)
     t_gen = time.time() - t0
-    main_arm = timed_arm(probs, args.precision, args, pg, local, ws, ctx)
+    lower = lower_entries(probs)
+    main_arm = timed_arm(probs, args.precision, args, pg, local, ws, ctx, lower)
     other = None
     if not args.no_compare:
-        other = timed_arm(probs, "mixed" if args.precision == "fp64" else "fp64", args, pg, local, ws, ctx)
-    # roofline of the solver kernel: algorithmic factorization flops per launch / launch time
+        other = timed_arm(probs, "mixed" if args.precision == "fp64" else "fp64", args, pg, local, ws, ctx, lower)
+    # roofline of the solver kernel: algorithmic factorization flops per launch / launch time, against
+    # the FP64 GEMM peak (FP64 arm) and the TF32 tensor-core peak (FP32 / mixed arm)
     peaks = measure_peaks()
-    peak_key = "tf32" if args.precision in ("fp32", "mixed") else "fp64"
-    achieved = main_arm["flops"] / (main_arm["ms"] / 1e3) / 1e12
-    traffic = None
-    if args.precision == "fp64" and TRAFFIC_BYTES_PER_INSTANCE_FP64 is not None:
-        traffic = TRAFFIC_BYTES_PER_INSTANCE_FP64 * args.count
-    roofline = {"bound": "tensor", "achieved": achieved, "peak": peaks[peak_key], "unit": "TFLOP/s",
-                "frac": achieved / peaks[peak_key], "traffic": traffic,
-                "peak_source": f"measured live: torch {peak_key} GEMM 8192^3 best of 5 on this GPU",
-                "kernel": "ipm_batch_kernel", "flops_per_launch": main_arm["flops"]}
-    if traffic is not None:
-        roofline["traffic_source"] = TRAFFIC_SOURCE
+
+    def roof(arm):
+        key = "fp64" if arm["precision"] == "fp64" else "tf32"
+        achieved = arm["flops"] / (arm["ms"] / 1e3) / 1e12
+        r = {"bound": "tensor", "achieved": achieved, "peak": peaks[key], "unit": "TFLOP/s",
+             "frac": achieved / peaks[key], "traffic": None,
+             "peak_source": f"measured live: torch {key} GEMM 8192^3 best of 5 on this GPU",
+             "kernel": "ipm_batch_kernel", "precision": arm["precision"], "flops_per_launch": arm["flops"],
+             "flops_fp32": arm["flops_fp32"], "flops_fp64": arm["flops_fp64"],
+             "factorizations": arm["factorizations"], "alg_bytes": arm["alg_bytes"],
+             "alg_bytes_source": "per factorization 8 B read (assembled B^T B) + 8 B (FP64) or 4 B (FP32) written "
+                                 "per stored lower-triangle entry of L; per triangular-solve sweep one read of L",
+             "hbm_achieved_gbs": arm["alg_bytes"] / (arm["ms"] / 1e3) / 1e9}
+        if arm["precision"] == "fp64" and TRAFFIC_BYTES_PER_INSTANCE_FP64 is not None:
+            r["traffic"] = TRAFFIC_BYTES_PER_INSTANCE_FP64 * args.count
+            r["traffic_source"] = TRAFFIC_SOURCE
+            r["traffic_over_alg"] = r["traffic"] / arm["alg_bytes"]
+        return r
+
+    roofline = roof(main_arm)
+    roofline_other = roof(other) if other is not None else None
     # end to end through the C ABI: host problems in, host results out
     e2e = None
     if not args.no_e2e:
@@ -465,11 +593,9 @@ def main():
         serve = serve_arm(args, ctx)
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
-        cores = os.cpu_count() or 1
-        r, done, busy = cpu_oracle_rate(args.cpu_seconds, cores)
-        cpu = {"value": r, "unit": "solves/s", "cores": cores, "kind": "port",
-               "sample": f"{done} instances of the same distribution, FP64 oracle, {cores} processes x 1 thread, "
-                         f"{args.cpu_seconds:.0f} s"}
+        k, ms, cores, sample = oracle_steps(args, 2, 1)
+        cpu = {"value": k / (statistics.mean(ms) / 1e3), "unit": "solves/s", "cores": cores, "kind": "port",
+               "sample": sample + "; 1 warm-up and 2 timed steps"}
     if rank == 0:
         st = main_arm["stats"]
         arms = {a["precision"]: {"solves_per_s": a["value"], "ms_per_step": a["ms_max"],
@@ -483,15 +609,14 @@ def main():
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": main_arm["ms_max"],
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
                 "data": "synthetic",
-                "config": {"workload": WORKLOAD, "instances_per_gpu": args.count, "precision": args.precision,
-                           "parallelism": f"instances sharded over {ws} GPU(s), one persistent launch per step",
-                           "l2": f"inputs larger than L2: {st['input_bytes'] / 1e9:.2f} GB uploaded + "
-                                 f"{(st['work_bytes'] + st['factor_bytes']) / 1e9:.2f} GB workspace per step",
-                           "optimal": f"{main_arm['optimal']}/{args.count}", "iters_mean": main_arm["iters_mean"],
-                           "setup_s": {"generate": round(t_gen, 2), "prepare": round(main_arm["prepare_s"], 2)}},
+                "config": main_config(args, ws),
+                "footprint": {"input_gb": st["input_bytes"] / 1e9,
+                              "workspace_gb": (st["work_bytes"] + st["factor_bytes"]) / 1e9},
+                "run": {"optimal": f"{main_arm['optimal']}/{args.count}", "iters_mean": main_arm["iters_mean"],
+                        "setup_s": {"generate": round(t_gen, 2), "prepare": round(main_arm["prepare_s"], 2)}},
                 "latency_ms": main_arm["latency_ms"], "solve_ms": main_arm["solve_ms"],
                 "precisions": arms, "serving": serve,
-                "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": args.steps,
+                "roofline": roofline, "roofline_other": roofline_other, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": args.steps,
                 "clocks": main_arm["clocks"], "step_ms": main_arm["ms_steps"]}
         print(json.dumps(line), flush=True)
     if pg is not None:

@@ -119,13 +119,15 @@ def _pow_dual_interior(rng, a):
     return [s1, s2, rng.uniform(-0.9, 0.9) * (s1 / a) ** a * (s2 / (1 - a)) ** (1 - a)]
 
 
-def exppow(nexp=3000, npow=1000, nfree=4000, npos=4000, m=5000, density=0.001, seed=0):
+def exppow(nexp=3000, npow=1000, nfree=4000, npos=4000, m=5000, density=0.001, seed=0, determined_free=True):
     """Exponential / power cone problem (defaults: n = 20000, m = 5000): ``nexp`` exponential cones and
     ``npow`` 3-d power cones with α ~ U(0.2, 0.8), plus free and nonnegative columns (the
     log-sum-exp / relative-entropy epigraph variables), A sparse N(0,1) at the given density.
     Feasible by construction: x0 in the cone interior, s0 in the dual-cone interior (0 on free
     columns), y0 ~ U(-1, 1), b = A x0, c = Aᵀ y0 + s0.  Free columns each carry an entry in a row of
-    their own, so the free variables are determined by the equalities."""
+    their own, so the free variables are determined by the equalities; ``determined_free=False``
+    keeps the random pattern alone (the same random stream up to that point), whose free block
+    may be structurally rank deficient."""
     rng = np.random.default_rng(seed)
     alphas = rng.uniform(0.2, 0.8, npow)
     kinds, sizes, params, x0, s0 = [], [], [], [], []
@@ -153,7 +155,7 @@ def exppow(nexp=3000, npow=1000, nfree=4000, npos=4000, m=5000, density=0.001, s
     # a zero Hessian block, so only BᵀB can make δH + BᵀB definite on it; with the random pattern
     # alone, seed 0 at n = 20000 has free columns with a single entry in the same row (structural
     # rank 3995 of 4000), δH + BᵀB is singular and every factorization needs the ρ retry.
-    if nfree and nfree <= m:
+    if determined_free and nfree and nfree <= m:
         f0 = 3 * (nexp + npow)
         rows = rng.permutation(m)[:nfree]
         for j in range(nfree):

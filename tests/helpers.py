@@ -42,7 +42,8 @@ def oracle_solve(prob_blocks, vperm=None, threads=1, **settings):
 TDC = {
     "exp_small": lambda: G.exppow(nexp=30, npow=0, nfree=0, npos=0, m=40, density=0.05, seed=1),
     "pow_small": lambda: G.exppow(nexp=0, npow=30, nfree=0, npos=0, m=40, density=0.05, seed=1),
-    "exppow_mix": lambda: G.exppow(nexp=30, npow=15, nfree=10, npos=20, m=60, density=0.05, seed=3),
+    "exppow_mix": lambda: G.exppow(nexp=30, npow=15, nfree=10, npos=20, m=60, density=0.05, seed=3,
+                                    determined_free=False),
 }
 # exponential / power cones stall in the certified line-search band just above a 1e-8 gap (the
 # reference's own power-cone examples run at 1e-5..1e-6); their parity runs use 1e-7

@@ -69,6 +69,8 @@ def parse():
                          "n = 20000 exponential/power-cone problem (1 GPU; 'all' runs the first three)")
     ap.add_argument("--config4-scale", type=float, default=1.0,
                     help="size of the exponential/power-cone problem relative to n = 20000")
+    ap.add_argument("--fp32-tiles", type=int, default=0, choices=[0, 1, 2],
+                    help="settings.fp32_tiles of every arm: 0 the runtime's choice, 1 FFMA, 2 tensor cores")
     ap.add_argument("--extras-count", type=int, default=1184, help="instances of the stable-factor arm")
     ap.add_argument("--comp-rows", type=int, default=1 << 20, help="rows = columns of the compensated-product matrix")
     return ap.parse_args()
@@ -277,7 +279,7 @@ def timed_arm(probs, precision, args, pg, local, ws, ctx, lower):
     """Prepare a batch at `precision`, warm up, time `steps` persistent launches (CUDA events on the
     launching stream, max over ranks) and read back statuses, iterations and latencies."""
     from mumblebee_b200.ipm import Batch, IPMSettings
-    settings = IPMSettings(precision=precision)
+    settings = IPMSettings(precision=precision, fp32_tiles=args.fp32_tiles)
     t0 = time.time()
     batch = Batch(probs, settings, ctx=ctx)
     t_prep = time.time() - t0
@@ -496,7 +498,7 @@ def config4_arm(args, ctx):
     t_sym = time.time() - t0
     clk = Clocks(0)
     t0 = time.time()
-    s = init(prob, IPMSettings())
+    s = init(prob, IPMSettings(precision=args.precision, fp32_tiles=args.fp32_tiles))
     r = s.solve()
     wall = time.time() - t0
     clocks = clk.stop()
@@ -505,7 +507,8 @@ def config4_arm(args, ctx):
     mhz = clocks.get("sm_mhz") or 1965.0
     fac_s = (tm["factor_update"] + tm["factor_diag"] + tm["factor_panel"]) / (mhz * 1e6)
     gap = (r.pobj - r.dobj) / max(1.0, min(abs(r.pobj), abs(r.dobj)))
-    print(json.dumps({"extra": "config4_exppow", "n": int(sum(pb["sizes"])), "m": int(pb["B"].shape[0]),
+    print(json.dumps({"extra": "config4_exppow", "precision": args.precision, "fp32_tiles": args.fp32_tiles,
+                      "nfp32": r.nfp32, "nfallback": r.nfallback, "n": int(sum(pb["sizes"])), "m": int(pb["B"].shape[0]),
                       "fronts": int(sym["nfront"]), "largest_front": int(r_.max()), "symbolic_s": t_sym,
                       "status": r.status.name, "niter": r.niter, "pobj": r.pobj, "dobj": r.dobj, "rel_gap": gap,
                       "pres": r.pres, "dres": r.dres, "mu": r.mu, "nfactor": r.nfactor,

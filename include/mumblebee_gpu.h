@@ -98,6 +98,13 @@ typedef struct mb_settings {
     double coop_wait;          /* 60  seconds a CTA of the grid-cooperative mode waits at a grid barrier;
                                       when a wait runs out every CTA returns and the call fails with
                                       MB_E_TIMEOUT (<= 0: 60) */
+    int32_t fp32_tiles;        /* 0   the FP32 factor's trailing-update tiles (MB_PREC_FP32, and the FP32
+                                      iterations of MB_PREC_MIXED) on fronts of order >= 128: 2 on the
+                                      tensor cores (tcgen05.mma kind::tf32, 3xTF32 split, per-step FP32
+                                      read-out; those kernels run one CTA per SM), 1 on FFMA (two CTAs
+                                      per SM), 0 the runtime's choice: the tensor cores for a lone
+                                      grid-cooperative instance, FFMA for batches */
+    int32_t reserved;          /* 0 */
 } mb_settings;
 
 /* BlockSparseMatrix{Float64,Int64} (BlockSparseArrays/src/block_sparse_matrix.jl:10-158), 1-based */

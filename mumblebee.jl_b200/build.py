@@ -20,11 +20,13 @@ NVCC = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 COMMON = ["-O3", "-std=c++17", "-Xcompiler", "-fPIC", "-lineinfo"]
 
-SOURCES_CU = ["mb_solver.cu", "mb_comp.cu"]
+SOURCES_CU = ["mb_solver.cu", "mb_solver_tc.cu", "mb_comp.cu"]
 SOURCES_CPP = ["mb_host.cpp"]
 # headers each source includes (a change rebuilds only the sources that use it)
+_SOLVER_DEPS = ["mb_internal.h", "mb_device.cuh", "mb_cones.cuh", "mb_tdc.cuh", "mb_sdp.cuh"]
 DEPS = {
-    "mb_solver.cu": ["mb_internal.h", "mb_device.cuh", "mb_cones.cuh", "mb_tdc.cuh", "mb_sdp.cuh"],
+    "mb_solver.cu": _SOLVER_DEPS,
+    "mb_solver_tc.cu": _SOLVER_DEPS + ["mb_solver.cu"],   # the tensor-core build of the same source
     "mb_comp.cu": ["mb_internal.h"],
     "mb_host.cpp": ["mb_internal.h", "mb_symbolic.hpp"],
 }
@@ -41,14 +43,15 @@ def _newer(target, deps):
 def build(verbose: bool = False, force: bool = False) -> str:
     api = os.path.join(HERE, "..", "include", "mumblebee_gpu.h")
     sources = [os.path.join(CSRC, f) for f in SOURCES_CU + SOURCES_CPP + HEADERS] + [api, os.path.abspath(__file__)]
-    # a library newer than every source is up to date even where the object files are absent (a
-    # copy of the tree that carries the built library but not the intermediate objects)
-    if not force and not _newer(LIB, sources):
+    # a copy of the tree that carries the built library but not the intermediate objects: the
+    # library is up to date when it is newer than every source (where the objects exist, each is
+    # checked against its own sources below, which also catches a source edited during a build)
+    objdir = os.path.join(HERE, "_build")
+    if not force and not os.path.isdir(objdir) and not _newer(LIB, sources):
         return LIB
     os.makedirs(LIBDIR, exist_ok=True)
-    objdir = os.path.join(HERE, "_build")
     os.makedirs(objdir, exist_ok=True)
-    objs = []
+    objs, cmds = [], []
     for src in SOURCES_CU + SOURCES_CPP:
         s = os.path.join(CSRC, src)
         o = os.path.join(objdir, src + ".o")
@@ -60,7 +63,13 @@ def build(verbose: bool = False, force: bool = False) -> str:
                 cmd += ["-Xptxas", "-v"] if verbose else []
             if verbose:
                 print(" ".join(cmd))
-            subprocess.run(cmd, check=True)
+            cmds.append(cmd)
+    # the translation units compile in parallel (the two solver builds take minutes each)
+    procs = [subprocess.Popen(c) for c in cmds]
+    rcs = [p.wait() for p in procs]
+    for c, rc in zip(cmds, rcs):
+        if rc:
+            raise subprocess.CalledProcessError(rc, c)
     if force or _newer(LIB, objs):
         cmd = [NVCC] + ARCH + ["-shared", "-cudart", "static", "-o", LIB] + objs
         if verbose:

@@ -31,6 +31,33 @@ extern "C" int mb_launch_coop(const mb::DevInst* d_inst, int mode, const mb::Set
                               int grid, cudaStream_t stream);
 extern "C" int mb_coop_grid(int device, int nsm);
 extern "C" int mb_launch_twomv(const mb::TwoMv* a, cudaStream_t st);
+// the tensor-core build of the solver kernels (mb_solver_tc.cu): same arguments
+extern "C" int mb_launch_batch_tc(const mb::DevInst* d_inst, int ninst, int mode, const mb::Settings* set,
+                                  int* d_counter, int grid, int fp32, cudaStream_t stream);
+extern "C" int mb_launch_coop_tc(const mb::DevInst* d_inst, int mode, const mb::Settings* set, mb::CoopCtl* d_ctl,
+                                 int grid, cudaStream_t stream);
+extern "C" int mb_coop_grid_tc(int device, int nsm);
+
+// Which build of the solver kernels a launch uses.  The tensor-core build (FP32 update tiles on
+// tcgen05) runs one CTA per SM, the default build two, which the batched path needs to hide its
+// latency; so with settings.fp32_tiles left to the runtime (0) the tensor cores serve only a lone
+// grid-cooperative instance with an FP32 factor, where the large fronts' update tiles dominate.
+// 1 always takes the FFMA tiles, 2 always the tensor cores (when an FP32 factor runs at all).
+static bool use_tc_build(const mb_settings& s, bool coop) {
+    if (s.precision == MB_PREC_FP64 || s.fp32_tiles == 1) return false;
+    return s.fp32_tiles == 2 || coop;
+}
+static int launch_coop(const mb_settings& s, const mb::DevInst* d_inst, int mode, const mb::Settings* ds,
+                       mb::CoopCtl* d_ctl, int device, int nsm, cudaStream_t st) {
+    return use_tc_build(s, true) ? mb_launch_coop_tc(d_inst, mode, ds, d_ctl, mb_coop_grid_tc(device, nsm), st)
+                                 : mb_launch_coop(d_inst, mode, ds, d_ctl, mb_coop_grid(device, nsm), st);
+}
+static int launch_batch(const mb_settings& s, const mb::DevInst* d_inst, int ninst, int mode, const mb::Settings* ds,
+                        int* d_counter, int grid, cudaStream_t st) {
+    const int fp32 = s.precision == MB_PREC_FP32;
+    return use_tc_build(s, false) ? mb_launch_batch_tc(d_inst, ninst, mode, ds, d_counter, grid, fp32, st)
+                                  : mb_launch_batch(d_inst, ninst, mode, ds, d_counter, grid, fp32, st);
+}
 
 using mbh::i64;
 
@@ -783,8 +810,9 @@ static int run_batch(mb_batch* b, int mode, int32_t grid, float* ms) {
     if (coop && !b->d_coop) CUDA_TRY(ctx, cudaMalloc((void**)&b->d_coop, sizeof(mb::CoopCtl)));
     cudaStream_t st = b->stream();
     CUDA_TRY(ctx, cudaEventRecord(b->e0, st));
-    int rc = coop ? mb_launch_coop(b->d_inst, mode, &s, b->d_coop, mb_coop_grid(ctx->device, ctx->nsm), st)
-                  : mb_launch_batch(b->d_inst, ninst, mode, &s, b->d_counter, g, b->set.precision == MB_PREC_FP32, st);
+    if (!coop && use_tc_build(b->set, false)) g = std::min({grid > 0 ? grid : ctx->nsm, ctx->nsm, ninst});   // one CTA per SM
+    int rc = coop ? launch_coop(b->set, b->d_inst, mode, &s, b->d_coop, ctx->device, ctx->nsm, st)
+                  : launch_batch(b->set, b->d_inst, ninst, mode, &s, b->d_counter, g, st);
     if (rc) return fail(ctx, MB_E_CUDA, std::string("launch failed: ") + cudaGetErrorString(cudaGetLastError()));
     b->launches++;
     CUDA_TRY(ctx, cudaEventRecord(b->e1, st));
@@ -796,6 +824,10 @@ static int run_batch(mb_batch* b, int mode, int32_t grid, float* ms) {
 
 static const char* COOP_TIMEOUT_MSG =
     "a grid-barrier wait of the grid-cooperative mode ran past settings.coop_wait; the solve was abandoned";
+static const char* TC_TIMEOUT_MSG =
+    "a tensor-core completion wait of the FP32 factor ran out; the solve was abandoned";
+// status word 7 of an instance: 1 a grid-barrier wait ran out, 2 a tensor-core completion wait did
+static const char* timeout_msg(int32_t w) { return w == 2 ? TC_TIMEOUT_MSG : COOP_TIMEOUT_MSG; }
 
 static int fetch_batch(mb_batch* b) {
     mb_ctx* ctx = b->ctx;
@@ -804,7 +836,7 @@ static int fetch_batch(mb_batch* b) {
     CUDA_TRY(ctx, cudaMemcpyAsync(b->h_i32, b->d_ost, std::max<size_t>(b->pk.ost.size(), 1) * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
     CUDA_TRY(ctx, cudaStreamSynchronize(st));
     for (const InstPlan& ip : b->pk.plans)
-        if (b->h_i32[ip.status + 7]) return fail(ctx, MB_E_TIMEOUT, COOP_TIMEOUT_MSG);
+        if (b->h_i32[ip.status + 7]) return fail(ctx, MB_E_TIMEOUT, timeout_msg(b->h_i32[ip.status + 7]));
     return MB_OK;
 }
 
@@ -1737,8 +1769,9 @@ extern "C" int mb_batch_solve_static(mb_ctx* ctx, mb_problem* const* probs, int3
     // the same choice as mb_batch_solve: a lone large instance runs grid-cooperatively, its control
     // block in the scratch
     const bool coop = ninst == 1 && !s.stable && (s.large == 1 || (s.large == 0 && pk.plans[0].fflops >= MB_LARGE_FLOPS));
-    const int lrc = coop ? mb_launch_coop(s_inst, mb::MODE_SOLVE, &ds, s_coop, mb_coop_grid(ctx->device, ctx->nsm), st)
-                         : mb_launch_batch(s_inst, ninst, mb::MODE_SOLVE, &ds, s_counter, g, s.precision == MB_PREC_FP32, st);
+    const int lrc = coop ? launch_coop(s, s_inst, mb::MODE_SOLVE, &ds, s_coop, ctx->device, ctx->nsm, st)
+                         : launch_batch(s, s_inst, ninst, mb::MODE_SOLVE, &ds, s_counter,
+                                        use_tc_build(s, false) ? std::min(g, ctx->nsm) : g, st);
     if (lrc) return fail(ctx, MB_E_CUDA, std::string("launch failed: ") + cudaGetErrorString(cudaGetLastError()));
     std::vector<double> h_out(std::max<size_t>(pk.out.size(), 1));
     std::vector<int32_t> h_ost(std::max<size_t>(pk.ost.size(), 1));
@@ -1746,7 +1779,7 @@ extern "C" int mb_batch_solve_static(mb_ctx* ctx, mb_problem* const* probs, int3
     CUDA_TRY(ctx, cudaMemcpyAsync(h_ost.data(), s_ost, h_ost.size() * sizeof(int32_t), cudaMemcpyDeviceToHost, st));
     CUDA_TRY(ctx, cudaStreamSynchronize(st));
     for (const InstPlan& ip : pk.plans)
-        if (h_ost[ip.status + 7]) return fail(ctx, MB_E_TIMEOUT, COOP_TIMEOUT_MSG);
+        if (h_ost[ip.status + 7]) return fail(ctx, MB_E_TIMEOUT, timeout_msg(h_ost[ip.status + 7]));
     for (size_t k = 0; k < pk.plans.size(); ++k)
         static_unpack(pk.plans[k], h_out.data(), h_ost.data(), s.max_iter, p_out ? p_out[k] : nullptr,
                       d_out ? d_out[k] : nullptr, y_out ? y_out[k] : nullptr, results ? &results[k] : nullptr);
@@ -1772,6 +1805,8 @@ extern "C" int mb_batch_solve_static(mb_ctx* ctx, mb_problem* const* probs, int3
 
 extern "C" int mb_launch_wave(const mb::DevInst* d_inst, int ninst, const mb::Settings* set, int* d_counter, int grid,
                               unsigned long long* done, long long seq0, int cap, cudaStream_t stream);
+extern "C" int mb_launch_wave_tc(const mb::DevInst* d_inst, int ninst, const mb::Settings* set, int* d_counter, int grid,
+                                 unsigned long long* done, long long seq0, int cap, cudaStream_t stream);
 
 namespace {
 
@@ -1954,7 +1989,9 @@ struct mb_server {
             uint64_t end = std::min<uint64_t>(s1, (s0 / cap + 1) * (uint64_t)cap);
             int n = (int)(end - s0);
             int g = std::min(n, grid_max);
-            if (mb_launch_wave(d_ring + s0 % cap, n, &ds, d_cnt + k, g, dv_done, (long long)s0, cap, ks[k])) {
+            const bool tcw = use_tc_build(set, false);
+            if ((tcw ? mb_launch_wave_tc : mb_launch_wave)(d_ring + s0 % cap, n, &ds, d_cnt + k, tcw ? std::min(g, grid_max / mb::CTA_PER_SM) : g,
+                                                           dv_done, (long long)s0, cap, ks[k])) {
                 fatal = std::string("serve launch: ") + cudaGetErrorString(cudaGetLastError());
                 return;
             }

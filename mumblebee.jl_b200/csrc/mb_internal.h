@@ -25,6 +25,8 @@ struct Settings {
     int32_t verbose, max_iter, scale_max_iter, refine_max_iter, newton_max_iter, stable, precision, large;
     double step_frac, feas_tol, gap_tol, near_factor, stall_tol, refine_stall_tol, aug_tol, infeas_abs, infeas_rel;
     double coop_wait;   // seconds at a grid barrier of the grid-cooperative mode (<= 0: 60)
+    int32_t fp32_tiles; // FP32 factor update tiles: 0 runtime's choice, 1 FFMA, 2 tensor cores (tcgen05)
+    int32_t reserved;
 };
 
 // One history row: the 17 fields of IPMHistoryRow (history/ipm.jl:1-4), stored as doubles.

@@ -15,6 +15,20 @@
 #include <cstdint>
 #include <cstdio>
 #include "mb_internal.h"
+
+// MB_TC = 1 builds the tensor-core variant of the solver kernels (mb_solver_tc.cu): the FP32
+// factor's update tiles on tcgen05.  A kernel that contains tcgen05 instructions runs one CTA per
+// SM (measured on B200: the occupancy calculator and the scheduler both drop from two to one), so
+// the default build, whose batched FP64 path needs two resident instances per SM to hide latency,
+// carries none; its extern "C" entry points get the suffix _tc in the variant.
+#ifndef MB_TC
+#define MB_TC 0
+#endif
+#if MB_TC
+#define MB_SFX(name) name##_tc
+#else
+#define MB_SFX(name) name
+#endif
 #include "mb_device.cuh"
 #include "mb_cones.cuh"
 #include "mb_tdc.cuh"
@@ -39,6 +53,13 @@ struct Shared {
     int flag;
     int ibuf[8];
     long long wait_ns;      // grid-cooperative mode: longest wait at a grid barrier
+    unsigned long long mbar[2];   // tensor-core update: completion of the MMAs that read stage 0 / 1
+    unsigned int tmem;      // tensor-core update: base address of the CTA's accumulator columns
+    unsigned int tc_ph;     // tensor-core update: parity of the next wait on mbar[b] at bit b
+    int tc_on;              // FP32 update tiles on the tensor cores: TMEM held, barriers set up
+    int tc_ok;              // tensor-core update: 0 once a completion wait ran out
+    int* tc_err;            // set to 2 when a completion wait runs out (instance status word 7, or the
+                            // grid-cooperative abort flag on a helper CTA)
 };
 
 // D += A·B on the FP64 tensor path (mma.m8n8k4, fragments: A[g][t], B[t][g], C[g][2t+i] with
@@ -470,9 +491,318 @@ __device__ __noinline__ void tiles_f32(float* M, int nf, int ntile, int K0, int 
     __syncthreads();
 }
 
+#if MB_TC
+// ---- FP32 update tiles on the 5th-generation tensor cores (tcgen05.mma kind::tf32) -----------
+// 3xTF32: a = ah + al with ah = a rounded to TF32 and al = the rest rounded to TF32; a·b is taken
+// as al·bh + ah·bl + ah·bh (al·bl lies below FP32 rounding).  The tensor cores accumulate one
+// 16-column K step of these products in FP32 in tensor memory (two 128 x 64 accumulators, 128 TMEM
+// columns, lane = tile row, column = tile column, alternating between steps); the CTA's threads
+// subtract each step's partial product from the tile in FP32 registers, round to nearest, so the
+// update keeps FP32-grade accuracy (the tensor cores' own accumulation truncates).  The threads
+// stage A (128 rows) and B (64 rows) of each step from the column-major front into shared memory in
+// the canonical K-major, no-swizzle layout (core matrices of 8 rows x 16 bytes), hi and lo parts
+// separately, two stages alternating; one thread issues the step's six MMAs and commits them to
+// the stage's mbarrier, on which every thread waits before reading the step's accumulator.  The
+// front's leading dimension is its order, so its columns are not 16-byte aligned in general and
+// the operands cannot come by TMA; the next step's loads and the previous step's read-out overlap
+// the MMAs.
+constexpr int TC_M = 128, TC_N = 64, TC_KC = 16;
+constexpr int TC_A_BYTES = TC_M * TC_KC * 4;                      // one part (hi or lo) of A, one stage
+constexpr int TC_B_BYTES = TC_N * TC_KC * 4;
+constexpr int TC_STAGE = 2 * TC_A_BYTES + 2 * TC_B_BYTES;        // A hi, A lo, B hi, B lo
+constexpr int TC_LBO_A = (TC_M / 8) * 128, TC_LBO_B = (TC_N / 8) * 128;   // between 16-byte K groups
+constexpr int TC_MIN_FRONT = 128;                                // smaller fronts stay on FFMA tiles
+constexpr long long TC_WAIT_NS = 1000000000LL;                   // bounded completion wait (1 s)
+// instruction descriptor: D F32 (bits 4-5 = 1), A and B TF32 (bits 7-9, 10-12 = 2), both K-major,
+// N >> 3 at bits 17-22, M >> 4 at bits 24-28
+constexpr uint32_t TC_IDESC = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(TC_N >> 3) << 17) |
+                              ((uint32_t)(TC_M >> 4) << 24);
+static_assert(NT == 256, "the staging maps assume 256 threads");
+static_assert(2 * TC_STAGE <= (int)sizeof(double) * 4 * TS * TLD, "two stages fit in Shared::tile");
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// shared-memory matrix descriptor: start address, leading (K-direction) and stride (8-row group)
+// byte offsets, all >> 4; version 1 (bit 46); no swizzle (bits 61-63 = 0)
+__device__ __forceinline__ uint64_t tc_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+    return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
+}
+__device__ __forceinline__ void tc_mma(uint32_t d, uint64_t a, uint64_t b, uint32_t acc) {
+    asm volatile("{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                 "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n"
+                 ::"r"(d), "l"(a), "l"(b), "r"(TC_IDESC), "r"(acc) : "memory");
+}
+__device__ __forceinline__ void tc_commit(unsigned long long* bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                 ::"r"(smem_u32(bar)) : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void mbar_init(unsigned long long* bar) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar)) : "memory");
+}
+// thread-local wait for the completion of the barrier phase of parity `ph`; false when it has not
+// completed within TC_WAIT_NS
+__device__ __forceinline__ bool mbar_wait(unsigned long long* bar, uint32_t ph) {
+    const uint32_t a = smem_u32(bar);
+    unsigned long long t0 = 0;
+    for (unsigned it = 0;; ++it) {
+        uint32_t ok;
+        asm volatile("{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                     "selp.u32 %0, 1, 0, p;\n\t}\n" : "=r"(ok) : "r"(a), "r"(ph) : "memory");
+        if (ok) return true;
+        if ((it & 255) == 0) {
+            unsigned long long t;
+            asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+            if (it == 0) t0 = t;
+            else if ((long long)(t - t0) > TC_WAIT_NS) return false;
+        }
+    }
+}
+// 32 lanes x 32 columns of FP32 accumulator from tensor memory (the warp's lane quarter), waited
+__device__ __forceinline__ void tc_ld32(uint32_t taddr, float (&v)[32]) {
+    uint32_t r[32];
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+                 "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];\n\t"
+                 "tcgen05.wait::ld.sync.aligned;\n"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+                   "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
+                   "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]),
+                   "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]),
+                   "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+                 : "r"(taddr) : "memory");
+#pragma unroll
+    for (int j = 0; j < 32; ++j) v[j] = __uint_as_float(r[j]);
+}
+// a = hi + lo + O(2^-22 |a|): hi = a rounded to nearest TF32, lo = the rest (exact in FP32) rounded
+// to nearest TF32; the tensor cores take both as they are
+__device__ __forceinline__ void tf32_split(float a, float& hi, float& lo) {
+    uint32_t h, l;
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(h) : "f"(a));
+    hi = __uint_as_float(h);
+    asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(l) : "f"(a - hi));
+    lo = __uint_as_float(l);
+}
+
+// The trailing-update tiles of tiles_f32, 128 rows each, on the tensor cores: M[r, c] -=
+// Σ_{k in [K0, K1)} M[r, k] M[c, k] for r in [rb, rb + 128), c in [J, J + nb), r >= c; every
+// (tile, 16-column K step) pair is one pipeline step.  Each step's product goes to its own
+// accumulator (two, alternating) and is subtracted from the tile in FP32 registers while the next
+// step's MMAs run, so the tensor cores' FP32 accumulation covers 16 products only.
+template <class TileAt>
+__device__ __noinline__ void tiles_tc32(float* M, int nf, int ntile, int K0, int K1, Shared& sh, TileAt at) {
+    if (ntile <= 0 || K1 <= K0) return;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int quad = warp & 3, half = warp >> 2;
+    const int nk = (K1 - K0 + TC_KC - 1) / TC_KC;
+    const int nstep = ntile * nk;
+    unsigned char* st = reinterpret_cast<unsigned char*>(sh.tile);
+    const uint32_t st0 = smem_u32(st);
+    // the accumulator columns and the two barriers belong to the CTA from tc_setup to tc_teardown;
+    // the barriers' phases carry over from the previous call
+    const uint32_t tmem = sh.tmem;
+    uint32_t ph[2] = {sh.tc_ph & 1u, (sh.tc_ph >> 1) & 1u};
+    // the operand rows this thread stages: A row ra (16-byte K groups ga and ga + 2), B row rb_
+    const int ra = tid & 127, ga = tid >> 7;
+    const int rb_ = tid & 63, gb = tid >> 6;
+    float va0[4], va1[4], vb[4];
+    int tile_next = -1;
+    UTile unext{0, 0, 0};
+    auto load = [&](int s) {
+        const int ti = s / nk;
+        if (ti != tile_next) { unext = at(ti); tile_next = ti; }
+        const int k0 = K0 + TC_KC * (s % nk);
+        const int cmax = min(nf, unext.J + unext.nb);
+        const int r = unext.rb + ra, c = unext.J + rb_;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int k1 = k0 + 4 * ga + j, k2 = k0 + 4 * (ga + 2) + j, k3 = k0 + 4 * gb + j;
+            va0[j] = (r < nf && k1 < K1) ? M[r + (int64_t)k1 * nf] : 0.f;
+            va1[j] = (r < nf && k2 < K1) ? M[r + (int64_t)k2 * nf] : 0.f;
+            vb[j] = (c < cmax && k3 < K1) ? M[c + (int64_t)k3 * nf] : 0.f;
+        }
+    };
+    // row r, K group g of an operand of R rows: hi part at base + off, lo part at base + part + off
+    auto put = [&](unsigned char* base, int r, int g, int R, const float (&v)[4], int part) {
+        float4 h, l;
+        tf32_split(v[0], h.x, l.x); tf32_split(v[1], h.y, l.y);
+        tf32_split(v[2], h.z, l.z); tf32_split(v[3], h.w, l.w);
+        const int off = g * (R / 8) * 128 + (r >> 3) * 128 + (r & 7) * 16;
+        *reinterpret_cast<float4*>(base + off) = h;
+        *reinterpret_cast<float4*>(base + part + off) = l;
+    };
+    // Read-out of step r: this thread's 32 outputs (tile row 32 quad + lane, columns 32 half + j)
+    // of the step's partial product leave tensor memory and are subtracted, in FP32 round-to-nearest,
+    // from acc, which holds M's values at the tile's first step and is stored back after its last
+    float acc[32];
+    UTile ur{0, 0, 0};
+    auto readout = [&](int r) {
+        const int b = r & 1, q = r % nk;
+        if (q == 0) {
+            ur = at(r / nk);
+            const int row = ur.rb + 32 * quad + lane, cmax = min(nf, ur.J + ur.nb);
+#pragma unroll
+            for (int j = 0; j < 32; ++j) {
+                const int col = ur.J + 32 * half + j;
+                acc[j] = (row < nf && col < cmax && row >= col) ? M[row + (int64_t)col * nf] : 0.f;
+            }
+        }
+        if (!mbar_wait(&sh.mbar[b], ph[b])) sh.tc_ok = 0;
+        ph[b] ^= 1u;
+        tc_fence_after();
+        __syncwarp();
+        float v[32];
+        tc_ld32(tmem + (uint32_t)(b * TC_N) + ((uint32_t)(32 * quad) << 16) + 32 * half, v);
+#pragma unroll
+        for (int j = 0; j < 32; ++j) acc[j] -= v[j];
+        tc_fence_before();
+        if (q == nk - 1) {
+            const int row = ur.rb + 32 * quad + lane, cmax = min(nf, ur.J + ur.nb);
+            if (row < nf) {
+#pragma unroll
+                for (int j = 0; j < 32; ++j) {
+                    const int col = ur.J + 32 * half + j;
+                    if (col < cmax && row >= col) M[row + (int64_t)col * nf] = acc[j];
+                }
+            }
+        }
+    };
+    load(0);
+    int s = 0;
+    for (; s < nstep; ++s) {
+        const int b = s & 1, q = s % nk;
+        // stage b and accumulator b are free: step s - 2 was read out by every thread (after its wait)
+        __syncthreads();
+        if (!sh.tc_ok) break;
+        unsigned char* sb = st + b * TC_STAGE;
+        put(sb, ra, ga, TC_M, va0, TC_A_BYTES);
+        put(sb, ra, ga + 2, TC_M, va1, TC_A_BYTES);
+        put(sb + 2 * TC_A_BYTES, rb_, gb, TC_N, vb, TC_B_BYTES);
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");   // generic writes -> tensor-core reads
+        __syncthreads();
+        if (tid == 0) {
+            tc_fence_after();
+            const uint32_t d = tmem + (uint32_t)(b * TC_N);
+            const uint32_t a_hi = st0 + b * TC_STAGE, a_lo = a_hi + TC_A_BYTES;
+            const uint32_t b_hi = a_hi + 2 * TC_A_BYTES, b_lo = b_hi + TC_B_BYTES;
+#pragma unroll
+            for (int kk = 0; kk < TC_KC / 8; ++kk) {
+                const uint32_t oa = kk * 2 * TC_LBO_A, ob = kk * 2 * TC_LBO_B;
+                tc_mma(d, tc_desc(a_lo + oa, TC_LBO_A, 128), tc_desc(b_hi + ob, TC_LBO_B, 128), kk > 0 ? 1u : 0u);
+                tc_mma(d, tc_desc(a_hi + oa, TC_LBO_A, 128), tc_desc(b_lo + ob, TC_LBO_B, 128), 1u);
+                tc_mma(d, tc_desc(a_hi + oa, TC_LBO_A, 128), tc_desc(b_hi + ob, TC_LBO_B, 128), 1u);
+            }
+            tc_commit(&sh.mbar[b]);
+        }
+        (void)q;
+        if (s + 1 < nstep) load(s + 1);
+        if (s >= 1) readout(s - 1);        // overlaps the MMAs of step s
+    }
+    __syncthreads();
+    if (s == nstep && sh.tc_ok) readout(nstep - 1);
+    __syncthreads();
+    // a wait that ran out: the solve is reported failed, and the barriers' phases are unknown, so
+    // this CTA's later updates use the FFMA tiles
+    if (tid == 0) {
+        if (!sh.tc_ok) {
+            if (sh.tc_err) atomicExch(sh.tc_err, 2);
+            sh.tc_on = 0;
+        }
+        sh.tc_ph = ph[0] | (ph[1] << 1);
+    }
+    __syncthreads();
+}
+
+// Set-up of the tensor-core update for the CTA's lifetime, by all its threads: warp 0 allocates
+// the accumulator's TMEM columns, thread 0 initialises the two stage barriers.  `on` = 0 leaves
+// the FFMA tiles in use and allocates nothing.
+__device__ void tc_setup(Shared& sh, bool on) {
+    __syncthreads();
+    if (threadIdx.x == 0) { sh.tc_on = on ? 1 : 0; sh.tc_ok = 1; sh.tc_ph = 0; sh.tc_err = nullptr; }
+    if (!on) { __syncthreads(); return; }
+    __syncwarp();                        // the .sync.aligned tcgen05 forms need converged warps
+    if ((threadIdx.x >> 5) == 0)
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                     ::"r"(smem_u32(&sh.tmem)), "r"(2 * TC_N) : "memory");
+    if (threadIdx.x == 0) {
+        mbar_init(&sh.mbar[0]);
+        mbar_init(&sh.mbar[1]);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+}
+
+// Release of the accumulator columns before the CTA exits (after tc_setup with on = 1; a CTA must
+// free its TMEM before it ends)
+__device__ void tc_teardown(Shared& sh, bool on) {
+    tc_fence_before();
+    __syncthreads();
+    if (!on) return;
+    tc_fence_after();
+    __syncwarp();
+    if ((threadIdx.x >> 5) == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(sh.tmem), "r"(2 * TC_N) : "memory");
+    __syncthreads();
+}
+
+// FP32 trailing update on the tensor cores: 128-row tiles from J0 down, dealt round-robin over
+// nranks CTAs
+__device__ void update_cols_tc32(float* M, int nf, int J0, int nb, int K0, int K1, Shared& sh, int rank, int nranks) {
+    if (K1 <= K0 || nb <= 0) return;
+    const int first = J0 + TC_M * rank, step = TC_M * nranks;
+    const int ntile = first < nf ? (nf - first + step - 1) / step : 0;
+    tiles_tc32(M, nf, ntile, K0, K1, sh, [=](int i) { return UTile{first + step * i, J0, nb}; });
+}
+
+// the separator's Schur complement on the tensor cores: the 128-row tiles of every 64-column block
+// of [J0, nf), in column-block order, dealt round-robin over nranks CTAs
+__device__ void schur_tiles_tc32(float* M, int nf, int J0, int K1, Shared& sh, int rank, int nranks) {
+    if (K1 <= 0 || J0 >= nf) return;
+    const int nblk = (nf - J0 + 63) / 64;
+    int total = 0;
+    for (int b = 0; b < nblk; ++b) total += (nf - J0 - 64 * b + TC_M - 1) / TC_M;
+    const int ntile = rank < total ? (total - rank + nranks - 1) / nranks : 0;
+    auto at = [=](int i) {
+        int gi = rank + nranks * i, b = 0;
+        for (;;) {
+            const int nt = (nf - J0 - 64 * b + TC_M - 1) / TC_M;
+            if (gi < nt) break;
+            gi -= nt;
+            ++b;
+        }
+        const int J = J0 + 64 * b;
+        return UTile{J + TC_M * gi, J, min(64, nf - J)};
+    };
+    tiles_tc32(M, nf, ntile, 0, K1, sh, at);
+}
+
+#else
+// the default build has no tensor-core tiles
+__device__ void update_cols_tc32(float*, int, int, int, int, int, Shared&, int, int) {}
+__device__ void schur_tiles_tc32(float*, int, int, int, Shared&, int, int) {}
+__device__ __forceinline__ void tc_setup(Shared& sh, bool) {
+    __syncthreads();
+    if (threadIdx.x == 0) { sh.tc_on = 0; sh.tc_ok = 1; sh.tc_ph = 0; sh.tc_err = nullptr; }
+    __syncthreads();
+}
+__device__ __forceinline__ void tc_teardown(Shared&, bool) { __syncthreads(); }
+#endif
+
+// FP32 update tiles go to the tensor cores for fronts from TC_MIN_FRONT up unless
+// settings.fp32_tiles selects the FFMA tiles
+__device__ __forceinline__ bool use_tc32(int nf, const Shared& sh) { return MB_TC && sh.tc_on && nf >= 128; }
+
 __device__ void update_cols_f32(float* M, int nf, int J0, int nb, int K0, int K1, Shared& sh, int rank = 0,
                                 int nranks = 1) {
     if (K1 <= K0 || nb <= 0) return;
+    if (use_tc32(nf, sh)) {
+        update_cols_tc32(M, nf, J0, nb, K0, K1, sh, rank, nranks);
+        __syncthreads();
+        return;
+    }
     const int first = J0 + TS * rank, step = TS * nranks;
     const int ntile = first < nf ? (nf - first + step - 1) / step : 0;
     tiles_f32(M, nf, ntile, K0, K1, sh, [=](int i) { return UTile{first + step * i, J0, nb}; });
@@ -495,6 +825,7 @@ __device__ void schur_tiles(FT* M, int nf, int J0, int K1, Shared& sh, int rank,
         return UTile{J + TS * gi, J, min(64, nf - J)};
     };
     if constexpr (sizeof(FT) == 8) tiles_f64((double*)M, nf, ntile, 0, K1, sh, at);
+    else if (use_tc32(nf, sh)) schur_tiles_tc32((float*)M, nf, J0, K1, sh, rank, nranks);
     else tiles_f32((float*)M, nf, ntile, 0, K1, sh, at);
     __syncthreads();
 }
@@ -2563,16 +2894,20 @@ struct BatchArgs {
     int cap;
 };
 
-__global__ void __launch_bounds__(NT, CTA_PER_SM) ipm_batch_kernel(BatchArgs a) {
+__global__ void __launch_bounds__(NT, CTA_PER_SM) MB_SFX(ipm_batch_kernel)(BatchArgs a) {
     extern __shared__ __align__(16) unsigned char mb_dsmem[];
     Shared& sh = *reinterpret_cast<Shared*>(mb_dsmem);
     __shared__ int next;
+    const bool tc = MB_TC && a.set.precision != 0;   // the tensor-core build, and an FP32 factor may run
+    tc_setup(sh, tc);
     for (;;) {
         if (threadIdx.x == 0) next = atomicAdd(a.counter, 1);
         __syncthreads();
         int k = next;
         __syncthreads();
         if (k >= a.ninst) break;
+        if (threadIdx.x == 0) sh.tc_err = a.inst[k].status + 7;
+        __syncthreads();
         unsigned long long t0 = globaltimer();
         solve_instance<false>(a.inst[k], a.set, sh, a.mode, nullptr);
         if (threadIdx.x == 0) {
@@ -2585,16 +2920,26 @@ __global__ void __launch_bounds__(NT, CTA_PER_SM) ipm_batch_kernel(BatchArgs a) 
             }
         }
     }
+    tc_teardown(sh, tc);
 }
 
 // One large instance on the whole GPU (cooperative launch): CTA 0 runs the solve and posts the
 // dense work of its large fronts to the other CTAs; COOP_EXIT releases them when it is done.
-__global__ void __launch_bounds__(NT, CTA_PER_SM) ipm_coop_kernel(BatchArgs a, CoopCtl* c) {
+__global__ void __launch_bounds__(NT, CTA_PER_SM) MB_SFX(ipm_coop_kernel)(BatchArgs a, CoopCtl* c) {
     extern __shared__ __align__(16) unsigned char mb_dsmem[];
     Shared& sh = *reinterpret_cast<Shared*>(mb_dsmem);
-    if (threadIdx.x == 0) sh.wait_ns = a.set.coop_wait > 0 ? (long long)(a.set.coop_wait * 1e9) : COOP_WAIT_NS;
+    const bool tc = MB_TC && a.set.precision != 0;   // the tensor-core build, and an FP32 factor may run
+    tc_setup(sh, tc);
+    if (threadIdx.x == 0) {
+        sh.wait_ns = a.set.coop_wait > 0 ? (long long)(a.set.coop_wait * 1e9) : COOP_WAIT_NS;
+        sh.tc_err = blockIdx.x == 0 ? a.inst[0].status + 7 : &c->abort;
+    }
     __syncthreads();
-    if (blockIdx.x != 0) { coop_helper(c, sh); return; }
+    if (blockIdx.x != 0) {
+        coop_helper(c, sh);
+        tc_teardown(sh, tc);
+        return;
+    }
     const DevInst& I = a.inst[0];
     const unsigned long long t0 = globaltimer();
     solve_instance<true>(I, a.set, sh, a.mode, c);
@@ -2606,22 +2951,23 @@ __global__ void __launch_bounds__(NT, CTA_PER_SM) ipm_coop_kernel(BatchArgs a, C
     }
     coop_barrier(c, sh);
     if (threadIdx.x == 0 && ld_volatile_i32(&c->abort) != 0) I.status[7] = 1;
+    tc_teardown(sh, tc);
 }
 
 }  // namespace mb
 
 // grid-cooperative launch of one instance: every CTA of the grid co-resident (grid <= 2 per SM)
-extern "C" int mb_launch_coop(const mb::DevInst* d_inst, int mode, const mb::Settings* set, mb::CoopCtl* d_ctl,
+extern "C" int MB_SFX(mb_launch_coop)(const mb::DevInst* d_inst, int mode, const mb::Settings* set, mb::CoopCtl* d_ctl,
                               int grid, cudaStream_t stream) {
     cudaError_t e = cudaMemsetAsync(d_ctl, 0, sizeof(mb::CoopCtl), stream);
     if (e != cudaSuccess) return -1;
-    e = cudaFuncSetAttribute(mb::ipm_coop_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(mb::Shared));
+    e = cudaFuncSetAttribute(mb::MB_SFX(ipm_coop_kernel), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(mb::Shared));
     if (e != cudaSuccess) return -1;
     mb::BatchArgs a;
     a.inst = d_inst; a.ninst = 1; a.mode = mode; a.set = *set; a.counter = nullptr;
     a.done = nullptr; a.seq0 = 0; a.cap = 1;
     void* args[] = {(void*)&a, (void*)&d_ctl};
-    e = cudaLaunchCooperativeKernel((const void*)mb::ipm_coop_kernel, dim3(grid), dim3(mb::NT), args,
+    e = cudaLaunchCooperativeKernel((const void*)mb::MB_SFX(ipm_coop_kernel), dim3(grid), dim3(mb::NT), args,
                                     sizeof(mb::Shared), stream);
     return e == cudaSuccess ? 0 : -2;
 }
@@ -2629,7 +2975,7 @@ extern "C" int mb_launch_coop(const mb::DevInst* d_inst, int mode, const mb::Set
 // ---------------------------------------------------------------------------------------------
 // launch entry used by the host runtime
 // ---------------------------------------------------------------------------------------------
-extern "C" int mb_launch_batch(const mb::DevInst* d_inst, int ninst, int mode, const mb::Settings* set,
+extern "C" int MB_SFX(mb_launch_batch)(const mb::DevInst* d_inst, int ninst, int mode, const mb::Settings* set,
                                int* d_counter, int grid, int fp32, cudaStream_t stream) {
     mb::BatchArgs a;
     a.inst = d_inst; a.ninst = ninst; a.mode = mode; a.set = *set; a.counter = d_counter;
@@ -2637,13 +2983,14 @@ extern "C" int mb_launch_batch(const mb::DevInst* d_inst, int ninst, int mode, c
     cudaError_t e = cudaMemsetAsync(d_counter, 0, sizeof(int), stream);
     if (e != cudaSuccess) return -1;
     (void)fp32;
-    e = cudaFuncSetAttribute(mb::ipm_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(mb::Shared));
+    e = cudaFuncSetAttribute(mb::MB_SFX(ipm_batch_kernel), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(mb::Shared));
     if (e != cudaSuccess) return -1;
-    mb::ipm_batch_kernel<<<grid, mb::NT, sizeof(mb::Shared), stream>>>(a);
+    mb::MB_SFX(ipm_batch_kernel)<<<grid, mb::NT, sizeof(mb::Shared), stream>>>(a);
     e = cudaGetLastError();
     return e == cudaSuccess ? 0 : -2;
 }
 
+#if !MB_TC
 // ---------------------------------------------------------------------------------------------
 // Fixed device scratch for mb_batch_solve_static (no counterpart in the reference).
 //
@@ -2681,28 +3028,30 @@ extern "C" int mb_static_scratch(int device, void** ptr, size_t* bytes) {
     return (int)cudaSuccess;
 }
 
+#endif  // !MB_TC
+
 // the serving loop's launch: one admission wave of ring slots [seq0, seq0 + ninst), each instance
 // stamping done[(seq0 + k) % cap] when it finishes
-extern "C" int mb_launch_wave(const mb::DevInst* d_inst, int ninst, const mb::Settings* set, int* d_counter, int grid,
+extern "C" int MB_SFX(mb_launch_wave)(const mb::DevInst* d_inst, int ninst, const mb::Settings* set, int* d_counter, int grid,
                               unsigned long long* done, long long seq0, int cap, cudaStream_t stream) {
     mb::BatchArgs a;
     a.inst = d_inst; a.ninst = ninst; a.mode = mb::MODE_SOLVE; a.set = *set; a.counter = d_counter;
     a.done = done; a.seq0 = seq0; a.cap = cap;
     cudaError_t e = cudaMemsetAsync(d_counter, 0, sizeof(int), stream);
     if (e != cudaSuccess) return -1;
-    e = cudaFuncSetAttribute(mb::ipm_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(mb::Shared));
+    e = cudaFuncSetAttribute(mb::MB_SFX(ipm_batch_kernel), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(mb::Shared));
     if (e != cudaSuccess) return -1;
-    mb::ipm_batch_kernel<<<grid, mb::NT, sizeof(mb::Shared), stream>>>(a);
+    mb::MB_SFX(ipm_batch_kernel)<<<grid, mb::NT, sizeof(mb::Shared), stream>>>(a);
     return cudaGetLastError() == cudaSuccess ? 0 : -2;
 }
 
 // CTAs of ipm_coop_kernel that can be co-resident (the grid of a cooperative launch)
-extern "C" int mb_coop_grid(int device, int nsm) {
+extern "C" int MB_SFX(mb_coop_grid)(int device, int nsm) {
     (void)device;
     int per_sm = 0;
-    if (cudaFuncSetAttribute(mb::ipm_coop_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(mb::Shared)) != cudaSuccess)
+    if (cudaFuncSetAttribute(mb::MB_SFX(ipm_coop_kernel), cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(mb::Shared)) != cudaSuccess)
         return nsm;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, mb::ipm_coop_kernel, mb::NT, sizeof(mb::Shared)) != cudaSuccess || per_sm < 1)
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, mb::MB_SFX(ipm_coop_kernel), mb::NT, sizeof(mb::Shared)) != cudaSuccess || per_sm < 1)
         return nsm;
     return nsm * (per_sm < mb::CTA_PER_SM ? per_sm : mb::CTA_PER_SM);
 }

@@ -21,7 +21,7 @@ class mb_settings(C.Structure):
                 ("newton_max_iter", I32), ("stable", I32), ("precision", I32), ("large", I32),
                 ("step_frac", F64), ("feas_tol", F64), ("gap_tol", F64), ("near_factor", F64),
                 ("stall_tol", F64), ("refine_stall_tol", F64), ("aug_tol", F64), ("infeas_abs", F64),
-                ("infeas_rel", F64), ("coop_wait", F64)]
+                ("infeas_rel", F64), ("coop_wait", F64), ("fp32_tiles", I32), ("reserved", I32)]
 
 
 class mb_bsm(C.Structure):

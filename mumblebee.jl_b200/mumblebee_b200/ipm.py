@@ -108,6 +108,7 @@ class IPMSettings:
     precision: str = "fp64"          # "fp64", "fp32" or "mixed" (factor precision; refinement stays FP64)
     large: int = 0                   # a lone large instance runs grid-cooperatively: 0 auto, 1 always, -1 never
     coop_wait: float = 60.0          # seconds a CTA of that mode waits at a grid barrier (then MB_E_TIMEOUT)
+    fp32_tiles: int = 0              # FP32 factor update tiles: 0 auto, 1 FFMA, 2 tensor cores (tcgen05, 3xTF32)
 
     def to_c(self) -> mb_settings:
         s = mb_settings()

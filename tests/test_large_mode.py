@@ -33,11 +33,13 @@ def test_large_mode_equals_one_cta(name):
         assert np.array_equal(x, y)
 
 
-def test_large_mode_mixed_precision_equals_one_cta():
-    """The FP32 tiles, panel rows and solves of the mixed path, shared with the helpers."""
+@pytest.mark.parametrize("tiles", [1, 2])
+def test_large_mode_mixed_precision_equals_one_cta(tiles):
+    """The FP32 tiles, panel rows and solves of the mixed path, shared with the helpers: FFMA tiles
+    (fp32_tiles = 1) and the tensor-core build (2), each against one CTA of the same build."""
     prob = IPMProblem.from_dict(block_problem(CASES["port300"]()), ctx=Context.default())
-    a = solve(prob, IPMSettings(large=-1, precision="mixed"))
-    b = solve(prob, IPMSettings(large=1, precision="mixed"))
+    a = solve(prob, IPMSettings(large=-1, precision="mixed", fp32_tiles=tiles))
+    b = solve(prob, IPMSettings(large=1, precision="mixed", fp32_tiles=tiles))
     assert a.status == b.status and a.niter == b.niter and a.nfp32 == b.nfp32
     assert a.pobj == b.pobj and np.array_equal(a.p, b.p)
 

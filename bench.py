@@ -58,6 +58,7 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-compare", action="store_true", help="skip the other precision's arm")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving arm")
+    ap.add_argument("--no-tune", action="store_true", help="launch configuration without the autotuner")
     ap.add_argument("--serve-rate", type=float, default=2000.0, help="offered requests per second")
     ap.add_argument("--serve-seconds", type=float, default=1.0, help="length of the arrival window")
     ap.add_argument("--serve-nmin", type=int, default=100)
@@ -277,25 +278,37 @@ def main_config(args, ws):
 
 def timed_arm(probs, precision, args, pg, local, ws, ctx, lower):
     """Prepare a batch at `precision`, warm up, time `steps` persistent launches (CUDA events on the
-    launching stream, max over ranks) and read back statuses, iterations and latencies."""
+    launching stream, max over ranks) and read back statuses, iterations and latencies.  The launch
+    configuration (kernel build and resident instances per SM) is the autotuner's choice from
+    timed trial launches on a sample of the same instances, unless --fp32-tiles fixes the build."""
+    from mumblebee_b200.autotune import tune
     from mumblebee_b200.ipm import Batch, IPMSettings
     settings = IPMSettings(precision=precision, fp32_tiles=args.fp32_tiles)
+    t0 = time.time()
+    tuned = None
+    grid = 0
+    if args.fp32_tiles == 0 and not args.no_tune:
+        import torch
+        nsm = torch.cuda.get_device_properties(local).multi_processor_count
+        choice = tune(probs, settings, nsm=nsm, seed=args.seed)
+        settings, grid = choice.settings, choice.grid
+        tuned = dict(choice.as_dict(), tune_s=round(time.time() - t0, 2))
     t0 = time.time()
     batch = Batch(probs, settings, ctx=ctx)
     t_prep = time.time() - t0
     st = batch.stats()
     for _ in range(args.warmup):
-        batch.run()
+        batch.run(grid=grid)
     barrier(pg, local)
     clk = Clocks(local)
-    ms_steps = [batch.run() for _ in range(args.steps)]
+    ms_steps = [batch.run(grid=grid) for _ in range(args.steps)]
     clocks = clk.stop()
     ms = sum(ms_steps) / len(ms_steps)
     ms_max = allreduce_max(pg, ms, local)
     res = batch.fetch(want_vectors=False)          # results of the last timed launch
     lat, svc = batch.latencies_ms()
     ntrsv = batch.timers()[:, batch.SECTIONS.index("ntrsv")]
-    out = {"precision": precision, "ms": ms, "ms_max": ms_max, "ms_steps": ms_steps, "clocks": clocks,
+    out = {"precision": precision, "autotune": tuned, "settings": settings, "grid": grid, "ms": ms, "ms_max": ms_max, "ms_steps": ms_steps, "clocks": clocks,
            "value": args.count * ws / (ms_max / 1e3), "res": res, "stats": st, "prepare_s": t_prep,
            "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
                           "max": float(lat.max())},
@@ -577,12 +590,17 @@ def main():
     # end to end through the C ABI: host problems in, host results out
     e2e = None
     if not args.no_e2e:
-        settings = IPMSettings(precision=args.precision)
-        batch_solve(probs, settings)          # warm-up
+        # the main arm's launch configuration; a grid left to the library (0: two CTAs per SM in the
+        # default build, one in the tensor-core build) keeps the call's chunked pipeline
+        settings, grid = main_arm["settings"], main_arm["grid"]
+        tuned = main_arm["autotune"]
+        if tuned is None or tuned["choice"] in ("ffma_2_per_sm", "tcgen05_1_per_sm"):
+            grid = 0
+        batch_solve(probs, settings, grid=grid)          # warm-up
         barrier(pg, local)
         t = time.perf_counter()
         for _ in range(max(1, min(args.steps, 2))):
-            batch_solve(probs, settings)
+            batch_solve(probs, settings, grid=grid)
         dt = (time.perf_counter() - t) / max(1, min(args.steps, 2))
         dt = allreduce_max(pg, dt, local)
         st = main_arm["stats"]
@@ -604,7 +622,7 @@ def main():
         arms = {a["precision"]: {"solves_per_s": a["value"], "ms_per_step": a["ms_max"],
                                  "latency_ms": a["latency_ms"], "solve_ms": a["solve_ms"],
                                  "optimal": f"{a['optimal']}/{args.count}", "near_optimal": a["near_optimal"],
-                                 "iters_mean": a["iters_mean"]}
+                                 "iters_mean": a["iters_mean"], "autotune": a["autotune"]}
                 for a in (main_arm, other) if a is not None}
         if "mixed" in arms and "fp64" in arms:
             arms["mixed_over_fp64"] = arms["mixed"]["solves_per_s"] / arms["fp64"]["solves_per_s"]

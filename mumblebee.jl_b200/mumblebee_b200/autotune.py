@@ -61,12 +61,13 @@ def _sample(probs, size, seed):
 
 def tune(probs, settings: IPMSettings | None = None, nsm: int = 148, sample: int = 0, repeats: int = 2,
          seed: int = 0, candidates=CANDIDATES) -> Choice:
-    """Time each candidate launch configuration on a sample of `probs` (by default twice the SM
-    count of instances, enough to fill every candidate's grid) and return the fastest.  An FP64
-    factor never runs the FP32 tiles, so for precision "fp64" only the resident-instance count is
-    tuned.  Each trial is a warm-up launch and `repeats` timed launches (CUDA events)."""
+    """Time each candidate launch configuration on a sample of `probs` (by default eight instances
+    per SM: a persistent CTA then runs several instances, as in a large batch, so that the trial
+    measures throughput rather than the latency of one instance per CTA) and return the fastest.
+    An FP64 factor never runs the FP32 tiles, so for precision "fp64" only the resident-instance
+    count is tuned.  Each trial is a warm-up launch and `repeats` timed launches (CUDA events)."""
     settings = settings or IPMSettings()
-    sub = _sample(probs, sample or 2 * nsm, seed)
+    sub = _sample(probs, sample or 8 * nsm, seed)
     trials, best = {}, None
     for name, tiles, per_sm in candidates:
         if settings.precision == "fp64" and tiles == 2:

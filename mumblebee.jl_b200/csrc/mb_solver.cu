@@ -759,8 +759,8 @@ __device__ void update_cols_tc32(float* M, int nf, int J0, int nb, int K0, int K
 
 // the separator's Schur complement on the tensor cores: the 128-row tiles of every 64-column block
 // of [J0, nf), in column-block order, dealt round-robin over nranks CTAs
-__device__ void schur_tiles_tc32(float* M, int nf, int J0, int K1, Shared& sh, int rank, int nranks) {
-    if (K1 <= 0 || J0 >= nf) return;
+__device__ void schur_tiles_tc32(float* M, int nf, int J0, int K0, int K1, Shared& sh, int rank, int nranks) {
+    if (K1 <= K0 || J0 >= nf) return;
     const int nblk = (nf - J0 + 63) / 64;
     int total = 0;
     for (int b = 0; b < nblk; ++b) total += (nf - J0 - 64 * b + TC_M - 1) / TC_M;
@@ -776,13 +776,13 @@ __device__ void schur_tiles_tc32(float* M, int nf, int J0, int K1, Shared& sh, i
         const int J = J0 + 64 * b;
         return UTile{J + TC_M * gi, J, min(64, nf - J)};
     };
-    tiles_tc32(M, nf, ntile, 0, K1, sh, at);
+    tiles_tc32(M, nf, ntile, K0, K1, sh, at);
 }
 
 #else
 // the default build has no tensor-core tiles
 __device__ void update_cols_tc32(float*, int, int, int, int, int, Shared&, int, int) {}
-__device__ void schur_tiles_tc32(float*, int, int, int, Shared&, int, int) {}
+__device__ void schur_tiles_tc32(float*, int, int, int, int, Shared&, int, int) {}
 __device__ __forceinline__ void tc_setup(Shared& sh, bool) {
     __syncthreads();
     if (threadIdx.x == 0) { sh.tc_on = 0; sh.tc_ok = 1; sh.tc_ph = 0; sh.tc_err = nullptr; }
@@ -809,24 +809,28 @@ __device__ void update_cols_f32(float* M, int nf, int J0, int nb, int K0, int K1
     __syncthreads();
 }
 
-// Schur complement of a front's separator block, M[r, c] -= Σ_{k < K1} M[r, k] M[c, k] for
+// Schur complement of a front's separator block, M[r, c] -= Σ_{k in [K0, K1)} M[r, k] M[c, k] for
 // J0 <= c <= r < nf: every (64-column block, row tile) pair in column-block order, dealt
-// round-robin over nranks CTAs, all of one CTA's tiles in one pipeline
+// round-robin over nranks CTAs, all of one CTA's tiles in one pipeline.  With K0 > 0 it is the
+// trailing update of a right-looking step.
 template <class FT>
-__device__ void schur_tiles(FT* M, int nf, int J0, int K1, Shared& sh, int rank, int nranks) {
-    if (K1 <= 0 || J0 >= nf) return;
+__device__ void schur_tiles(FT* M, int nf, int J0, int K0, int K1, Shared& sh, int rank, int nranks) {
+    if (K1 <= K0 || J0 >= nf) return;
     const int nblk = (nf - J0 + 63) / 64;               // column blocks; block b has nblk - b row tiles
     const int total = nblk * (nblk + 1) / 2;
     const int ntile = rank < total ? (total - rank + nranks - 1) / nranks : 0;
-    auto at = [=](int i) {
-        int gi = rank + nranks * i, b = 0;
-        while (gi >= nblk - b) { gi -= nblk - b; ++b; }
+    // tile gi of the sequence: the column block b and its first tile `base` are kept from the
+    // previous call (the pipelines ask for tiles in increasing order; a smaller one restarts)
+    auto at = [=, b = 0, base = 0](int i) mutable {
+        const int gi = rank + nranks * i;
+        if (gi < base) { b = 0; base = 0; }
+        while (gi - base >= nblk - b) { base += nblk - b; ++b; }
         const int J = J0 + 64 * b;
-        return UTile{J + TS * gi, J, min(64, nf - J)};
+        return UTile{J + TS * (gi - base), J, min(64, nf - J)};
     };
-    if constexpr (sizeof(FT) == 8) tiles_f64((double*)M, nf, ntile, 0, K1, sh, at);
-    else if (use_tc32(nf, sh)) schur_tiles_tc32((float*)M, nf, J0, K1, sh, rank, nranks);
-    else tiles_f32((float*)M, nf, ntile, 0, K1, sh, at);
+    if constexpr (sizeof(FT) == 8) tiles_f64((double*)M, nf, ntile, K0, K1, sh, at);
+    else if (use_tc32(nf, sh)) schur_tiles_tc32((float*)M, nf, J0, K0, K1, sh, rank, nranks);
+    else tiles_f32((float*)M, nf, ntile, K0, K1, sh, at);
     __syncthreads();
 }
 
@@ -919,12 +923,12 @@ __device__ bool coop_barrier(CoopCtl* c, const Shared& sh) {
             atomicAdd(&c->gen, 1u);
         } else {
             const unsigned long long t0 = gtimer();
-            unsigned int nap = 100;   // ns; backs off to 8 us so idle helpers poll the hot word rarely
+            unsigned int nap = 100;   // ns; backs off to 1 us so idle helpers poll the hot word rarely
             while (ld_acquire_u32(&c->gen) == g) {
                 if (ld_volatile_i32(&c->abort) != 0) break;
                 if ((long long)(gtimer() - t0) > sh.wait_ns) { atomicExch(&c->abort, 1); break; }
                 __nanosleep(nap);
-                if (nap < 8000) nap *= 2;
+                if (nap < 1000) nap *= 2;
             }
         }
     }
@@ -963,9 +967,9 @@ __device__ void coop_exec(CoopCtl* c, Shared& sh, int rank, int nranks) {
     } else if (cmd == COOP_PANEL) {         // panel_rows(p0, nf=ia1, k0=ia2, kb=ia3); ia0 = FP32
         if (ia[0]) panel_rows<float>((float*)p0, ia[1], ia[2], ia[3], sh, rank, nranks, rank != 0);
         else panel_rows<double>((double*)p0, ia[1], ia[2], ia[3], sh, rank, nranks, rank != 0);
-    } else if (cmd == COOP_SCHUR) {         // schur_tiles(p0, nf=ia1, J0=ia2, K1=ia3)
-        if (ia[0]) schur_tiles<float>((float*)p0, ia[1], ia[2], ia[3], sh, rank, nranks);
-        else schur_tiles<double>((double*)p0, ia[1], ia[2], ia[3], sh, rank, nranks);
+    } else if (cmd == COOP_SCHUR) {         // schur_tiles(p0, nf=ia1, J0=ia2, K0=ia4, K1=ia3)
+        if (ia[0]) schur_tiles<float>((float*)p0, ia[1], ia[2], ia[4], ia[3], sh, rank, nranks);
+        else schur_tiles<double>((double*)p0, ia[1], ia[2], ia[4], ia[3], sh, rank, nranks);
     } else if (cmd == COOP_LROWS) {         // lsolve_rows(p0, nf=ia1, nres=ia2, r0=ia3, sep=p1, x=p2, k0=ia4, kb=ia5)
         if (ia[0]) lsolve_rows<float>((const float*)p0, ia[1], ia[2], ia[3], (const int*)p1, (double*)p2, ia[4], ia[5], sh, rank, nranks, true);
         else lsolve_rows<double>((const double*)p0, ia[1], ia[2], ia[3], (const int*)p1, (double*)p2, ia[4], ia[5], sh, rank, nranks, true);
@@ -1239,14 +1243,23 @@ __device__ __forceinline__ void update_cols<float>(float* M, int nf, int J0, int
 }
 
 constexpr int COOP_ABORTED = -1;   // front_chol result when the grid barrier timed out
+constexpr int COOP_RL_FRONT = 1024; // grid-cooperative fronts from this order up factor right-looking
 
 // Front factorization: left-looking over 64-column blocks (each column updated once, from final L
 // columns), 32-column diagonal/panel steps inside a block, then the separator's Schur complement
 // (the update matrix handed to the parent by extend-add).  With `coop` and a front of at least
-// COOP_MIN_FRONT, the update tiles and panel rows are shared with the helper CTAs.
+// COOP_MIN_FRONT, the update tiles and panel rows are shared with the helper CTAs.  A shared front
+// of at least COOP_RL_FRONT factors right-looking instead: after each 64-column block its trailing
+// matrix, separator included, takes the block's rank-64 update as one command of tiles over the
+// whole grid.  A left-looking step has (nf - J) / 64 row tiles of depth J, so near the end of a
+// large front a few CTAs carry all the work while the rest wait; the trailing update has
+// ((nf - J) / 64)² / 2 tiles of depth 64 at every step.  The factor is the one-CTA factor bit for
+// bit: an entry's accumulator starts from the front's value and takes the products in increasing k
+// with the same chunk boundaries either way, and storing it between steps is exact.
 template <class FT, bool COOP>
 __device__ int front_chol_ll(FT* M, int nf, int nres, Shared& sh, CoopCtl* coop, long long* tf) {
     const bool big = COOP && coop != nullptr && nf >= COOP_MIN_FRONT;
+    const bool rl = big && nf >= COOP_RL_FRONT;
     // tf[0..2]: SM clocks in the trailing updates, the diagonal blocks and the panel rows
     auto tic = [&]() -> long long { __syncthreads(); return clock64(); };
     auto toc = [&](int k, long long t0) { __syncthreads(); tf[k] += clock64() - t0; };
@@ -1262,9 +1275,18 @@ __device__ int front_chol_ll(FT* M, int nf, int nres, Shared& sh, CoopCtl* coop,
         toc(0, t0);
         return ok;
     };
+    auto trail = [&](int J0, int K0, int K1) -> bool {   // right-looking step: columns [J0, nf)
+        const long long t0 = tic();
+        const bool ok = coop_call(coop, sh, [&](CoopCtl* c) {
+            c->cmd = COOP_SCHUR; c->pa[0] = M;
+            c->ia[0] = IsF32<FT>::v; c->ia[1] = nf; c->ia[2] = J0; c->ia[3] = K1; c->ia[4] = K0;
+        });
+        toc(0, t0);
+        return ok;
+    };
     for (int J = 0; J < nres; J += 64) {
         const int nb = min(64, nres - J);
-        if (!upd(J, nb, 0, J)) return COOP_ABORTED;
+        if (!rl && !upd(J, nb, 0, J)) return COOP_ABORTED;
         for (int h = 0; h < nb; h += 32) {
             const int k0 = J + h, kb = min(32, nb - h);
             if (h > 0 && !upd(k0, kb, J, J + 32)) return COOP_ABORTED;
@@ -1283,14 +1305,16 @@ __device__ int front_chol_ll(FT* M, int nf, int nres, Shared& sh, CoopCtl* coop,
                 return COOP_ABORTED;
             tf[2] += clock64() - t0;
         }
+        if (rl && J + nb < nf && !trail(J + nb, J, J + nb)) return COOP_ABORTED;
     }
+    if (rl) return 0;                    // the trailing updates covered the separator block
     const long long t0 = tic();
     if (!big) {
-        schur_tiles<FT>(M, nf, nres, nres, sh, 0, 1);
+        schur_tiles<FT>(M, nf, nres, 0, nres, sh, 0, 1);
     } else if (nres > 0 && nf > nres &&
                !coop_call(coop, sh, [&](CoopCtl* c) {   // the whole separator block in one command
                    c->cmd = COOP_SCHUR; c->pa[0] = M;
-                   c->ia[0] = IsF32<FT>::v; c->ia[1] = nf; c->ia[2] = nres; c->ia[3] = nres;
+                   c->ia[0] = IsF32<FT>::v; c->ia[1] = nf; c->ia[2] = nres; c->ia[3] = nres; c->ia[4] = 0;
                })) {
         return COOP_ABORTED;
     }

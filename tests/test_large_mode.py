@@ -1,7 +1,10 @@
 """Grid-cooperative mode for one large instance (settings `large`): the leader CTA runs the solve and
 the helper CTAs take update tiles, panel rows, extend-adds and the assembly copy of its large
 fronts.  Each of those elements is still computed by exactly one CTA in the same order, so the
-result must equal the one-CTA path bit for bit."""
+result must equal the one-CTA path bit for bit.  That holds for the right-looking factor of fronts
+of order 1024 and more too: an entry's accumulator starts from the front's value and takes the
+products in increasing k with the same chunk boundaries, and storing it between the 64-column
+steps is exact."""
 import numpy as np
 import pytest
 
@@ -31,6 +34,19 @@ def test_large_mode_equals_one_cta(name):
     assert a.pobj == b.pobj and a.dobj == b.dobj
     for x, y in ((a.p, b.p), (a.d, b.d), (a.y, b.y)):
         assert np.array_equal(x, y)
+
+
+@pytest.mark.parametrize("tiles", [1, 2])
+def test_right_looking_mixed_precision_matches_one_cta(tiles):
+    """A portfolio front of order 1211 in the grid-cooperative mode, mixed precision: the
+    right-looking FP32 and FP64 factors (FFMA or tensor-core tiles) give the one-CTA result bit
+    for bit."""
+    prob = IPMProblem.from_dict(block_problem(G.portfolio(600, seed=8)), ctx=Context.default())
+    a = solve(prob, IPMSettings(large=-1, precision="mixed", fp32_tiles=tiles))
+    b = solve(prob, IPMSettings(large=1, precision="mixed", fp32_tiles=tiles))
+    assert a.status == b.status == IPMStatus.OPTIMAL
+    assert a.niter == b.niter and a.nfp32 == b.nfp32
+    assert a.pobj == b.pobj and np.array_equal(a.p, b.p)
 
 
 @pytest.mark.parametrize("tiles", [1, 2])

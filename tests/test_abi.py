@@ -35,7 +35,8 @@ def test_binding_covers_every_declared_symbol():
 
 
 def test_struct_layouts_match_header():
-    # mb_settings: 8 int32 then 10 doubles; mb_result: 8 int32 then 6 doubles; history rows: 17 doubles
-    assert ctypes.sizeof(_lib.mb_settings) == 8 * 4 + 10 * 8
+    # mb_settings: 8 int32, 10 doubles, then 2 int32; mb_result: 8 int32 then 6 doubles; history
+    # rows: 17 doubles
+    assert ctypes.sizeof(_lib.mb_settings) == 8 * 4 + 10 * 8 + 2 * 4
     assert ctypes.sizeof(_lib.mb_result) == 8 * 4 + 6 * 8
     assert ctypes.sizeof(_lib.mb_history_row) == 17 * 8

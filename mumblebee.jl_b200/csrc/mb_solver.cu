@@ -69,47 +69,45 @@ __device__ __forceinline__ void dmma(double& c0, double& c1, double a, double b)
                  : "+d"(c0), "+d"(c1) : "d"(a), "d"(b));
 }
 
-// Factor the kb x kb diagonal block at k0 (warp 0: lane l holds row l in registers; each finished
-// column is broadcast through sh.col).  The factor is left in sh.diag, with 1 / L[c][c] in
-// sh.dinv for the panel solve, and written back to M; its inverse goes to the block's upper
-// triangle for the triangular solves.  Returns the failing pivot (1-based in the front) or 0.  Not
-// inlined, so the register-resident rows get their own allocation.
+// Factor the kb x kb diagonal block at k0 in shared memory (sh.diag, S[r * 33 + c] = L[k0 + r][k0 + c]),
+// all warps: per column the pivot's square root and reciprocal (every thread computes the same),
+// the column scaled by the reciprocal, then the trailing triangle's rank-1 update, two barriers per
+// column.  Each entry takes its updates in increasing column order, as a row held in registers
+// would, with the same fused forms.  The factor is left in sh.diag, with 1 / L[c][c] in sh.dinv for
+// the panel, and written back to M; its inverse goes to the block's upper triangle for the
+// triangular solves.  Returns the failing pivot (1-based in the front) or 0.
 template <class FT>
 __device__ __noinline__ int diag_factor(FT* M, int nf, int k0, int kb, Shared& sh) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     FT* S = reinterpret_cast<FT*>(sh.diag);
-    FT* col = reinterpret_cast<FT*>(sh.col);
     FT* dinv = reinterpret_cast<FT*>(sh.dinv);
-    if (warp == 0) {
-        FT v[32];
-#pragma unroll
-        for (int c = 0; c < 32; ++c) v[c] = (lane < kb && c <= lane) ? M[(k0 + lane) + (int64_t)(k0 + c) * nf] : FT(0);
-        int fail = 0;
-#pragma unroll
-        for (int c = 0; c < 32; ++c) {
-            if (c >= kb || fail) continue;
-            const FT dd = __shfl_sync(0xffffffffu, v[c], c);   // the updated pivot, from lane c
-            if (!(dd > FT(0))) { fail = c + 1; continue; }
-            const FT dc = sqrt(dd);
-            const FT r = FT(1) / dc;
-            if (lane == c) { v[c] = dc; dinv[c] = r; }
-            else if (lane > c) v[c] = v[c] * r;                  // L[lane][c]
-            col[lane] = v[c];
-            __syncwarp();
-#pragma unroll
-            for (int cc = c + 1; cc < 32; ++cc) {
-                const FT lcc = col[cc];                            // L[cc][c], one broadcast read
-                if (lane >= cc) v[cc] -= v[c] * lcc;
-            }
-            __syncwarp();
-        }
-        if (!fail && lane < kb) {
-#pragma unroll
-            for (int c = 0; c < 32; ++c)
-                if (c <= lane) { S[lane * 33 + c] = v[c]; M[(k0 + lane) + (int64_t)(k0 + c) * nf] = v[c]; }
-        }
-        if (lane == 0) sh.flag = fail ? k0 + fail : 0;
+    for (int t = tid; t < 32 * 32; t += NT) {
+        const int r = t & 31, c = t >> 5;
+        if (r < kb && c <= r) S[r * 33 + c] = M[(k0 + r) + (int64_t)(k0 + c) * nf];
     }
+    __syncthreads();
+    int fail = 0;
+    for (int c = 0; c < kb; ++c) {
+        const FT dd = S[c * 33 + c];
+        if (!(dd > FT(0))) { fail = c + 1; break; }
+        const FT dc = sqrt(dd);
+        const FT r = FT(1) / dc;
+        if (tid == c) { S[c * 33 + c] = dc; dinv[c] = r; }
+        else if (tid > c && tid < kb) S[tid * 33 + c] = S[tid * 33 + c] * r;   // L[tid][c]
+        __syncthreads();
+        for (int t = tid; t < 32 * 32; t += NT) {
+            const int i = t & 31, j = t >> 5;
+            if (j > c && i >= j && i < kb) S[i * 33 + j] -= S[i * 33 + c] * S[j * 33 + c];
+        }
+        __syncthreads();
+    }
+    if (!fail) {
+        for (int t = tid; t < 32 * 32; t += NT) {
+            const int r = t & 31, c = t >> 5;
+            if (r < kb && c <= r) M[(k0 + r) + (int64_t)(k0 + c) * nf] = S[r * 33 + c];
+        }
+    }
+    if (tid == 0) sh.flag = fail ? k0 + fail : 0;
     __syncthreads();
     const int flag = sh.flag;
     if (warp == 1 && !flag) {
@@ -230,7 +228,18 @@ __device__ __noinline__ void qr_apply_panel(double* W, int64_t ld, int nfr, int 
 // Panel solve L21 = A21 L11^{-T} for the rows [k0 + kb, nf) owned by this rank (row blocks of NT
 // rows dealt round-robin over nranks CTAs), multiplying by the reciprocal pivots.  With `load`, the
 // factored diagonal block is first read back from M into sh.diag (a helper CTA that did not
-// factor it) and its reciprocal pivots recomputed.
+// factor it) and its reciprocal pivots recomputed.  Each block of NT rows is first staged into
+// shared memory by cp.async, all 32 columns in flight at once; a thread then solves its row in
+// column (axpy) order, so the updates after each pivot are independent of one another, while every
+// entry still takes its terms in increasing column order, as the row's dot products would.
+template <class FT>
+__device__ __forceinline__ void cp_async_ft(FT* sdst, const FT* gsrc, bool valid) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(sdst);
+    if constexpr (sizeof(FT) == 8)
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(sa), "l"(gsrc), "r"(valid ? 8 : 0) : "memory");
+    else
+        asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;\n" ::"r"(sa), "l"(gsrc), "r"(valid ? 4 : 0) : "memory");
+}
 template <class FT>
 __device__ __noinline__ void panel_rows(FT* M, int nf, int k0, int kb, Shared& sh, int rank, int nranks, bool load) {
     const int tid = threadIdx.x;
@@ -245,26 +254,37 @@ __device__ __noinline__ void panel_rows(FT* M, int nf, int k0, int kb, Shared& s
         if (tid < kb) dinv[tid] = FT(1) / S[tid * 33 + tid];   // as diag_factor computes it
         __syncthreads();
     }
-    {
-        const int j0 = k0 + kb;
-        for (int i = j0 + rank * NT + tid; i < nf; i += NT * nranks) {
-            // keeps the triangle's shared-memory reads inside the row loop: hoisted out of it, its
-            // 528 entries do not fit in registers and spill
-            asm volatile("" ::: "memory");
+    constexpr int LD = NT + 1;                 // staged rows: T[c * LD + r], r < NT
+    static_assert(32 * LD * 8 <= (int)sizeof(double) * 4 * TS * TLD, "a staged row block fits in Shared::tile");
+    FT* T = reinterpret_cast<FT*>(sh.tile);
+    const int j0 = k0 + kb;
+    for (int base = j0 + rank * NT; base < nf; base += NT * nranks) {
+        for (int idx = tid; idx < 32 * NT; idx += NT) {
+            const int c = idx / NT, r = idx - c * NT, row = base + r;
+            const bool v = row < nf && c < kb;
+            cp_async_ft<FT>(T + c * LD + r, v ? M + row + (int64_t)(k0 + c) * nf : M, v);
+        }
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
+        asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+        __syncthreads();
+        const int i = base + tid;
+        if (i < nf) {
             FT x[32];
 #pragma unroll
-            for (int c = 0; c < 32; ++c) {
-                if (c < kb) {
-                    FT t = M[i + (int64_t)(k0 + c) * nf];
+            for (int c = 0; c < 32; ++c) x[c] = T[c * LD + tid];
 #pragma unroll
-                    for (int cc = 0; cc < c; ++cc) t -= x[cc] * S[c * 33 + cc];
-                    x[c] = t * dinv[c];
+            for (int cc = 0; cc < 32; ++cc) {
+                if (cc < kb) {
+                    x[cc] = x[cc] * dinv[cc];
+#pragma unroll
+                    for (int c = cc + 1; c < 32; ++c) x[c] -= x[cc] * S[c * 33 + cc];
                 }
             }
+            FT* wp = M + i + (int64_t)k0 * nf;
 #pragma unroll
-            for (int c = 0; c < 32; ++c) if (c < kb) M[i + (int64_t)(k0 + c) * nf] = x[c];
+            for (int c = 0; c < 32; ++c) if (c < kb) wp[(int64_t)c * nf] = x[c];
         }
-        __syncthreads();
+        __syncthreads();                       // the block is read before the next one is staged
     }
 }
 

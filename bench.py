@@ -39,8 +39,8 @@ METRIC = "IPM solves/s & p50/p99 latency at 1e-8 gap: mixed vs FP64 GPU; factor 
 # DRAM bytes (read + write) of one ipm_batch_kernel launch per instance of this workload, FP64
 # factor: an ncu capture of a smaller launch of the same instance distribution, divided by its
 # instance count (profiles/ipm_batch_kernel_portfolio_fp64.txt gives the command and the figures)
-TRAFFIC_BYTES_PER_INSTANCE_FP64 = 89.50e9 / 296
-TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of one 296-instance launch (89.50 GB), "
+TRAFFIC_BYTES_PER_INSTANCE_FP64 = 81.00e9 / 296
+TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of one 296-instance launch (81.00 GB), "
                   "scaled to this launch by instance count")
 
 
@@ -307,8 +307,16 @@ def timed_arm(probs, precision, args, pg, local, ws, ctx, lower):
     ms_max = allreduce_max(pg, ms, local)
     res = batch.fetch(want_vectors=False)          # results of the last timed launch
     lat, svc = batch.latencies_ms()
-    ntrsv = batch.timers()[:, batch.SECTIONS.index("ntrsv")]
-    out = {"precision": precision, "autotune": tuned, "settings": settings, "grid": grid, "ms": ms, "ms_max": ms_max, "ms_steps": ms_steps, "clocks": clocks,
+    tm = batch.timers()
+    ntrsv = tm[:, batch.SECTIONS.index("ntrsv")]
+    # section clocks of the largest quarter of the instances (by n), mean per instance, Mclk
+    nsz = np.array([z["n"] for z in batch.sizes])
+    big = nsz >= np.percentile(nsz, 75)
+    sections = {k: round(float(tm[big, j].mean()) / (1e6 if not k.startswith("n") else 1.0), 2)
+                for j, k in enumerate(batch.SECTIONS)}
+    sections["instances"] = int(big.sum())
+    sections["iters_mean"] = float(np.mean([r.niter for r, b in zip(res, big) if b]))
+    out = {"precision": precision, "autotune": tuned, "settings": settings, "grid": grid, "sections_mclk": sections, "ms": ms, "ms_max": ms_max, "ms_steps": ms_steps, "clocks": clocks,
            "value": args.count * ws / (ms_max / 1e3), "res": res, "stats": st, "prepare_s": t_prep,
            "latency_ms": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99)),
                           "max": float(lat.max())},
@@ -622,7 +630,8 @@ def main():
         arms = {a["precision"]: {"solves_per_s": a["value"], "ms_per_step": a["ms_max"],
                                  "latency_ms": a["latency_ms"], "solve_ms": a["solve_ms"],
                                  "optimal": f"{a['optimal']}/{args.count}", "near_optimal": a["near_optimal"],
-                                 "iters_mean": a["iters_mean"], "autotune": a["autotune"]}
+                                 "iters_mean": a["iters_mean"], "autotune": a["autotune"],
+                                 "sections_mclk": a["sections_mclk"]}
                 for a in (main_arm, other) if a is not None}
         if "mixed" in arms and "fp64" in arms:
             arms["mixed_over_fp64"] = arms["mixed"]["solves_per_s"] / arms["fp64"]["solves_per_s"]

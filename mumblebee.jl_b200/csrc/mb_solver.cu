@@ -1345,6 +1345,32 @@ __device__ int front_chol_ll(FT* M, int nf, int nres, Shared& sh, CoopCtl* coop,
 // ---------------------------------------------------------------------------------------------
 // the per-instance solver
 // ---------------------------------------------------------------------------------------------
+// body(v, nc, t) for every entry t < nc² of every vertex block v (nc = its column count) with
+// pred(v): blocks of one or two columns a thread each, blocks below 1024 entries a warp each, larger
+// ones over the whole CTA, then a barrier.  A vertex of one scalar column otherwise costs a pass of
+// the whole CTA over a dependent load chain; the entries are disjoint and each is written once, so
+// the split changes no result.
+template <class Pred, class Body>
+__device__ void for_vertex_blocks(const int* xcol, int nv, Pred pred, Body body) {
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (int v = tid; v < nv; v += NT) {
+        const int nc = xcol[v + 1] - xcol[v];
+        if (nc <= 2 && pred(v))
+            for (int t = 0; t < nc * nc; ++t) body(v, nc, t);
+    }
+    for (int v = warp; v < nv; v += NW) {
+        const int nc = xcol[v + 1] - xcol[v];
+        if (nc > 2 && nc * nc < 1024 && pred(v))
+            for (int t = lane; t < nc * nc; t += 32) body(v, nc, t);
+    }
+    for (int v = 0; v < nv; ++v) {
+        const int nc = xcol[v + 1] - xcol[v];
+        if (nc * nc >= 1024 && pred(v))
+            for (int t = tid; t < nc * nc; t += NT) body(v, nc, t);
+    }
+    __syncthreads();
+}
+
 template <bool COOP>   // COOP: the leader of a grid-cooperative launch (else no cooperative code is built)
 struct Ctx {
     const DevInst& I;
@@ -1495,14 +1521,8 @@ struct Ctx {
                 const double su = vswp[I.colvtx[i]];
                 for (int k = Q.rptr[i]; k < Q.rptr[i + 1]; ++k) Q.val[k] *= su * vswp[I.colvtx[Q.cidx[k]]];
             }
-            for (int v = 0; v < nv; ++v) {
-                const int c0 = I.xcol[v], nc = I.xcol[v + 1] - c0;
-                if (I.hflag[c0] & 2) continue;   // zero block
-                double sc = vswp[v] * vswp[v];
-                double* qd = I.Qd + I.hdoff[v];
-                for (int t = tid; t < nc * nc; t += NT) qd[t] *= sc;
-            }
-            __syncthreads();
+            for_vertex_blocks(I.xcol, nv, [&](int v) { return !(I.hflag[I.xcol[v]] & 2); },   // a zero block stays
+                              [&](int v, int, int t) { I.Qd[I.hdoff[v] + t] *= vswp[v] * vswp[v]; });
             if (dd < tol) break;
         }
         for (int j = tid; j < n; j += NT) { I.pscl[j] = vscl[I.colvtx[j]]; I.f[j] *= I.pscl[j]; }
@@ -1872,16 +1892,11 @@ struct Ctx {
     // ---- cone fan-outs  (cone/cone.jl:146-553) -------------------------------------------
     __device__ bool scale_all(double& spsd_sum) {
         const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-        // H_vv ← Q_vv for every cone block (cone.jl:146-174)
-        for (int v = 0; v < nv; ++v) {
-            // SOC blocks are written below; structured SDP blocks are assigned by b_sdpscale
-            if (I.kind[v] == CONE_FREE || I.kind[v] == CONE_SOC || vsocz[v] == 2.0) continue;
-            int nc = I.xcol[v + 1] - I.xcol[v];
-            const double* q = I.Qd + I.hdoff[v];
-            double* h = I.Hd + I.hdoff[v];
-            for (int t = tid; t < nc * nc; t += NT) h[t] = q[t];
-        }
-        __syncthreads();
+        // H_vv ← Q_vv for every cone block (cone.jl:146-174); SOC blocks are written below and
+        // structured SDP blocks are assigned by b_sdpscale
+        for_vertex_blocks(I.xcol, nv,
+                          [&](int v) { return !(I.kind[v] == CONE_FREE || I.kind[v] == CONE_SOC || vsocz[v] == 2.0); },
+                          [&](int v, int, int t) { I.Hd[I.hdoff[v] + t] = I.Qd[I.hdoff[v] + t]; });
         // per cone: scaling point and ⟨p*, d*⟩
         for (int v = warp; v < nv; v += NW) {
             int k = I.kind[v];
@@ -2079,19 +2094,13 @@ struct Ctx {
         }
         __syncthreads();
         // + δ H: diagonal blocks (lower part) and the off-diagonal nonzeros of Q (chordal.jl:1-80)
-        for (int v = 0; v < nv; ++v) {
-            int nc = I.xcol[v + 1] - I.xcol[v];
-            int64_t base = I.hdpos[v];
-            int ld = I.hdld[v];
-            const double* h = I.Hd + I.hdoff[v];
-            for (int t = tid; t < nc * nc; t += NT) {
-                int r = t % nc, c = t / nc;
-                if (r >= c) {
-                    int64_t q = base + r + (int64_t)c * ld;
-                    F[q] = (FT)(I.Finit[q] + dl * h[t]);
-                }
+        for_vertex_blocks(I.xcol, nv, [](int) { return true; }, [&](int v, int nc, int t) {
+            const int r = t % nc, c = t / nc;
+            if (r >= c) {
+                const int64_t q = I.hdpos[v] + r + (int64_t)c * I.hdld[v];
+                F[q] = (FT)(I.Finit[q] + dl * I.Hd[I.hdoff[v] + t]);
             }
-        }
+        });
         for (int t = tid; t < I.nqoff; t += NT) {
             int64_t q = I.qoffpos[t];
             F[q] = (FT)(I.Finit[q] + dl * I.Q.val[I.qoffk[t]]);

@@ -421,9 +421,9 @@ static int plan_instance(const mb_problem* P, const mb_settings& set, const doub
                 }
             }
         if (!found && P->kind[vp[v]] != MB_CONE_FREE) { err = "Q lacks the diagonal block of a cone vertex"; return MB_E_ARG; }
-        i64 f = fr.vfront[v], nf = fr.nres[f] + (i64)fr.sep[f].size();
-        hdpos[v] = fr.fptr[f] + (B.xcol[v] - fr.res0[f]) * (nf + 1);
-        hdld[v] = nf;
+        i64 f = fr.vfront[v], ld = mb::front_ld(fr.nres[f] + (i64)fr.sep[f].size());
+        hdpos[v] = fr.fptr[f] + (B.xcol[v] - fr.res0[f]) * (ld + 1);
+        hdld[v] = ld;
     }
     // off-diagonal-block nonzeros of Q in the lower triangle and their F offsets
     std::vector<i64> qoffk, qoffpos;
@@ -431,11 +431,11 @@ static int plan_instance(const mb_problem* P, const mb_settings& set, const doub
         for (i64 k = Qrptr[i]; k < Qrptr[i + 1]; ++k) {
             i64 j = Qcidx[k];
             if (i < j) continue;
-            i64 f = cfront[j], nf = fr.nres[f] + (i64)fr.sep[f].size();
+            i64 f = cfront[j], ld = mb::front_ld(fr.nres[f] + (i64)fr.sep[f].size());
             i64 rp = rowpos(f, i);
             if (rp < 0) { err = "internal: Q entry outside the front structure"; return MB_E_ARG; }
             qoffk.push_back(k);
-            qoffpos.push_back(fr.fptr[f] + rp + (j - fr.res0[f]) * nf);
+            qoffpos.push_back(fr.fptr[f] + rp + (j - fr.res0[f]) * ld);
         }
     ip.nqoff = (i64)qoffk.size();
     // rows and columns with more than LONG_ROW terms in the sparse products: a warp each on the device.

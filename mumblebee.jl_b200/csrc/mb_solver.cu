@@ -12,6 +12,7 @@
 // Precision: iterates, residuals, refinement, cone algebra and termination checks are FP64.  The
 // KKT factor is stored and computed in FT (double, or float for the mixed-precision path).
 #include <cuda_runtime.h>
+#include <cstddef>
 #include <cstdint>
 #include <cstdio>
 #include "mb_internal.h"
@@ -38,7 +39,7 @@ namespace mb {
 
 constexpr int TS = 64;   // trailing-update tile
 constexpr double MIXED_MAX_SOLVES = 4;   // KKT solves (IR passes + CG steps) an FP32 iteration may take
-constexpr int TLD = 36;  // tile row stride (doubles): 8-byte fragment loads of 8 rows x 4 columns hit 32 distinct banks
+constexpr int TLD = 36;  // sizes Shared::tile: four 64 x 36 double tiles (FP64, FP32 and tensor-core stages fit in it)
 
 // Block-shared scratch (dynamic shared memory: it exceeds the 48 KB static limit).  `tile` holds the
 // two stages (A and B operand each) of the double-buffered front update.
@@ -61,6 +62,7 @@ struct Shared {
     int* tc_err;            // set to 2 when a completion wait runs out (instance status word 7, or the
                             // grid-cooperative abort flag on a helper CTA)
 };
+static_assert(offsetof(Shared, tile) % 16 == 0, "16-byte copies stage into Shared::tile");
 
 // D += A·B on the FP64 tensor path (mma.m8n8k4, fragments: A[g][t], B[t][g], C[g][2t+i] with
 // g = lane/4, t = lane%4)
@@ -78,12 +80,13 @@ __device__ __forceinline__ void dmma(double& c0, double& c1, double a, double b)
 // triangular solves.  Returns the failing pivot (1-based in the front) or 0.
 template <class FT>
 __device__ __noinline__ int diag_factor(FT* M, int nf, int k0, int kb, Shared& sh) {
+    const int64_t ld = front_ld(nf);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     FT* S = reinterpret_cast<FT*>(sh.diag);
     FT* dinv = reinterpret_cast<FT*>(sh.dinv);
     for (int t = tid; t < 32 * 32; t += NT) {
         const int r = t & 31, c = t >> 5;
-        if (r < kb && c <= r) S[r * 33 + c] = M[(k0 + r) + (int64_t)(k0 + c) * nf];
+        if (r < kb && c <= r) S[r * 33 + c] = M[(k0 + r) + (int64_t)(k0 + c) * ld];
     }
     __syncthreads();
     int fail = 0;
@@ -104,7 +107,7 @@ __device__ __noinline__ int diag_factor(FT* M, int nf, int k0, int kb, Shared& s
     if (!fail) {
         for (int t = tid; t < 32 * 32; t += NT) {
             const int r = t & 31, c = t >> 5;
-            if (r < kb && c <= r) M[(k0 + r) + (int64_t)(k0 + c) * nf] = S[r * 33 + c];
+            if (r < kb && c <= r) M[(k0 + r) + (int64_t)(k0 + c) * ld] = S[r * 33 + c];
         }
     }
     if (tid == 0) sh.flag = fail ? k0 + fail : 0;
@@ -124,7 +127,7 @@ __device__ __noinline__ int diag_factor(FT* M, int nf, int k0, int kb, Shared& s
         for (int k = 0; k < 32; ++k) {
             if (k >= kb) continue;
             const FT xk = k < c ? FT(0) : (k == c ? dinv[c] : -acc[k] * dinv[k]);
-            if (k > c && c < kb) M[(k0 + c) + (int64_t)(k0 + k) * nf] = xk;
+            if (k > c && c < kb) M[(k0 + c) + (int64_t)(k0 + k) * ld] = xk;
 #pragma unroll
             for (int i = k + 1; i < 32; ++i) acc[i] = fma(S[i * 33 + k], xk, acc[i]);
         }
@@ -136,6 +139,7 @@ __device__ __noinline__ int diag_factor(FT* M, int nf, int k0, int kb, Shared& s
 // (the stable factor writes L directly): the layout diag_factor leaves, a warp per block, lane c
 // forming column c of X = L⁻¹ in the same axpy order and storing X[k][c], k > c, at M[k0 + c, k0 + k].
 __device__ __noinline__ void front_block_inverses(double* M, int nf, int nres) {
+    const int64_t ld = front_ld(nf);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (int b = warp; b * 32 < nres; b += NW) {
         const int k0 = b * 32, kb = min(32, nres - k0), c = lane;
@@ -145,12 +149,12 @@ __device__ __noinline__ void front_block_inverses(double* M, int nf, int nres) {
 #pragma unroll
         for (int k = 0; k < 32; ++k) {
             if (k >= kb) continue;
-            const double dk = 1.0 / M[(k0 + k) + (int64_t)(k0 + k) * nf];
+            const double dk = 1.0 / M[(k0 + k) + (int64_t)(k0 + k) * ld];
             const double xk = k < c ? 0.0 : (k == c ? dk : -acc[k] * dk);
-            if (k > c && c < kb) M[(k0 + c) + (int64_t)(k0 + k) * nf] = xk;
+            if (k > c && c < kb) M[(k0 + c) + (int64_t)(k0 + k) * ld] = xk;
 #pragma unroll
             for (int i = k + 1; i < 32; ++i)
-                if (i < kb) acc[i] = fma(M[(k0 + i) + (int64_t)(k0 + k) * nf], xk, acc[i]);
+                if (i < kb) acc[i] = fma(M[(k0 + i) + (int64_t)(k0 + k) * ld], xk, acc[i]);
         }
     }
     __syncthreads();
@@ -232,6 +236,11 @@ __device__ __noinline__ void qr_apply_panel(double* W, int64_t ld, int nfr, int 
 // shared memory by cp.async, all 32 columns in flight at once; a thread then solves its row in
 // column (axpy) order, so the updates after each pivot are independent of one another, while every
 // entry still takes its terms in increasing column order, as the row's dot products would.
+__device__ __forceinline__ void cp_async16(void* sdst, const void* gsrc, int bytes) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(sdst);   // bytes < 16: the rest zero-filled
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(sa), "l"(gsrc), "r"(bytes) : "memory");
+}
+
 template <class FT>
 __device__ __forceinline__ void cp_async_ft(FT* sdst, const FT* gsrc, bool valid) {
     const unsigned sa = (unsigned)__cvta_generic_to_shared(sdst);
@@ -242,27 +251,43 @@ __device__ __forceinline__ void cp_async_ft(FT* sdst, const FT* gsrc, bool valid
 }
 template <class FT>
 __device__ __noinline__ void panel_rows(FT* M, int nf, int k0, int kb, Shared& sh, int rank, int nranks, bool load) {
+    const int64_t ld = front_ld(nf);
     const int tid = threadIdx.x;
     FT* S = reinterpret_cast<FT*>(sh.diag);
     FT* dinv = reinterpret_cast<FT*>(sh.dinv);
     if (load) {
         for (int t = tid; t < 32 * 32; t += NT) {
             const int r = t & 31, c = t >> 5;
-            if (r < kb && c <= r) S[r * 33 + c] = M[(k0 + r) + (int64_t)(k0 + c) * nf];
+            if (r < kb && c <= r) S[r * 33 + c] = M[(k0 + r) + (int64_t)(k0 + c) * ld];
         }
         __syncthreads();
         if (tid < kb) dinv[tid] = FT(1) / S[tid * 33 + tid];   // as diag_factor computes it
         __syncthreads();
     }
-    constexpr int LD = NT + 1;                 // staged rows: T[c * LD + r], r < NT
+    // staged rows: T[c * LD + sft + r], r < NT.  FP64 blocks come in 16-byte copies of row pairs
+    // (LD even keeps each staged column 16-byte aligned); pairs start at even rows, so a block that
+    // starts at an odd row is staged from the row before, sft = 1, with a 129th pair per column
+    constexpr int LD = sizeof(FT) == 8 ? NT + 2 : NT + 1, NP = NT / 2;
     static_assert(32 * LD * 8 <= (int)sizeof(double) * 4 * TS * TLD, "a staged row block fits in Shared::tile");
     FT* T = reinterpret_cast<FT*>(sh.tile);
     const int j0 = k0 + kb;
     for (int base = j0 + rank * NT; base < nf; base += NT * nranks) {
-        for (int idx = tid; idx < 32 * NT; idx += NT) {
-            const int c = idx / NT, r = idx - c * NT, row = base + r;
-            const bool v = row < nf && c < kb;
-            cp_async_ft<FT>(T + c * LD + r, v ? M + row + (int64_t)(k0 + c) * nf : M, v);
+        int sft = 0;
+        if constexpr (sizeof(FT) == 8) {
+            sft = base & 1;
+            const int b0 = base - sft;
+            for (int idx = tid; idx < 32 * NP + 32 * sft; idx += NT) {
+                const bool last = idx >= 32 * NP;
+                const int c = last ? idx - 32 * NP : idx / NP, u = last ? NP : idx % NP, gr = b0 + 2 * u;
+                const int nv = c < kb ? min(2, max(0, nf - gr)) : 0;
+                cp_async16(T + c * LD + 2 * u, nv ? M + gr + (int64_t)(k0 + c) * ld : M, 8 * nv);
+            }
+        } else {
+            for (int idx = tid; idx < 32 * NT; idx += NT) {
+                const int c = idx / NT, r = idx - c * NT, row = base + r;
+                const bool v = row < nf && c < kb;
+                cp_async_ft<FT>(T + c * LD + r, v ? M + row + (int64_t)(k0 + c) * ld : M, v);
+            }
         }
         asm volatile("cp.async.commit_group;\n" ::: "memory");
         asm volatile("cp.async.wait_group 0;\n" ::: "memory");
@@ -271,7 +296,7 @@ __device__ __noinline__ void panel_rows(FT* M, int nf, int k0, int kb, Shared& s
         if (i < nf) {
             FT x[32];
 #pragma unroll
-            for (int c = 0; c < 32; ++c) x[c] = T[c * LD + tid];
+            for (int c = 0; c < 32; ++c) x[c] = T[c * LD + sft + tid];
 #pragma unroll
             for (int cc = 0; cc < 32; ++cc) {
                 if (cc < kb) {
@@ -280,20 +305,12 @@ __device__ __noinline__ void panel_rows(FT* M, int nf, int k0, int kb, Shared& s
                     for (int c = cc + 1; c < 32; ++c) x[c] -= x[cc] * S[c * 33 + cc];
                 }
             }
-            FT* wp = M + i + (int64_t)k0 * nf;
+            FT* wp = M + i + (int64_t)k0 * ld;
 #pragma unroll
-            for (int c = 0; c < 32; ++c) if (c < kb) wp[(int64_t)c * nf] = x[c];
+            for (int c = 0; c < 32; ++c) if (c < kb) wp[(int64_t)c * ld] = x[c];
         }
         __syncthreads();                       // the block is read before the next one is staged
     }
-}
-
-template <class FT>
-__device__ int diag_panel(FT* M, int nf, int k0, int kb, Shared& sh) {
-    int info = diag_factor<FT>(M, nf, k0, kb, sh);
-    if (info) return info;
-    panel_rows<FT>(M, nf, k0, kb, sh, 0, 1, false);
-    return 0;
 }
 
 // ---- FP64 left-looking front factorization ---------------------------------------------------
@@ -306,24 +323,30 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
-// Stage rows [r0, r0 + 64) x columns [k0, k0 + 32) of the column-major M (leading dimension nf)
-// as buf[r * TLD + c], zero where the row is >= rmax or the column >= kmax.  A warp copies 8 rows x
-// 4 columns per instruction: 64-byte runs in global memory, conflict-free 16-lane phases in
-// shared memory.
-__device__ __forceinline__ void stage_tile_f64(double* buf, const double* M, int nf, int r0, int rmax, int k0,
+// Stage rows [r0, r0 + 64) x columns [k0, k0 + 32) of the column-major front M (16-byte aligned,
+// even leading dimension ld) into buf column by column: row r of column c at
+// buf[c * CLD + (r0 & 1) + r - r0], zero where the row is >= rmax or the column >= kmax.  16-byte
+// copies of row pairs, which start on a 16-byte boundary at even rows: a warp copies one column's
+// 64 rows (512 contiguous bytes) per instruction; for an odd r0 the pairs start one row early and
+// lane 0 copies a 33rd pair.
+constexpr int CLD = 68;   // staged column stride (doubles): fragment loads of 8 rows x 4 columns hit 32 distinct banks
+static_assert(4 * 32 * CLD <= 4 * TS * TLD, "four staged tiles fit in Shared::tile");
+__device__ __forceinline__ void stage_tile_f64(double* buf, const double* M, int64_t ld, int r0, int rmax, int k0,
                                                int kmax) {
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int rl = lane >> 2, cl = lane & 3;
-    for (int i = warp; i < 64; i += NW) {
-        const int r = (i & 7) * 8 + rl, c = (i >> 3) * 4 + cl;
-        const int gr = r0 + r, gc = k0 + c;
-        const bool v = gr < rmax && gc < kmax;
-        cp_async8(buf + r * TLD + c, v ? M + gr + (int64_t)gc * nf : M, v);
+    const int p = r0 & 1, base = r0 - p;
+    for (int c = warp; c < 32; c += NW) {
+        const int gc = k0 + c;
+        for (int u = lane; u < 32 + p; u += 32) {
+            const int gr = base + 2 * u;
+            const int nv = gc < kmax ? min(2, max(0, rmax - gr)) : 0;
+            cp_async16(buf + c * CLD + 2 * u, nv ? M + gr + (int64_t)gc * ld : M, 8 * nv);
+        }
     }
 }
 
 // One 64 x nb tile of the trailing update: rows [rb, rb + 64) x columns [J, J + nb) (nb <= 64) of
-// the column-major front M (leading dimension nf), M[r, c] -= Σ_{k in [K0, K1)} M[r, k] M[c, k] for
+// the column-major front M (order nf), M[r, c] -= Σ_{k in [K0, K1)} M[r, k] M[c, k] for
 // r >= c.  The K columns must be final (K1 <= J).
 struct UTile { int rb, J, nb; };
 
@@ -335,6 +358,7 @@ struct UTile { int rb, J, nb; };
 // with negated B fragments, so the epilogue is a plain store.
 template <class TileAt>
 __device__ __noinline__ void tiles_f64(double* M, int nf, int ntile, int K0, int K1, Shared& sh, TileAt at) {
+    const int64_t ld = front_ld(nf);
     constexpr int WRN = NW / 4, RW = TS / WRN, MR = RW / 8;
     if (ntile <= 0 || K1 <= K0) return;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -342,13 +366,13 @@ __device__ __noinline__ void tiles_f64(double* M, int nf, int ntile, int K0, int
     const int wr = warp >> 2, wc = warp & 3;
     const int nk = (K1 - K0 + 31) / 32;
     const int nstep = ntile * nk;
-    double* A[2] = {sh.tile, sh.tile + 2 * TS * TLD};
-    double* B[2] = {sh.tile + TS * TLD, sh.tile + 3 * TS * TLD};
+    double* A[2] = {sh.tile, sh.tile + 2 * 32 * CLD};
+    double* B[2] = {sh.tile + 32 * CLD, sh.tile + 3 * 32 * CLD};
     auto stage = [&](int s, int buf) {
         const UTile u = at(s / nk);
         const int k0 = K0 + 32 * (s % nk);
-        stage_tile_f64(A[buf], M, nf, u.rb, nf, k0, K1);
-        stage_tile_f64(B[buf], M, nf, u.J, min(nf, u.J + u.nb), k0, K1);
+        stage_tile_f64(A[buf], M, ld, u.rb, nf, k0, K1);
+        stage_tile_f64(B[buf], M, ld, u.J, min(nf, u.J + u.nb), k0, K1);
         cp_async_commit();
     };
     double acc[MR][2][2];
@@ -369,7 +393,7 @@ __device__ __noinline__ void tiles_f64(double* M, int nf, int ntile, int K0, int
                     for (int e = 0; e < 2; ++e) {
                         const int row = u.rb + wr * RW + a * 8 + g;
                         const int col = u.J + wc * 16 + b * 8 + 2 * t + e;
-                        acc[a][b][e] = (!skip && row < nf && col < cmax && row >= col) ? M[row + (int64_t)col * nf] : 0.0;
+                        acc[a][b][e] = (!skip && row < nf && col < cmax && row >= col) ? M[row + (int64_t)col * ld] : 0.0;
                     }
         }
         if (s + 1 < nstep) {
@@ -380,14 +404,14 @@ __device__ __noinline__ void tiles_f64(double* M, int nf, int ntile, int K0, int
         }
         __syncthreads();
         if (!skip) {
-            const double* ta = A[cur];
-            const double* tb = B[cur];
+            const double* ta = A[cur] + (u.rb & 1) + wr * RW + g + t * CLD;
+            const double* tb = B[cur] + (u.J & 1) + wc * 16 + g + t * CLD;
             const int kb4 = (min(32, K1 - K0 - 32 * q) + 3) & ~3;
             for (int k = 0; k < kb4; k += 4) {
-                const double b0 = -tb[(wc * 16 + g) * TLD + k + t], b1 = -tb[(wc * 16 + 8 + g) * TLD + k + t];
+                const double b0 = -tb[k * CLD], b1 = -tb[k * CLD + 8];
 #pragma unroll
                 for (int a = 0; a < MR; ++a) {
-                    const double av = ta[(wr * RW + a * 8 + g) * TLD + k + t];
+                    const double av = ta[k * CLD + a * 8];
                     dmma(acc[a][0][0], acc[a][0][1], av, b0);
                     dmma(acc[a][1][0], acc[a][1][1], av, b1);
                 }
@@ -404,7 +428,7 @@ __device__ __noinline__ void tiles_f64(double* M, int nf, int ntile, int K0, int
                     for (int e = 0; e < 2; ++e) {
                         const int row = u.rb + wr * RW + a * 8 + g;
                         const int col = u.J + wc * 16 + b * 8 + 2 * t + e;
-                        if (row < nf && col < cmax && row >= col) M[row + (int64_t)col * nf] = acc[a][b][e];
+                        if (row < nf && col < cmax && row >= col) M[row + (int64_t)col * ld] = acc[a][b][e];
                     }
         }
     }
@@ -431,12 +455,12 @@ __device__ __forceinline__ void cp_async4(void* sdst, const void* gsrc, bool val
 // FP32 stage: rows [r0, r0 + 64) x columns [k0, k0 + 32) of M as buf[c * 68 + r] (k-major, so a
 // thread reads its 4 rows as one float4), zero where the row is >= rmax or the column >= kmax
 constexpr int T32LD = 68;
-__device__ __forceinline__ void stage_tile_f32(float* buf, const float* M, int nf, int r0, int rmax, int k0, int kmax) {
+__device__ __forceinline__ void stage_tile_f32(float* buf, const float* M, int64_t ld, int r0, int rmax, int k0, int kmax) {
     for (int i = threadIdx.x; i < 64 * 32; i += NT) {
         const int r = i & 63, c = i >> 6;
         const int gr = r0 + r, gc = k0 + c;
         const bool v = gr < rmax && gc < kmax;
-        cp_async4(buf + c * T32LD + r, v ? M + gr + (int64_t)gc * nf : M, v);
+        cp_async4(buf + c * T32LD + r, v ? M + gr + (int64_t)gc * ld : M, v);
     }
 }
 
@@ -444,6 +468,7 @@ __device__ __forceinline__ void stage_tile_f32(float* buf, const float* M, int n
 // cross-tile pipeline, accumulators started from M
 template <class TileAt>
 __device__ __noinline__ void tiles_f32(float* M, int nf, int ntile, int K0, int K1, Shared& sh, TileAt at) {
+    const int64_t ld = front_ld(nf);
     if (ntile <= 0 || K1 <= K0) return;
     const int tr = threadIdx.x & 15, tc = threadIdx.x >> 4;
     const int nk = (K1 - K0 + 31) / 32;
@@ -453,8 +478,8 @@ __device__ __noinline__ void tiles_f32(float* M, int nf, int ntile, int K0, int 
     auto stage = [&](int s, int buf) {
         const UTile u = at(s / nk);
         const int k0 = K0 + 32 * (s % nk);
-        stage_tile_f32(A[buf], M, nf, u.rb, nf, k0, K1);
-        stage_tile_f32(B[buf], M, nf, u.J, min(nf, u.J + u.nb), k0, K1);
+        stage_tile_f32(A[buf], M, ld, u.rb, nf, k0, K1);
+        stage_tile_f32(B[buf], M, ld, u.J, min(nf, u.J + u.nb), k0, K1);
         cp_async_commit();
     };
     float acc[4][4];
@@ -472,7 +497,7 @@ __device__ __noinline__ void tiles_f32(float* M, int nf, int ntile, int K0, int 
 #pragma unroll
                 for (int b = 0; b < 4; ++b) {
                     const int row = u.rb + tr * 4 + a, col = u.J + tc * 4 + b;
-                    acc[a][b] = (!skip && row < nf && col < cmax && row >= col) ? M[row + (int64_t)col * nf] : 0.f;
+                    acc[a][b] = (!skip && row < nf && col < cmax && row >= col) ? M[row + (int64_t)col * ld] : 0.f;
                 }
         }
         if (s + 1 < nstep) {
@@ -504,7 +529,7 @@ __device__ __noinline__ void tiles_f32(float* M, int nf, int ntile, int K0, int 
 #pragma unroll
                 for (int a = 0; a < 4; ++a) {
                     const int row = u.rb + tr * 4 + a, col = u.J + tc * 4 + b;
-                    if (row < nf && col < cmax && row >= col) M[row + (int64_t)col * nf] = acc[a][b];
+                    if (row < nf && col < cmax && row >= col) M[row + (int64_t)col * ld] = acc[a][b];
                 }
         }
     }
@@ -523,9 +548,8 @@ __device__ __noinline__ void tiles_f32(float* M, int nf, int ntile, int K0, int 
 // the canonical K-major, no-swizzle layout (core matrices of 8 rows x 16 bytes), hi and lo parts
 // separately, two stages alternating; one thread issues the step's six MMAs and commits them to
 // the stage's mbarrier, on which every thread waits before reading the step's accumulator.  The
-// front's leading dimension is its order, so its columns are not 16-byte aligned in general and
-// the operands cannot come by TMA; the next step's loads and the previous step's read-out overlap
-// the MMAs.
+// operands pass through registers for the hi/lo split, so they are staged by the threads rather
+// than by TMA; the next step's loads and the previous step's read-out overlap the MMAs.
 constexpr int TC_M = 128, TC_N = 64, TC_KC = 16;
 constexpr int TC_A_BYTES = TC_M * TC_KC * 4;                      // one part (hi or lo) of A, one stage
 constexpr int TC_B_BYTES = TC_N * TC_KC * 4;
@@ -612,6 +636,7 @@ __device__ __forceinline__ void tf32_split(float a, float& hi, float& lo) {
 // step's MMAs run, so the tensor cores' FP32 accumulation covers 16 products only.
 template <class TileAt>
 __device__ __noinline__ void tiles_tc32(float* M, int nf, int ntile, int K0, int K1, Shared& sh, TileAt at) {
+    const int64_t ld = front_ld(nf);
     if (ntile <= 0 || K1 <= K0) return;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int quad = warp & 3, half = warp >> 2;
@@ -638,9 +663,9 @@ __device__ __noinline__ void tiles_tc32(float* M, int nf, int ntile, int K0, int
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
             const int k1 = k0 + 4 * ga + j, k2 = k0 + 4 * (ga + 2) + j, k3 = k0 + 4 * gb + j;
-            va0[j] = (r < nf && k1 < K1) ? M[r + (int64_t)k1 * nf] : 0.f;
-            va1[j] = (r < nf && k2 < K1) ? M[r + (int64_t)k2 * nf] : 0.f;
-            vb[j] = (c < cmax && k3 < K1) ? M[c + (int64_t)k3 * nf] : 0.f;
+            va0[j] = (r < nf && k1 < K1) ? M[r + (int64_t)k1 * ld] : 0.f;
+            va1[j] = (r < nf && k2 < K1) ? M[r + (int64_t)k2 * ld] : 0.f;
+            vb[j] = (c < cmax && k3 < K1) ? M[c + (int64_t)k3 * ld] : 0.f;
         }
     };
     // row r, K group g of an operand of R rows: hi part at base + off, lo part at base + part + off
@@ -665,7 +690,7 @@ __device__ __noinline__ void tiles_tc32(float* M, int nf, int ntile, int K0, int
 #pragma unroll
             for (int j = 0; j < 32; ++j) {
                 const int col = ur.J + 32 * half + j;
-                acc[j] = (row < nf && col < cmax && row >= col) ? M[row + (int64_t)col * nf] : 0.f;
+                acc[j] = (row < nf && col < cmax && row >= col) ? M[row + (int64_t)col * ld] : 0.f;
             }
         }
         if (!mbar_wait(&sh.mbar[b], ph[b])) sh.tc_ok = 0;
@@ -683,7 +708,7 @@ __device__ __noinline__ void tiles_tc32(float* M, int nf, int ntile, int K0, int
 #pragma unroll
                 for (int j = 0; j < 32; ++j) {
                     const int col = ur.J + 32 * half + j;
-                    if (col < cmax && row >= col) M[row + (int64_t)col * nf] = acc[j];
+                    if (col < cmax && row >= col) M[row + (int64_t)col * ld] = acc[j];
                 }
             }
         }
@@ -862,22 +887,23 @@ __device__ void schur_tiles(FT* M, int nf, int J0, int K0, int K1, Shared& sh, i
 template <class FT>
 __device__ void lsolve_rows(const FT* M, int nf, int nres, int r0, const int* sep, double* x, int k0, int kb,
                             Shared& sh, int rank, int nranks, bool load) {
+    const int64_t ld = front_ld(nf);
     const int tid = threadIdx.x;
     if (load) {
         if (tid < kb) sh.xs[tid] = x[r0 + k0 + tid];
         __syncthreads();
     }
     for (int i = k0 + kb + rank * NT + tid; i < nf; i += NT * nranks) {
-        const FT* Mi = M + i + (int64_t)k0 * nf;
+        const FT* Mi = M + i + (int64_t)k0 * ld;
         double t = 0;
         if (kb == 32) {   // all 32 loads in flight before the FMA chain
             FT v[32];
 #pragma unroll
-            for (int c = 0; c < 32; ++c) v[c] = Mi[(int64_t)c * nf];
+            for (int c = 0; c < 32; ++c) v[c] = Mi[(int64_t)c * ld];
 #pragma unroll
             for (int c = 0; c < 32; ++c) t = fma((double)v[c], sh.xs[c], t);
         } else {
-            for (int c = 0; c < kb; ++c) t = fma((double)Mi[(int64_t)c * nf], sh.xs[c], t);
+            for (int c = 0; c < kb; ++c) t = fma((double)Mi[(int64_t)c * ld], sh.xs[c], t);
         }
         int tg = i < nres ? r0 + i : sep[i - nres];
         x[tg] -= t;
@@ -890,9 +916,10 @@ __device__ void lsolve_rows(const FT* M, int nf, int nres, int r0, const int* se
 template <class FT>
 __device__ void usolve_dots(const FT* M, int nf, int nres, int r0, const int* sep, const double* x, int k0, int kb,
                             double* out, int gw, int gws) {
+    const int64_t ld = front_ld(nf);
     const int lane = threadIdx.x & 31;
     for (int c = gw; c < kb; c += gws) {
-        const FT* Mc = M + (int64_t)(k0 + c) * nf;
+        const FT* Mc = M + (int64_t)(k0 + c) * ld;
         double t0 = 0, t1 = 0, t2 = 0, t3 = 0;
         int i = k0 + kb + lane;
         for (; i + 96 < nf; i += 128) {   // four rows per lane in flight
@@ -1003,7 +1030,7 @@ __device__ void coop_exec(CoopCtl* c, Shared& sh, int rank, int nranks) {
         for (long long t = (long long)rank * NT + tid; t < (long long)nsep * nsep; t += (long long)NT * nranks) {
             const int i = (int)(t % nsep), j = (int)(t / nsep);
             if (i < j) continue;
-            const long long dst = rel[i] + (long long)rel[j] * np, src = (nres + i) + (long long)(nres + j) * nfr;
+            const long long dst = rel[i] + (long long)rel[j] * front_ld(np), src = (nres + i) + (long long)(nres + j) * front_ld(nfr);
             if (ia[0]) ((float*)p1)[dst] += ((const float*)p0)[src];
             else ((double*)p1)[dst] += ((const double*)p0)[src];
         }
@@ -1041,13 +1068,14 @@ template <> struct IsF32<float> { static constexpr int v = 1; };
 template <class FT, bool COOP = false>
 __device__ void front_lsolve(const FT* M, int nf, int nres, int r0, const int* sep, double* x, Shared& sh,
                              CoopCtl* coop = nullptr) {
+    const int64_t ld = front_ld(nf);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     double* T = sh.diag;   // the 32x32 diagonal triangle, T[c*33 + r] = L[k0+r, k0+c]
     for (int k0 = 0; k0 < nres; k0 += 32) {
         const int kb = min(32, nres - k0);
         for (int idx = tid; idx < 32 * 32; idx += NT) {
             int r = idx & 31, c = idx >> 5;
-            if (r < kb && c < kb && r >= c) T[c * 33 + r] = (double)M[(k0 + r) + (int64_t)(k0 + c) * nf];
+            if (r < kb && c < kb && r >= c) T[c * 33 + r] = (double)M[(k0 + r) + (int64_t)(k0 + c) * ld];
         }
         __syncthreads();
         if (warp == 0) {
@@ -1075,6 +1103,7 @@ __device__ void front_lsolve(const FT* M, int nf, int nres, int r0, const int* s
 template <class FT, bool COOP = false>
 __device__ void front_usolve(const FT* M, int nf, int nres, int r0, const int* sep, double* x, Shared& sh,
                              CoopCtl* coop = nullptr) {
+    const int64_t ld = front_ld(nf);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int nblk = (nres + 31) / 32;
     double* T = sh.diag;   // T[c*33 + r] = L[k0+r, k0+c]
@@ -1082,7 +1111,7 @@ __device__ void front_usolve(const FT* M, int nf, int nres, int r0, const int* s
         const int k0 = bk * 32, kb = min(32, nres - k0);
         for (int idx = tid; idx < 32 * 32; idx += NT) {
             int r = idx & 31, c = idx >> 5;
-            if (r < kb && c < kb && r >= c) T[c * 33 + r] = (double)M[(k0 + r) + (int64_t)(k0 + c) * nf];
+            if (r < kb && c < kb && r >= c) T[c * 33 + r] = (double)M[(k0 + r) + (int64_t)(k0 + c) * ld];
         }
         if (!COOP || !coop) {
             usolve_dots<FT>(M, nf, nres, r0, sep, x, k0, kb, sh.acc, warp, NW);
@@ -1120,6 +1149,7 @@ static_assert(COOP_MIN_SOLVE + 8 * 32 <= XSM_CAP, "front slice of x and dot part
 
 template <class FT>
 __device__ __noinline__ void front_lsolve_sm(const FT* M, int nf, int nres, int r0, const int* sep, double* x, Shared& sh) {
+    const int64_t ld = front_ld(nf);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     double* xf = sh.tile;
     double* T = sh.diag;   // T[c*33 + r] = L[k0+r, k0+c]
@@ -1130,15 +1160,15 @@ __device__ __noinline__ void front_lsolve_sm(const FT* M, int nf, int nres, int 
         const int i0 = k0 + kb + tid;
         FT v[32];
         if (kb == 32 && i0 < nf) {   // first panel row of this thread, in flight during the diagonal solve
-            const FT* Mi = M + i0 + (int64_t)k0 * nf;
+            const FT* Mi = M + i0 + (int64_t)k0 * ld;
 #pragma unroll
-            for (int c = 0; c < 32; ++c) v[c] = Mi[(int64_t)c * nf];
+            for (int c = 0; c < 32; ++c) v[c] = Mi[(int64_t)c * ld];
         }
         for (int idx = tid; idx < 32 * 32; idx += NT) {   // T[r*33 + c] = X[r][c], c < r (L⁻¹ of the block)
             int c = idx & 31, r = idx >> 5;
-            if (r < kb && c < r) T[r * 33 + c] = (double)M[(k0 + c) + (int64_t)(k0 + r) * nf];
+            if (r < kb && c < r) T[r * 33 + c] = (double)M[(k0 + c) + (int64_t)(k0 + r) * ld];
         }
-        if (tid < kb) sh.dinv[tid] = 1.0 / (double)M[(k0 + tid) + (int64_t)(k0 + tid) * nf];
+        if (tid < kb) sh.dinv[tid] = 1.0 / (double)M[(k0 + tid) + (int64_t)(k0 + tid) * ld];
         __syncthreads();
         if (warp == 0 && lane < kb) {   // x = L⁻¹ b for the block, a lane per row
             const int r = lane;
@@ -1151,17 +1181,17 @@ __device__ __noinline__ void front_lsolve_sm(const FT* M, int nf, int nres, int 
         __syncthreads();
         if (tid < kb) xf[k0 + tid] = sh.xs[tid];
         for (int i = i0; i < nf; i += NT) {
-            const FT* Mi = M + i + (int64_t)k0 * nf;
+            const FT* Mi = M + i + (int64_t)k0 * ld;
             double t = 0;
             if (kb == 32) {
                 if (i != i0) {
 #pragma unroll
-                    for (int c = 0; c < 32; ++c) v[c] = Mi[(int64_t)c * nf];
+                    for (int c = 0; c < 32; ++c) v[c] = Mi[(int64_t)c * ld];
                 }
 #pragma unroll
                 for (int c = 0; c < 32; ++c) t = fma((double)v[c], sh.xs[c], t);
             } else {
-                for (int c = 0; c < kb; ++c) t = fma((double)Mi[(int64_t)c * nf], sh.xs[c], t);
+                for (int c = 0; c < kb; ++c) t = fma((double)Mi[(int64_t)c * ld], sh.xs[c], t);
             }
             xf[i] -= t;
         }
@@ -1176,6 +1206,7 @@ __device__ __noinline__ void front_lsolve_sm(const FT* M, int nf, int nres, int 
 // across warps), then the transposed diagonal solve
 template <class FT>
 __device__ __noinline__ void front_usolve_sm(const FT* M, int nf, int nres, int r0, const int* sep, double* x, Shared& sh) {
+    const int64_t ld = front_ld(nf);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int nblk = (nres + 31) / 32;
     double* xf = sh.tile;
@@ -1191,18 +1222,18 @@ __device__ __noinline__ void front_usolve_sm(const FT* M, int nf, int nres, int 
 #pragma unroll
             for (int j = 0; j < 16; ++j) acc[j] = 0;
             for (int i = k0 + kb + tid; i < nf; i += NT) {
-                const FT* Mi = M + i + (int64_t)(k0 + h) * nf;
+                const FT* Mi = M + i + (int64_t)(k0 + h) * ld;
                 const double xi = xf[i];
                 if (hb == 16) {
                     FT v[16];
 #pragma unroll
-                    for (int j = 0; j < 16; ++j) v[j] = Mi[(int64_t)j * nf];
+                    for (int j = 0; j < 16; ++j) v[j] = Mi[(int64_t)j * ld];
 #pragma unroll
                     for (int j = 0; j < 16; ++j) acc[j] = fma((double)v[j], xi, acc[j]);
                 } else {
 #pragma unroll
                     for (int j = 0; j < 16; ++j)
-                        if (j < hb) acc[j] = fma((double)Mi[(int64_t)j * nf], xi, acc[j]);
+                        if (j < hb) acc[j] = fma((double)Mi[(int64_t)j * ld], xi, acc[j]);
                 }
             }
             // reduce over the warp: afterwards lane l (and l + 16) holds column h + (l & 15)
@@ -1222,9 +1253,9 @@ __device__ __noinline__ void front_usolve_sm(const FT* M, int nf, int nres, int 
         }
         for (int idx = tid; idx < 32 * 32; idx += NT) {   // T[r*33 + c] = X[r][c], c < r (L⁻¹ of the block)
             int c = idx & 31, r = idx >> 5;
-            if (r < kb && c < r) T[r * 33 + c] = (double)M[(k0 + c) + (int64_t)(k0 + r) * nf];
+            if (r < kb && c < r) T[r * 33 + c] = (double)M[(k0 + c) + (int64_t)(k0 + r) * ld];
         }
-        if (tid < kb) sh.dinv[tid] = 1.0 / (double)M[(k0 + tid) + (int64_t)(k0 + tid) * nf];
+        if (tid < kb) sh.dinv[tid] = 1.0 / (double)M[(k0 + tid) + (int64_t)(k0 + tid) * ld];
         __syncthreads();
         if (warp == 0) {   // x = L⁻ᵀ y for the block, a lane per row: x_c = Σ_{r ≥ c} X[r][c] y_r
             double dot = 0;
@@ -1540,8 +1571,8 @@ struct Ctx {
     }
     __device__ int64_t fpos(int i, int j) const {   // offset in F of entry (i, j), i >= j
         int f = I.cfront[j];
-        int nfr = I.fnres[f] + I.fnsep[f];
-        return I.fptr[f] + rowpos(f, i) + (int64_t)(j - I.fres0[f]) * nfr;
+        const int64_t ld = front_ld(I.fnres[f] + I.fnsep[f]);
+        return I.fptr[f] + rowpos(f, i) + (int64_t)(j - I.fres0[f]) * ld;
     }
 
     // Finit ← lower part of BᵀB in front layout  (uzawa.jl:29 `B' * B`; gemm.jl:48-82; chordal.jl:1-80).
@@ -2074,15 +2105,16 @@ struct Ctx {
             const int lane = tid & 31, warp = tid >> 5;
             for (int f = 0; f < I.nfront; ++f) {
                 const int nfr = I.fnres[f] + I.fnsep[f];
+                const int64_t ld = front_ld(nfr);
                 FT* M = F + I.fptr[f];
                 const double* M0 = I.Finit + I.fptr[f];
                 if (nfr < 64) {
-                    for (int t = tid; t < nfr * nfr; t += NT) M[t] = (FT)M0[t];
+                    for (int t = tid; t < ld * nfr; t += NT) M[t] = (FT)M0[t];
                     continue;
                 }
                 for (int j = warp; j < nfr; j += NW) {
-                    FT* Mj = M + (int64_t)j * nfr;
-                    const double* Aj = M0 + (int64_t)j * nfr;
+                    FT* Mj = M + (int64_t)j * ld;
+                    const double* Aj = M0 + (int64_t)j * ld;
                     int i = j + lane;
                     for (; i + 96 < nfr; i += 128) {
                         const double a0 = Aj[i], a1 = Aj[i + 32], a2 = Aj[i + 64], a3 = Aj[i + 96];
@@ -2108,9 +2140,10 @@ struct Ctx {
         __syncthreads();
         if (rho != 0) {
             for (int f = 0; f < I.nfront; ++f) {
-                int nres = I.fnres[f], nfr = nres + I.fnsep[f];
+                const int nres = I.fnres[f];
+                const int64_t ld = front_ld(nres + I.fnsep[f]);
                 FT* M = F + I.fptr[f];
-                for (int j = tid; j < nres; j += NT) M[j + (int64_t)j * nfr] = (FT)((double)M[j + (int64_t)j * nfr] + rho);
+                for (int j = tid; j < nres; j += NT) M[j + (int64_t)j * ld] = (FT)((double)M[j + (int64_t)j * ld] + rho);
             }
             __syncthreads();
         }
@@ -2124,10 +2157,11 @@ struct Ctx {
         double s = 0;
         for (int f = 0; f < I.nfront; ++f) {
             int nres = I.fnres[f], nfr = nres + I.fnsep[f];
+            const int64_t ld = front_ld(nfr);
             const FT* M = F + I.fptr[f];
             for (int64_t t = threadIdx.x; t < (int64_t)nres * nfr; t += NT) {
                 int i = (int)(t % nfr), j = (int)(t / nfr);
-                if (i >= j) { double x = (double)M[t]; s += x * x; }
+                if (i >= j) { double x = (double)M[i + (int64_t)j * ld]; s += x * x; }
             }
         }
         return sqrt(block_reduce(s, red, OpSum(), 0.0));
@@ -2159,9 +2193,10 @@ struct Ctx {
                     toc(SEC_FEXTEND, te);
                     continue;
                 }
+                const int64_t ldc = front_ld(nfr), ldp = front_ld(np);
                 for (int j = threadIdx.x >> 5; j < nsep; j += NW) {   // column j of the update matrix per warp
-                    const FT* Mj = M + nres + (int64_t)(nres + j) * nfr;
-                    FT* Pj = P + (int64_t)rel[j] * np;
+                    const FT* Mj = M + nres + (int64_t)(nres + j) * ldc;
+                    FT* Pj = P + (int64_t)rel[j] * ldp;
                     for (int i = j + (threadIdx.x & 31); i < nsep; i += 32) Pj[rel[i]] += Mj[i];
                 }
                 toc(SEC_FEXTEND, te);
@@ -2247,7 +2282,7 @@ struct Ctx {
                 const int* rel = I.frel + I.fsepp[c];
                 for (int t = tid; t < cs * cs; t += NT) {
                     const int r = t % cs, j = t / cs;
-                    if (r <= j) W[(rc + r) + (int64_t)rel[j] * ld] = Mc[(cres + r) + (int64_t)(cres + j) * cn];
+                    if (r <= j) W[(rc + r) + (int64_t)rel[j] * ld] = Mc[(cres + r) + (int64_t)(cres + j) * front_ld(cn)];
                 }
                 rc += cs;
             }
@@ -2318,13 +2353,14 @@ struct Ctx {
             }
             __syncthreads();
             double* M = F + I.fptr[f];
+            const int64_t ldm = front_ld(nfr);
             for (int64_t t = tid; t < (int64_t)nfr * nres; t += NT) {
                 const int i = (int)(t % nfr), j = (int)(t / nfr);
-                if (i >= j) M[t] = (W[j + (int64_t)j * ld] < 0.0 ? -1.0 : 1.0) * W[j + (int64_t)i * ld];
+                if (i >= j) M[i + (int64_t)j * ldm] = (W[j + (int64_t)j * ld] < 0.0 ? -1.0 : 1.0) * W[j + (int64_t)i * ld];
             }
             for (int t = tid; t < nsep * nsep; t += NT) {
                 const int r = t % nsep, c = t / nsep;
-                if (r <= c) M[(nres + r) + (int64_t)(nres + c) * nfr] = nres + r < jmax ? W[(nres + r) + (int64_t)(nres + c) * ld] : 0.0;
+                if (r <= c) M[(nres + r) + (int64_t)(nres + c) * ldm] = nres + r < jmax ? W[(nres + r) + (int64_t)(nres + c) * ld] : 0.0;
             }
             __syncthreads();
             front_block_inverses(M, nfr, nres);

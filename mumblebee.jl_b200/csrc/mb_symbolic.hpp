@@ -13,6 +13,7 @@
 #include <algorithm>
 #include <cstdint>
 #include <vector>
+#include "mb_internal.h"
 
 namespace mbh {
 
@@ -512,7 +513,7 @@ inline Fronts analyze(const std::vector<std::vector<i64>>& adj0, const std::vect
     for (i64 f = 0; f < S.nfront; ++f) {
         S.fptr[f] = off;
         i64 nf = S.nres[f] + (i64)S.sep[f].size();
-        off += (nf * nf + 31) / 32 * 32;
+        off += (mb::front_ld(nf) * nf + 31) / 32 * 32;   // column-major, leading dimension front_ld(nf)
     }
     S.fptr[S.nfront] = off; S.fsize = off;
     return S;

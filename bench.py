@@ -39,8 +39,8 @@ METRIC = "IPM solves/s & p50/p99 latency at 1e-8 gap: mixed vs FP64 GPU; factor 
 # DRAM bytes (read + write) of one ipm_batch_kernel launch per instance of this workload, FP64
 # factor: an ncu capture of a smaller launch of the same instance distribution, divided by its
 # instance count (profiles/ipm_batch_kernel_portfolio_fp64.txt gives the command and the figures)
-TRAFFIC_BYTES_PER_INSTANCE_FP64 = 81.00e9 / 296
-TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of one 296-instance launch (81.00 GB), "
+TRAFFIC_BYTES_PER_INSTANCE_FP64 = 82.35e9 / 296
+TRAFFIC_SOURCE = ("ncu dram__bytes_read.sum + dram__bytes_write.sum of one 296-instance launch (82.35 GB), "
                   "scaled to this launch by instance count")
 
 

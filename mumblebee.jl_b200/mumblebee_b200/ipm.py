@@ -246,9 +246,17 @@ class IPMProblem:
                                params=d.get("param"))
 
     def info(self):
-        a = np.zeros(8, dtype=np.int64)
-        self.ctx.L.mb_problem_info(self.h, _p(a, C.c_int64))
-        return dict(zip(["n", "m", "nvtx", "nout", "narcB", "nbnzB", "narcQ", "nbnzQ"], a.tolist()))
+        """n, m, vertices, outputs and block counts (read once: a problem's shape never changes)"""
+        if getattr(self, "_info", None) is None:
+            a = np.zeros(8, dtype=np.int64)
+            self.ctx.L.mb_problem_info(self.h, _p(a, C.c_int64))
+            self._info = dict(zip(["n", "m", "nvtx", "nout", "narcB", "nbnzB", "narcQ", "nbnzQ"], a.tolist()))
+        return dict(self._info)
+
+    def _nm(self):
+        if getattr(self, "_info", None) is None:
+            self.info()
+        return self._info["n"], self._info["m"]
 
     @property
     def n(self):
@@ -573,6 +581,44 @@ class Batch:
             self.h = None
 
 
+_RESULT_DTYPE = np.dtype([(f, "<i4") for f in ("status", "niter", "nsolve", "nfactor_retry", "nfactor", "nfp32",
+                                                 "nfallback", "reserved")] +
+                         [(f, "<f8") for f in ("mu", "pres", "dres", "pobj", "dobj", "factor_flops")])
+assert _RESULT_DTYPE.itemsize == C.sizeof(mb_result)
+_STATUS = {s.value: s for s in IPMStatus}
+
+
+def _batch_call(fn, probs, settings, grid, ctx, what):
+    """Run a batched C entry point over `probs` with outputs in three contiguous host buffers (one
+    allocation each; every problem's p, d and y are views into them) and the results read back
+    through a structured view of the mb_result array."""
+    probs = list(probs)
+    if not probs:
+        return []
+    ctx = ctx or probs[0].ctx
+    settings = settings or IPMSettings()
+    cs = settings.to_c()
+    k = len(probs)
+    nm = np.array([p._nm() for p in probs], dtype=np.int64).reshape(k, 2)
+    on = np.zeros(k + 1, np.int64); np.cumsum(nm[:, 0], out=on[1:])
+    om = np.zeros(k + 1, np.int64); np.cumsum(nm[:, 1], out=om[1:])
+    P, D, Y = np.zeros(max(int(on[-1]), 1)), np.zeros(max(int(on[-1]), 1)), np.zeros(max(int(om[-1]), 1))
+    pa = (P.ctypes.data + 8 * on[:-1]).astype(np.uint64)
+    da = (D.ctypes.data + 8 * on[:-1]).astype(np.uint64)
+    ya = (Y.ctypes.data + 8 * om[:-1]).astype(np.uint64)
+    pp = lambda a: C.cast(a.ctypes.data, C.POINTER(C.POINTER(C.c_double)))
+    res = (mb_result * k)()
+    arr = (C.c_void_p * k)(*[p.h.value for p in probs])
+    check(fn(ctx.h, arr, k, C.byref(cs), grid, pp(pa), pp(da), pp(ya), res), ctx.h, what)
+    r = np.frombuffer(res, dtype=_RESULT_DTYPE)
+    col = {f: r[f].tolist() for f in _RESULT_DTYPE.names}
+    ps, ds, ys = np.split(P, on[1:-1]), np.split(D, on[1:-1]), np.split(Y, om[1:-1])
+    return [IPMResult(ps[i], ds[i], ys[i], _STATUS[col["status"][i]], col["niter"][i], col["nsolve"][i], IPMHistory(),
+                      col["mu"][i], col["pres"][i], col["dres"][i], col["pobj"][i], col["dobj"][i],
+                      col["nfactor_retry"][i], col["nfactor"][i], col["factor_flops"][i], col["nfp32"][i],
+                      col["nfallback"][i]) for i in range(k)]
+
+
 def batch_solve(probs, settings: IPMSettings | None = None, grid: int = 0, ctx: Context | None = None):
     """solve over many problems (solver/ipm.jl:798-804) through mb_batch_solve: planning, upload,
     one persistent launch per chunk, results.  With grid = 0 and 1024 or more problems the library
@@ -581,20 +627,7 @@ def batch_solve(probs, settings: IPMSettings | None = None, grid: int = 0, ctx: 
     if not probs:
         return []
     ctx = ctx or probs[0].ctx
-    settings = settings or IPMSettings()
-    cs = settings.to_c()
-    k = len(probs)
-    sizes = [p.info() for p in probs]
-    ps = [np.zeros(s["n"]) for s in sizes]
-    ds = [np.zeros(s["n"]) for s in sizes]
-    ys = [np.zeros(s["m"]) for s in sizes]
-    mk = lambda lst: (C.POINTER(C.c_double) * k)(*[_p(a, C.c_double) for a in lst])
-    res = (mb_result * k)()
-    arr = (C.c_void_p * k)(*[p.h.value for p in probs])
-    check(ctx.L.mb_batch_solve(ctx.h, arr, k, C.byref(cs), grid, mk(ps), mk(ds), mk(ys), res), ctx.h, "batch solve")
-    return [IPMResult(ps[i], ds[i], ys[i], IPMStatus(res[i].status), res[i].niter, res[i].nsolve, IPMHistory(),
-                      res[i].mu, res[i].pres, res[i].dres, res[i].pobj, res[i].dobj, res[i].nfactor_retry,
-                      res[i].nfactor, res[i].factor_flops, res[i].nfp32, res[i].nfallback) for i in range(k)]
+    return _batch_call(ctx.L.mb_batch_solve, probs, settings, grid, ctx, "batch solve")
 
 
 def batch_solve_static(probs, settings: IPMSettings | None = None, grid: int = 0, ctx: Context | None = None):
@@ -606,21 +639,7 @@ def batch_solve_static(probs, settings: IPMSettings | None = None, grid: int = 0
     if not probs:
         return []
     ctx = ctx or probs[0].ctx
-    settings = settings or IPMSettings()
-    cs = settings.to_c()
-    k = len(probs)
-    sizes = [p.info() for p in probs]
-    ps = [np.zeros(s["n"]) for s in sizes]
-    ds = [np.zeros(s["n"]) for s in sizes]
-    ys = [np.zeros(s["m"]) for s in sizes]
-    mk = lambda lst: (C.POINTER(C.c_double) * k)(*[_p(a, C.c_double) for a in lst])
-    res = (mb_result * k)()
-    arr = (C.c_void_p * k)(*[p.h.value for p in probs])
-    check(ctx.L.mb_batch_solve_static(ctx.h, arr, k, C.byref(cs), grid, mk(ps), mk(ds), mk(ys), res), ctx.h,
-          "static batch solve")
-    return [IPMResult(ps[i], ds[i], ys[i], IPMStatus(res[i].status), res[i].niter, res[i].nsolve, IPMHistory(),
-                      res[i].mu, res[i].pres, res[i].dres, res[i].pobj, res[i].dobj, res[i].nfactor_retry,
-                      res[i].nfactor, res[i].factor_flops, res[i].nfp32, res[i].nfallback) for i in range(k)]
+    return _batch_call(ctx.L.mb_batch_solve_static, probs, settings, grid, ctx, "static batch solve")
 
 
 # ---------------------------------------------------------------------------------------- serving

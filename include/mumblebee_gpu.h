@@ -218,8 +218,8 @@ int mb_solver_destroy(mb_solver* s);
 
 /* batched solve: every problem solved by a persistent launch (one CTA per instance at a time).
  * With grid = 0 and 1024 or more problems the call is split into two or four chunks (problems
- * dealt round-robin), each planned, uploaded and launched on its own stream, so host planning
- * overlaps device work; each instance is solved exactly as alone.  Outputs per problem i:
+ * taken largest first by an estimate of their cost), each planned, uploaded and launched on its
+ * own stream, so host planning overlaps device work; each instance is solved exactly as alone.  Outputs per problem i:
  * p_out[i] (n_i), d_out[i] (n_i), y_out[i] (m_i), results[i]; any output pointer may be NULL to
  * skip it.  `grid` = CTAs of the persistent launch (0 = two per SM). */
 int mb_batch_solve(mb_ctx* ctx, mb_problem* const* probs, int32_t nprob, const mb_settings* settings,

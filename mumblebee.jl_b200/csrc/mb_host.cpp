@@ -675,9 +675,14 @@ static int upload(mb_batch* b) {
     CUDA_TRY(ctx, dalloc(&b->d_F, std::max<size_t>(pk.fbytes, 256)));
     CUDA_TRY(ctx, dalloc((void**)&b->d_counter, sizeof(int)));
     CUDA_TRY(ctx, halloc((void**)&b->h_out, std::max<size_t>(pk.out.size(), 1) * sizeof(double)));
-    CUDA_TRY(ctx, dalloc((void**)&b->d_ost, std::max<size_t>(pk.ost.size(), 1) * sizeof(int32_t)));
-    CUDA_TRY(ctx, cudaMemsetAsync(b->d_ost, 0, std::max<size_t>(pk.ost.size(), 1) * sizeof(int32_t), st));
-    CUDA_TRY(ctx, halloc((void**)&b->h_i32, std::max<size_t>(pk.ost.size(), 1) * sizeof(int32_t)));
+    const size_t ost_bytes = std::max<size_t>(pk.ost.size(), 1) * sizeof(int32_t);
+    CUDA_TRY(ctx, dalloc((void**)&b->d_ost, ost_bytes));
+    CUDA_TRY(ctx, halloc((void**)&b->h_i32, ost_bytes));
+    // status words zeroed by a copy from the zeroed pinned mirror, not a memset: a memset runs as a
+    // kernel, which waits for SMs that a running chunk's persistent grid holds, and the pageable
+    // copies queued after it would then hold up the host, and the planning of the next chunk, too
+    std::memset(b->h_i32, 0, ost_bytes);
+    CUDA_TRY(ctx, cudaMemcpyAsync(b->d_ost, b->h_i32, ost_bytes, cudaMemcpyHostToDevice, st));
     std::vector<mb::DevInst> hi(pk.plans.size());
     for (size_t k = 0; k < pk.plans.size(); ++k)
         hi[k] = static_devinst(pk.plans[k], b->d_i32, b->d_i64, b->d_din, b->d_work, b->d_out, b->d_ost, (char*)b->d_F);
@@ -1561,10 +1566,11 @@ int mb_batch_destroy(mb_batch* b) {
     return MB_OK;
 }
 
-// A large call is split into up to four chunks (instances dealt round-robin, so each holds a like
-// mix), each planned, uploaded and launched on its own stream: the host plans chunk c + 1 while the
-// device runs chunk c, and the chunks' persistent grids fill each other's tails.  Every instance
-// is solved exactly as in a single launch.
+// A large call is split into two or four chunks of decreasing estimated cost, each planned,
+// uploaded and launched on its own stream: the host plans chunk c + 1 while the device runs chunk
+// c, and the chunks' persistent grids fill each other's tails.  Nothing on a chunk's stream before
+// its launch needs an SM (no memset kernels), so a running chunk never holds up the planning of the
+// next.  Every instance is solved exactly as in a single launch.
 int mb_batch_solve(mb_ctx* ctx, mb_problem* const* probs, int32_t nprob, const mb_settings* settings, int32_t grid,
                    double* const* p_out, double* const* d_out, double* const* y_out, mb_result* results) {
     const int nch = nprob >= 2048 ? 4 : (nprob >= 1024 ? 2 : 1);
@@ -1579,8 +1585,24 @@ int mb_batch_solve(mb_ctx* ctx, mb_problem* const* probs, int32_t nprob, const m
     }
     if (!probs) return fail(ctx, MB_E_ARG, "bad arguments");
     std::vector<std::unique_ptr<mb_batch>> chunks(nch);
+    // chunks in decreasing estimated cost (n³ of the problem's columns; only which chunk a problem
+    // lands in depends on it): a small first chunk of the largest problems starts the device early,
+    // the middle chunks carry the bulk while the host plans the next one, and a small last chunk of
+    // the smallest problems fills the grid's tail and leaves little to read back at the end
+    std::vector<int32_t> ord(nprob);
+    for (int32_t k = 0; k < nprob; ++k) ord[k] = k;
+    auto est = [&](int32_t k) { const double n = (double)probs[k]->B.ncol; return n * n * n; };
+    std::stable_sort(ord.begin(), ord.end(), [&](int32_t a, int32_t b) { return est(a) > est(b); });
+    std::vector<int32_t> cnt;
+    if (nch == 2) cnt = {nprob / 8, nprob - nprob / 8};
+    else {
+        const int32_t c0 = nprob / 16, c3 = nprob / 8, c1 = (nprob - c0 - c3) / 2;
+        cnt = {c0, c1, nprob - c0 - c3 - c1, c3};
+    }
     std::vector<std::vector<int32_t>> idx(nch);
-    for (int32_t k = 0; k < nprob; ++k) idx[k % nch].push_back(k);
+    for (int c = 0, k = 0; c < nch; ++c)
+        for (int32_t j = 0; j < cnt[c]; ++j) idx[c].push_back(ord[k++]);
+    const double t0 = host_time();
     for (int c = 0; c < nch; ++c) {
         std::vector<mb_problem*> sub(idx[c].size());
         for (size_t j = 0; j < sub.size(); ++j) sub[j] = probs[idx[c][j]];
@@ -1589,6 +1611,8 @@ int mb_batch_solve(mb_ctx* ctx, mb_problem* const* probs, int32_t nprob, const m
         if (rc) return rc;
         chunks[c].reset(b);
         if ((rc = run_batch(b, mb::MODE_SOLVE, 0, nullptr))) return rc;   // returns after the launch
+        if (trace_on()) fprintf(stderr, "mb_batch_solve: chunk %d (%zu problems) launched at %.1f ms\n", c, sub.size(),
+                                1e3 * (host_time() - t0));
     }
     for (int c = 0; c < nch; ++c) {
         const size_t nk = idx[c].size();
@@ -1603,6 +1627,13 @@ int mb_batch_solve(mb_ctx* ctx, mb_problem* const* probs, int32_t nprob, const m
                                 y_out ? yy.data() : nullptr, results ? rr.data() : nullptr);
         if (rc) return rc;
         if (results) for (size_t j = 0; j < nk; ++j) results[idx[c][j]] = rr[j];
+        if (trace_on()) {
+            float a = 0, z = 0;
+            cudaEventElapsedTime(&a, chunks[0]->e0, chunks[c]->e0);
+            cudaEventElapsedTime(&z, chunks[0]->e0, chunks[c]->e1);
+            fprintf(stderr, "mb_batch_solve: chunk %d fetched at %.1f ms; on the device from %.1f to %.1f ms after chunk 0's launch\n",
+                    c, 1e3 * (host_time() - t0), a, z);
+        }
     }
     return MB_OK;
 }
@@ -1884,6 +1915,8 @@ struct mb_server {
     int* d_cnt = nullptr;                    // one work counter per stream
     unsigned long long* h_done = nullptr;    // mapped
     unsigned long long* dv_done = nullptr;   // its device alias
+    int32_t* h_zero = nullptr;               // pinned zeros: a request's status words are cleared by a copy
+    static constexpr size_t ZERO_WORDS = 256;
     int cap = 0;
     uint64_t next_seq = 0;
     std::map<uint64_t, Request*> inflight;   // by seq
@@ -1911,6 +1944,7 @@ struct mb_server {
         if (cstream) cudaStreamSynchronize(cstream);
         cudaFree(d_arena); cudaFree(d_ring); cudaFree(d_cnt);
         if (h_done) cudaFreeHost(h_done);
+        if (h_zero) cudaFreeHost(h_zero);
         for (int i = 0; i < SERVE_STREAMS; ++i) {
             if (klast[i]) cudaEventDestroy(klast[i]);
             if (ks[i]) cudaStreamDestroy(ks[i]);
@@ -1961,7 +1995,12 @@ struct mb_server {
         if (pk.i32.size() && !e) e = cudaMemcpyAsync(s_i32, pk.i32.h.data(), pk.i32.size() * 4, cudaMemcpyHostToDevice, cstream);
         if (pk.i64a.size() && !e) e = cudaMemcpyAsync(s_i64, pk.i64a.h.data(), pk.i64a.size() * 8, cudaMemcpyHostToDevice, cstream);
         if (pk.din.size() && !e) e = cudaMemcpyAsync(s_din, pk.din.h.data(), pk.din.size() * 8, cudaMemcpyHostToDevice, cstream);
-        if (!e) e = cudaMemsetAsync(s_ost, 0, std::max<size_t>(pk.ost.size(), 1) * 4, cstream);
+        // zeroed by a copy, not a memset: a memset runs as a kernel, which waits for SMs that running
+        // waves hold, and the pageable copy of the ring slot below would then hold up admission
+        const size_t ost_words = std::max<size_t>(pk.ost.size(), 1);
+        if (!e) e = ost_words <= mb_server::ZERO_WORDS
+                        ? cudaMemcpyAsync(s_ost, h_zero, ost_words * 4, cudaMemcpyHostToDevice, cstream)
+                        : cudaMemsetAsync(s_ost, 0, ost_words * 4, cstream);
         r->seq = next_seq;
         if (!e) e = cudaMemcpyAsync(d_ring + r->seq % cap, &I, sizeof(I), cudaMemcpyHostToDevice, cstream);
         if (e) { fatal = std::string("serve staging: ") + cudaGetErrorString(e); return MB_E_CUDA; }
@@ -2103,6 +2142,8 @@ int mb_server_create(mb_ctx* ctx, const mb_settings* settings, int64_t arena_byt
     CUDA_TRY(ctx, cudaMalloc((void**)&sv->d_cnt, sizeof(int) * SERVE_STREAMS));
     CUDA_TRY(ctx, cudaHostAlloc((void**)&sv->h_done, sizeof(unsigned long long) * capacity, cudaHostAllocMapped));
     std::memset(sv->h_done, 0, sizeof(unsigned long long) * capacity);
+    CUDA_TRY(ctx, cudaMallocHost((void**)&sv->h_zero, mb_server::ZERO_WORDS * sizeof(int32_t)));
+    std::memset(sv->h_zero, 0, mb_server::ZERO_WORDS * sizeof(int32_t));
     CUDA_TRY(ctx, cudaHostGetDevicePointer((void**)&sv->dv_done, sv->h_done, 0));
     sv->arena.init((size_t)arena_bytes);
     int np = nplanners > 0 ? nplanners : (int)std::max(1u, std::thread::hardware_concurrency() / 2);

@@ -394,7 +394,7 @@ struct Fronts {
     std::vector<i64> res0, nres, parent;
     std::vector<std::vector<i64>> sep;   // scalar separator rows, ascending
     std::vector<std::vector<i64>> rel;   // positions of sep rows in the parent's row list
-    std::vector<i64> fptr;               // storage offsets of the (nres+nsep)^2 fronts
+    std::vector<i64> fptr;               // storage offsets of the fronts (order nres+nsep, leading dimension front_ld)
     i64 fsize = 0;
     std::vector<i64> vfront;             // per postordered vertex
 };

@@ -612,11 +612,11 @@ def _batch_call(fn, probs, settings, grid, ctx, what):
     check(fn(ctx.h, arr, k, C.byref(cs), grid, pp(pa), pp(da), pp(ya), res), ctx.h, what)
     r = np.frombuffer(res, dtype=_RESULT_DTYPE)
     col = {f: r[f].tolist() for f in _RESULT_DTYPE.names}
-    ps, ds, ys = np.split(P, on[1:-1]), np.split(D, on[1:-1]), np.split(Y, om[1:-1])
-    return [IPMResult(ps[i], ds[i], ys[i], _STATUS[col["status"][i]], col["niter"][i], col["nsolve"][i], IPMHistory(),
-                      col["mu"][i], col["pres"][i], col["dres"][i], col["pobj"][i], col["dobj"][i],
-                      col["nfactor_retry"][i], col["nfactor"][i], col["factor_flops"][i], col["nfp32"][i],
-                      col["nfallback"][i]) for i in range(k)]
+    on, om = on.tolist(), om.tolist()
+    return [IPMResult(P[on[i]:on[i + 1]], D[on[i]:on[i + 1]], Y[om[i]:om[i + 1]], _STATUS[col["status"][i]],
+                      col["niter"][i], col["nsolve"][i], IPMHistory(), col["mu"][i], col["pres"][i], col["dres"][i],
+                      col["pobj"][i], col["dobj"][i], col["nfactor_retry"][i], col["nfactor"][i],
+                      col["factor_flops"][i], col["nfp32"][i], col["nfallback"][i]) for i in range(k)]
 
 
 def batch_solve(probs, settings: IPMSettings | None = None, grid: int = 0, ctx: Context | None = None):

@@ -231,6 +231,7 @@ inline BSM selectvtxs(const BSM& A, const std::vector<i64>& sel) {
     B.nvtx = (i64)sel.size();
     B.xcol.assign(B.nvtx + 1, 0); B.xsrc.assign(B.nvtx + 1, 0);
     i64 c = 0, ee = 0, bb = 0;
+    B.tgt.reserve(A.narc); B.xblk.reserve(A.narc + 1); B.val.reserve(A.val.size());
     for (i64 v = 0; v < B.nvtx; ++v) {
         i64 av = sel[v];
         B.xcol[v] = c; B.xsrc[v] = ee; c += A.ncols(av);
@@ -277,6 +278,36 @@ inline BSM halfselectvtxs(const BSM& A, const std::vector<i64>& sel) {
     for (i64 au = 0; au < R.nout; ++au) { R.xrow[au] = ar; ar += A.ncols(sel[au]); }
     R.xrow[R.nout] = R.nrow;
     R.xcol = A.xrow;
+    return R;
+}
+
+// halfselectvtxs(halfselectvtxs(Q, sel), sel) for a square Q whose only arcs are diagonal blocks:
+// the two block transposes cancel, so vertex v takes the diagonal block of sel[v] as it is stored,
+// with row and column splits both the sizes of the selected vertices in order
+inline bool blockdiag(const BSM& Q) {
+    for (i64 v = 0; v < Q.nvtx; ++v)
+        for (i64 e = Q.xsrc[v]; e < Q.xsrc[v + 1]; ++e)
+            if (Q.tgt[e] != v) return false;
+    return Q.nout == Q.nvtx;
+}
+inline BSM select_blockdiag(const BSM& Q, const std::vector<i64>& sel) {
+    BSM R;
+    R.nout = R.nvtx = (i64)sel.size();
+    R.xcol.assign(R.nvtx + 1, 0); R.xsrc.assign(R.nvtx + 1, 0);
+    R.tgt.reserve(Q.narc); R.xblk.reserve(Q.narc + 1); R.val.reserve(Q.val.size());
+    i64 c = 0, ee = 0, bb = 0;
+    for (i64 v = 0; v < R.nvtx; ++v) {
+        const i64 w = sel[v];
+        R.xcol[v] = c; R.xsrc[v] = ee; c += Q.ncols(w);
+        for (i64 e = Q.xsrc[w]; e < Q.xsrc[w + 1]; ++e) {
+            R.tgt.push_back(v); R.xblk.push_back(bb); ++ee;
+            R.val.insert(R.val.end(), Q.val.begin() + Q.xblk[e], Q.val.begin() + Q.xblk[e + 1]);
+            bb += Q.xblk[e + 1] - Q.xblk[e];
+        }
+    }
+    R.xcol[R.nvtx] = c; R.xsrc[R.nvtx] = ee; R.xblk.push_back(bb);
+    R.xrow = R.xcol;
+    R.ncol = R.nrow = c; R.narc = ee; R.nbnz = bb;
     return R;
 }
 

@@ -362,34 +362,35 @@ static int plan_instance(const mb_problem* P, const mb_settings& set, const doub
     for (i64 v = 0; v < nv; ++v) for (i64 j = B.xcol[v]; j < B.xcol[v + 1]; ++j) { colvtx[j] = v; cfront[j] = fr.vfront[v]; }
     // scalar nonzeros: CSR + CSC (CSC entries carry their CSR position).  With `skipdiag`, the
     // entries inside the diagonal blocks are left out (they live in the dense Qd blocks).  Each
-    // stored block is read once, contiguously, in two passes (column counts, then placement);
-    // within a column the entries come arc by arc in the vertex's arc order and each block's rows
-    // in order, the order a column-by-column scan of the arcs gives.
+    // stored block is read once, contiguously; its nonzeros, gathered arc by arc in the vertex's
+    // arc order, are counting-sorted (stably) by column, so within a column the entries come arc by
+    // arc and each block's rows in order: the order a column-by-column scan of the arcs gives.
     auto scalar = [&](const mbh::BSM& A, bool skipdiag, std::vector<i64>& rptr, std::vector<i64>& cidx,
                       std::vector<double>& val, std::vector<i64>& cptr, std::vector<i64>& ridx, std::vector<i64>& cpos) {
+        std::vector<i64> tr, tc; std::vector<double> tv;   // nonzeros in arc order
         rptr.assign(A.nrow + 1, 0); cptr.assign(A.ncol + 1, 0);
-        auto blocks = [&](auto&& visit) {
-            for (i64 v = 0; v < A.nvtx; ++v) {
-                const i64 nc = A.ncols(v), c0 = A.xcol[v];
-                for (i64 e = A.xsrc[v]; e < A.xsrc[v + 1]; ++e) {
-                    const i64 u = A.tgt[e];
-                    if (skipdiag && u == v) continue;
-                    const i64 nr = A.nrows(u), r0 = A.xrow[u];
-                    const double* blk = A.val.data() + A.xblk[e];
-                    for (i64 jl = 0; jl < nc; ++jl)
-                        for (i64 il = 0; il < nr; ++il)
-                            if (blk[jl * nr + il] != 0) visit(r0 + il, c0 + jl, blk[jl * nr + il]);
-                }
+        for (i64 v = 0; v < A.nvtx; ++v) {
+            const i64 nc = A.ncols(v), c0 = A.xcol[v];
+            for (i64 e = A.xsrc[v]; e < A.xsrc[v + 1]; ++e) {
+                const i64 u = A.tgt[e];
+                if (skipdiag && u == v) continue;
+                const i64 nr = A.nrows(u), r0 = A.xrow[u];
+                const double* blk = A.val.data() + A.xblk[e];
+                for (i64 jl = 0; jl < nc; ++jl)
+                    for (i64 il = 0; il < nr; ++il)
+                        if (blk[jl * nr + il] != 0) {
+                            tr.push_back(r0 + il); tc.push_back(c0 + jl); tv.push_back(blk[jl * nr + il]);
+                            rptr[r0 + il + 1]++; cptr[c0 + jl + 1]++;
+                        }
             }
-        };
-        blocks([&](i64 r, i64 c, double) { rptr[r + 1]++; cptr[c + 1]++; });
+        }
         for (i64 i = 0; i < A.nrow; ++i) rptr[i + 1] += rptr[i];
         for (i64 j = 0; j < A.ncol; ++j) cptr[j + 1] += cptr[j];
-        const i64 nnz = cptr[A.ncol];
+        const i64 nnz = (i64)tr.size();
         std::vector<double> cv(nnz);
         ridx.assign(nnz, 0);
         std::vector<i64> pc(cptr.begin(), cptr.end() - 1);
-        blocks([&](i64 r, i64 c, double x) { const i64 k = pc[c]++; ridx[k] = r; cv[k] = x; });
+        for (i64 t = 0; t < nnz; ++t) { const i64 k = pc[tc[t]]++; ridx[k] = tr[t]; cv[k] = tv[t]; }
         cidx.assign(nnz, 0); val.assign(nnz, 0); cpos.assign(nnz, 0);
         std::vector<i64> rc(rptr.begin(), rptr.end() - 1);
         for (i64 j = 0; j < A.ncol; ++j)   // CSR by a stable counting sort of the CSC entries

@@ -1402,6 +1402,12 @@ __device__ void for_vertex_blocks(const int* xcol, int nv, Pred pred, Body body)
     __syncthreads();
 }
 
+// row pair q of an FT column that starts on a pair boundary, from two FP64 values
+__device__ __forceinline__ void store_pair(double* m, int q, double2 a) { reinterpret_cast<double2*>(m)[q] = a; }
+__device__ __forceinline__ void store_pair(float* m, int q, double2 a) {
+    reinterpret_cast<float2*>(m)[q] = make_float2((float)a.x, (float)a.y);
+}
+
 template <bool COOP>   // COOP: the leader of a grid-cooperative launch (else no cooperative code is built)
 struct Ctx {
     const DevInst& I;
@@ -2101,7 +2107,11 @@ struct Ctx {
             });
         } else {
             // only the lower triangle of each front is ever read (factor, solves, extend-add, norms):
-            // large fronts copy it a warp per column, small ones whole and flat
+            // large fronts copy it a warp per column in 16-byte row pairs, from the even row at or
+            // above the diagonal (columns start on 16-byte boundaries: even leading dimension, Finit
+            // and F aligned) to the padding row of an odd order, so at most one upper-triangle entry,
+            // which the factor rewrites before anything reads it, and the unread padding row come
+            // along; small fronts are copied whole and flat
             const int lane = tid & 31, warp = tid >> 5;
             for (int f = 0; f < I.nfront; ++f) {
                 const int nfr = I.fnres[f] + I.fnsep[f];
@@ -2113,14 +2123,15 @@ struct Ctx {
                     continue;
                 }
                 for (int j = warp; j < nfr; j += NW) {
-                    FT* Mj = M + (int64_t)j * ld;
-                    const double* Aj = M0 + (int64_t)j * ld;
-                    int i = j + lane;
-                    for (; i + 96 < nfr; i += 128) {
-                        const double a0 = Aj[i], a1 = Aj[i + 32], a2 = Aj[i + 64], a3 = Aj[i + 96];
-                        Mj[i] = (FT)a0; Mj[i + 32] = (FT)a1; Mj[i + 64] = (FT)a2; Mj[i + 96] = (FT)a3;
+                    const int i0 = j & ~1, np = (((nfr + 1) & ~1) - i0) >> 1;
+                    const double2* A2 = reinterpret_cast<const double2*>(M0 + (int64_t)j * ld + i0);
+                    FT* Mj = M + (int64_t)j * ld + i0;
+                    int q = lane;
+                    for (; q + 96 < np; q += 128) {
+                        const double2 a0 = A2[q], a1 = A2[q + 32], a2 = A2[q + 64], a3 = A2[q + 96];
+                        store_pair(Mj, q, a0); store_pair(Mj, q + 32, a1); store_pair(Mj, q + 64, a2); store_pair(Mj, q + 96, a3);
                     }
-                    for (; i < nfr; i += 32) Mj[i] = (FT)Aj[i];
+                    for (; q < np; q += 32) store_pair(Mj, q, A2[q]);
                 }
             }
         }

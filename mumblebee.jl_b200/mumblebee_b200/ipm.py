@@ -622,7 +622,9 @@ def _batch_call(fn, probs, settings, grid, ctx, what):
 def batch_solve(probs, settings: IPMSettings | None = None, grid: int = 0, ctx: Context | None = None):
     """solve over many problems (solver/ipm.jl:798-804) through mb_batch_solve: planning, upload,
     one persistent launch per chunk, results.  With grid = 0 and 1024 or more problems the library
-    splits the call into chunks on their own streams, so host planning overlaps device work."""
+    splits the call into chunks on their own streams, so host planning overlaps device work.  Each
+    result's p, d and y are non-overlapping views into three arrays shared by the call's results
+    (copy one to keep it apart from the others' memory)."""
     probs = list(probs)
     if not probs:
         return []
